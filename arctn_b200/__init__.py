@@ -1,0 +1,42 @@
+"""arctn_b200: B200-native executor for ArcTN's numerical contraction path.
+
+The compute path is the in-tree CUDA library ``libarctn_b200.so`` (sm_100a),
+reached through the C ABI of ``include/arctn_b200.h``.  There is no CPU
+fallback: executing without a CUDA device raises ``ValueError``.
+"""
+
+from ._capi import ArcTNB200Error
+from .api import (
+    ArcTNCompiledContraction,
+    CompiledContraction,
+    Finalize,
+    InputPrep,
+    PairStep,
+    SlicedProgram,
+    arctn_contract,
+    contract_sliced,
+    find_slices_to_size,
+    greedy,
+    linear_to_ssa,
+    simulate_path,
+    slice_parallel_chunks,
+    ssa_to_linear,
+)
+
+__all__ = [
+    "ArcTNB200Error",
+    "ArcTNCompiledContraction",
+    "CompiledContraction",
+    "Finalize",
+    "InputPrep",
+    "PairStep",
+    "SlicedProgram",
+    "arctn_contract",
+    "contract_sliced",
+    "find_slices_to_size",
+    "greedy",
+    "linear_to_ssa",
+    "simulate_path",
+    "slice_parallel_chunks",
+    "ssa_to_linear",
+]

@@ -1,0 +1,758 @@
+"""Python surface of the B200 executor, mirroring ArcTN's execution entry points.
+
+Reference surfaces mirrored (paths inside the ArcTN repository):
+
+* ``CompiledContraction.compile(inputs, output, size_dict, *, ssa_path)`` /
+  ``.execute(arrays)`` / ``.stats()`` -- ``pybind/src/lib.rs:355-454``;
+  the stage API ``input_preps()`` / ``pair_steps()`` / ``finalize()`` with
+  their accessors -- ``src/compiled.rs:33-250``.
+* ``contract_sliced(inputs, output, size_dict, arrays, sliced_legs, path=None,
+  ssa_path=None)`` -- ``pybind/src/lib.rs:667-765``.
+* ``ArcTNCompiledContraction.compile(..., backend=)`` and
+  ``arctn_contract(..., backend=)`` -- ``pybind/python/arctn/__init__.py:749-1072``,
+  with ``backend="b200"`` selecting this executor explicitly.
+
+Arrays may be NumPy arrays (copied to the GPU and the result copied back) or
+CUDA ``torch`` tensors (used in place; the result stays on the device).  Every
+error is raised as ``ValueError`` before anything is launched, as the
+reference raises ``ValueError`` from its preflight (``pybind/src/lib.rs:246-330``).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import operator
+import threading
+import time
+
+import numpy as np
+
+from . import _capi as C
+
+_NP_CODES = {np.dtype(np.float32): C.F32, np.dtype(np.float64): C.F64, np.dtype(np.complex64): C.C64,
+             np.dtype(np.complex128): C.C128}
+_PRECISIONS = {"fp32": C.PREC_FP32, "tf32x3": C.PREC_TF32X3}
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+def _torch_code(dtype):
+    torch = _torch()
+    table = {torch.float32: C.F32, torch.float64: C.F64, torch.complex64: C.C64, torch.complex128: C.C128}
+    if dtype not in table:
+        raise ValueError(f"dtype {dtype} is not supported; use float32, float64, complex64 or complex128")
+    return table[dtype]
+
+
+def _torch_dtype(code, wide=False):
+    torch = _torch()
+    if wide:
+        return torch.complex128 if code in (C.C64, C.C128) else torch.float64
+    return {C.F32: torch.float32, C.F64: torch.float64, C.C64: torch.complex64, C.C128: torch.complex128}[code]
+
+
+def _precision(p):
+    if isinstance(p, int):
+        return p
+    if p not in _PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}, got {p!r}")
+    return _PRECISIONS[p]
+
+
+def _is_torch(x):
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        return False
+    return isinstance(x, torch.Tensor)
+
+
+def _expected_shapes(inputs, size_dict):
+    return [tuple(int(size_dict[l]) for l in t) for t in inputs]
+
+
+def _preflight(arrays, inputs, size_dict, context):
+    """Validate count, dtype, layout and every shape before any copy (pybind/src/lib.rs:246-330)."""
+    try:
+        arrays = list(arrays)
+    except TypeError as exc:
+        raise TypeError("arrays must be a sequence of tensors") from exc
+    if len(arrays) != len(inputs):
+        raise ValueError(f"{context}: {len(arrays)} arrays given for {len(inputs)} input tensors")
+    if not arrays:
+        raise ValueError(f"{context}: arrays is empty")
+    torch_mode = _is_torch(arrays[0])
+    code = None
+    for i, (a, shape) in enumerate(zip(arrays, _expected_shapes(inputs, size_dict))):
+        if torch_mode != _is_torch(a):
+            raise ValueError(f"{context}: arrays[{i}] mixes torch tensors and NumPy arrays")
+        if torch_mode:
+            c = _torch_code(a.dtype)
+            if not a.is_cuda:
+                raise ValueError(f"{context}: arrays[{i}] is a CPU torch tensor; pass CUDA tensors or NumPy arrays")
+            if not a.is_contiguous():
+                raise ValueError(f"{context}: arrays[{i}] must be contiguous (call .contiguous())")
+        else:
+            a = np.asarray(a)
+            if a.dtype not in _NP_CODES:
+                raise ValueError(f"{context}: arrays[{i}] dtype {a.dtype} is not supported; "
+                                 "use float32, float64, complex64 or complex128")
+            c = _NP_CODES[a.dtype]
+        if code is None:
+            code = c
+        elif c != code:
+            raise ValueError(f"{context}: arrays[{i}] dtype differs from the first tensor's")
+        if tuple(int(d) for d in a.shape) != shape:
+            raise ValueError(f"{context}: arrays[{i}] shape {tuple(a.shape)} does not match the network's {shape} "
+                             "(invalid input layout)")
+    return arrays, code, torch_mode
+
+
+class _DeviceCall:
+    """Moves NumPy inputs to the GPU (via pinned staging) or passes CUDA tensors through."""
+
+    def __init__(self, arrays, torch_mode, device=None):
+        torch = _torch()
+        if torch_mode:
+            self.device = arrays[0].device
+            for a in arrays:
+                if a.device != self.device:
+                    raise ValueError("all arrays must live on one CUDA device")
+            self.tensors = list(arrays)
+        else:
+            if not torch.cuda.is_available():
+                raise ValueError("the B200 executor needs a CUDA device; none is visible")
+            self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+            self.tensors = []
+            for a in arrays:
+                host = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+                self.tensors.append(host.to(self.device, non_blocking=True))
+        self.stream = torch.cuda.current_stream(self.device)
+        self.ptrs = (ctypes.c_void_p * len(self.tensors))(*[t.data_ptr() for t in self.tensors])
+
+    def empty(self, shape, dtype):
+        return _torch().empty(shape, dtype=dtype, device=self.device)
+
+    def workspace(self, nbytes):
+        return _torch().empty(max(int(nbytes), 1), dtype=_torch().uint8, device=self.device)
+
+
+def _to_output(t, torch_mode):
+    if torch_mode:
+        return t
+    return t.cpu().numpy()
+
+
+# ---------------------------------------------------------------------------- planning support
+
+
+def simulate_path(inputs, output, size_dict, ssa_path):
+    """Path metrics (``simulate_path_full``, src/path.rs:239-434) as a dict."""
+    net = C.NetworkArgs(inputs, output, size_dict)
+    n, p = C.path_array(ssa_path)
+    st = (ctypes.c_double * 6)()
+    C.check(C.lib().arctn_b200_simulate_path(net.ptr, n, p.ctypes.data_as(C.u64p), st), "invalid path")
+    keys = ("log10_flops", "log2_max_size", "log2_max_contraction_size", "log2_total_size", "log2_read_write",
+            "log2_peak_size")
+    return dict(zip(keys, list(st)))
+
+
+def greedy(inputs, output, size_dict):
+    """Deterministic greedy SSA path (src/paths/greedy.rs:307-320)."""
+    net = C.NetworkArgs(inputs, output, size_dict)
+    buf = np.zeros(2 * max(1, len(net.inputs)), dtype=np.uint64)
+    ns = C.u64(0)
+    C.check(C.lib().arctn_b200_greedy(net.ptr, buf.ctypes.data_as(C.u64p), ctypes.byref(ns)), "invalid network")
+    return [(int(buf[2 * s]), int(buf[2 * s + 1])) for s in range(ns.value)]
+
+
+def find_slices_to_size(inputs, output, size_dict, ssa_path, target_size):
+    """Sliced legs meeting ``target_size`` elements per intermediate, or None (src/slice.rs:209-215)."""
+    net = C.NetworkArgs(inputs, output, size_dict)
+    n, p = C.path_array(ssa_path)
+    buf = np.zeros(max(1, len(net.size_dict)), dtype=np.uint32)
+    nl = C.u64(0)
+    found = ctypes.c_int(0)
+    C.check(C.lib().arctn_b200_find_slices_to_size(net.ptr, n, p.ctypes.data_as(C.u64p), int(target_size),
+                                                   buf.ctypes.data_as(C.u32p), ctypes.byref(nl),
+                                                   ctypes.byref(found)), "slice search")
+    return [int(x) for x in buf[: nl.value]] if found.value else None
+
+
+def slice_parallel_chunks(n_slices, out_numel):
+    """Deterministic chunk count of the sliced sum (src/slice.rs:893-905)."""
+    return int(C.lib().arctn_b200_slice_parallel_chunks(int(n_slices), int(out_numel)))
+
+
+# ---------------------------------------------------------------------------- programs
+
+
+class SlicedProgram:
+    """A network + SSA path + sliced legs bound to a dtype, precision and GPU.
+
+    ``execute`` runs all slices (slices batched, slice-invariant subtrees run
+    once, FP64 cross-slice sum in the reference's chunk order) and returns the
+    full output, like ``contract_network_sliced`` (src/slice.rs:960-1173).
+    """
+
+    def __init__(self, inputs, output, size_dict, ssa_path, sliced_legs=(), *, dtype="complex64",
+                 precision="fp32", device=None, use_graph=True, max_slices_per_group=0, workspace_budget=0,
+                 slice_begin=0, slice_end=0):
+        torch = _torch()
+        self.inputs = [[int(l) for l in t] for t in inputs]
+        self.output = [int(l) for l in output]
+        self.size_dict = {int(k): int(v) for k, v in size_dict.items()}
+        self.ssa_path = [(int(a), int(b)) for a, b in ssa_path]
+        self.sliced_legs = [int(l) for l in sliced_legs]
+        if isinstance(dtype, int):
+            self.code = dtype
+        else:
+            self.code = _NP_CODES.get(np.dtype(dtype)) if not _is_torch_dtype(dtype) else _torch_code(dtype)
+            if self.code is None:
+                raise ValueError(f"unsupported dtype {dtype}")
+        self.precision = _precision(precision)
+        if device is None:
+            device = torch.cuda.current_device() if torch.cuda.is_available() else 0
+        self.device = int(device)
+        net = C.NetworkArgs(self.inputs, self.output, self.size_dict)
+        n, p = C.path_array(self.ssa_path)
+        sl = np.asarray(self.sliced_legs or [0], dtype=np.uint32)
+        opts = C.ProgramOptions(self.code, self.precision, self.device, 1 if use_graph else 0,
+                                int(max_slices_per_group), int(workspace_budget), int(slice_begin), int(slice_end))
+        h = C.vp()
+        C.check(C.lib().arctn_b200_program_create(net.ptr, n, p.ctypes.data_as(C.u64p), len(self.sliced_legs),
+                                                  sl.ctypes.data_as(C.u32p), ctypes.byref(opts), ctypes.byref(h)),
+                "sliced contraction failed")
+        self._h = h
+        self._lock = threading.Lock()
+        L = C.lib()
+        self.workspace_bytes = int(L.arctn_b200_program_workspace_size(h))
+        self.n_slices = int(L.arctn_b200_program_n_slices(h))
+        self.slices_per_group = int(L.arctn_b200_program_slices_per_group(h))
+        self.flops = float(L.arctn_b200_program_flops(h))
+        self.launches = int(L.arctn_b200_program_launches(h))
+        self.output_shape = tuple(self.size_dict[l] for l in self.output)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            C.lib().arctn_b200_program_destroy(h)
+            self._h = None
+
+    def execute(self, arrays, *, f64_out=False, workspace=None, stream=None):
+        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "sliced contraction failed")
+        if code != self.code:
+            raise ValueError("sliced contraction failed: arrays dtype differs from the program's dtype")
+        call = _DeviceCall(arrays, torch_mode, self.device)
+        torch = _torch()
+        out = call.empty(self.output_shape, _torch_dtype(code, wide=f64_out))
+        ws = workspace if workspace is not None else call.workspace(self.workspace_bytes)
+        st = stream if stream is not None else call.stream
+        fn = C.lib().arctn_b200_program_execute_f64out if f64_out else C.lib().arctn_b200_program_execute
+        with torch.cuda.device(call.device):
+            C.check(fn(self._h, call.ptrs, out.data_ptr(), ws.data_ptr(), ws.numel(), st.cuda_stream),
+                    "sliced contraction failed")
+        self._keep = (call, ws)  # keep device buffers alive until the next call on this stream
+        return _to_output(out, torch_mode)
+
+    def profile(self, arrays, *, workspace=None):
+        """Op-by-op run with CUDA events between launches: (ms, kind, algorithmic work) per launch."""
+        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "profile failed")
+        call = _DeviceCall(arrays, torch_mode, self.device)
+        out = call.empty(self.output_shape, _torch_dtype(code))
+        ws = workspace if workspace is not None else call.workspace(self.workspace_bytes)
+        n = self.launches
+        ms = (ctypes.c_float * n)()
+        kind = (ctypes.c_int * n)()
+        work = (ctypes.c_double * n)()
+        with _torch().cuda.device(call.device):
+            C.check(C.lib().arctn_b200_program_profile(self._h, call.ptrs, out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                                       call.stream.cuda_stream, ms, kind, work), "profile failed")
+        return list(ms), list(kind), list(work)
+
+    def execute_stripped(self, arrays):
+        """Mantissa tensor and decimal exponent (src/compiled.rs:376-441); unsliced programs only."""
+        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "compiled contraction failed")
+        call = _DeviceCall(arrays, torch_mode, self.device)
+        out = call.empty(self.output_shape, _torch_dtype(code))
+        ws = call.workspace(self.workspace_bytes)
+        e = ctypes.c_double(0.0)
+        with _torch().cuda.device(call.device):
+            C.check(C.lib().arctn_b200_program_execute_stripped(self._h, call.ptrs, out.data_ptr(), ws.data_ptr(),
+                                                                ws.numel(), call.stream.cuda_stream,
+                                                                ctypes.byref(e)), "compiled contraction failed")
+        return _to_output(out, torch_mode), e.value
+
+
+def _is_torch_dtype(d):
+    try:
+        import torch
+    except ImportError:  # pragma: no cover
+        return False
+    return isinstance(d, torch.dtype)
+
+
+# ---------------------------------------------------------------------------- CompiledContraction
+
+
+class InputPrep:
+    """CompiledInputPrep (src/compiled.rs:33-75)."""
+
+    def __init__(self, owner, index, info):
+        self._owner, self._i = owner, index
+        self._input_shape = tuple(info.input_shape[j] for j in range(info.n_input_shape))
+        self._traces = [tuple(info.traces[3 * t + j] for j in range(3)) for t in range(info.n_traces)]
+        self._legs = tuple(int(info.legs[j]) for j in range(info.n_legs))
+        self._shape = tuple(int(info.shape[j]) for j in range(info.n_legs))
+
+    def is_identity(self):
+        return not self._traces
+
+    def input_shape(self):
+        return self._input_shape
+
+    def traces(self):
+        return list(self._traces)
+
+    def legs(self):
+        return self._legs
+
+    def shape(self):
+        return self._shape
+
+    def execute(self, tensor):
+        return self._owner._stage("prep", self._i, [tensor], self._input_shape, self._shape)
+
+
+class PairStep:
+    """CompiledPairContraction (src/compiled.rs:77-172)."""
+
+    def __init__(self, owner, index, s):
+        self._owner, self._i = owner, index
+        rng = lambda p, n: tuple(int(p[j]) for j in range(n))  # noqa: E731
+        self._left_slot, self._right_slot, self._result_slot = int(s.left_slot), int(s.right_slot), int(s.result_slot)
+        self._left_legs = rng(s.left_legs, s.n_left)
+        self._right_legs = rng(s.right_legs, s.n_right)
+        self._result_legs = rng(s.result_legs, s.n_result)
+        self._left_shape = rng(s.left_shape, s.n_left)
+        self._right_shape = rng(s.right_shape, s.n_right)
+        self._result_shape = rng(s.result_shape, s.n_result)
+        self._sum_a = rng(s.sum_a, s.n_sum_a)
+        self._sum_b = rng(s.sum_b, s.n_sum_b)
+        self._a_perm = rng(s.a_perm, s.n_left - s.n_sum_a)
+        self._b_perm = rng(s.b_perm, s.n_right - s.n_sum_b)
+        self._dims = (int(s.bt), int(s.m), int(s.k), int(s.n))
+
+    def left_slot(self):
+        return self._left_slot
+
+    def right_slot(self):
+        return self._right_slot
+
+    def result_slot(self):
+        return self._result_slot
+
+    def left_legs(self):
+        return self._left_legs
+
+    def right_legs(self):
+        return self._right_legs
+
+    def result_legs(self):
+        return self._result_legs
+
+    def left_shape(self):
+        return self._left_shape
+
+    def right_shape(self):
+        return self._right_shape
+
+    def result_shape(self):
+        return self._result_shape
+
+    def sum_a(self):
+        return self._sum_a
+
+    def sum_b(self):
+        return self._sum_b
+
+    def a_perm(self):
+        return self._a_perm
+
+    def b_perm(self):
+        return self._b_perm
+
+    def gemm_dims(self):
+        return self._dims
+
+    def execute(self, left, right, *, precision="fp32"):
+        return self._owner._stage("step", self._i, [left, right], None, self._result_shape, precision=precision)
+
+
+class Finalize:
+    """CompiledFinalize (src/compiled.rs:174-219)."""
+
+    def __init__(self, owner, f):
+        self._owner = owner
+        self._slot = int(f.slot)
+        self._input_legs = tuple(int(f.input_legs[j]) for j in range(f.n_input))
+        self._input_shape = tuple(int(f.input_shape[j]) for j in range(f.n_input))
+        self._sum = tuple(int(f.sum[j]) for j in range(f.n_sum))
+        self._perm = tuple(int(f.perm[j]) for j in range(f.n_output))
+        self._output_shape = tuple(int(f.output_shape[j]) for j in range(f.n_output))
+
+    def slot(self):
+        return self._slot
+
+    def input_legs(self):
+        return self._input_legs
+
+    def input_shape(self):
+        return self._input_shape
+
+    def output_shape(self):
+        return self._output_shape
+
+    def sum_axes(self):
+        return self._sum
+
+    def perm(self):
+        return self._perm
+
+    def is_identity(self):
+        return not self._sum and all(i == p for i, p in enumerate(self._perm))
+
+    def execute(self, tensor):
+        return self._owner._stage("finalize", 0, [tensor], self._input_shape, self._output_shape)
+
+
+class CompiledContraction:
+    """A reusable exact contraction compiled from an SSA path (pybind/src/lib.rs:355-454)."""
+
+    def __init__(self, inputs, output, size_dict, ssa_path, handle):
+        self.inputs = [[int(l) for l in t] for t in inputs]
+        self.output = [int(l) for l in output]
+        self.size_dict = {int(k): int(v) for k, v in size_dict.items()}
+        self.ssa_path = [(int(a), int(b)) for a, b in ssa_path]
+        self._h = handle
+        self._programs = {}
+        self._lock = threading.Lock()
+        L = C.lib()
+        self._n_inputs = int(L.arctn_b200_plan_n_inputs(handle))
+        self._n_steps = int(L.arctn_b200_plan_n_steps(handle))
+        self.log10_flops = float(L.arctn_b200_plan_log10_flops(handle))
+        self.log2_peak_size = float(L.arctn_b200_plan_log2_peak_size(handle))
+        self._preps = []
+        for i in range(self._n_inputs):
+            info = C.PrepInfo()
+            C.check(L.arctn_b200_plan_prep_info(handle, i, ctypes.byref(info)))
+            self._preps.append(InputPrep(self, i, info))
+        self._steps = []
+        for s in range(self._n_steps):
+            info = C.StepInfo()
+            C.check(L.arctn_b200_plan_step_info(handle, s, ctypes.byref(info)))
+            self._steps.append(PairStep(self, s, info))
+        fi = C.FinalizeInfo()
+        C.check(L.arctn_b200_plan_finalize_info(handle, ctypes.byref(fi)))
+        self._finalize = Finalize(self, fi)
+
+    @staticmethod
+    def compile(inputs, output, size_dict, *, ssa_path):
+        """Compile a reusable contraction from an **SSA** path (keyword required, as the reference)."""
+        net = C.NetworkArgs(inputs, output, size_dict)
+        n, p = C.path_array(ssa_path)
+        h = C.vp()
+        C.check(C.lib().arctn_b200_plan_compile(net.ptr, n, p.ctypes.data_as(C.u64p), ctypes.byref(h)),
+                "invalid compiled path")
+        return CompiledContraction(inputs, output, size_dict, ssa_path, h)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            C.lib().arctn_b200_plan_destroy(h)
+            self._h = None
+
+    def n_inputs(self):
+        return self._n_inputs
+
+    def n_steps(self):
+        return self._n_steps
+
+    def input_preps(self):
+        return list(self._preps)
+
+    def pair_steps(self):
+        return list(self._steps)
+
+    def finalize(self):
+        return self._finalize
+
+    def program(self, code, precision="fp32", device=None):
+        key = (code, _precision(precision), device)
+        with self._lock:
+            prog = self._programs.get(key)
+            if prog is None:
+                prog = SlicedProgram(self.inputs, self.output, self.size_dict, self.ssa_path, (), dtype=code,
+                                     precision=precision, device=device)
+                self._programs[key] = prog
+        return prog
+
+    def execute(self, arrays, *, precision="fp32", f64_out=False):
+        """Execute on arrays with the frozen shapes; one dtype for all inputs."""
+        if len(list(arrays)) != self._n_inputs:
+            raise ValueError(f"{len(list(arrays))} arrays given for a plan with {self._n_inputs} inputs")
+        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "compiled contraction failed")
+        dev = arrays[0].device.index if torch_mode else None
+        return self.program(code, precision, dev).execute(arrays, f64_out=f64_out)
+
+    __call__ = execute
+
+    def execute_stripped(self, arrays):
+        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "compiled contraction failed")
+        dev = arrays[0].device.index if torch_mode else None
+        return self.program(code, "fp32", dev).execute_stripped(arrays)
+
+    def stats(self):
+        return {"path_format": "ssa-v1", "n_inputs": self._n_inputs, "n_steps": self._n_steps,
+                "log10_flops": self.log10_flops, "log2_peak_size": self.log2_peak_size}
+
+    def __repr__(self):
+        return f"CompiledContraction(path_format='ssa-v1', n_inputs={self._n_inputs}, n_steps={self._n_steps})"
+
+    # Stage execution ---------------------------------------------------------------------------
+    def _stage(self, kind, idx, tensors, want_shape, out_shape, precision="fp32"):
+        torch = _torch()
+        torch_mode = _is_torch(tensors[0])
+        code = None
+        for t in tensors:
+            c = _torch_code(t.dtype) if _is_torch(t) else _NP_CODES.get(np.asarray(t).dtype)
+            if c is None:
+                raise ValueError("unsupported dtype")
+            if code is None:
+                code = c
+            elif c != code:
+                raise ValueError("stage operands differ in dtype")
+        if kind == "step":
+            st = self._steps[idx]
+            shapes = [st.left_shape(), st.right_shape()]
+            labels = ["left operand", "right operand"]
+        elif kind == "prep":
+            shapes, labels = [want_shape], ["input tensor"]
+        else:
+            shapes, labels = [want_shape], ["finalize tensor"]
+        for t, shp, lab in zip(tensors, shapes, labels):
+            if tuple(int(d) for d in t.shape) != tuple(shp):
+                raise ValueError(f"{lab} shape {tuple(t.shape)} does not match the compiled plan's {tuple(shp)}")
+            if _is_torch(t) and not t.is_contiguous():
+                raise ValueError(f"{lab} must be contiguous")
+        call = _DeviceCall(tensors, torch_mode)
+        out = call.empty(tuple(out_shape), _torch_dtype(code))
+        L = C.lib()
+        with torch.cuda.device(call.device):
+            if kind == "step":
+                p = _precision(precision)
+                nbytes = int(L.arctn_b200_plan_step_workspace_size(self._h, code, p, idx))
+                ws = call.workspace(nbytes)
+                rc = L.arctn_b200_plan_step_execute(self._h, code, p, idx, call.ptrs[0], call.ptrs[1],
+                                                    out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                                    call.stream.cuda_stream)
+            elif kind == "prep":
+                nbytes = int(L.arctn_b200_plan_prep_workspace_size(self._h, code, idx))
+                ws = call.workspace(nbytes)
+                rc = L.arctn_b200_plan_prep_execute(self._h, code, idx, call.ptrs[0], out.data_ptr(), ws.data_ptr(),
+                                                    ws.numel(), call.stream.cuda_stream)
+            else:
+                nbytes = int(L.arctn_b200_plan_finalize_workspace_size(self._h, code))
+                ws = call.workspace(nbytes)
+                rc = L.arctn_b200_plan_finalize_execute(self._h, code, call.ptrs[0], out.data_ptr(), ws.data_ptr(),
+                                                        ws.numel(), call.stream.cuda_stream)
+        C.check(rc, f"{kind} stage failed")
+        return _to_output(out, torch_mode)
+
+
+# ---------------------------------------------------------------------------- functional API
+
+
+def linear_to_ssa(linear_path, n):
+    """Inverse of ssa_to_linear (pybind/src/lib.rs:153-175)."""
+    ids = list(range(n))
+    out = []
+    for nxt, (a, b) in enumerate(linear_path, start=n):
+        lo, hi = (a, b) if a < b else (b, a)
+        if hi >= len(ids) or lo == hi:
+            raise ValueError(f"linear path index out of range or self-contraction: ({a},{b}); "
+                             f"{len(ids)} tensors are alive (pass SSA paths through ssa_path=)")
+        out.append((ids[lo], ids[hi]))
+        del ids[hi]
+        del ids[lo]
+        ids.append(nxt)
+    return out
+
+
+def ssa_to_linear(ssa_path, n):
+    """Recycled linear form of an SSA path (pybind/src/lib.rs:137-151)."""
+    ids = list(range(n))
+    out = []
+    for nxt, (a, b) in enumerate(ssa_path, start=n):
+        ia, ib = ids.index(a), ids.index(b)
+        lo, hi = (ia, ib) if ia < ib else (ib, ia)
+        out.append((lo, hi))
+        del ids[hi]
+        del ids[lo]
+        ids.append(nxt)
+    return out
+
+
+def contract_sliced(inputs, output, size_dict, arrays, sliced_legs, path=None, ssa_path=None, *,
+                    precision="fp32", f64_out=False):
+    """Execute a supplied path over every slice assignment (pybind/src/lib.rs:692-765)."""
+    n = len(inputs)
+    arrays = list(arrays)
+    if len(arrays) != n:
+        raise ValueError(f"{len(arrays)} arrays given for {n} inputs")
+    if path is not None and ssa_path is not None:
+        raise ValueError("path and ssa_path are mutually exclusive (path = linear form, ssa_path = SSA form)")
+    for leg in sliced_legs:
+        if int(leg) not in {int(k) for k in size_dict}:
+            raise ValueError(f"sliced leg {leg} is not in the network's size_dict")
+    arrays, code, torch_mode = _preflight(arrays, inputs, size_dict, "sliced contraction failed")
+    if ssa_path is not None:
+        ssa = [tuple(p) for p in ssa_path]
+    elif path is not None:
+        ssa = linear_to_ssa(path, n)
+    else:
+        raise ValueError("give path= (linear form) or ssa_path= (SSA form)")
+    dev = arrays[0].device.index if torch_mode else None
+    prog = SlicedProgram(inputs, output, size_dict, ssa, sliced_legs, dtype=code, precision=precision, device=dev,
+                         use_graph=False)
+    return prog.execute(arrays, f64_out=f64_out)
+
+
+def _to_int_labels(inputs, output, size_dict):
+    """Arbitrary hashable labels -> dense u32 ids (pybind/python/arctn/__init__.py:186-235)."""
+    if not hasattr(size_dict, "items"):
+        raise TypeError("size_dict must be a mapping from leg label to positive integer dimension")
+    label_of = {}
+
+    def idx(lab):
+        i = label_of.get(lab)
+        if i is None:
+            i = len(label_of)
+            label_of[lab] = i
+        return i
+
+    inputs_i = [[idx(l) for l in term] for term in inputs]
+    output_i = [idx(l) for l in output]
+    missing = [lab for lab in label_of if lab not in size_dict]
+    if missing:
+        raise ValueError(f"size_dict lacks dimensions of used legs: {missing!r}")
+    unused = [lab for lab in size_dict if lab not in label_of]
+    if unused:
+        raise ValueError(f"size_dict holds legs not used in inputs/output: {unused!r}")
+    size_i = {}
+    for lab, i in label_of.items():
+        raw = size_dict[lab]
+        if isinstance(raw, bool):
+            raise ValueError(f"dimension of leg {lab!r} must be a positive integer, not bool")
+        dim = operator.index(raw)
+        if dim <= 0:
+            raise ValueError(f"dimension of leg {lab!r} must be positive, got {dim}")
+        size_i[i] = dim
+    return inputs_i, output_i, size_i, label_of
+
+
+def _validate_backend(backend):
+    if not isinstance(backend, str) or not backend or backend != backend.strip():
+        raise ValueError(f"backend must be a non-empty string without surrounding spaces, got {backend!r}")
+    if backend == "auto":
+        raise ValueError("backend must be chosen explicitly; this package executes backend='b200'")
+    if backend != "b200":
+        raise ValueError(f"backend {backend!r} is not provided by arctn_b200; use backend='b200'")
+    return backend
+
+
+class ArcTNCompiledContraction:
+    """``ArcTNCompiledContraction`` with ``backend='b200'`` (pybind/python/arctn/__init__.py:749-853)."""
+
+    def __init__(self, backend, inputs, output, size_dict, ssa_path, implementation, compile_wall_s):
+        self.backend = backend
+        self.inputs = tuple(tuple(t) for t in inputs)
+        self.output = tuple(output)
+        self.size_dict = dict(size_dict)
+        self.ssa_path = tuple(tuple(p) for p in ssa_path)
+        self._implementation = implementation
+        self.compile_wall_s = float(compile_wall_s)
+        self.last_execute_wall_s = None
+        self.last_dispatch_wall_s = None
+
+    @classmethod
+    def compile(cls, inputs, output, size_dict, *, ssa_path, backend="b200"):
+        backend = _validate_backend(backend)
+        inputs_i, output_i, size_i, _ = _to_int_labels(inputs, output, size_dict)
+        ssa_path = [tuple(p) for p in ssa_path]
+        t0 = time.perf_counter()
+        impl = CompiledContraction.compile(inputs_i, output_i, size_i, ssa_path=ssa_path)
+        return cls(backend, inputs_i, output_i, size_i, ssa_path, impl, time.perf_counter() - t0)
+
+    def execute(self, arrays, *, precision="fp32"):
+        t0 = time.perf_counter()
+        result = self._implementation.execute(arrays, precision=precision)
+        self.last_dispatch_wall_s = time.perf_counter() - t0
+        self.last_execute_wall_s = self.last_dispatch_wall_s
+        return result
+
+    __call__ = execute
+
+    def stats(self):
+        out = {"backend": self.backend, "path_format": "ssa-v1", "n_inputs": len(self.inputs),
+               "n_steps": len(self.ssa_path), "compile_wall_s": self.compile_wall_s,
+               "last_execute_wall_s": self.last_execute_wall_s, "last_dispatch_wall_s": self.last_dispatch_wall_s}
+        out.update(self._implementation.stats())
+        return out
+
+    def __repr__(self):
+        return (f"ArcTNCompiledContraction(backend={self.backend!r}, n_inputs={len(self.inputs)}, "
+                f"n_steps={len(self.ssa_path)})")
+
+
+def arctn_contract(inputs, output, size_dict, arrays, *, target_size=None, backend="b200", ssa_path=None,
+                   sliced_legs=None, precision="fp32", return_info=False):
+    """Plan (when no path is given), optionally slice, and execute on the B200 executor.
+
+    Mirrors ``arctn_contract`` (pybind/python/arctn/__init__.py:903-1072).  The
+    reference plans with its closed-source engine; here the public greedy
+    planner (src/paths/greedy.rs:317-320) and ``find_slices_to_size``
+    (src/slice.rs:209-215) produce the path and slices unless they are given.
+    """
+    backend = _validate_backend(backend)
+    inputs_i, output_i, size_i, _ = _to_int_labels(inputs, output, size_dict)
+    if target_size is not None:
+        target_size = operator.index(target_size)
+        if target_size < 1:
+            raise ValueError(f"target_size must be >= 1, got {target_size}")
+    t0 = time.perf_counter()
+    ssa = [tuple(p) for p in ssa_path] if ssa_path is not None else greedy(inputs_i, output_i, size_i)
+    if sliced_legs is None:
+        sliced_legs = []
+        if target_size is not None:
+            found = find_slices_to_size(inputs_i, output_i, size_i, ssa, target_size)
+            if found is None:
+                raise ValueError(f"target_size (log2={math.log2(target_size):.6g}) is unreachable: no slicing "
+                                 "meets it")
+            sliced_legs = found
+    plan_wall = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    result = contract_sliced(inputs_i, output_i, size_i, arrays, sliced_legs, ssa_path=ssa, precision=precision)
+    exec_wall = time.perf_counter() - t1
+    if return_info:
+        info = {"path": ssa, "sliced_legs": list(sliced_legs), "execution_backend": backend,
+                "execution_implementation": "arctn_b200.contract_sliced", "planning_wall_s": plan_wall,
+                "execution_wall_s": exec_wall, "target_size": target_size}
+        info.update(simulate_path(inputs_i, output_i, size_i, ssa))
+        return result, info
+    return result

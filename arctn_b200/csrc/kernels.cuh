@@ -1,0 +1,293 @@
+// SIMT kernels of the B200 executor (sm_100a).
+//
+// Every kernel reads its operands through offset tables built on the host: a
+// pairwise step C[s,b,i,j] = sum_l A[s,b,i,l] * B[s,b,l,j] reads
+//   A[sliceoff_A(s) + aB[b] + aM[i] + aK[l]]   and   B[sliceoff_B(s) + bB[b] + bK[l] + bN[j]]
+// so the reference's permute (src/tensor.rs:453-492) and slice selection
+// (src/tensor.rs:636-669, src/slice.rs:1005-1012) are folded into the GEMM's
+// loads instead of being materialised in HBM.  `s` runs over the slices of one
+// group; slices are an extra batch dimension of every step.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ab2 {
+
+typedef long long ll;
+
+// ---------------------------------------------------------------- scalar types
+struct __align__(8) cf32 { float re, im; };
+struct __align__(16) cf64 { double re, im; };
+
+template <class T> struct Num;
+template <> struct Num<float> {
+  using acc = float; using wide = double;
+  __device__ static float zero() { return 0.f; }
+  __device__ static void fma(float& c, float a, float b) { c = fmaf(a, b, c); }
+  __device__ static double widen(float v) { return (double)v; }
+  __device__ static float narrow(double v) { return (float)v; }
+  __device__ static float add(float a, float b) { return a + b; }
+  __device__ static double mag(float v) { return fabs((double)v); }
+  __device__ static float scale(float v, double s) { return v * (float)s; }
+};
+template <> struct Num<double> {
+  using acc = double; using wide = double;
+  __device__ static double zero() { return 0.0; }
+  __device__ static void fma(double& c, double a, double b) { c = fma_rn(a, b, c); }
+  __device__ static double fma_rn(double a, double b, double c) { return ::fma(a, b, c); }
+  __device__ static double widen(double v) { return v; }
+  __device__ static double narrow(double v) { return v; }
+  __device__ static double add(double a, double b) { return a + b; }
+  __device__ static double mag(double v) { return fabs(v); }
+  __device__ static double scale(double v, double s) { return v * s; }
+};
+template <> struct Num<cf32> {
+  using acc = cf32; using wide = cf64;
+  __device__ static cf32 zero() { return {0.f, 0.f}; }
+  __device__ static void fma(cf32& c, cf32 a, cf32 b) {
+    c.re = fmaf(a.re, b.re, c.re);
+    c.re = fmaf(-a.im, b.im, c.re);
+    c.im = fmaf(a.re, b.im, c.im);
+    c.im = fmaf(a.im, b.re, c.im);
+  }
+  __device__ static cf64 widen(cf32 v) { return {(double)v.re, (double)v.im}; }
+  __device__ static cf32 narrow(cf64 v) { return {(float)v.re, (float)v.im}; }
+  __device__ static cf32 add(cf32 a, cf32 b) { return {a.re + b.re, a.im + b.im}; }
+  __device__ static double mag(cf32 v) { return hypot((double)v.re, (double)v.im); }
+  __device__ static cf32 scale(cf32 v, double s) { float f = (float)s; return {v.re * f, v.im * f}; }
+};
+template <> struct Num<cf64> {
+  using acc = cf64; using wide = cf64;
+  __device__ static cf64 zero() { return {0.0, 0.0}; }
+  __device__ static void fma(cf64& c, cf64 a, cf64 b) {
+    c.re = ::fma(a.re, b.re, c.re);
+    c.re = ::fma(-a.im, b.im, c.re);
+    c.im = ::fma(a.re, b.im, c.im);
+    c.im = ::fma(a.im, b.re, c.im);
+  }
+  __device__ static cf64 widen(cf64 v) { return v; }
+  __device__ static cf64 narrow(cf64 v) { return v; }
+  __device__ static cf64 add(cf64 a, cf64 b) { return {a.re + b.re, a.im + b.im}; }
+  __device__ static double mag(cf64 v) { return hypot(v.re, v.im); }
+  __device__ static cf64 scale(cf64 v, double s) { return {v.re * s, v.im * s}; }
+};
+
+__device__ inline double wadd(double a, double b) { return a + b; }
+__device__ inline cf64 wadd(cf64 a, cf64 b) { return {a.re + b.re, a.im + b.im}; }
+__device__ inline double wzero(double*) { return 0.0; }
+__device__ inline cf64 wzero(cf64*) { return {0.0, 0.0}; }
+
+// ---------------------------------------------------------------- slice offsets
+// Element offset of slice `s` (local index inside a group) of one operand:
+//   s * local_stride + sum_t ((g0 + s) / div_t % mod_t) * stride_t
+// The first term addresses per-slice intermediates laid out [S][numel]; the
+// terms decode the global slice number into sliced-leg values for an input
+// tensor (last sliced leg fastest, src/slice.rs:881-888).
+constexpr int kMaxSliceTerms = 12;
+struct SliceTerm { ll div, mod, stride; };
+struct SliceOff {
+  ll local_stride;
+  int n;
+  SliceTerm t[kMaxSliceTerms];
+};
+
+__device__ __forceinline__ ll slice_offset(const SliceOff& so, ll g0, ll s) {
+  ll off = s * so.local_stride;
+  const ll g = g0 + s;
+  for (int i = 0; i < so.n; ++i) off += ((g / so.t[i].div) % so.t[i].mod) * so.t[i].stride;
+  return off;
+}
+
+// ---------------------------------------------------------------- gather-reduce
+// out[s*n_out + e] = sum_{r < n_red} in[sliceoff(s) + offE[e] + offR[r]]
+// Used for input traces / diagonals (src/tensor.rs:503-590), dangling-leg sums
+// (src/tensor.rs:593-633) and the final sum + permute (src/compiled.rs:211-218).
+template <class T, class TO>
+struct OutCast;
+template <class T> struct OutCast<T, T> { __device__ static T cast(T v) { return v; } };
+template <> struct OutCast<float, double> { __device__ static double cast(float v) { return v; } };
+template <> struct OutCast<cf32, cf64> { __device__ static cf64 cast(cf32 v) { return {(double)v.re, (double)v.im}; } };
+
+template <class T, class TO>
+__global__ void k_gather_reduce(const T* __restrict__ in, TO* __restrict__ out, const ll* __restrict__ offE,
+                                const ll* __restrict__ offR, ll n_out, ll n_red, ll S, SliceOff so, ll g0) {
+  const ll total = S * n_out;
+  for (ll idx = (ll)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (ll)gridDim.x * blockDim.x) {
+    const ll s = idx / n_out, e = idx - s * n_out;
+    const T* base = in + slice_offset(so, g0, s) + offE[e];
+    T acc = base[offR[0]];
+    for (ll r = 1; r < n_red; ++r) acc = Num<T>::add(acc, base[offR[r]]);
+    out[idx] = OutCast<T, TO>::cast(acc);
+  }
+}
+
+// ---------------------------------------------------------------- GEMM tables
+struct GemmArgs {
+  const void* A;
+  const void* B;
+  void* C;
+  ll bt, m, k, n, S, g0;
+  const ll* aB; const ll* aM; const ll* aK;
+  const ll* bB; const ll* bK; const ll* bN;
+  SliceOff sa, sb;
+};
+
+// Thin steps: one thread per output element, k-loop through the tables.
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm_small(GemmArgs g) {
+  using A = typename Num<T>::acc;
+  const T* Ap = (const T*)g.A;
+  const T* Bp = (const T*)g.B;
+  T* Cp = (T*)g.C;
+  const ll mn = g.m * g.n, per_s = g.bt * mn, total = g.S * per_s;
+  extern __shared__ ll sh_tab[];  // aK[0..k) then bK[0..k) when they fit
+  const bool tab_in_smem = g.k <= 1024;
+  if (tab_in_smem) {
+    for (ll l = threadIdx.x; l < g.k; l += blockDim.x) { sh_tab[l] = g.aK[l]; sh_tab[g.k + l] = g.bK[l]; }
+    __syncthreads();
+  }
+  const ll* aK = tab_in_smem ? sh_tab : g.aK;
+  const ll* bK = tab_in_smem ? sh_tab + g.k : g.bK;
+  for (ll idx = (ll)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (ll)gridDim.x * blockDim.x) {
+    const ll s = idx / per_s;
+    ll r = idx - s * per_s;
+    const ll b = r / mn;
+    r -= b * mn;
+    const ll i = r / g.n, j = r - i * g.n;
+    const T* a = Ap + slice_offset(g.sa, g.g0, s) + g.aB[b] + g.aM[i];
+    const T* bb = Bp + slice_offset(g.sb, g.g0, s) + g.bB[b] + g.bN[j];
+    A acc = Num<T>::zero();
+    for (ll l = 0; l < g.k; ++l) Num<T>::fma(acc, a[aK[l]], bb[bK[l]]);
+    Cp[idx] = acc;
+  }
+}
+
+// Dense-enough steps on the CUDA cores: TM x TN output tile per CTA, TK-deep
+// k-slabs staged through shared memory, (TM/16) x (TN/16) outputs per thread.
+// This is the plain-FP32 (or FP64) form of the step GEMM.
+template <class T, int TM, int TN, int TK>
+__global__ void __launch_bounds__(256) k_gemm_tile(GemmArgs g) {
+  constexpr int RM = TM / 16, RN = TN / 16;
+  __shared__ T As[TK][TM + 1];
+  __shared__ T Bs[TK][TN + 1];
+  const T* Ap = (const T*)g.A;
+  const T* Bp = (const T*)g.B;
+  T* Cp = (T*)g.C;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const ll tiles_n = (g.n + TN - 1) / TN, tiles_m = (g.m + TM - 1) / TM;
+  const ll n_tiles = tiles_n * tiles_m * g.S * g.bt;
+  for (ll t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    ll r = t;
+    const ll tn = r % tiles_n; r /= tiles_n;
+    const ll tm = r % tiles_m; r /= tiles_m;
+    const ll sb = r, s = sb / g.bt, b = sb - s * g.bt;
+    const ll i0 = tm * TM, j0 = tn * TN;
+    const T* abase = Ap + slice_offset(g.sa, g.g0, s) + g.aB[b];
+    const T* bbase = Bp + slice_offset(g.sb, g.g0, s) + g.bB[b];
+    typename Num<T>::acc acc[RM][RN];
+#pragma unroll
+    for (int x = 0; x < RM; ++x)
+#pragma unroll
+      for (int y = 0; y < RN; ++y) acc[x][y] = Num<T>::zero();
+    for (ll l0 = 0; l0 < g.k; l0 += TK) {
+      for (int q = threadIdx.x; q < TM * TK; q += 256) {
+        const int ii = q / TK, ll_ = q % TK;
+        const ll i = i0 + ii, l = l0 + ll_;
+        As[ll_][ii] = (i < g.m && l < g.k) ? abase[g.aM[i] + g.aK[l]] : Num<T>::zero();
+      }
+      for (int q = threadIdx.x; q < TN * TK; q += 256) {
+        const int jj = q % TN, ll_ = q / TN;
+        const ll j = j0 + jj, l = l0 + ll_;
+        Bs[ll_][jj] = (j < g.n && l < g.k) ? bbase[g.bK[l] + g.bN[j]] : Num<T>::zero();
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int l = 0; l < TK; ++l) {
+        T av[RM], bv[RN];
+#pragma unroll
+        for (int x = 0; x < RM; ++x) av[x] = As[l][ty + 16 * x];
+#pragma unroll
+        for (int y = 0; y < RN; ++y) bv[y] = Bs[l][tx + 16 * y];
+#pragma unroll
+        for (int x = 0; x < RM; ++x)
+#pragma unroll
+          for (int y = 0; y < RN; ++y) Num<T>::fma(acc[x][y], av[x], bv[y]);
+      }
+      __syncthreads();
+    }
+    T* cbase = Cp + (s * g.bt + b) * g.m * g.n;
+#pragma unroll
+    for (int x = 0; x < RM; ++x)
+#pragma unroll
+      for (int y = 0; y < RN; ++y) {
+        const ll i = i0 + ty + 16 * x, j = j0 + tx + 16 * y;
+        if (i < g.m && j < g.n) cbase[i * g.n + j] = acc[x][y];
+      }
+  }
+}
+
+// ---------------------------------------------------------------- cross-slice sum
+// FP64 accumulation of per-slice results into chunk partials, in slice order
+// within each chunk (src/slice.rs:1020-1064).  A segment is one (block, chunk)
+// intersected with the current group: partial[seg.part] += sum_{s in [lo,hi)} F[s].
+struct Segment { ll part, lo, hi; };  // lo/hi are local slice indices in the group
+
+template <class T>
+__global__ void k_slice_accumulate(const T* __restrict__ F, typename Num<T>::wide* __restrict__ P,
+                                   const Segment* __restrict__ segs, ll n_segs, ll n_e) {
+  using W = typename Num<T>::wide;
+  const ll total = n_segs * n_e;
+  for (ll idx = (ll)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (ll)gridDim.x * blockDim.x) {
+    const ll sg = idx / n_e, e = idx - sg * n_e;
+    const Segment seg = segs[sg];
+    W acc = P[seg.part * n_e + e];
+    for (ll s = seg.lo; s < seg.hi; ++s) acc = wadd(acc, Num<T>::widen(F[s * n_e + e]));
+    P[seg.part * n_e + e] = acc;
+  }
+}
+
+// out[blockbase[blk] + scatter[e]] = sum_c P[blk][c][e], chunks merged in order.
+template <class T, class TO>
+__global__ void k_slice_output(const typename Num<T>::wide* __restrict__ P, TO* __restrict__ out,
+                               const ll* __restrict__ block_base, const ll* __restrict__ scatter, ll n_blocks,
+                               ll n_chunks, ll n_e) {
+  using W = typename Num<T>::wide;
+  const ll total = n_blocks * n_e;
+  for (ll idx = (ll)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (ll)gridDim.x * blockDim.x) {
+    const ll blk = idx / n_e, e = idx - blk * n_e;
+    const W* p = P + blk * n_chunks * n_e + e;
+    W acc = p[0];
+    for (ll c = 1; c < n_chunks; ++c) acc = wadd(acc, p[c * n_e]);
+    TO v;
+    if constexpr (sizeof(TO) == sizeof(W)) v = *reinterpret_cast<TO*>(&acc);
+    else v = Num<T>::narrow(acc);
+    out[block_base[blk] + scatter[e]] = v;
+  }
+}
+
+// ---------------------------------------------------------------- stripped execution
+// max |c| over a step result (src/compiled.rs:412-421), reduced into *mx as
+// the bit pattern of a non-negative double (monotone under unsigned compare).
+template <class T>
+__global__ void k_maxabs(const T* __restrict__ c, ll n, unsigned long long* mx) {
+  double m = 0.0;
+  for (ll i = (ll)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (ll)gridDim.x * blockDim.x) {
+    double v = Num<T>::mag(c[i]);
+    if (!(v <= m)) m = v;  // propagates NaN as a large value
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(mx, (unsigned long long)__double_as_longlong(m));
+}
+
+// Divide by the max and accumulate log10(max) (src/compiled.rs:422-429).
+template <class T>
+__global__ void k_strip_scale(T* __restrict__ c, ll n, const unsigned long long* mx, double* exponent, int last_block_adds) {
+  const double f = __longlong_as_double((long long)*mx);
+  if (!(f > 0.0) || isinf(f) || isnan(f)) return;
+  const double inv = 1.0 / f;
+  for (ll i = (ll)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (ll)gridDim.x * blockDim.x) c[i] = Num<T>::scale(c[i], inv);
+  if (last_block_adds && blockIdx.x == 0 && threadIdx.x == 0) *exponent += log10(f);
+}
+
+}  // namespace ab2

@@ -1,0 +1,811 @@
+// Device program: build (host) and execution (launch sequence / CUDA graph).
+//
+// Execution model.  Every slice of a sliced contraction runs the same plan
+// (src/slice.rs:997-1016), so slices are executed as an extra batch dimension
+// of each pairwise step rather than one after another.  A slot that holds no
+// sliced leg is slice-invariant: the steps producing it run once, in a first
+// phase, and their results are shared by all slices.  The remaining
+// (slice-variant) steps run per group of S consecutive slices; each group's
+// per-slice results are folded into FP64 chunk partials in the reference's
+// deterministic chunk order (src/slice.rs:1020-1064, 1070-1173).
+#include "program.hpp"
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+#include <set>
+
+namespace ab2 {
+
+#define CK(x)                                                                                   \
+  do {                                                                                          \
+    cudaError_t e_ = (x);                                                                       \
+    if (e_ != cudaSuccess) throw Error(E_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+size_t dtype_bytes(int dt) {
+  switch (dt) {
+    case DT_F32: return 4;
+    case DT_F64: return 8;
+    case DT_C64: return 8;
+    case DT_C128: return 16;
+  }
+  throw Error(E_INVALID, "unsupported dtype code " + std::to_string(dt));
+}
+static size_t wide_bytes(int dt) { return dtype_complex(dt) ? 16 : 8; }
+
+namespace {
+
+constexpr u64 kAlign = 256;
+constexpr u64 kInf = ~0ull;
+inline u64 align_up(u64 x) { return (x + kAlign - 1) / kAlign * kAlign; }
+
+// Per-slice strided view of a slot.
+struct View {
+  Ref ref;
+  std::vector<u64> shape;
+  std::vector<ll> strides;
+  SliceOff so{};
+  bool variant = false;
+};
+
+u64 prod(const std::vector<u64>& v) {
+  unsigned __int128 p = 1;
+  for (u64 x : v) {
+    p *= x;
+    if (p > (unsigned __int128)INT64_MAX) throw Error(E_UNSUPPORTED, "tensor element count exceeds the device index range");
+  }
+  return (u64)p;
+}
+
+// Offsets of every multi-index over (dims, strides), last axis fastest.
+std::vector<ll> offsets(const std::vector<u64>& dims, const std::vector<ll>& strides) {
+  const u64 n = prod(dims);
+  std::vector<ll> out(n);
+  std::vector<u64> idx(dims.size(), 0);
+  ll off = 0;
+  for (u64 e = 0; e < n; ++e) {
+    out[e] = off;
+    for (size_t d = dims.size(); d-- > 0;) {
+      ++idx[d];
+      off += strides[d];
+      if (idx[d] < dims[d]) break;
+      off -= strides[d] * (ll)dims[d];
+      idx[d] = 0;
+    }
+  }
+  return out;
+}
+
+std::vector<ll> rm_strides(const std::vector<u64>& shape) {
+  std::vector<ll> s(shape.size(), 1);
+  for (size_t i = shape.size(); i-- > 1;) s[i - 1] = s[i] * (ll)shape[i];
+  return s;
+}
+
+// Axis indices left after removing `seq` one at a time (sum_axis order).
+void split_removed(size_t rank, const std::vector<u64>& seq, std::vector<size_t>& kept, std::vector<size_t>& removed) {
+  kept.resize(rank);
+  std::iota(kept.begin(), kept.end(), 0);
+  removed.clear();
+  for (u64 r : seq) {
+    removed.push_back(kept[r]);
+    kept.erase(kept.begin() + r);
+  }
+}
+
+template <class F>
+void pick(const View& v, const std::vector<size_t>& axes, std::vector<u64>& dims, std::vector<ll>& strides, F&&) {
+  dims.clear();
+  strides.clear();
+  for (size_t a : axes) { dims.push_back(v.shape[a]); strides.push_back(v.strides[a]); }
+}
+
+}  // namespace
+
+Program::Program(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced, const ProgramOptions& opt)
+    : opt_(opt) {
+  dtype_bytes(opt_.dtype);
+  if (opt_.precision != PREC_FP32 && opt_.precision != PREC_TF32X3)
+    throw Error(E_INVALID, "unsupported precision mode " + std::to_string(opt_.precision));
+  build(net, path, sliced);
+  int prev = 0;
+  CK(cudaGetDevice(&prev));
+  CK(cudaSetDevice(opt_.device));
+  cudaError_t e = cudaMalloc(&dev_tab_, std::max<size_t>(host_tab_.size(), 256));
+  if (e == cudaSuccess) e = cudaMemcpy(dev_tab_, host_tab_.data(), host_tab_.size(), cudaMemcpyHostToDevice);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) throw Error(E_CUDA, std::string("uploading offset tables: ") + cudaGetErrorString(e));
+}
+
+Program::~Program() {
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(opt_.device);
+  if (gexec_) cudaGraphExecDestroy(gexec_);
+  if (dev_tab_) cudaFree(dev_tab_);
+  cudaSetDevice(prev);
+}
+
+void Program::build(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced) {
+  net.validate();
+  validate_slice_legs(net, sliced);
+  const int dt = opt_.dtype;
+  const u64 eb = dtype_bytes(dt);
+  std::set<Leg> sl(sliced.begin(), sliced.end());
+  std::vector<Leg> outer, internal;
+  for (Leg l : net.output)
+    if (sl.count(l)) outer.push_back(l);
+  for (Leg l : sliced)
+    if (std::find(outer.begin(), outer.end(), l) == outer.end()) internal.push_back(l);
+  {
+    unsigned __int128 t = 1;
+    for (Leg l : sliced) {
+      t *= net.dim(l);
+      if (t > (unsigned __int128)UINT64_MAX) fail("slice count overflows usize");
+    }
+  }
+  std::vector<u64> full_out_shape;
+  for (Leg l : net.output) full_out_shape.push_back(net.dim(l));
+  const u64 full_out_numel = checked_numel(full_out_shape);
+  if (!outer.empty() && (unsigned __int128)full_out_numel * eb > (unsigned __int128)INT64_MAX)
+    fail("the full output tensor's byte size exceeds the allocatable capacity");
+
+  // Per-slice network: every sliced leg removed (src/slice.rs:990-996, 1113-1120).
+  Network sub = net;
+  for (auto& t : sub.inputs) t.erase(std::remove_if(t.begin(), t.end(), [&](Leg l) { return sl.count(l) > 0; }), t.end());
+  sub.output.erase(std::remove_if(sub.output.begin(), sub.output.end(), [&](Leg l) { return sl.count(l) > 0; }), sub.output.end());
+  for (Leg l : sliced) sub.size.erase(l);
+  plan_ = compile_plan(sub, path);
+
+  sliced_ = !sliced.empty();
+  n_int_ = 1;
+  for (Leg l : internal) n_int_ *= net.dim(l);
+  n_blocks_ = 1;
+  for (Leg l : outer) n_blocks_ *= net.dim(l);
+  n_total_ = n_int_ * n_blocks_;
+  range_begin_ = 0;
+  range_end_ = n_total_;
+  if (opt_.slice_begin || opt_.slice_end) {
+    if (opt_.slice_end <= opt_.slice_begin || opt_.slice_end > n_total_)
+      fail("slice range [" + std::to_string(opt_.slice_begin) + ", " + std::to_string(opt_.slice_end) +
+           ") is outside [0, " + std::to_string(n_total_) + ")");
+    range_begin_ = opt_.slice_begin;
+    range_end_ = opt_.slice_end;
+  }
+  std::vector<u64> sub_out_shape;
+  for (Leg l : sub.output) sub_out_shape.push_back(net.dim(l));
+  const u64 n_e = std::max<u64>(prod(sub_out_shape), 1);
+  n_chunks_ = internal.empty() ? 1 : slice_parallel_chunks(n_int_, n_e);
+
+  double macs = 0;
+  for (auto& st : plan_.steps) macs += (double)st.bt * st.m * st.k * st.n;
+  flops_ = (dtype_complex(dt) ? 8.0 : 2.0) * macs * (double)(range_end_ - range_begin_);
+
+  // ---------------------------------------------------------------- buffers / ops
+  std::vector<Buf> bufs;
+  std::vector<Op> ops1, ops2, strip1;
+  const bool want_strip = !sliced_;
+  auto new_buf = [&](bool region2, u64 bytes, u64 first) {
+    bufs.push_back(Buf{bytes, first, first, region2, 0});
+    return (u64)bufs.size() - 1;
+  };
+  // A region-1 buffer read by a phase-2 op must outlive phase 1.
+  auto touch = [&](const Ref& r, bool phase2, u64 at) {
+    if (r.kind != Ref::WS) return;
+    Buf& b = bufs[r.index];
+    if (!b.region2 && phase2) b.last = kInf;
+    else if (b.last != kInf) b.last = std::max(b.last, at);
+  };
+  auto tab_ll = [&](const std::vector<ll>& v) {
+    u64 off = align_up(host_tab_.size());
+    host_tab_.resize(off + v.size() * sizeof(ll));
+    std::memcpy(host_tab_.data() + off, v.data(), v.size() * sizeof(ll));
+    return off;
+  };
+  auto emit = [&](bool phase2, const Op& op, bool also_strip) {
+    if (phase2) ops2.push_back(op);
+    else {
+      ops1.push_back(op);
+      if (also_strip) strip1.push_back(op);
+    }
+  };
+  auto opidx = [&](bool phase2) { return (u64)(phase2 ? ops2.size() : ops1.size()); };
+
+  // Slice decode of every sliced leg: value = (g / div) % dim.
+  std::map<Leg, std::pair<ll, ll>> decode;  // leg -> (div, mod)
+  {
+    ll div = 1;
+    for (size_t q = internal.size(); q-- > 0;) { decode[internal[q]] = {div, (ll)net.dim(internal[q])}; div *= (ll)net.dim(internal[q]); }
+    div = (ll)n_int_;
+    for (size_t q = outer.size(); q-- > 0;) { decode[outer[q]] = {div, (ll)net.dim(outer[q])}; div *= (ll)net.dim(outer[q]); }
+  }
+
+  // FP64 partials [n_blocks][n_chunks][n_e] live through the whole run.
+  u64 part_buf = kInf;
+  if (sliced_) {
+    part_buf = new_buf(false, n_blocks_ * n_chunks_ * n_e * wide_bytes(dt), 0);
+    bufs[part_buf].last = kInf;
+    Op z{Op::MEMSET};
+    z.c = Ref{Ref::WS, part_buf};
+    z.bytes = bufs[part_buf].bytes;
+    emit(false, z, false);
+  }
+  if (want_strip) {
+    u64 b = new_buf(false, 16, 0);
+    bufs[b].last = kInf;
+    strip_exp_off_ = b;  // patched to a byte offset after layout
+    Op z{Op::MEMSET};
+    z.c = Ref{Ref::WS, b};
+    z.bytes = 16;
+    strip1.push_back(z);
+  }
+
+  // ---------------------------------------------------------------- input views
+  std::set<Leg> outs(net.output.begin(), net.output.end());
+  std::map<Leg, u64> holders;
+  for (auto& t : net.inputs) {
+    std::set<Leg> u(t.begin(), t.end());
+    for (Leg l : u) ++holders[l];
+  }
+  const size_t n_slots = plan_.n_inputs + plan_.steps.size();
+  std::vector<View> view(n_slots);
+  for (size_t i = 0; i < net.n_tensors(); ++i) {
+    struct Ax { u64 dim; ll stride; Leg leg; };
+    std::vector<Ax> ax, red;
+    std::vector<u64> shape0;
+    for (Leg l : net.inputs[i]) shape0.push_back(net.dim(l));
+    auto st0 = rm_strides(shape0);
+    for (size_t a = 0; a < shape0.size(); ++a) ax.push_back({shape0[a], st0[a], net.inputs[i][a]});
+    std::vector<Leg> legs = net.inputs[i];
+    auto traces = plan_traces(legs, [&](Leg l) { return holders[l] > 1 || outs.count(l) > 0; });
+    for (size_t t = 0; t < traces.size(); t += 3) {
+      size_t ai = traces[t], aj = traces[t + 1];
+      if (traces[t + 2]) {  // diagonal keeps axis ai and walks both strides
+        ax[ai].stride += ax[aj].stride;
+        ax.erase(ax.begin() + aj);
+      } else {              // trace sums the diagonal and drops both axes
+        red.push_back({ax[ai].dim, ax[ai].stride + ax[aj].stride, ax[ai].leg});
+        ax.erase(ax.begin() + aj);
+        ax.erase(ax.begin() + ai);
+      }
+    }
+    View v;
+    v.ref = Ref{Ref::INPUT, i};
+    std::vector<u64> pdims;
+    std::vector<ll> pstr;
+    for (auto& a : ax) { pdims.push_back(a.dim); pstr.push_back(a.stride); }
+    if (!traces.empty()) {
+      // Materialise the prepared full tensor once (slice-invariant work).
+      std::vector<u64> rd;
+      std::vector<ll> rs;
+      for (auto& r : red) { rd.push_back(r.dim); rs.push_back(r.stride); }
+      u64 numel = prod(pdims);
+      u64 b = new_buf(false, numel * eb, opidx(false));
+      bufs[b].last = kInf;
+      Op g{Op::GATHER};
+      g.a = v.ref;
+      g.c = Ref{Ref::WS, b};
+      g.tab[0] = tab_ll(offsets(pdims, pstr));
+      g.tab[1] = tab_ll(rd.empty() ? std::vector<ll>{0} : offsets(rd, rs));
+      g.n_out = (ll)numel;
+      g.n_red = rd.empty() ? 1 : (ll)prod(rd);
+      g.S = 1;
+      emit(false, g, true);
+      v.ref = Ref{Ref::WS, b};
+      pstr = rm_strides(pdims);
+    }
+    std::vector<std::pair<ll, std::pair<ll, ll>>> terms;  // (stride, (div, mod))
+    for (size_t a = 0; a < ax.size(); ++a) {
+      if (sl.count(ax[a].leg)) {
+        auto dm = decode.at(ax[a].leg);
+        terms.push_back({pstr[a], dm});
+      } else {
+        v.shape.push_back(pdims[a]);
+        v.strides.push_back(pstr[a]);
+      }
+    }
+    // Merge terms that address one contiguous run of sliced legs.
+    std::sort(terms.begin(), terms.end(), [](auto& x, auto& y) { return x.second.first < y.second.first; });
+    std::vector<SliceTerm> merged;
+    for (auto& t : terms) {
+      SliceTerm nt{t.second.first, t.second.second, t.first};
+      if (!merged.empty()) {
+        SliceTerm& p = merged.back();
+        if (p.div * p.mod == nt.div && p.stride * p.mod == nt.stride) { p.mod *= nt.mod; continue; }
+      }
+      merged.push_back(nt);
+    }
+    if (merged.size() > (size_t)kMaxSliceTerms)
+      throw Error(E_UNSUPPORTED, "input " + std::to_string(i) + " holds sliced legs that need more than " +
+                                     std::to_string(kMaxSliceTerms) + " slice-offset terms");
+    v.so.local_stride = 0;
+    v.so.n = (int)merged.size();
+    for (size_t t = 0; t < merged.size(); ++t) v.so.t[t] = merged[t];
+    v.variant = !merged.empty();
+    if (v.shape != plan_.preps[i].shape) throw Error(E_INVALID, "internal: prepared input shape mismatch");
+    view[i] = v;
+  }
+
+  // ---------------------------------------------------------------- pairwise steps
+  auto reduce_view = [&](View v, const std::vector<u64>& seq, bool phase2, Op* strip_dummy) -> View {
+    (void)strip_dummy;
+    if (seq.empty()) return v;
+    std::vector<size_t> kept, removed;
+    split_removed(v.shape.size(), seq, kept, removed);
+    std::vector<u64> kd, rd;
+    std::vector<ll> ks, rs;
+    pick(v, kept, kd, ks, 0);
+    pick(v, removed, rd, rs, 0);
+    u64 numel = prod(kd);
+    u64 b = new_buf(phase2, numel * eb, opidx(phase2));
+    Op g{Op::GATHER};
+    g.a = v.ref;
+    g.sa = v.so;
+    g.c = Ref{Ref::WS, b};
+    g.tab[0] = tab_ll(offsets(kd, ks));
+    g.tab[1] = tab_ll(offsets(rd, rs));
+    g.n_out = (ll)numel;
+    g.n_red = (ll)prod(rd);
+    touch(v.ref, phase2, opidx(phase2));
+    emit(phase2, g, true);
+    View r;
+    r.ref = g.c;
+    r.shape = kd;
+    r.strides = rm_strides(kd);
+    r.so.local_stride = v.variant ? (ll)numel : 0;
+    r.so.n = 0;
+    r.variant = v.variant;
+    return r;
+  };
+
+  for (size_t s = 0; s < plan_.steps.size(); ++s) {
+    const PairStep& st = plan_.steps[s];
+    View A = view[st.left_slot], B = view[st.right_slot];
+    const bool ph2 = A.variant || B.variant;
+    A = reduce_view(A, st.sum_a, ph2, nullptr);
+    B = reduce_view(B, st.sum_b, ph2, nullptr);
+    std::vector<u64> da, db;
+    std::vector<ll> sa, sb;
+    for (u64 p : st.a_perm) { da.push_back(A.shape[p]); sa.push_back(A.strides[p]); }
+    for (u64 p : st.b_perm) { db.push_back(B.shape[p]); sb.push_back(B.strides[p]); }
+    const size_t nb = st.n_batch, nfa = st.n_free_a, nc = st.n_con;
+    auto part = [](const std::vector<u64>& d, const std::vector<ll>& s_, size_t lo, size_t hi) {
+      return offsets(std::vector<u64>(d.begin() + lo, d.begin() + hi), std::vector<ll>(s_.begin() + lo, s_.begin() + hi));
+    };
+    Op g{Op::GEMM_SMALL};
+    g.tab[0] = tab_ll(part(da, sa, 0, nb));
+    g.tab[1] = tab_ll(part(da, sa, nb, nb + nfa));
+    g.tab[2] = tab_ll(part(da, sa, nb + nfa, da.size()));
+    g.tab[3] = tab_ll(part(db, sb, 0, nb));
+    g.tab[4] = tab_ll(part(db, sb, nb, nb + nc));
+    g.tab[5] = tab_ll(part(db, sb, nb + nc, db.size()));
+    g.bt = (ll)st.bt;
+    g.m = (ll)st.m;
+    g.k = (ll)st.k;
+    g.n = (ll)st.n;
+    g.a = A.ref;
+    g.b = B.ref;
+    g.sa = A.so;
+    g.sb = B.so;
+    if (st.m >= 64 && st.n >= 64) g.kind = Op::GEMM_TILE64;
+    else if (st.m >= 24 && st.n >= 24) g.kind = Op::GEMM_TILE32;
+    const u64 cnumel = prod({st.bt, st.m, st.n});
+    u64 cb = new_buf(ph2, cnumel * eb, opidx(ph2));
+    g.c = Ref{Ref::WS, cb};
+    touch(A.ref, ph2, opidx(ph2));
+    touch(B.ref, ph2, opidx(ph2));
+    touch(view[st.left_slot].ref, ph2, opidx(ph2));
+    touch(view[st.right_slot].ref, ph2, opidx(ph2));
+    emit(ph2, g, true);
+    if (!ph2 && want_strip) {
+      Op z{Op::MEMSET};
+      z.c = Ref{Ref::WS, (u64)strip_exp_off_};
+      z.bytes = 8;  // the max word (first 8 bytes); the exponent sits in the second 8
+      strip1.push_back(z);
+      Op mx{Op::MAXABS};
+      mx.c = g.c;
+      mx.n_out = (ll)cnumel;
+      mx.a = Ref{Ref::WS, (u64)strip_exp_off_};
+      strip1.push_back(mx);
+      Op sc{Op::STRIP};
+      sc.c = g.c;
+      sc.n_out = (ll)cnumel;
+      sc.a = Ref{Ref::WS, (u64)strip_exp_off_};
+      strip1.push_back(sc);
+    }
+    View C;
+    C.ref = g.c;
+    C.shape = st.result_shape;
+    C.strides = rm_strides(st.result_shape);
+    C.so.local_stride = ph2 ? (ll)cnumel : 0;
+    C.so.n = 0;
+    C.variant = ph2;
+    view[st.result_slot] = C;
+  }
+
+  // ---------------------------------------------------------------- finalize
+  const Finalize& fin = plan_.fin;
+  View Fv = view[fin.slot];
+  std::vector<size_t> kept, removed;
+  split_removed(Fv.shape.size(), fin.sum, kept, removed);
+  std::vector<u64> od, rd;
+  std::vector<ll> os, rs;
+  for (u64 p : fin.perm) { od.push_back(Fv.shape[kept[p]]); os.push_back(Fv.strides[kept[p]]); }
+  pick(Fv, removed, rd, rs, 0);
+  Op fg{Op::GATHER};
+  fg.a = Fv.ref;
+  fg.sa = Fv.so;
+  fg.tab[0] = tab_ll(offsets(od, os));
+  fg.tab[1] = tab_ll(rd.empty() ? std::vector<ll>{0} : offsets(rd, rs));
+  fg.n_out = (ll)n_e;
+  fg.n_red = rd.empty() ? 1 : (ll)prod(rd);
+  const bool fin_ph2 = sliced_;
+  touch(Fv.ref, fin_ph2, opidx(fin_ph2));
+  u64 fbuf = kInf;
+  if (!sliced_) {
+    fg.c = Ref{Ref::OUTPUT, 0};
+    emit(false, fg, true);
+  } else {
+    fbuf = new_buf(true, n_e * eb, opidx(true));
+    fg.c = Ref{Ref::WS, fbuf};
+    emit(true, fg, false);
+    Op ac{Op::ACCUM};
+    ac.a = Ref{Ref::WS, fbuf};
+    ac.c = Ref{Ref::WS, part_buf};
+    ac.n_e = (ll)n_e;
+    touch(ac.a, true, opidx(true));
+    emit(true, ac, false);
+  }
+
+  // ---------------------------------------------------------------- group size and layout
+  u64 region1 = 0, per_slice2 = 0;
+  auto layout = [&](bool region2, u64 mult) {
+    std::vector<size_t> ids;
+    for (size_t b = 0; b < bufs.size(); ++b)
+      if (bufs[b].region2 == region2) ids.push_back(b);
+    std::sort(ids.begin(), ids.end(), [&](size_t x, size_t y) { return bufs[x].bytes > bufs[y].bytes || (bufs[x].bytes == bufs[y].bytes && x < y); });
+    std::vector<size_t> placed;
+    u64 top = 0;
+    for (size_t id : ids) {
+      Buf& b = bufs[id];
+      const u64 sz = align_up(b.bytes * mult);
+      std::vector<std::pair<u64, u64>> busy;
+      for (size_t p : placed) {
+        const Buf& o = bufs[p];
+        if (o.first <= b.last && b.first <= o.last) busy.push_back({o.offset, o.offset + align_up(o.bytes * mult)});
+      }
+      std::sort(busy.begin(), busy.end());
+      u64 off = 0;
+      for (auto& iv : busy) {
+        if (off + sz <= iv.first) break;
+        off = std::max(off, iv.second);
+      }
+      b.offset = off;
+      top = std::max(top, off + sz);
+      placed.push_back(id);
+    }
+    return top;
+  };
+  region1 = layout(false, 1);
+  per_slice2 = layout(true, 1);
+  const u64 budget = opt_.workspace_budget ? opt_.workspace_budget : (8ull << 30);
+  S_ = 1;
+  if (sliced_) {
+    u64 room = budget > region1 ? budget - region1 : 0;
+    const u64 n_range = range_end_ - range_begin_;
+    u64 s_fit = per_slice2 ? std::max<u64>(room / (per_slice2 + kAlign), 1) : n_range;
+    S_ = std::min<u64>(n_range, s_fit);
+    if (opt_.max_slices_per_group) S_ = std::min<u64>(S_, opt_.max_slices_per_group);
+    S_ = std::max<u64>(S_, 1);
+  }
+  const u64 region2 = sliced_ ? layout(true, S_) : 0;
+  ws_total_ = align_up(region1) + region2;
+  n_groups_ = sliced_ ? (range_end_ - range_begin_ + S_ - 1) / S_ : 1;
+
+  auto resolve = [&](Ref& r) {
+    if (r.kind != Ref::WS) return;
+    const Buf& b = bufs[r.index];
+    r.index = b.region2 ? align_up(region1) + b.offset : b.offset;
+  };
+  auto finish = [&](Op& op) {
+    resolve(op.a);
+    resolve(op.b);
+    resolve(op.c);
+  };
+  if (want_strip) strip_exp_off_ = bufs[strip_exp_off_].offset;
+
+  // ---------------------------------------------------------------- final op sequence
+  for (Op op : ops1) { finish(op); ops_.push_back(op); }
+  if (want_strip) {
+    for (Op op : strip1) { finish(op); strip_ops_.push_back(op); }
+  }
+  if (sliced_) {
+    const ll chunk = (ll)((n_int_ + n_chunks_ - 1) / n_chunks_);
+    for (u64 gi = 0; gi < n_groups_; ++gi) {
+      const ll g0 = (ll)(range_begin_ + gi * S_), g1 = std::min<ll>(g0 + (ll)S_, (ll)range_end_);
+      std::vector<ll> segs;  // triples (part, lo, hi)
+      for (ll cur = g0; cur < g1;) {
+        const ll blk = cur / (ll)n_int_, i = cur % (ll)n_int_, c = i / chunk;
+        const ll end_i = std::min<ll>((c + 1) * chunk, (ll)n_int_);
+        const ll run_end = std::min<ll>(blk * (ll)n_int_ + end_i, g1);
+        segs.push_back(blk * (ll)n_chunks_ + c);
+        segs.push_back(cur - g0);
+        segs.push_back(run_end - g0);
+        cur = run_end;
+      }
+      const u64 seg_tab = tab_ll(segs);
+      for (Op op : ops2) {
+        finish(op);
+        op.S = g1 - g0;
+        op.g0 = g0;
+        if (op.kind == Op::ACCUM) {
+          op.tab[0] = seg_tab;
+          op.n_segs = (ll)segs.size() / 3;
+        }
+        ops_.push_back(op);
+      }
+    }
+    // Output assembly: block bases and the scatter of kept output axes.
+    auto full_st = rm_strides(full_out_shape);
+    std::vector<u64> odims;
+    std::vector<ll> ostr, kstr;
+    std::vector<u64> kdims;
+    for (size_t a = 0; a < net.output.size(); ++a) {
+      if (sl.count(net.output[a])) { odims.push_back(full_out_shape[a]); ostr.push_back(full_st[a]); }
+      else { kdims.push_back(full_out_shape[a]); kstr.push_back(full_st[a]); }
+    }
+    Op out{Op::OUTPUT};
+    out.a = Ref{Ref::WS, part_buf};
+    finish(out);
+    out.c = Ref{Ref::OUTPUT, 0};
+    out.tab[0] = tab_ll(odims.empty() ? std::vector<ll>{0} : offsets(odims, ostr));
+    out.tab[1] = tab_ll(kdims.empty() ? std::vector<ll>{0} : offsets(kdims, kstr));
+    out.n_blocks = (ll)n_blocks_;
+    out.n_chunks = (ll)n_chunks_;
+    out.n_e = (ll)n_e;
+    ops_.push_back(out);
+  }
+  (void)fbuf;
+}
+
+u64 Program::launches() const {
+  u64 n = 0;
+  for (auto& op : ops_) n += op.kind != Op::MEMSET;
+  return n;
+}
+
+// ---------------------------------------------------------------- launching
+namespace {
+
+inline int grid_for(ll total, int per_block = 256, int cap = 148 * 16) {
+  ll g = (total + per_block - 1) / per_block;
+  return (int)std::max<ll>(1, std::min<ll>(g, cap));
+}
+
+template <class T>
+void launch_typed(const Op& op, const void* A, const void* B, void* C, const char* tab, bool out_f64, cudaStream_t st) {
+  using W = typename Num<T>::wide;
+  auto T_ = [&](int i) { return (const ll*)(tab + op.tab[i]); };
+  switch (op.kind) {
+    case Op::GATHER: {
+      const ll total = op.S * op.n_out;
+      if (out_f64 && op.c.kind == Ref::OUTPUT)
+        k_gather_reduce<T, W><<<grid_for(total), 256, 0, st>>>((const T*)A, (W*)C, T_(0), T_(1), op.n_out, op.n_red, op.S, op.sa, op.g0);
+      else
+        k_gather_reduce<T, T><<<grid_for(total), 256, 0, st>>>((const T*)A, (T*)C, T_(0), T_(1), op.n_out, op.n_red, op.S, op.sa, op.g0);
+      break;
+    }
+    case Op::GEMM_SMALL:
+    case Op::GEMM_TILE64:
+    case Op::GEMM_TILE32: {
+      GemmArgs g;
+      g.A = A; g.B = B; g.C = C;
+      g.bt = op.bt; g.m = op.m; g.k = op.k; g.n = op.n; g.S = op.S; g.g0 = op.g0;
+      g.aB = T_(0); g.aM = T_(1); g.aK = T_(2); g.bB = T_(3); g.bK = T_(4); g.bN = T_(5);
+      g.sa = op.sa; g.sb = op.sb;
+      if (op.kind == Op::GEMM_SMALL) {
+        const ll total = op.S * op.bt * op.m * op.n;
+        const size_t smem = op.k <= 1024 ? (size_t)(2 * op.k * sizeof(ll)) : 0;
+        k_gemm_small<T><<<grid_for(total, 256, 148 * 32), 256, smem, st>>>(g);
+      } else if (op.kind == Op::GEMM_TILE64) {
+        const ll tiles = ((op.n + 63) / 64) * ((op.m + 63) / 64) * op.S * op.bt;
+        k_gemm_tile<T, 64, 64, 16><<<(int)std::min<ll>(tiles, 148 * 8), 256, 0, st>>>(g);
+      } else {
+        const ll tiles = ((op.n + 31) / 32) * ((op.m + 31) / 32) * op.S * op.bt;
+        k_gemm_tile<T, 32, 32, 16><<<(int)std::min<ll>(tiles, 148 * 16), 256, 0, st>>>(g);
+      }
+      break;
+    }
+    case Op::ACCUM: {
+      const ll total = op.n_segs * op.n_e;
+      k_slice_accumulate<T><<<grid_for(total), 256, 0, st>>>((const T*)A, (W*)C, (const Segment*)(tab + op.tab[0]), op.n_segs, op.n_e);
+      break;
+    }
+    case Op::OUTPUT: {
+      const ll total = op.n_blocks * op.n_e;
+      if (out_f64)
+        k_slice_output<T, W><<<grid_for(total), 256, 0, st>>>((const W*)A, (W*)C, T_(0), T_(1), op.n_blocks, op.n_chunks, op.n_e);
+      else
+        k_slice_output<T, T><<<grid_for(total), 256, 0, st>>>((const W*)A, (T*)C, T_(0), T_(1), op.n_blocks, op.n_chunks, op.n_e);
+      break;
+    }
+    case Op::MAXABS:
+      k_maxabs<T><<<grid_for(op.n_out), 256, 0, st>>>((const T*)C, op.n_out, (unsigned long long*)A);
+      break;
+    case Op::STRIP:
+      k_strip_scale<T><<<grid_for(op.n_out), 256, 0, st>>>((T*)C, op.n_out, (const unsigned long long*)A,
+                                                             (double*)((char*)A + 8), 1);
+      break;
+    case Op::MEMSET:
+      break;
+  }
+}
+
+}  // namespace
+
+void Program::launch_op(const Op& op, const void* const* inputs, void* output, char* ws, cudaStream_t st) {
+  auto ptr = [&](const Ref& r) -> void* {
+    switch (r.kind) {
+      case Ref::INPUT: return const_cast<void*>(inputs[r.index]);
+      case Ref::WS: return ws + r.index;
+      case Ref::OUTPUT: return output;
+      default: return nullptr;
+    }
+  };
+  if (op.kind == Op::MEMSET) {
+    CK(cudaMemsetAsync(ptr(op.c), 0, op.bytes, st));
+    return;
+  }
+  const bool out_f64 = out_f64_flag_;
+  switch (opt_.dtype) {
+    case DT_F32: launch_typed<float>(op, ptr(op.a), ptr(op.b), ptr(op.c), dev_tab_, out_f64, st); break;
+    case DT_F64: launch_typed<double>(op, ptr(op.a), ptr(op.b), ptr(op.c), dev_tab_, out_f64, st); break;
+    case DT_C64: launch_typed<cf32>(op, ptr(op.a), ptr(op.b), ptr(op.c), dev_tab_, out_f64, st); break;
+    case DT_C128: launch_typed<cf64>(op, ptr(op.a), ptr(op.b), ptr(op.c), dev_tab_, out_f64, st); break;
+  }
+  CK(cudaGetLastError());
+}
+
+void Program::enqueue(const std::vector<Op>& ops, const void* const* inputs, void* output, char* ws, cudaStream_t st) {
+  for (const Op& op : ops) launch_op(op, inputs, output, ws, st);
+}
+
+namespace {
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+}  // namespace
+
+void Program::execute(const void* const* inputs, void* output, bool f64_out, void* ws, u64 ws_bytes, cudaStream_t st) {
+  if (ws_bytes < ws_total_)
+    throw Error(E_WORKSPACE, "workspace of " + std::to_string(ws_bytes) + " bytes is smaller than the required " + std::to_string(ws_total_));
+  if (!output) throw Error(E_INVALID, "output pointer is null");
+  for (u64 i = 0; i < plan_.n_inputs; ++i)
+    if (!inputs[i]) throw Error(E_INVALID, "input " + std::to_string(i) + " pointer is null");
+  if (ws_total_ && !ws) throw Error(E_INVALID, "workspace pointer is null");
+  DeviceGuard guard(opt_.device);
+  std::lock_guard<std::mutex> lk(mu_);
+  out_f64_flag_ = f64_out;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (st) CK(cudaStreamIsCapturing(st, &cs));
+  const bool graph = opt_.use_graph && st != nullptr && cs == cudaStreamCaptureStatusNone;
+  if (!graph) {
+    enqueue(ops_, inputs, output, (char*)ws, st);
+    return;
+  }
+  std::vector<const void*> key(inputs, inputs + plan_.n_inputs);
+  key.push_back(output);
+  key.push_back(ws);
+  key.push_back((const void*)(uintptr_t)f64_out);
+  if (!gexec_ || key != gkey_) {
+    cudaGraph_t graph_h = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue(ops_, inputs, output, (char*)ws, st);
+    } catch (...) {
+      cudaStreamEndCapture(st, &graph_h);
+      if (graph_h) cudaGraphDestroy(graph_h);
+      throw;
+    }
+    CK(cudaStreamEndCapture(st, &graph_h));
+    bool updated = false;
+    if (gexec_) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(gexec_, graph_h, &info) == cudaSuccess) updated = true;
+      else {
+        cudaGetLastError();
+        cudaGraphExecDestroy(gexec_);
+        gexec_ = nullptr;
+      }
+    }
+    if (!updated) {
+      cudaError_t e = cudaGraphInstantiate(&gexec_, graph_h, 0);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(graph_h);
+        gexec_ = nullptr;
+        throw Error(E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      }
+    }
+    cudaGraphDestroy(graph_h);
+    gkey_ = key;
+  }
+  CK(cudaGraphLaunch(gexec_, st));
+}
+
+namespace {
+double op_work(const Op& op, int dt) {
+  const double eb = (double)dtype_bytes(dt);
+  switch (op.kind) {
+    case Op::GEMM_SMALL:
+    case Op::GEMM_TILE64:
+    case Op::GEMM_TILE32:
+      return (dtype_complex(dt) ? 8.0 : 2.0) * (double)op.S * op.bt * op.m * op.k * op.n;
+    case Op::GATHER: return (double)op.S * op.n_out * (op.n_red + 1) * eb;
+    case Op::ACCUM: return (double)op.n_segs * op.n_e * (2.0 * wide_bytes(dt)) + (double)op.S * op.n_e * eb;
+    case Op::OUTPUT: return (double)op.n_blocks * op.n_chunks * op.n_e * wide_bytes(dt);
+    default: return (double)op.n_out * eb;
+  }
+}
+}  // namespace
+
+void Program::profile(const void* const* inputs, void* output, void* ws, u64 ws_bytes, cudaStream_t st, float* ms,
+                      int* kind, double* work) {
+  if (ws_bytes < ws_total_) throw Error(E_WORKSPACE, "workspace is smaller than required");
+  DeviceGuard guard(opt_.device);
+  std::lock_guard<std::mutex> lk(mu_);
+  out_f64_flag_ = false;
+  std::vector<cudaEvent_t> ev;
+  for (size_t i = 0; i <= ops_.size(); ++i) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    ev.push_back(e);
+  }
+  try {
+    for (size_t i = 0; i < ops_.size(); ++i) {
+      CK(cudaEventRecord(ev[i], st));
+      launch_op(ops_[i], inputs, output, (char*)ws, st);
+    }
+    CK(cudaEventRecord(ev[ops_.size()], st));
+    CK(cudaEventSynchronize(ev[ops_.size()]));
+    size_t j = 0;
+    for (size_t i = 0; i < ops_.size(); ++i) {
+      if (ops_[i].kind == Op::MEMSET) continue;
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+      ms[j] = t;
+      kind[j] = (int)ops_[i].kind;
+      work[j] = op_work(ops_[i], opt_.dtype);
+      ++j;
+    }
+  } catch (...) {
+    for (auto e : ev) cudaEventDestroy(e);
+    throw;
+  }
+  for (auto e : ev) cudaEventDestroy(e);
+}
+
+void Program::execute_stripped(const void* const* inputs, void* output, void* ws, u64 ws_bytes, cudaStream_t st,
+                               double* exponent) {
+  if (sliced_) throw Error(E_UNSUPPORTED, "execute_stripped applies to unsliced programs only");
+  if (ws_bytes < ws_total_) throw Error(E_WORKSPACE, "workspace is smaller than required");
+  DeviceGuard guard(opt_.device);
+  std::lock_guard<std::mutex> lk(mu_);
+  out_f64_flag_ = false;
+  enqueue(strip_ops_, inputs, output, (char*)ws, st);
+  double e = 0.0;
+  CK(cudaMemcpyAsync(&e, (char*)ws + strip_exp_off_ + 8, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  *exponent = e;
+}
+
+}  // namespace ab2

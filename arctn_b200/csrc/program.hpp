@@ -1,0 +1,99 @@
+// Device program: a compiled plan bound to slices, a dtype and a GPU.
+//
+// Built once on the host (all validation, slice decoding, offset tables and
+// the workspace layout), then executed any number of times as a fixed
+// sequence of kernel launches on the caller's stream, optionally replayed
+// from a captured CUDA graph.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "host.hpp"
+#include "kernels.cuh"
+
+namespace ab2 {
+
+enum : int { DT_F32 = 0, DT_F64 = 1, DT_C64 = 2, DT_C128 = 3 };
+enum : int { PREC_FP32 = 0, PREC_TF32X3 = 1 };
+
+size_t dtype_bytes(int dt);
+inline bool dtype_complex(int dt) { return dt == DT_C64 || dt == DT_C128; }
+
+struct ProgramOptions {
+  int dtype = DT_C64;
+  int precision = PREC_FP32;
+  int device = 0;
+  bool use_graph = true;
+  u64 max_slices_per_group = 0;
+  u64 workspace_budget = 0;
+  u64 slice_begin = 0, slice_end = 0;  // both 0: every slice
+};
+
+// Where an operand lives at run time.
+struct Ref {
+  enum Kind : int { NONE = 0, INPUT = 1, WS = 2, OUTPUT = 3 } kind = NONE;
+  u64 index = 0;  // input index, or byte offset into the workspace
+};
+
+struct Op {
+  enum Kind : int { GATHER, GEMM_SMALL, GEMM_TILE64, GEMM_TILE32, ACCUM, OUTPUT, MEMSET, MAXABS, STRIP } kind;
+  Ref a, b, c;
+  u64 tab[6] = {0, 0, 0, 0, 0, 0};  // byte offsets of offset tables in the program's table buffer
+  ll bt = 1, m = 1, k = 1, n = 1, S = 1, g0 = 0;
+  SliceOff sa{}, sb{};
+  ll n_out = 0, n_red = 0;  // GATHER
+  ll n_segs = 0, n_e = 0, n_blocks = 0, n_chunks = 0;  // ACCUM / OUTPUT
+  u64 bytes = 0;            // MEMSET
+  bool out_f64 = false;     // GATHER / OUTPUT writing FP64
+};
+
+class Program {
+ public:
+  Program(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced, const ProgramOptions& opt);
+  ~Program();
+  Program(const Program&) = delete;
+  Program& operator=(const Program&) = delete;
+
+  u64 workspace_size() const { return ws_total_; }
+  u64 n_slices() const { return n_total_; }
+  u64 slices_per_group() const { return S_; }
+  double flops() const { return flops_; }
+  u64 launches() const;
+  const Plan& plan() const { return plan_; }
+
+  void execute(const void* const* inputs, void* output, bool f64_out, void* ws, u64 ws_bytes, cudaStream_t st);
+  void execute_stripped(const void* const* inputs, void* output, void* ws, u64 ws_bytes, cudaStream_t st,
+                        double* exponent);
+  // Op-by-op run with an event between launches; per launch: ms, kind, algorithmic work.
+  void profile(const void* const* inputs, void* output, void* ws, u64 ws_bytes, cudaStream_t st, float* ms,
+               int* kind, double* work);
+
+ private:
+  struct Buf { u64 bytes, first, last; bool region2; u64 offset; };
+
+  void build(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced);
+  void enqueue(const std::vector<Op>& ops, const void* const* inputs, void* output, char* ws, cudaStream_t st);
+  void launch_op(const Op& op, const void* const* inputs, void* output, char* ws, cudaStream_t st);
+
+  ProgramOptions opt_;
+  Plan plan_;
+  u64 n_total_ = 1, n_int_ = 1, n_blocks_ = 1, n_chunks_ = 1, S_ = 1, n_groups_ = 1;
+  u64 range_begin_ = 0, range_end_ = 1;
+  bool sliced_ = false;
+  double flops_ = 0;
+  std::vector<Op> ops_;          // full launch sequence for one execute (all groups)
+  std::vector<Op> strip_ops_;    // unsliced stripped variant
+  std::vector<char> host_tab_;   // offset tables, uploaded once
+  char* dev_tab_ = nullptr;
+  u64 ws_total_ = 0;
+  u64 strip_mx_off_ = 0, strip_exp_off_ = 0;
+
+  std::mutex mu_;
+  bool out_f64_flag_ = false;
+  cudaGraphExec_t gexec_ = nullptr;
+  std::vector<const void*> gkey_;
+};
+
+}  // namespace ab2

@@ -1,0 +1,231 @@
+/*
+ * arctn_b200 -- B200-native executor for ArcTN's numerical contraction path.
+ *
+ * C ABI.  Plain pointers and sizes only; no C++ or torch types cross this
+ * boundary.  Every entry point returns an int status (ARCTN_B200_OK == 0) and
+ * records a message readable through arctn_b200_last_error() on the calling
+ * thread.  No exception or unwinding crosses the ABI.
+ *
+ * Reference interfaces replaced (paths inside the ArcTN repository):
+ *   TensorNetwork{inputs,output,size_dict}         src/network.rs:134-143
+ *   CompiledContraction::compile                    src/compiled.rs:254
+ *   CompiledContraction::execute / execute_stripped src/compiled.rs:369-381
+ *   input_preps() / pair_steps() / finalize()       src/compiled.rs:241-250
+ *   CompiledPairContraction accessors + execute     src/compiled.rs:102-153
+ *   CompiledInputPrep::execute                      src/compiled.rs:60-63
+ *   CompiledFinalize::execute                       src/compiled.rs:206-209
+ *   contract_network_sliced                         src/slice.rs:960
+ *   slice_parallel_chunks                           src/slice.rs:893-905
+ *   simulate_path_full (metrics)                    src/path.rs:239-434
+ *   greedy                                          src/paths/greedy.rs:317-320
+ *   find_slices_to_size                             src/slice.rs:209-215
+ *   PyO3 CompiledContraction.compile/execute/stats  pybind/src/lib.rs:384-454
+ *   PyO3 contract_sliced                            pybind/src/lib.rs:692-765
+ */
+#ifndef ARCTN_B200_H
+#define ARCTN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ARCTN_B200_ABI_VERSION 1u
+
+/* Status codes. */
+enum {
+  ARCTN_B200_OK = 0,
+  ARCTN_B200_ERR_INVALID = 1,        /* network / path / shape / argument rejected before any launch */
+  ARCTN_B200_ERR_CUDA = 2,           /* a CUDA runtime call failed */
+  ARCTN_B200_ERR_UNSUPPORTED = 3,    /* valid input outside what this build executes */
+  ARCTN_B200_ERR_DEVICE_TIMEOUT = 4, /* a bounded device-side wait expired */
+  ARCTN_B200_ERR_WORKSPACE = 5       /* caller workspace smaller than required */
+};
+
+/* Element types; every input of one call shares the dtype
+ * (pybind/src/lib.rs:287-330).  Complex values are (re, im) pairs. */
+enum {
+  ARCTN_B200_F32 = 0,
+  ARCTN_B200_F64 = 1,
+  ARCTN_B200_C64 = 2,  /* complex64  = 2 x f32 */
+  ARCTN_B200_C128 = 3  /* complex128 = 2 x f64 */
+};
+
+/* Arithmetic used for the pairwise GEMMs of f32 / c64 contractions.
+ * f64 / c128 always compute in FP64. */
+enum {
+  ARCTN_B200_PREC_FP32 = 0,  /* plain FP32 FFMA on the CUDA cores */
+  ARCTN_B200_PREC_TF32X3 = 1 /* split-TF32 (3 products) on tcgen05 tensor cores, FP32 accumulate,
+                                for steps dense enough to fill a tensor-core tile; thin steps FP32 */
+};
+
+/* A tensor network (TensorNetwork, src/network.rs:134-143).
+ * inputs are CSR: tensor i holds input_legs[input_offsets[i] .. input_offsets[i+1]].
+ * size_dict is given as parallel arrays (size_legs[j] -> size_dims[j]). */
+typedef struct {
+  uint64_t n_inputs;
+  const uint64_t* input_offsets; /* n_inputs + 1 entries */
+  const uint32_t* input_legs;
+  uint64_t n_output;
+  const uint32_t* output;
+  uint64_t n_sizes;
+  const uint32_t* size_legs;
+  const uint64_t* size_dims;
+} arctn_b200_network;
+
+typedef struct arctn_b200_plan arctn_b200_plan;       /* CompiledContraction (immutable, shareable) */
+typedef struct arctn_b200_program arctn_b200_program; /* plan + slices + dtype bound to a device */
+
+uint32_t arctn_b200_abi_version(void);
+/* Last error message of the calling thread ("" when none). */
+const char* arctn_b200_last_error(void);
+
+/* ------------------------------------------------------------ planning support (host only) */
+
+/* Path metrics in the order: log10_flops, log2_max_size, log2_max_contraction_size,
+ * log2_total_size, log2_read_write, log2_peak_size (src/path.rs:14-29). */
+int arctn_b200_simulate_path(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
+                             double stats_out[6]);
+/* Deterministic greedy SSA path (src/paths/greedy.rs:317-320).  ssa_out holds 2*(n_inputs-1) entries. */
+int arctn_b200_greedy(const arctn_b200_network* net, uint64_t* ssa_out, uint64_t* n_steps_out);
+/* find_slices_to_size (src/slice.rs:209-215).  legs_out holds n_sizes entries; *found = 0 where the
+ * reference returns None. */
+int arctn_b200_find_slices_to_size(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
+                                   uint64_t target_size, uint32_t* legs_out, uint64_t* n_legs_out, int* found);
+/* Deterministic chunk count of sliced summation (src/slice.rs:893-905). */
+uint64_t arctn_b200_slice_parallel_chunks(uint64_t n_slices, uint64_t out_numel);
+
+/* ------------------------------------------------------------ CompiledContraction */
+
+int arctn_b200_plan_compile(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
+                            arctn_b200_plan** plan_out);
+void arctn_b200_plan_destroy(arctn_b200_plan* plan);
+
+uint64_t arctn_b200_plan_n_inputs(const arctn_b200_plan* plan);
+uint64_t arctn_b200_plan_n_steps(const arctn_b200_plan* plan);
+double arctn_b200_plan_log10_flops(const arctn_b200_plan* plan);
+double arctn_b200_plan_log2_peak_size(const arctn_b200_plan* plan);
+
+/* Views into the plan's immutable metadata; valid until arctn_b200_plan_destroy. */
+typedef struct {
+  uint64_t left_slot, right_slot, result_slot;
+  uint64_t n_left, n_right, n_result;        /* ranks */
+  const uint32_t* left_legs;
+  const uint32_t* right_legs;
+  const uint32_t* result_legs;               /* [batch, free_left, free_right] */
+  const uint64_t* left_shape;
+  const uint64_t* right_shape;
+  const uint64_t* result_shape;
+  uint64_t n_sum_a, n_sum_b;
+  const uint64_t* sum_a;                     /* axes reduced from the left operand, in order */
+  const uint64_t* sum_b;
+  const uint64_t* a_perm;                    /* n_left - n_sum_a entries -> [batch, free_a, con] */
+  const uint64_t* b_perm;                    /* n_right - n_sum_b entries -> [batch, con, free_b] */
+  uint64_t bt, m, k, n;                      /* gemm_dims() */
+} arctn_b200_step_info;
+
+typedef struct {
+  uint64_t n_input_shape;
+  const uint64_t* input_shape;
+  uint64_t n_traces;
+  const uint64_t* traces;                    /* n_traces triples (ax_i, ax_j, is_diag) */
+  uint64_t n_legs;
+  const uint32_t* legs;
+  const uint64_t* shape;
+} arctn_b200_prep_info;
+
+typedef struct {
+  uint64_t slot;
+  uint64_t n_input;
+  const uint32_t* input_legs;
+  const uint64_t* input_shape;
+  uint64_t n_sum;
+  const uint64_t* sum;
+  uint64_t n_output;
+  const uint64_t* perm;
+  const uint64_t* output_shape;
+} arctn_b200_finalize_info;
+
+int arctn_b200_plan_step_info(const arctn_b200_plan* plan, uint64_t step, arctn_b200_step_info* out);
+int arctn_b200_plan_prep_info(const arctn_b200_plan* plan, uint64_t input, arctn_b200_prep_info* out);
+int arctn_b200_plan_finalize_info(const arctn_b200_plan* plan, arctn_b200_finalize_info* out);
+
+/* Stage-by-stage execution on device buffers (CompiledInputPrep::execute, CompiledPairContraction::execute,
+ * CompiledFinalize::execute).  Operands are contiguous row-major device tensors with the shapes the plan
+ * records.  Each stage may need scratch: pass at least the matching *_workspace_size bytes (0 is allowed
+ * when the size is 0).  Results are bit-identical to the corresponding stage inside a program execute. */
+uint64_t arctn_b200_plan_prep_workspace_size(const arctn_b200_plan* plan, int dtype, uint64_t input);
+uint64_t arctn_b200_plan_step_workspace_size(const arctn_b200_plan* plan, int dtype, int precision, uint64_t step);
+uint64_t arctn_b200_plan_finalize_workspace_size(const arctn_b200_plan* plan, int dtype);
+int arctn_b200_plan_prep_execute(const arctn_b200_plan* plan, int dtype, uint64_t input, const void* in, void* out,
+                                 void* workspace, uint64_t workspace_bytes, void* cuda_stream);
+int arctn_b200_plan_step_execute(const arctn_b200_plan* plan, int dtype, int precision, uint64_t step,
+                                 const void* left, const void* right, void* out, void* workspace,
+                                 uint64_t workspace_bytes, void* cuda_stream);
+int arctn_b200_plan_finalize_execute(const arctn_b200_plan* plan, int dtype, const void* in, void* out,
+                                     void* workspace, uint64_t workspace_bytes, void* cuda_stream);
+
+/* ------------------------------------------------------------ device programs (execute / contract_sliced) */
+
+typedef struct {
+  int dtype;                     /* ARCTN_B200_F32 .. ARCTN_B200_C128 */
+  int precision;                 /* ARCTN_B200_PREC_* */
+  int device;                    /* CUDA device ordinal the program is bound to */
+  int use_graph;                 /* capture the launch sequence once and replay it as a CUDA graph */
+  uint64_t max_slices_per_group; /* 0: all slices in one group when the workspace budget allows */
+  uint64_t workspace_budget;     /* bytes; 0: 8 GiB */
+  uint64_t slice_begin;          /* run only global slices [slice_begin, slice_end); both 0: all slices.  A */
+  uint64_t slice_end;            /* partial range sums only its slices (one rank of a sharded contraction). */
+} arctn_b200_program_options;
+
+/* Builds a program that contracts `net` along `ssa_path`, summing internal sliced legs and assembling
+ * output-leg slices as blocks (contract_network_sliced, src/slice.rs:960-1173).  n_sliced == 0 gives the
+ * unsliced CompiledContraction::execute.  Validation happens here, before anything is launched. */
+int arctn_b200_program_create(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
+                              uint64_t n_sliced, const uint32_t* sliced_legs,
+                              const arctn_b200_program_options* options, arctn_b200_program** program_out);
+void arctn_b200_program_destroy(arctn_b200_program* program);
+uint64_t arctn_b200_program_workspace_size(const arctn_b200_program* program);
+uint64_t arctn_b200_program_n_slices(const arctn_b200_program* program);
+uint64_t arctn_b200_program_slices_per_group(const arctn_b200_program* program);
+/* Algorithmic real flops of one execution: 8 (complex) or 2 (real) x sum_steps bt*m*k*n x slices. */
+double arctn_b200_program_flops(const arctn_b200_program* program);
+/* Number of kernels one execute launches. */
+uint64_t arctn_b200_program_launches(const arctn_b200_program* program);
+
+/* Runs on `cuda_stream` (cudaStream_t; NULL = legacy default stream).  inputs[i] are contiguous device
+ * tensors in net order; output receives the full output (native dtype).  The call is asynchronous. */
+int arctn_b200_program_execute(arctn_b200_program* program, const void* const* inputs, void* output,
+                               void* workspace, uint64_t workspace_bytes, void* cuda_stream);
+/* Same, but writes the result in FP64 (f64 / c128) from the FP64 cross-slice sum. */
+int arctn_b200_program_execute_f64out(arctn_b200_program* program, const void* const* inputs, void* output_f64,
+                                      void* workspace, uint64_t workspace_bytes, void* cuda_stream);
+/* execute_stripped (src/compiled.rs:376-441): unsliced programs only.  Synchronises the stream and writes
+ * the accumulated decimal exponent to *log10_exponent. */
+int arctn_b200_program_execute_stripped(arctn_b200_program* program, const void* const* inputs, void* output,
+                                        void* workspace, uint64_t workspace_bytes, void* cuda_stream,
+                                        double* log10_exponent);
+
+/* Profiled execute: launches op by op (no graph) with a CUDA event between consecutive kernels on
+ * `cuda_stream`, synchronises, and writes per-launch duration (ms), kind and algorithmic work (real flops
+ * for GEMM kinds, bytes moved for the others).  Arrays hold arctn_b200_program_launches entries.
+ * Kinds: 0 gather, 1 gemm_small, 2 gemm_tile64, 3 gemm_tile32, 4 slice_accumulate, 5 slice_output,
+ * 7 maxabs, 8 strip, 9 gemm_tc. */
+int arctn_b200_program_profile(arctn_b200_program* program, const void* const* inputs, void* output, void* workspace,
+                               uint64_t workspace_bytes, void* cuda_stream, float* ms_out, int* kind_out,
+                               double* work_out);
+
+/* One-shot host-buffer call (the reference-facing e2e path of contract_sliced): copies host inputs to the
+ * device, executes, copies the result back and synchronises.  Allocates its own device memory. */
+int arctn_b200_contract_sliced_host(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
+                                    uint64_t n_sliced, const uint32_t* sliced_legs,
+                                    const arctn_b200_program_options* options, const void* const* host_inputs,
+                                    void* host_output);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ARCTN_B200_H */

@@ -1,0 +1,86 @@
+"""Shared helpers for the test suite (network fixtures and comparisons)."""
+
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def known_answers():
+    with open(os.path.join(HERE, "golden", "known_answers.json")) as f:
+        return json.load(f)
+
+
+def sd(d):
+    return {int(k): int(v) for k, v in d.items()}
+
+
+def case_arrays(case):
+    dt = np.dtype(case["dtype"])
+    out = []
+    for a, shape in zip(case["arrays"], case["shapes"]):
+        arr = np.asarray(a, dtype=np.float64)
+        if np.issubdtype(dt, np.complexfloating):
+            arr = arr[..., 0] + 1j * arr[..., 1]
+        out.append(np.ascontiguousarray(arr.reshape(shape).astype(dt)))
+    return out
+
+
+def case_expected(case):
+    exp = case["expected"]
+    if exp is None:
+        return None
+    arr = np.asarray(exp, dtype=np.float64)
+    if case["dtype"].startswith("complex"):
+        arr = arr[..., 0] + 1j * arr[..., 1]
+    return arr
+
+
+def random_arrays(inputs, size_dict, dtype, seed, scale=1.0):
+    """Reference-style test data: uniform(-1, 1) entries (src/tensor.rs:117-119, 310-312)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dt = np.dtype(dtype)
+    out = []
+    for t in inputs:
+        shape = tuple(size_dict[l] for l in t)
+        if np.issubdtype(dt, np.complexfloating):
+            v = rng.uniform(-1, 1, shape) + 1j * rng.uniform(-1, 1, shape)
+        else:
+            v = rng.uniform(-1, 1, shape)
+        out.append(np.ascontiguousarray((np.asarray(v) * scale).astype(dt)))
+    return out
+
+
+def rel_err(got, want):
+    got = np.asarray(got, dtype=np.complex128)
+    want = np.asarray(want, dtype=np.complex128)
+    scale = max(1.0, float(np.max(np.abs(want)))) if want.size else 1.0
+    return float(np.max(np.abs(got - want))) / scale if want.size else 0.0
+
+
+def mixed_network():
+    """A diagonal, a trace, a dangling leg, a batch leg and a hyperedge (tests/compiled_pair_steps.rs:67-93)."""
+    inputs = [[0, 0, 1], [0, 2, 3, 3], [1, 2, 4, 5], [4, 6, 9], [6, 8, 9], [9, 10]]
+    output = [8, 6, 10]
+    size_dict = {0: 3, 1: 2, 2: 3, 3: 2, 4: 2, 5: 3, 6: 2, 8: 3, 9: 2, 10: 3}
+    return inputs, output, size_dict
+
+
+SMALL_NETWORKS = {
+    "matmul": ([[0, 1], [1, 2]], [0, 2], {0: 3, 1: 4, 2: 5}),
+    "chain3": ([[0, 1], [1, 2], [2, 3]], [0, 3], {0: 2, 1: 3, 2: 5, 3: 7}),
+    "hyper": ([[0, 1], [0, 2], [0]], [], {0: 3, 1: 2, 2: 4}),
+    "trace": ([[0, 0, 1], [1]], [], {0: 3, 1: 4}),
+    "diag_shared": ([[0, 0, 1], [0, 2]], [1, 2], {0: 3, 1: 2, 2: 4}),
+    "diag_output": ([[0, 0, 1], [1, 2]], [0, 2], {0: 4, 1: 3, 2: 5}),
+    "trace_and_diag": ([[0, 0, 1, 1], [1, 2]], [2], {0: 3, 1: 2, 2: 4}),
+    "single": ([[0, 1]], [0], {0: 3, 1: 5}),
+    "single_perm": ([[0, 1, 2]], [2, 0], {0: 2, 1: 3, 2: 4}),
+    "dangling": ([[0, 1], [1, 2]], [2], {0: 7, 1: 3, 2: 5}),
+    "scalar_inputs": ([[], []], [], {}),
+    "scalar_and_vec": ([[], [0]], [0], {0: 5}),
+    "mixed": mixed_network(),
+    "tiny6": ([[0, 1], [1, 2], [2, 3], [3, 4], [4, 5], [5, 0, 6]], [6], {0: 4, 1: 5, 2: 4, 3: 6, 4: 4, 5: 5, 6: 3}),
+}
