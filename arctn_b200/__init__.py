@@ -20,6 +20,7 @@ from .api import (
     linear_to_ssa,
     simulate_path,
     slice_parallel_chunks,
+    slice_range,
     ssa_to_linear,
 )
 
@@ -38,5 +39,6 @@ __all__ = [
     "linear_to_ssa",
     "simulate_path",
     "slice_parallel_chunks",
+    "slice_range",
     "ssa_to_linear",
 ]

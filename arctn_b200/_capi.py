@@ -52,7 +52,7 @@ class FinalizeInfo(ctypes.Structure):
 class ProgramOptions(ctypes.Structure):
     _fields_ = [("dtype", c_int), ("precision", c_int), ("device", c_int), ("use_graph", c_int),
                 ("max_slices_per_group", u64), ("workspace_budget", u64), ("slice_begin", u64),
-                ("slice_end", u64)]
+                ("slice_end", u64), ("gradient", c_int)]
 
 
 # (name, restype, argtypes) for every symbol the header declares.
@@ -90,6 +90,8 @@ SIGNATURES = [
     ("arctn_b200_program_execute", c_int, [vp, vpp, vp, vp, u64, vp]),
     ("arctn_b200_program_execute_f64out", c_int, [vp, vpp, vp, vp, u64, vp]),
     ("arctn_b200_program_execute_stripped", c_int, [vp, vpp, vp, vp, u64, vp, ctypes.POINTER(c_double)]),
+    ("arctn_b200_program_gradient", c_int, [vp, c_int, vpp, vp, vpp, vp, vp, u64, vp]),
+    ("arctn_b200_program_device_status", c_int, [vp, vp, vp, ctypes.POINTER(c_int)]),
     ("arctn_b200_program_profile", c_int, [vp, vpp, vp, vp, u64, vp, ctypes.POINTER(ctypes.c_float),
                                            ctypes.POINTER(c_int), ctypes.POINTER(c_double)]),
     ("arctn_b200_contract_sliced_host", c_int, [NETP, u64, u64p, u64, u32p, ctypes.POINTER(ProgramOptions), vpp,

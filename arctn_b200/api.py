@@ -130,7 +130,7 @@ class _DeviceCall:
             self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
             self.tensors = []
             for a in arrays:
-                host = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+                host = torch.from_numpy(np.array(a, order="C", copy=None)).pin_memory()
                 self.tensors.append(host.to(self.device, non_blocking=True))
         self.stream = torch.cuda.current_stream(self.device)
         self.ptrs = (ctypes.c_void_p * len(self.tensors))(*[t.data_ptr() for t in self.tensors])
@@ -184,6 +184,15 @@ def find_slices_to_size(inputs, output, size_dict, ssa_path, target_size):
     return [int(x) for x in buf[: nl.value]] if found.value else None
 
 
+def slice_range(count, ranks, rank):
+    """Contiguous slice range [begin, end) of one rank (src/bin/tnmpi.rs:278-284); empty when ranks > count."""
+    if ranks < 1 or not 0 <= rank < ranks:
+        raise ValueError(f"rank {rank} outside [0, {ranks})")
+    chunk, extra = divmod(int(count), int(ranks))
+    begin = rank * chunk + min(rank, extra)
+    return begin, begin + chunk + (1 if rank < extra else 0)
+
+
 def slice_parallel_chunks(n_slices, out_numel):
     """Deterministic chunk count of the sliced sum (src/slice.rs:893-905)."""
     return int(C.lib().arctn_b200_slice_parallel_chunks(int(n_slices), int(out_numel)))
@@ -202,7 +211,7 @@ class SlicedProgram:
 
     def __init__(self, inputs, output, size_dict, ssa_path, sliced_legs=(), *, dtype="complex64",
                  precision="fp32", device=None, use_graph=True, max_slices_per_group=0, workspace_budget=0,
-                 slice_begin=0, slice_end=0):
+                 slice_begin=0, slice_end=0, gradient=False):
         torch = _torch()
         self.inputs = [[int(l) for l in t] for t in inputs]
         self.output = [int(l) for l in output]
@@ -222,8 +231,10 @@ class SlicedProgram:
         net = C.NetworkArgs(self.inputs, self.output, self.size_dict)
         n, p = C.path_array(self.ssa_path)
         sl = np.asarray(self.sliced_legs or [0], dtype=np.uint32)
+        self.has_gradient = bool(gradient)
         opts = C.ProgramOptions(self.code, self.precision, self.device, 1 if use_graph else 0,
-                                int(max_slices_per_group), int(workspace_budget), int(slice_begin), int(slice_end))
+                                int(max_slices_per_group), int(workspace_budget), int(slice_begin), int(slice_end),
+                                1 if gradient else 0)
         h = C.vp()
         C.check(C.lib().arctn_b200_program_create(net.ptr, n, p.ctypes.data_as(C.u64p), len(self.sliced_legs),
                                                   sl.ctypes.data_as(C.u32p), ctypes.byref(opts), ctypes.byref(h)),
@@ -259,6 +270,52 @@ class SlicedProgram:
                     "sliced contraction failed")
         self._keep = (call, ws)  # keep device buffers alive until the next call on this stream
         return _to_output(out, torch_mode)
+
+    def gradient(self, arrays, grad_output=None, *, part=0, workspace=None, output=None, stream=None):
+        """Adjoint sweep (programs built with ``gradient=True``).
+
+        Returns ``(output, [dL/d conj(T_i)])`` for part 0 (forward + reverse), ``(output, None)`` for
+        part 1 (forward, intermediates kept in ``workspace``) and ``(None, grads)`` for part 2 (reverse
+        only, with the workspace of a preceding part-1 call).  ``grad_output`` defaults to ones.
+        """
+        if not self.has_gradient:
+            raise ValueError("program was built without gradient=True")
+        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "gradient failed")
+        torch = _torch()
+        call = _DeviceCall(arrays, torch_mode, self.device)
+        out = output if output is not None else call.empty(self.output_shape, _torch_dtype(code))
+        ws = workspace if workspace is not None else call.workspace(self.workspace_bytes)
+        st = stream if stream is not None else call.stream
+        grads, gptr, g = None, None, None
+        if part != 1:
+            if grad_output is None:
+                g = torch.ones(self.output_shape, dtype=_torch_dtype(code), device=call.device)
+            elif _is_torch(grad_output):
+                g = grad_output.to(call.device, _torch_dtype(code)).contiguous()
+            else:
+                np_dt = {C.F32: np.float32, C.F64: np.float64, C.C64: np.complex64, C.C128: np.complex128}[code]
+                g = torch.from_numpy(np.array(grad_output, dtype=np_dt, order="C")).to(call.device)
+            grads = [torch.empty_like(t) for t in call.tensors]
+            gptr = (ctypes.c_void_p * len(grads))(*[t.data_ptr() for t in grads])
+        with torch.cuda.device(call.device):
+            C.check(C.lib().arctn_b200_program_gradient(self._h, int(part), call.ptrs,
+                                                        g.data_ptr() if g is not None else None, gptr,
+                                                        out.data_ptr() if part != 2 else None, ws.data_ptr(),
+                                                        ws.numel(), st.cuda_stream), "gradient failed")
+        self._keep = (call, ws, g)
+        if torch_mode:
+            return (out if part != 2 else None), grads
+        return (_to_output(out, False) if part != 2 else None), ([_to_output(x, False) for x in grads]
+                                                                 if grads is not None else None)
+
+    def device_status(self, workspace, stream=None):
+        """Synchronise and return 0, or raise when a bounded device-side wait expired in the last execute."""
+        torch = _torch()
+        st = stream if stream is not None else torch.cuda.current_stream(torch.device("cuda", self.device))
+        code = ctypes.c_int(0)
+        C.check(C.lib().arctn_b200_program_device_status(self._h, workspace.data_ptr(), st.cuda_stream,
+                                                         ctypes.byref(code)), "device status")
+        return code.value
 
     def profile(self, arrays, *, workspace=None):
         """Op-by-op run with CUDA events between launches: (ms, kind, algorithmic work) per launch."""

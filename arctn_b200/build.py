@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libarctn_b200.so")
 SOURCES = ["host.cpp", "program.cu", "capi.cu"]
-HEADERS = ["host.hpp", "program.hpp", "kernels.cuh"]
+HEADERS = ["host.hpp", "program.hpp", "kernels.cuh", "tc_gemm.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

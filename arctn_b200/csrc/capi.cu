@@ -18,6 +18,11 @@ using namespace ab2;
 
 static thread_local std::string g_last_error;
 
+namespace ab2 {
+// Lets other translation units of the library report through arctn_b200_last_error().
+void set_last_error(const std::string& m) { g_last_error = m; }
+}  // namespace ab2
+
 struct arctn_b200_plan {
   Network net;
   SsaPath path;
@@ -88,6 +93,7 @@ ProgramOptions to_options(const arctn_b200_program_options* o) {
     po.workspace_budget = o->workspace_budget;
     po.slice_begin = o->slice_begin;
     po.slice_end = o->slice_end;
+    po.gradient = o->gradient != 0;
   }
   return po;
 }
@@ -340,6 +346,31 @@ int arctn_b200_program_execute_stripped(arctn_b200_program* p, const void* const
     if (!p || !inputs || !log10_exponent) fail("null argument");
     p->p->execute_stripped(inputs, output, workspace, workspace_bytes, (cudaStream_t)cuda_stream, log10_exponent);
   });
+}
+
+int arctn_b200_program_gradient(arctn_b200_program* p, int part, const void* const* inputs, const void* grad_output,
+                                void* const* grad_inputs, void* output, void* workspace, uint64_t workspace_bytes,
+                                void* cuda_stream) {
+  return guarded([&] {
+    if (!p || !inputs) fail("null argument");
+    if (part < 0 || part > 2) fail("part must be 0, 1 or 2");
+    p->p->execute_gradient(part, inputs, grad_output, grad_inputs, output, workspace, workspace_bytes,
+                           (cudaStream_t)cuda_stream);
+  });
+}
+
+int arctn_b200_program_device_status(arctn_b200_program* p, void* workspace, void* cuda_stream, int* code) {
+  int c = 0;
+  int rc = guarded([&] {
+    if (!p || !workspace || !code) fail("null argument");
+    c = p->p->device_status(workspace, (cudaStream_t)cuda_stream);
+    *code = c;
+  });
+  if (rc == ARCTN_B200_OK && c != 0) {
+    g_last_error = "a bounded device-side wait expired (code " + std::to_string(c) + ")";
+    return ARCTN_B200_ERR_DEVICE_TIMEOUT;
+  }
+  return rc;
 }
 
 int arctn_b200_program_profile(arctn_b200_program* p, const void* const* inputs, void* output, void* workspace,

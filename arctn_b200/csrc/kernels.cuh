@@ -73,6 +73,12 @@ template <> struct Num<cf64> {
   __device__ static cf64 scale(cf64 v, double s) { return {v.re * s, v.im * s}; }
 };
 
+// Complex conjugate when `c` is set; identity for real types.
+__device__ __forceinline__ float cj(float v, int) { return v; }
+__device__ __forceinline__ double cj(double v, int) { return v; }
+__device__ __forceinline__ cf32 cj(cf32 v, int c) { return c ? cf32{v.re, -v.im} : v; }
+__device__ __forceinline__ cf64 cj(cf64 v, int c) { return c ? cf64{v.re, -v.im} : v; }
+
 __device__ inline double wadd(double a, double b) { return a + b; }
 __device__ inline cf64 wadd(cf64 a, cf64 b) { return {a.re + b.re, a.im + b.im}; }
 __device__ inline double wzero(double*) { return 0.0; }
@@ -122,6 +128,19 @@ __global__ void k_gather_reduce(const T* __restrict__ in, TO* __restrict__ out, 
   }
 }
 
+// out[offE[e] + offR[r]] = in[e] for every (e, r): the adjoint of a trace (every diagonal element
+// receives the traced gradient) or of a diagonal extraction (the diagonal receives it).  The
+// (e, r) -> position map is injective, so plain stores suffice after the output is zeroed.
+template <class T>
+__global__ void k_scatter(const T* __restrict__ in, T* __restrict__ out, const ll* __restrict__ offE,
+                          const ll* __restrict__ offR, ll n_in, ll n_red) {
+  const ll total = n_in * n_red;
+  for (ll idx = (ll)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (ll)gridDim.x * blockDim.x) {
+    const ll e = idx / n_red, r = idx - e * n_red;
+    out[offE[e] + offR[r]] = in[e];
+  }
+}
+
 // ---------------------------------------------------------------- GEMM tables
 struct GemmArgs {
   const void* A;
@@ -131,6 +150,7 @@ struct GemmArgs {
   const ll* aB; const ll* aM; const ll* aK;
   const ll* bB; const ll* bK; const ll* bN;
   SliceOff sa, sb;
+  int conj_a = 0, conj_b = 0;  // read an operand conjugated (adjoint steps)
 };
 
 // Thin steps: one thread per output element, k-loop through the tables.
@@ -158,8 +178,40 @@ __global__ void __launch_bounds__(256) k_gemm_small(GemmArgs g) {
     const T* a = Ap + slice_offset(g.sa, g.g0, s) + g.aB[b] + g.aM[i];
     const T* bb = Bp + slice_offset(g.sb, g.g0, s) + g.bB[b] + g.bN[j];
     A acc = Num<T>::zero();
-    for (ll l = 0; l < g.k; ++l) Num<T>::fma(acc, a[aK[l]], bb[bK[l]]);
+    for (ll l = 0; l < g.k; ++l) Num<T>::fma(acc, cj(a[aK[l]], g.conj_a), cj(bb[bK[l]], g.conj_b));
     Cp[idx] = acc;
+  }
+}
+
+// Few outputs with a long contraction (a dot product per slice, k up to 2^19):
+// one CTA per output element, the k range strided over 256 threads and
+// folded by a fixed shared-memory tree, so the sum order never varies.
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm_dot(GemmArgs g) {
+  using A = typename Num<T>::acc;
+  __shared__ A red[256];
+  const T* Ap = (const T*)g.A;
+  const T* Bp = (const T*)g.B;
+  T* Cp = (T*)g.C;
+  const ll mn = g.m * g.n, per_s = g.bt * mn, total = g.S * per_s;
+  for (ll idx = blockIdx.x; idx < total; idx += gridDim.x) {
+    const ll s = idx / per_s;
+    ll r = idx - s * per_s;
+    const ll b = r / mn;
+    r -= b * mn;
+    const ll i = r / g.n, j = r - i * g.n;
+    const T* a = Ap + slice_offset(g.sa, g.g0, s) + g.aB[b] + g.aM[i];
+    const T* bb = Bp + slice_offset(g.sb, g.g0, s) + g.bB[b] + g.bN[j];
+    A acc = Num<T>::zero();
+    for (ll l = threadIdx.x; l < g.k; l += 256) Num<T>::fma(acc, cj(a[g.aK[l]], g.conj_a), cj(bb[g.bK[l]], g.conj_b));
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (threadIdx.x < w) red[threadIdx.x] = Num<T>::add(red[threadIdx.x], red[threadIdx.x + w]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) Cp[idx] = red[0];
+    __syncthreads();
   }
 }
 
@@ -194,12 +246,12 @@ __global__ void __launch_bounds__(256) k_gemm_tile(GemmArgs g) {
       for (int q = threadIdx.x; q < TM * TK; q += 256) {
         const int ii = q / TK, ll_ = q % TK;
         const ll i = i0 + ii, l = l0 + ll_;
-        As[ll_][ii] = (i < g.m && l < g.k) ? abase[g.aM[i] + g.aK[l]] : Num<T>::zero();
+        As[ll_][ii] = (i < g.m && l < g.k) ? cj(abase[g.aM[i] + g.aK[l]], g.conj_a) : Num<T>::zero();
       }
       for (int q = threadIdx.x; q < TN * TK; q += 256) {
         const int jj = q % TN, ll_ = q / TN;
         const ll j = j0 + jj, l = l0 + ll_;
-        Bs[ll_][jj] = (j < g.n && l < g.k) ? bbase[g.bK[l] + g.bN[j]] : Num<T>::zero();
+        Bs[ll_][jj] = (j < g.n && l < g.k) ? cj(bbase[g.bK[l] + g.bN[j]], g.conj_b) : Num<T>::zero();
       }
       __syncthreads();
 #pragma unroll 4

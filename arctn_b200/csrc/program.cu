@@ -12,8 +12,11 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 #include <set>
+
+#include "tc_gemm.cuh"
 
 namespace ab2 {
 
@@ -184,6 +187,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
 
   // ---------------------------------------------------------------- buffers / ops
   std::vector<Buf> bufs;
+  std::vector<u64> saved;  // forward buffers the reverse sweep reads (step results, summed operands)
   std::vector<Op> ops1, ops2, strip1;
   const bool want_strip = !sliced_;
   auto new_buf = [&](bool region2, u64 bytes, u64 first) {
@@ -231,6 +235,15 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     z.bytes = bufs[part_buf].bytes;
     emit(false, z, false);
   }
+  // Device error word: bounded waits record where they gave up.
+  const u64 err_buf = new_buf(false, 16, 0);
+  bufs[err_buf].last = kInf;
+  {
+    Op z{Op::MEMSET};
+    z.c = Ref{Ref::WS, err_buf};
+    z.bytes = 16;
+    emit(false, z, true);
+  }
   if (want_strip) {
     u64 b = new_buf(false, 16, 0);
     bufs[b].last = kInf;
@@ -250,6 +263,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
   }
   const size_t n_slots = plan_.n_inputs + plan_.steps.size();
   std::vector<View> view(n_slots);
+  std::vector<Op> prep_gather(net.n_tensors(), Op{Op::MEMSET});  // kind GATHER where an input has traces
   for (size_t i = 0; i < net.n_tensors(); ++i) {
     struct Ax { u64 dim; ll stride; Leg leg; };
     std::vector<Ax> ax, red;
@@ -292,6 +306,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       g.n_red = rd.empty() ? 1 : (ll)prod(rd);
       g.S = 1;
       emit(false, g, true);
+      prep_gather[i] = g;  // the reverse sweep scatters through the same tables
       v.ref = Ref{Ref::WS, b};
       pstr = rm_strides(pdims);
     }
@@ -339,6 +354,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     pick(v, removed, rd, rs, 0);
     u64 numel = prod(kd);
     u64 b = new_buf(phase2, numel * eb, opidx(phase2));
+    saved.push_back(b);
     Op g{Op::GATHER};
     g.a = v.ref;
     g.sa = v.so;
@@ -359,6 +375,98 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     return r;
   };
 
+  auto part = [](const std::vector<u64>& d, const std::vector<ll>& s_, size_t lo, size_t hi) {
+    return offsets(std::vector<u64>(d.begin() + lo, d.begin() + hi), std::vector<ll>(s_.begin() + lo, s_.begin() + hi));
+  };
+  // A GEMM operand read through offset tables: batch, rows (M of A / N of B) and K.
+  struct Operand {
+    Ref ref;
+    SliceOff so;
+    bool variant;
+    std::vector<ll> tB, tR, tK;
+  };
+  // Emits C[s,b,i,j] = sum_l A(s,b,i,l) * B(s,b,l,j) into `out`.  Dense complex64 GEMMs under tf32x3
+  // go through the planar pack (permute + split, conjugating on the fly) and the tcgen05 kernel.
+  auto emit_gemm = [&](bool ph2, const Operand& A, const Operand& B, u64 bt, u64 m, u64 k, u64 n, Ref out,
+                       bool conj_a, bool conj_b) {
+    auto rows_contiguous = [](const std::vector<ll>& r, const std::vector<ll>& c) {
+      const bool r1 = r.size() > 1 && r[1] - r[0] == 1, c1 = c.size() > 1 && c[1] - c[0] == 1;
+      return r1 && !c1;  // the pack then reads the source along rows
+    };
+    Op g{Op::GEMM_SMALL};
+    g.tab[0] = tab_ll(A.tB);
+    g.tab[1] = tab_ll(A.tR);
+    g.tab[2] = tab_ll(A.tK);
+    g.tab[3] = tab_ll(B.tB);
+    g.tab[4] = tab_ll(B.tK);
+    g.tab[5] = tab_ll(B.tR);
+    g.bt = (ll)bt;
+    g.m = (ll)m;
+    g.k = (ll)k;
+    g.n = (ll)n;
+    g.a = A.ref;
+    g.b = B.ref;
+    g.sa = A.so;
+    g.sb = B.so;
+    g.c = out;
+    g.conj_a = conj_a && dtype_complex(dt);
+    g.conj_b = conj_b && dtype_complex(dt);
+    if (m >= 64 && n >= 64) g.kind = Op::GEMM_TILE64;
+    else if (m >= 24 && n >= 24) g.kind = Op::GEMM_TILE32;
+    else if (k >= 2048 && bt * m * n <= 64) g.kind = Op::GEMM_DOT;
+    const bool use_tc = opt_.precision == PREC_TF32X3 && dt == DT_C64 && m >= 96 && n >= 96 && k >= 32;
+    if (use_tc) {
+      const ll kpad = ((ll)k + tc::BK - 1) / tc::BK * tc::BK;
+      const ll rpa = ((ll)m + tc::BM - 1) / tc::BM * tc::BM;
+      const ll rpb = ((ll)n + tc::BN - 1) / tc::BN * tc::BN;
+      auto pack = [&](const Operand& X, ll rows, ll rpad, bool conj) {
+        const u64 pbuf = new_buf(ph2, (u64)(2 * (ll)bt * rpad * kpad * 4), opidx(ph2));
+        bufs[pbuf].fixed = ph2 && !X.variant;
+        Op p{Op::PACK};
+        p.a = X.ref;
+        p.sa = X.so;
+        p.c = Ref{Ref::WS, pbuf};
+        p.tab[0] = tab_ll(X.tB);
+        p.tab[1] = tab_ll(X.tR);
+        p.tab[2] = tab_ll(X.tK);
+        p.bt = (ll)bt;
+        p.rows = rows;
+        p.cols = (ll)k;
+        p.rpad = rpad;
+        p.kpad = kpad;
+        p.a_var = X.variant;
+        p.b_var = rows_contiguous(X.tR, X.tK);
+        p.conj_a = conj && dtype_complex(dt);
+        touch(X.ref, ph2, opidx(ph2));
+        emit(ph2, p, true);
+        return pbuf;
+      };
+      const u64 pa = pack(A, (ll)m, rpa, conj_a);
+      const u64 pb = pack(B, (ll)n, rpb, conj_b);
+      touch(Ref{Ref::WS, pa}, ph2, opidx(ph2));
+      g.kind = Op::GEMM_TC;
+      g.a = Ref{Ref::WS, pa};
+      g.b = Ref{Ref::WS, pb};
+      g.rpad = rpa;
+      g.rpad_b = rpb;
+      g.kpad = kpad;
+      g.a_var = A.variant;
+      g.b_var = B.variant;
+      g.conj_a = g.conj_b = false;  // conjugation happened in the packs
+      touch(g.a, ph2, opidx(ph2));
+      touch(g.b, ph2, opidx(ph2));
+    }
+    touch(A.ref, ph2, opidx(ph2));
+    touch(B.ref, ph2, opidx(ph2));
+    emit(ph2, g, true);
+    return g;
+  };
+  struct StepRec {
+    Operand a, b;          // the GEMM operands of the forward step (after dangling sums, in perm order)
+    std::vector<u64> da, db;  // their shapes in [batch, free_a, con] / [batch, con, free_b] order
+  };
+  std::vector<StepRec> recs;
+
   for (size_t s = 0; s < plan_.steps.size(); ++s) {
     const PairStep& st = plan_.steps[s];
     View A = view[st.left_slot], B = view[st.right_slot];
@@ -370,34 +478,15 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     for (u64 p : st.a_perm) { da.push_back(A.shape[p]); sa.push_back(A.strides[p]); }
     for (u64 p : st.b_perm) { db.push_back(B.shape[p]); sb.push_back(B.strides[p]); }
     const size_t nb = st.n_batch, nfa = st.n_free_a, nc = st.n_con;
-    auto part = [](const std::vector<u64>& d, const std::vector<ll>& s_, size_t lo, size_t hi) {
-      return offsets(std::vector<u64>(d.begin() + lo, d.begin() + hi), std::vector<ll>(s_.begin() + lo, s_.begin() + hi));
-    };
-    Op g{Op::GEMM_SMALL};
-    g.tab[0] = tab_ll(part(da, sa, 0, nb));
-    g.tab[1] = tab_ll(part(da, sa, nb, nb + nfa));
-    g.tab[2] = tab_ll(part(da, sa, nb + nfa, da.size()));
-    g.tab[3] = tab_ll(part(db, sb, 0, nb));
-    g.tab[4] = tab_ll(part(db, sb, nb, nb + nc));
-    g.tab[5] = tab_ll(part(db, sb, nb + nc, db.size()));
-    g.bt = (ll)st.bt;
-    g.m = (ll)st.m;
-    g.k = (ll)st.k;
-    g.n = (ll)st.n;
-    g.a = A.ref;
-    g.b = B.ref;
-    g.sa = A.so;
-    g.sb = B.so;
-    if (st.m >= 64 && st.n >= 64) g.kind = Op::GEMM_TILE64;
-    else if (st.m >= 24 && st.n >= 24) g.kind = Op::GEMM_TILE32;
+    Operand oa{A.ref, A.so, A.variant, part(da, sa, 0, nb), part(da, sa, nb, nb + nfa), part(da, sa, nb + nfa, da.size())};
+    Operand ob{B.ref, B.so, B.variant, part(db, sb, 0, nb), part(db, sb, nb + nc, db.size()), part(db, sb, nb, nb + nc)};
     const u64 cnumel = prod({st.bt, st.m, st.n});
     u64 cb = new_buf(ph2, cnumel * eb, opidx(ph2));
-    g.c = Ref{Ref::WS, cb};
-    touch(A.ref, ph2, opidx(ph2));
-    touch(B.ref, ph2, opidx(ph2));
+    saved.push_back(cb);
     touch(view[st.left_slot].ref, ph2, opidx(ph2));
     touch(view[st.right_slot].ref, ph2, opidx(ph2));
-    emit(ph2, g, true);
+    Op g = emit_gemm(ph2, oa, ob, st.bt, st.m, st.k, st.n, Ref{Ref::WS, cb}, false, false);
+    recs.push_back(StepRec{oa, ob, da, db});
     if (!ph2 && want_strip) {
       Op z{Op::MEMSET};
       z.c = Ref{Ref::WS, (u64)strip_exp_off_};
@@ -458,6 +547,130 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     emit(true, ac, false);
   }
 
+  // ---------------------------------------------------------------- adjoint (reverse) sweep
+  // Reverse-mode through the step loop with PyTorch's complex convention (grad = dL/d conj(x)):
+  // for C = A.B:  dA = dC . conj(B)^T,  dB = conj(A)^T . dC, mapped back through the step's permutes,
+  // broadcast over the legs the step summed away, then through the input traces / diagonals.
+  if (opt_.gradient) {
+    if (sliced_) throw Error(E_UNSUPPORTED, "gradients of sliced contractions are not supported by this build");
+    for (u64 b : saved) bufs[b].last = kInf;  // forward intermediates stay alive for the sweep
+    bwd_begin_ = ops1.size();
+    std::vector<View> dv(n_slots);
+    auto contiguous = [&](u64 buf, const std::vector<u64>& shape) {
+      View v;
+      v.ref = Ref{Ref::WS, buf};
+      v.shape = shape;
+      v.strides = rm_strides(shape);
+      v.so.local_stride = 0;
+      v.so.n = 0;
+      return v;
+    };
+    // Final slot: the incoming gradient broadcast over finalize's summed legs, permuted to slot order.
+    {
+      const auto& shp = fin.input_shape;
+      auto full_st = rm_strides(full_out_shape);
+      std::vector<ll> st(shp.size(), 0);
+      std::vector<size_t> k2, r2;
+      split_removed(shp.size(), fin.sum, k2, r2);
+      for (size_t j = 0; j < k2.size(); ++j) {
+        const Leg leg = fin.input_legs[k2[j]];
+        const size_t q = std::find(net.output.begin(), net.output.end(), leg) - net.output.begin();
+        st[k2[j]] = full_st[q];
+      }
+      const u64 numel = prod(shp);
+      const u64 b = new_buf(false, numel * eb, opidx(false));
+      Op g{Op::GATHER};
+      g.a = Ref{Ref::GRAD_OUT, 0};
+      g.c = Ref{Ref::WS, b};
+      g.tab[0] = tab_ll(offsets(shp, st));
+      g.tab[1] = tab_ll({0});
+      g.n_out = (ll)numel;
+      g.n_red = 1;
+      emit(false, g, false);
+      dv[fin.slot] = contiguous(b, shp);
+    }
+    // Scatter a GEMM result laid out in `order` dims (rm strides) back into a slot's own leg order,
+    // broadcasting over the legs the forward step summed away (`sum_seq`).
+    auto to_slot = [&](u64 src_buf, const std::vector<u64>& order_dims, const std::vector<u64>& perm,
+                       const std::vector<u64>& sum_seq, const std::vector<u64>& slot_shape) {
+      const auto src_st = rm_strides(order_dims);
+      std::vector<size_t> k2, r2;
+      split_removed(slot_shape.size(), sum_seq, k2, r2);
+      std::vector<ll> st(slot_shape.size(), 0);
+      for (size_t j = 0; j < k2.size(); ++j) {
+        const size_t p = std::find(perm.begin(), perm.end(), (u64)j) - perm.begin();
+        st[k2[j]] = src_st[p];
+      }
+      const u64 numel = prod(slot_shape);
+      const u64 b = new_buf(false, numel * eb, opidx(false));
+      Op g{Op::GATHER};
+      g.a = Ref{Ref::WS, src_buf};
+      g.c = Ref{Ref::WS, b};
+      g.tab[0] = tab_ll(offsets(slot_shape, st));
+      g.tab[1] = tab_ll({0});
+      g.n_out = (ll)numel;
+      g.n_red = 1;
+      touch(g.a, false, opidx(false));
+      emit(false, g, false);
+      return contiguous(b, slot_shape);
+    };
+    for (size_t s = plan_.steps.size(); s-- > 0;) {
+      const PairStep& st = plan_.steps[s];
+      const StepRec& rec = recs[s];
+      const View dC = dv[st.result_slot];
+      const size_t nb = st.n_batch, nfa = st.n_free_a;
+      const auto& rsh = st.result_shape;
+      const auto rst = rm_strides(rsh);
+      const std::vector<ll> dcB = part(rsh, rst, 0, nb), dcM = part(rsh, rst, nb, nb + nfa),
+                            dcN = part(rsh, rst, nb + nfa, rsh.size());
+      // dA' [batch, free_a, con] = dC [batch, free_a, free_b] . conj(B') [batch, con, free_b]^T
+      {
+        Operand a{dC.ref, dC.so, false, dcB, dcM, dcN};
+        Operand b{rec.b.ref, rec.b.so, false, rec.b.tB, rec.b.tK, rec.b.tR};
+        const u64 tbuf = new_buf(false, prod({st.bt, st.m, st.k}) * eb, opidx(false));
+        emit_gemm(false, a, b, st.bt, st.m, st.n, st.k, Ref{Ref::WS, tbuf}, false, true);
+        dv[st.left_slot] = to_slot(tbuf, rec.da, st.a_perm, st.sum_a, st.left_shape);
+      }
+      // dB' [batch, con, free_b] = conj(A') [batch, free_a, con]^T . dC [batch, free_a, free_b]
+      {
+        Operand a{rec.a.ref, rec.a.so, false, rec.a.tB, rec.a.tK, rec.a.tR};
+        Operand b{dC.ref, dC.so, false, dcB, dcN, dcM};
+        const u64 tbuf = new_buf(false, prod({st.bt, st.k, st.n}) * eb, opidx(false));
+        emit_gemm(false, a, b, st.bt, st.k, st.m, st.n, Ref{Ref::WS, tbuf}, true, false);
+        dv[st.right_slot] = to_slot(tbuf, rec.db, st.b_perm, st.sum_b, st.right_shape);
+      }
+    }
+    // Inputs: copy to the caller's gradient buffers, or scatter through an input's traces / diagonals.
+    for (size_t i = 0; i < net.n_tensors(); ++i) {
+      const View& d = dv[i];
+      std::vector<u64> shape0;
+      for (Leg l : net.inputs[i]) shape0.push_back(net.dim(l));
+      const u64 numel0 = prod(shape0);
+      if (prep_gather[i].kind != Op::GATHER) {
+        Op g{Op::GATHER};
+        g.a = d.ref;
+        g.c = Ref{Ref::GRADS, i};
+        g.tab[0] = tab_ll(offsets(shape0, rm_strides(shape0)));
+        g.tab[1] = tab_ll({0});
+        g.n_out = (ll)numel0;
+        g.n_red = 1;
+        touch(g.a, false, opidx(false));
+        emit(false, g, false);
+      } else {
+        Op z{Op::MEMSET};
+        z.c = Ref{Ref::GRADS, i};
+        z.bytes = numel0 * eb;
+        emit(false, z, false);
+        Op sc = prep_gather[i];
+        sc.kind = Op::SCATTER;
+        sc.a = d.ref;
+        sc.c = Ref{Ref::GRADS, i};
+        touch(sc.a, false, opidx(false));
+        emit(false, sc, false);
+      }
+    }
+  }
+
   // ---------------------------------------------------------------- group size and layout
   u64 region1 = 0, per_slice2 = 0;
   auto layout = [&](bool region2, u64 mult) {
@@ -469,11 +682,12 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     u64 top = 0;
     for (size_t id : ids) {
       Buf& b = bufs[id];
-      const u64 sz = align_up(b.bytes * mult);
+      const u64 sz = align_up(b.fixed ? b.bytes : b.bytes * mult);
       std::vector<std::pair<u64, u64>> busy;
       for (size_t p : placed) {
         const Buf& o = bufs[p];
-        if (o.first <= b.last && b.first <= o.last) busy.push_back({o.offset, o.offset + align_up(o.bytes * mult)});
+        if (o.first <= b.last && b.first <= o.last)
+          busy.push_back({o.offset, o.offset + align_up(o.fixed ? o.bytes : o.bytes * mult)});
       }
       std::sort(busy.begin(), busy.end());
       u64 off = 0;
@@ -514,6 +728,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     resolve(op.c);
   };
   if (want_strip) strip_exp_off_ = bufs[strip_exp_off_].offset;
+  err_off_ = bufs[err_buf].offset;
 
   // ---------------------------------------------------------------- final op sequence
   for (Op op : ops1) { finish(op); ops_.push_back(op); }
@@ -597,6 +812,7 @@ void launch_typed(const Op& op, const void* A, const void* B, void* C, const cha
       break;
     }
     case Op::GEMM_SMALL:
+    case Op::GEMM_DOT:
     case Op::GEMM_TILE64:
     case Op::GEMM_TILE32: {
       GemmArgs g;
@@ -604,10 +820,15 @@ void launch_typed(const Op& op, const void* A, const void* B, void* C, const cha
       g.bt = op.bt; g.m = op.m; g.k = op.k; g.n = op.n; g.S = op.S; g.g0 = op.g0;
       g.aB = T_(0); g.aM = T_(1); g.aK = T_(2); g.bB = T_(3); g.bK = T_(4); g.bN = T_(5);
       g.sa = op.sa; g.sb = op.sb;
+      g.conj_a = op.conj_a ? 1 : 0;
+      g.conj_b = op.conj_b ? 1 : 0;
       if (op.kind == Op::GEMM_SMALL) {
         const ll total = op.S * op.bt * op.m * op.n;
         const size_t smem = op.k <= 1024 ? (size_t)(2 * op.k * sizeof(ll)) : 0;
         k_gemm_small<T><<<grid_for(total, 256, 148 * 32), 256, smem, st>>>(g);
+      } else if (op.kind == Op::GEMM_DOT) {
+        const ll total = op.S * op.bt * op.m * op.n;
+        k_gemm_dot<T><<<(int)std::min<ll>(total, 148 * 16), 256, 0, st>>>(g);
       } else if (op.kind == Op::GEMM_TILE64) {
         const ll tiles = ((op.n + 63) / 64) * ((op.m + 63) / 64) * op.S * op.bt;
         k_gemm_tile<T, 64, 64, 16><<<(int)std::min<ll>(tiles, 148 * 8), 256, 0, st>>>(g);
@@ -633,6 +854,9 @@ void launch_typed(const Op& op, const void* A, const void* B, void* C, const cha
     case Op::MAXABS:
       k_maxabs<T><<<grid_for(op.n_out), 256, 0, st>>>((const T*)C, op.n_out, (unsigned long long*)A);
       break;
+    case Op::SCATTER:
+      k_scatter<T><<<grid_for(op.n_out * op.n_red), 256, 0, st>>>((const T*)A, (T*)C, T_(0), T_(1), op.n_out, op.n_red);
+      break;
     case Op::STRIP:
       k_strip_scale<T><<<grid_for(op.n_out), 256, 0, st>>>((T*)C, op.n_out, (const unsigned long long*)A,
                                                              (double*)((char*)A + 8), 1);
@@ -644,17 +868,98 @@ void launch_typed(const Op& op, const void* A, const void* B, void* C, const cha
 
 }  // namespace
 
+namespace {
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiled)p;
+  });
+  if (!fn) throw Error(E_CUDA, "cuTensorMapEncodeTiled is unavailable from the driver");
+  return fn;
+}
+
+// [re|im][z][rows][kpad] fp32 planes, boxes of 16 x 128 with 64-byte swizzle.
+CUtensorMap plane_map(void* base, ll kpad, ll rows, ll zplanes) {
+  CUtensorMap m;
+  cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows, (cuuint64_t)zplanes};
+  cuuint64_t strides[2] = {(cuuint64_t)(kpad * 4), (cuuint64_t)(kpad * rows * 4)};
+  cuuint32_t box[3] = {(cuuint32_t)tc::BK, (cuuint32_t)tc::BM, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error(E_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+  return m;
+}
+
+void launch_tc(const Op& op, void* A, void* B, void* C, const char* tab, int* err, cudaStream_t st) {
+  if (op.kind == Op::PACK) {
+    const ll Z = (op.a_var ? op.S : 1) * op.bt;
+    const ll tiles = Z * (op.rpad / 32) * ((op.kpad + 31) / 32);
+    tc::k_pack_planar<<<(int)std::min<ll>(tiles, 148 * 16), 256, 0, st>>>(
+        (const cf32*)A, (float*)C, (const ll*)(tab + op.tab[0]), (const ll*)(tab + op.tab[1]),
+        (const ll*)(tab + op.tab[2]), op.bt, op.rows, op.cols, op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0,
+        op.conj_a ? 1 : 0);
+    return;
+  }
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 64 && !attr_set[dev]) {
+    CK(cudaFuncSetAttribute(tc::k_tc_cgemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    attr_set[dev] = true;
+  }
+  const ll s_eff = (op.a_var || op.b_var) ? op.S : 1;
+  const ll za = (op.a_var ? op.S : 1) * op.bt, zb = (op.b_var ? op.S : 1) * op.bt;
+  const CUtensorMap ma = plane_map(A, op.kpad, op.rpad, 2 * za);
+  const CUtensorMap mb = plane_map(B, op.kpad, op.rpad_b, 2 * zb);
+  tc::TcArgs args;
+  args.C = (cf32*)C;
+  args.m = op.m;
+  args.n = op.n;
+  args.k_tiles = (int)(op.kpad / tc::BK);
+  args.za = (int)za;
+  args.zb = (int)zb;
+  args.bt = (int)op.bt;
+  args.a_var = op.a_var;
+  args.b_var = op.b_var;
+  args.err = err;
+  const ll zc = s_eff * op.bt;
+  if (zc > 65535) throw Error(E_UNSUPPORTED, "tensor-core GEMM batch exceeds the grid limit");
+  dim3 grid((unsigned)((op.n + tc::BN - 1) / tc::BN), (unsigned)((op.m + tc::BM - 1) / tc::BM), (unsigned)zc);
+  tc::k_tc_cgemm_tf32x3<<<grid, 192, tc::SMEM_BYTES, st>>>(ma, mb, args);
+}
+
+}  // namespace
+
 void Program::launch_op(const Op& op, const void* const* inputs, void* output, char* ws, cudaStream_t st) {
   auto ptr = [&](const Ref& r) -> void* {
     switch (r.kind) {
       case Ref::INPUT: return const_cast<void*>(inputs[r.index]);
       case Ref::WS: return ws + r.index;
       case Ref::OUTPUT: return output;
+      case Ref::GRAD_OUT: return const_cast<void*>(grad_out_);
+      case Ref::GRADS: return grads_ ? grads_[r.index] : nullptr;
       default: return nullptr;
     }
   };
   if (op.kind == Op::MEMSET) {
     CK(cudaMemsetAsync(ptr(op.c), 0, op.bytes, st));
+    return;
+  }
+  if (op.kind == Op::PACK || op.kind == Op::GEMM_TC) {
+    launch_tc(op, ptr(op.a), ptr(op.b), ptr(op.c), dev_tab_, (int*)(ws + err_off_), st);
+    CK(cudaGetLastError());
     return;
   }
   const bool out_f64 = out_f64_flag_;
@@ -696,6 +1001,10 @@ void Program::execute(const void* const* inputs, void* output, bool f64_out, voi
   DeviceGuard guard(opt_.device);
   std::lock_guard<std::mutex> lk(mu_);
   out_f64_flag_ = f64_out;
+  if (opt_.gradient) {  // plain execute of a gradient program: the forward part only
+    for (size_t i = 0; i < bwd_begin_; ++i) launch_op(ops_[i], inputs, output, (char*)ws, st);
+    return;
+  }
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (st) CK(cudaStreamIsCapturing(st, &cs));
   const bool graph = opt_.use_graph && st != nullptr && cs == cudaStreamCaptureStatusNone;
@@ -747,6 +1056,8 @@ double op_work(const Op& op, int dt) {
   const double eb = (double)dtype_bytes(dt);
   switch (op.kind) {
     case Op::GEMM_SMALL:
+    case Op::GEMM_DOT:
+    case Op::GEMM_TC:
     case Op::GEMM_TILE64:
     case Op::GEMM_TILE32:
       return (dtype_complex(dt) ? 8.0 : 2.0) * (double)op.S * op.bt * op.m * op.k * op.n;
@@ -792,6 +1103,58 @@ void Program::profile(const void* const* inputs, void* output, void* ws, u64 ws_
     throw;
   }
   for (auto e : ev) cudaEventDestroy(e);
+}
+
+u64 Program::forward_launches() const {
+  u64 n = 0;
+  for (size_t i = 0; i < std::min(bwd_begin_, ops_.size()); ++i) n += ops_[i].kind != Op::MEMSET;
+  return n;
+}
+
+u64 Program::backward_launches() const {
+  u64 n = 0;
+  for (size_t i = bwd_begin_; i < ops_.size(); ++i) n += ops_[i].kind != Op::MEMSET;
+  return n;
+}
+
+void Program::execute_gradient(int part, const void* const* inputs, const void* grad_out, void* const* grads,
+                               void* output, void* ws, u64 ws_bytes, cudaStream_t st) {
+  if (!opt_.gradient) throw Error(E_INVALID, "the program was built without gradient support");
+  if (ws_bytes < ws_total_)
+    throw Error(E_WORKSPACE, "workspace of " + std::to_string(ws_bytes) + " bytes is smaller than the required " +
+                                 std::to_string(ws_total_));
+  for (u64 i = 0; i < plan_.n_inputs; ++i)
+    if (!inputs[i]) throw Error(E_INVALID, "input " + std::to_string(i) + " pointer is null");
+  if (part != 2 && !output) throw Error(E_INVALID, "output pointer is null");
+  if (part != 1) {
+    if (!grad_out) throw Error(E_INVALID, "grad_output pointer is null");
+    for (u64 i = 0; i < plan_.n_inputs; ++i)
+      if (!grads || !grads[i]) throw Error(E_INVALID, "gradient buffer " + std::to_string(i) + " is null");
+  }
+  if (ws_total_ && !ws) throw Error(E_INVALID, "workspace pointer is null");
+  DeviceGuard guard(opt_.device);
+  std::lock_guard<std::mutex> lk(mu_);
+  out_f64_flag_ = false;
+  grad_out_ = grad_out;
+  grads_ = grads;
+  const size_t lo = part == 2 ? bwd_begin_ : 0, hi = part == 1 ? bwd_begin_ : ops_.size();
+  try {
+    for (size_t i = lo; i < hi; ++i) launch_op(ops_[i], inputs, output, (char*)ws, st);
+  } catch (...) {
+    grad_out_ = nullptr;
+    grads_ = nullptr;
+    throw;
+  }
+  grad_out_ = nullptr;
+  grads_ = nullptr;
+}
+
+int Program::device_status(void* ws, cudaStream_t st) {
+  DeviceGuard guard(opt_.device);
+  int code = 0;
+  CK(cudaMemcpyAsync(&code, (char*)ws + err_off_, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return code;
 }
 
 void Program::execute_stripped(const void* const* inputs, void* output, void* ws, u64 ws_bytes, cudaStream_t st,

@@ -29,16 +29,20 @@ struct ProgramOptions {
   u64 max_slices_per_group = 0;
   u64 workspace_budget = 0;
   u64 slice_begin = 0, slice_end = 0;  // both 0: every slice
+  bool gradient = false;               // also build the adjoint (reverse) sweep
 };
 
 // Where an operand lives at run time.
 struct Ref {
-  enum Kind : int { NONE = 0, INPUT = 1, WS = 2, OUTPUT = 3 } kind = NONE;
-  u64 index = 0;  // input index, or byte offset into the workspace
+  enum Kind : int { NONE = 0, INPUT = 1, WS = 2, OUTPUT = 3, GRAD_OUT = 4, GRADS = 5 } kind = NONE;
+  u64 index = 0;  // input / gradient index, or byte offset into the workspace
 };
 
 struct Op {
-  enum Kind : int { GATHER, GEMM_SMALL, GEMM_TILE64, GEMM_TILE32, ACCUM, OUTPUT, MEMSET, MAXABS, STRIP } kind;
+  enum Kind : int {
+    GATHER = 0, GEMM_SMALL = 1, GEMM_TILE64 = 2, GEMM_TILE32 = 3, ACCUM = 4, OUTPUT = 5, MEMSET = 6, MAXABS = 7,
+    STRIP = 8, GEMM_TC = 9, GEMM_DOT = 10, PACK = 11, SCATTER = 12
+  } kind;
   Ref a, b, c;
   u64 tab[6] = {0, 0, 0, 0, 0, 0};  // byte offsets of offset tables in the program's table buffer
   ll bt = 1, m = 1, k = 1, n = 1, S = 1, g0 = 0;
@@ -47,6 +51,10 @@ struct Op {
   ll n_segs = 0, n_e = 0, n_blocks = 0, n_chunks = 0;  // ACCUM / OUTPUT
   u64 bytes = 0;            // MEMSET
   bool out_f64 = false;     // GATHER / OUTPUT writing FP64
+  // PACK: rows x cols gathered into [re|im][z][rpad][kpad]; GEMM_TC: padded operand geometry.
+  ll rows = 0, cols = 0, rpad = 0, kpad = 0, rpad_b = 0;
+  bool a_var = false, b_var = false;
+  bool conj_a = false, conj_b = false;  // GEMM operands read conjugated (adjoint); PACK uses conj_a
 };
 
 class Program {
@@ -69,9 +77,18 @@ class Program {
   // Op-by-op run with an event between launches; per launch: ms, kind, algorithmic work.
   void profile(const void* const* inputs, void* output, void* ws, u64 ws_bytes, cudaStream_t st, float* ms,
                int* kind, double* work);
+  // Gradient programs: part 0 = forward (keeps intermediates in ws) + reverse sweep, 1 = forward only,
+  // 2 = reverse sweep only (needs the ws of a preceding part-1 run and the same inputs).
+  void execute_gradient(int part, const void* const* inputs, const void* grad_out, void* const* grads, void* output,
+                        void* ws, u64 ws_bytes, cudaStream_t st);
+  bool has_gradient() const { return opt_.gradient; }
+  u64 forward_launches() const;
+  u64 backward_launches() const;
 
  private:
-  struct Buf { u64 bytes, first, last; bool region2; u64 offset; };
+  // Workspace buffer with an op-index lifetime; region-2 sizes scale with the
+  // group size unless `fixed` (operands shared by every slice of a group).
+  struct Buf { u64 bytes, first, last; bool region2; u64 offset; bool fixed = false; };
 
   void build(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced);
   void enqueue(const std::vector<Op>& ops, const void* const* inputs, void* output, char* ws, cudaStream_t st);
@@ -89,6 +106,17 @@ class Program {
   char* dev_tab_ = nullptr;
   u64 ws_total_ = 0;
   u64 strip_mx_off_ = 0, strip_exp_off_ = 0;
+  u64 err_off_ = 0;  // device error word (bounded-wait expiry codes), cleared by every execute
+
+ public:
+  // Synchronises `st` and returns the device error word of the last execute on `ws`.
+  int device_status(void* ws, cudaStream_t st);
+
+ private:
+
+  size_t bwd_begin_ = 0;             // gradient programs: first op of the reverse sweep in ops_
+  const void* grad_out_ = nullptr;   // bound during execute_gradient
+  void* const* grads_ = nullptr;
 
   std::mutex mu_;
   bool out_f64_flag_ = false;

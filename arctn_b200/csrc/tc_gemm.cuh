@@ -1,0 +1,332 @@
+// tcgen05 complex GEMM with split-TF32 products (sm_100a).
+//
+// C[z] (m x n, complex64) = A[z] (m x k) . B[z] (k x n) for every batch z.
+// Operands arrive packed by k_pack_planar as K-major fp32 planes
+// [re | im][z][rows][k] (rows padded to 128, k padded to 16).  Per 16-wide K
+// slab the CTA splits every value x into hi = x with its 13 low mantissa bits
+// cleared (exactly representable in TF32) and lo = x - hi (exact in FP32), and
+// issues the 4M complex product as 12 TF32 MMAs into two TMEM accumulators:
+//   Cr += Ar*Br - Ai*Bi,  Ci += Ar*Bi + Ai*Br   for (hi,hi), (hi,lo), (lo,hi),
+// the minus through the instruction's negate-A bit.  Accumulation is FP32.
+//
+// Warp roles (192 threads, one CTA per 128x128 output tile):
+//   warp 0      TMA producer: 4 plane tiles per stage, 3-stage ring
+//   warp 1      TMEM allocation + single-thread MMA issue
+//   warps 2..5  hi/lo split in shared memory, then the epilogue (TMEM -> HBM)
+// Every mbarrier wait is bounded (about one second of global time); on expiry
+// the kernel records a code in *err, drains what it issued and returns.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "kernels.cuh"
+
+namespace ab2 {
+namespace tc {
+
+constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3, LO_SLOTS = 2;
+constexpr int PLANE_BYTES = BM * BK * 4;          // 8 KB: 128 rows x 64 B
+constexpr int STAGE_BYTES = 4 * PLANE_BYTES;       // Ar, Ai, Br, Bi
+constexpr int SMEM_BYTES = (STAGES + LO_SLOTS) * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*align*/;
+// Cr: [0,128), Ci: [128,256) take the (hi,hi) products; Cr', Ci': [256,384), [384,512) take the
+// (hi,lo) and (lo,hi) products, which are 2^-10 smaller, so the large accumulators see 4 of the 12
+// additions per K step and the rounding of each accumulation stays at the scale of its own sum.
+constexpr uint32_t TMEM_COLS = 512;
+constexpr unsigned long long kWaitNs = 1000000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait; false (and *err = code) once about a second has passed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err, int code) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = now_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try(bar, parity)) return true;
+    if ((i & 255) == 0) {
+      if (now_ns() - t0 > kWaitNs) {
+        atomicCAS(err, 0, code);
+        return false;
+      }
+      __nanosleep(128);
+    }
+  }
+}
+
+__device__ __forceinline__ void tma_load_3d(const CUtensorMap* map, uint64_t* bar, void* dst, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+// K-major operand tile, 64-byte swizzle: rows of 64 B, 8-row groups 512 B apart.
+__device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFF) >> 4) | (1ull << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46) |
+         (4ull << 61);
+}
+// kind::tf32, FP32 accumulate, K-major A and B, M = 128, N = 128.
+__host__ __device__ constexpr uint32_t idesc_tf32(bool neg_a) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(BN >> 3) << 17) |
+         ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+#define AB2_TMEM_LD32(taddr, r)                                                                                   \
+  asm volatile(                                                                                                   \
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18," \
+      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                                             \
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),          \
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),    \
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),  \
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])   \
+      : "r"(taddr))
+
+struct TcArgs {
+  cf32* C;
+  ll m, n;           // logical output rows / complex columns
+  int k_tiles;       // padded K / BK
+  int za, zb;        // plane batches of A and B (the imaginary plane starts at z + za / z + zb)
+  int bt;            // GEMM batch per slice
+  int a_var, b_var;  // operand differs per slice (else it is shared by all slices)
+  int* err;
+};
+
+static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_constant__ CUtensorMap tmA,
+                                                          const __grid_constant__ CUtensorMap tmB, TcArgs args) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* raw = smem;                                   // STAGES x {Ar, Ai, Br, Bi}
+  unsigned char* lo = smem + STAGES * STAGE_BYTES;             // LO_SLOTS x {Ar, Ai, Br, Bi}
+  uint64_t* bars = (uint64_t*)(smem + (STAGES + LO_SLOTS) * STAGE_BYTES);
+  uint64_t* full = bars;                     // TMA landed          (count 1 + tx)
+  uint64_t* empty = bars + STAGES;           // MMAs done reading   (commit)
+  uint64_t* lofull = bars + 2 * STAGES;      // split done          (count 128)
+  uint64_t* loempty = lofull + LO_SLOTS;     // MMAs done with slot (commit)
+  uint64_t* accfull = loempty + LO_SLOTS;    // all MMAs done       (commit)
+  uint64_t* drain = accfull + 1;             // abort drain         (commit)
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(drain + 1);
+  volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int tile_n = blockIdx.x, tile_m = blockIdx.y, z = blockIdx.z;
+  const int s_idx = z / args.bt, b_idx = z % args.bt;
+  const int zA = args.a_var ? z : b_idx;
+  const int zB = args.b_var ? z : b_idx;
+  (void)s_idx;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < STAGES; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
+    for (int i = 0; i < LO_SLOTS; ++i) { mbar_init(&lofull[i], 128); mbar_init(&loempty[i], 1); }
+    mbar_init(accfull, 1);
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32((const void*)tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const int KT = args.k_tiles;
+
+  if (warp == 0) {
+    // ------------------------------------------------------------ TMA producer
+    if (lane == 0) {
+      int issued = 0;
+      for (int t = 0; t < KT; ++t) {
+        const int s = t % STAGES;
+        if (t >= STAGES && !mbar_wait(&empty[s], ((t / STAGES) - 1) & 1, args.err, 1)) { *abort_flag = 1; break; }
+        if (*abort_flag) break;
+        unsigned char* dst = raw + s * STAGE_BYTES;
+        mbar_expect_tx(&full[s], STAGE_BYTES);
+        const int k0 = t * BK;
+        tma_load_3d(&tmA, &full[s], dst + 0 * PLANE_BYTES, k0, tile_m * BM, zA);
+        tma_load_3d(&tmA, &full[s], dst + 1 * PLANE_BYTES, k0, tile_m * BM, zA + args.za);
+        tma_load_3d(&tmB, &full[s], dst + 2 * PLANE_BYTES, k0, tile_n * BN, zB);
+        tma_load_3d(&tmB, &full[s], dst + 3 * PLANE_BYTES, k0, tile_n * BN, zB + args.zb);
+        issued = t + 1;
+      }
+      if (*abort_flag) {  // let issued copies land before the CTA retires
+        for (int t = (issued > STAGES ? issued - STAGES : 0); t < issued; ++t)
+          mbar_wait(&full[t % STAGES], (t / STAGES) & 1, args.err, 7);
+      }
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      const uint32_t id_pos = idesc_tf32(false), id_neg = idesc_tf32(true);
+      const uint32_t cr = tmem, ci = tmem + BN, crs = tmem + 2 * BN, cis = tmem + 3 * BN;
+      bool first = true;
+      for (int t = 0; t < KT && !*abort_flag; ++t) {
+        const int s = t % STAGES, q = t % LO_SLOTS;
+        if (!mbar_wait(&lofull[q], (t / LO_SLOTS) & 1, args.err, 2)) { *abort_flag = 1; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t rb = smem_u32(raw + s * STAGE_BYTES), lb = smem_u32(lo + q * STAGE_BYTES);
+        const uint32_t hAr = rb, hAi = rb + PLANE_BYTES, hBr = rb + 2 * PLANE_BYTES, hBi = rb + 3 * PLANE_BYTES;
+        const uint32_t lAr = lb, lAi = lb + PLANE_BYTES, lBr = lb + 2 * PLANE_BYTES, lBi = lb + 3 * PLANE_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < BK / 8; ++kk) {
+          const uint32_t o = kk * 32;  // 8 tf32 = 32 bytes along the swizzled row
+          const uint32_t acc = first ? 0u : 1u;
+          // correction terms (lo,hi) and (hi,lo) into Cr', Ci'
+          umma(crs, sw64_desc(lAr + o), sw64_desc(hBr + o), id_pos, acc);
+          umma(cis, sw64_desc(lAr + o), sw64_desc(hBi + o), id_pos, acc);
+          umma(crs, sw64_desc(lAi + o), sw64_desc(hBi + o), id_neg, 1);
+          umma(cis, sw64_desc(lAi + o), sw64_desc(hBr + o), id_pos, 1);
+          umma(crs, sw64_desc(hAr + o), sw64_desc(lBr + o), id_pos, 1);
+          umma(cis, sw64_desc(hAr + o), sw64_desc(lBi + o), id_pos, 1);
+          umma(crs, sw64_desc(hAi + o), sw64_desc(lBi + o), id_neg, 1);
+          umma(cis, sw64_desc(hAi + o), sw64_desc(lBr + o), id_pos, 1);
+          // leading terms (hi,hi) into Cr, Ci
+          umma(cr, sw64_desc(hAr + o), sw64_desc(hBr + o), id_pos, acc);
+          umma(ci, sw64_desc(hAr + o), sw64_desc(hBi + o), id_pos, acc);
+          umma(cr, sw64_desc(hAi + o), sw64_desc(hBi + o), id_neg, 1);
+          umma(ci, sw64_desc(hAi + o), sw64_desc(hBr + o), id_pos, 1);
+          first = false;
+        }
+        umma_commit(&empty[s]);
+        umma_commit(&loempty[q]);
+      }
+      umma_commit(*abort_flag ? drain : accfull);
+      if (*abort_flag) mbar_wait(drain, 0, args.err, 8);
+    }
+  } else {
+    // ------------------------------------------------------------ hi/lo split (128 threads)
+    const int tid = threadIdx.x - 64;
+    for (int t = 0; t < KT; ++t) {
+      const int s = t % STAGES, q = t % LO_SLOTS;
+      bool ok = mbar_wait(&full[s], (t / STAGES) & 1, args.err, 3);
+      if (ok && t >= LO_SLOTS) ok = mbar_wait(&loempty[q], ((t / LO_SLOTS) - 1) & 1, args.err, 4);
+      if (!ok || *abort_flag) { *abort_flag = 1; break; }
+      uint4* rp = (uint4*)(raw + s * STAGE_BYTES);
+      uint4* lp = (uint4*)(lo + q * STAGE_BYTES);
+#pragma unroll 4
+      for (int v = tid; v < STAGE_BYTES / 16; v += 128) {
+        uint4 x = rp[v];
+        uint4 h = make_uint4(x.x & 0xFFFFE000u, x.y & 0xFFFFE000u, x.z & 0xFFFFE000u, x.w & 0xFFFFE000u);
+        float4 l = make_float4(__uint_as_float(x.x) - __uint_as_float(h.x), __uint_as_float(x.y) - __uint_as_float(h.y),
+                               __uint_as_float(x.z) - __uint_as_float(h.z), __uint_as_float(x.w) - __uint_as_float(h.w));
+        rp[v] = h;
+        lp[v] = *reinterpret_cast<uint4*>(&l);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_arrive(&lofull[q]);
+    }
+    // ------------------------------------------------------------ epilogue
+    const bool ok = !*abort_flag && mbar_wait(accfull, 0, args.err, 5);
+    if (ok) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int quad = warp % 4;
+      const ll row = (ll)tile_m * BM + quad * 32 + lane;
+      cf32* crow = args.C + ((ll)z * args.m + row) * args.n;
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        uint32_t vr[32], vi[32], sr[32], si[32];
+        const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + c0;
+        AB2_TMEM_LD32(ta, vr);
+        AB2_TMEM_LD32(ta + BN, vi);
+        AB2_TMEM_LD32(ta + 2 * BN, sr);
+        AB2_TMEM_LD32(ta + 3 * BN, si);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < args.m) {
+          const ll col0 = (ll)tile_n * BN + c0;
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (col0 + j < args.n)
+              crow[col0 + j] = cf32{__uint_as_float(vr[j]) + __uint_as_float(sr[j]),
+                                    __uint_as_float(vi[j]) + __uint_as_float(si[j])};
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+// Gather one operand of a pairwise step into K-major fp32 planes:
+//   dst[(p*Z + z)*Rpad*Kpad + r*Kpad + c] = (p == 0 ? re : im) of src(z, r, c), zero in the padding,
+// where src(z, r, c) = src[sliceoff(z / bt) + tabB[z % bt] + tabR[r] + tabC[c]].
+// This is the permute of the reference step (src/tensor.rs:453-492) fused with the planar split.
+// A 32 x 32 (r, c) tile goes through shared memory: it is read along whichever index the source
+// walks with unit stride (r_major) and written along c, so both sides stay coalesced.
+static __global__ void __launch_bounds__(256) k_pack_planar(const cf32* __restrict__ src, float* __restrict__ dst,
+                                                     const ll* __restrict__ tabB, const ll* __restrict__ tabR,
+                                                     const ll* __restrict__ tabC, ll bt, ll R, ll K, ll Rpad, ll Kpad,
+                                                     ll Z, SliceOff so, ll g0, int r_major, int conj) {
+  const float im_sign = conj ? -1.f : 1.f;
+  __shared__ cf32 tile[32][33];
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;  // 32 x 8
+  const ll tiles_c = (Kpad + 31) / 32, tiles_r = Rpad / 32, per_z = tiles_c * tiles_r;
+  const ll plane = Z * Rpad * Kpad;
+  for (ll t = blockIdx.x; t < Z * per_z; t += gridDim.x) {
+    const ll zz = t / per_z, rem = t - zz * per_z;
+    const ll r0 = (rem / tiles_c) * 32, c0 = (rem % tiles_c) * 32;
+    const ll s = zz / bt, b = zz - s * bt;
+    const cf32* base = src + slice_offset(so, g0, s) + tabB[b];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int u = ty + 8 * j;
+      const ll r = r0 + (r_major ? tx : u), c = c0 + (r_major ? u : tx);
+      cf32 v{0.f, 0.f};
+      if (r < R && c < K) v = base[tabR[r] + tabC[c]];
+      if (r_major) tile[tx][u] = v;
+      else tile[u][tx] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int u = ty + 8 * j;
+      const ll r = r0 + u, c = c0 + tx;
+      if (c < Kpad) {
+        const ll o = (zz * Rpad + r) * Kpad + c;
+        dst[o] = tile[u][tx].re;
+        dst[plane + o] = im_sign * tile[u][tx].im;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace tc
+}  // namespace ab2

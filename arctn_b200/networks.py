@@ -164,7 +164,7 @@ def gaussian_tensors(net, dtype, seed, scale_base=None):
             v = (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)) * scale
         else:
             v = rng.standard_normal(shape) * scale
-        out.append(np.ascontiguousarray(np.asarray(v).astype(dtype)))
+        out.append(np.array(np.asarray(v), dtype=dtype, order="C"))
     return out
 
 

@@ -178,6 +178,7 @@ typedef struct {
   uint64_t workspace_budget;     /* bytes; 0: 8 GiB */
   uint64_t slice_begin;          /* run only global slices [slice_begin, slice_end); both 0: all slices.  A */
   uint64_t slice_end;            /* partial range sums only its slices (one rank of a sharded contraction). */
+  int gradient;                  /* also build the adjoint sweep (arctn_b200_program_gradient); unsliced only */
 } arctn_b200_program_options;
 
 /* Builds a program that contracts `net` along `ssa_path`, summing internal sliced legs and assembling
@@ -207,6 +208,22 @@ int arctn_b200_program_execute_f64out(arctn_b200_program* program, const void* c
 int arctn_b200_program_execute_stripped(arctn_b200_program* program, const void* const* inputs, void* output,
                                         void* workspace, uint64_t workspace_bytes, void* cuda_stream,
                                         double* log10_exponent);
+
+/* Adjoint of the contraction (programs created with options.gradient = 1).  With grad_output G (the
+ * output's shape), writes grad_inputs[i] = dL/d conj(T_i) in PyTorch's complex convention: for a step
+ * C = A.B the sweep forms dA = dC.conj(B)^T and dB = conj(A)^T.dC, undoing each step's permutes and
+ * broadcasting over the legs it summed away (src/compiled.rs:155-171 is the forward it reverses).
+ * part 0: forward (result into `output`) then the reverse sweep; part 1: forward only, keeping the
+ * intermediates in `workspace`; part 2: reverse sweep only, reusing the workspace of a preceding
+ * part-1 call with the same inputs.  No counterpart in the reference, which has no differentiation. */
+int arctn_b200_program_gradient(arctn_b200_program* program, int part, const void* const* inputs,
+                                const void* grad_output, void* const* grad_inputs, void* output, void* workspace,
+                                uint64_t workspace_bytes, void* cuda_stream);
+
+/* Synchronises `cuda_stream` and reports the device status word the last execute on `workspace` left:
+ * *code = 0 when every bounded device-side wait completed, else the code of the first wait that expired
+ * (the call then returns ARCTN_B200_ERR_DEVICE_TIMEOUT). */
+int arctn_b200_program_device_status(arctn_b200_program* program, void* workspace, void* cuda_stream, int* code);
 
 /* Profiled execute: launches op by op (no graph) with a CUDA event between consecutive kernels on
  * `cuda_stream`, synchronises, and writes per-launch duration (ms), kind and algorithmic work (real flops

@@ -114,7 +114,7 @@ def _path_arr(path):
 
 
 def _inputs(net: _Net, arrays):
-    arrays = [np.ascontiguousarray(a) for a in arrays]
+    arrays = [np.array(a, order="C", copy=None) for a in arrays]  # keeps 0-d shapes
     dt = arrays[0].dtype
     if dt not in DTYPE_CODES:
         raise OracleError(f"unsupported dtype {dt}")

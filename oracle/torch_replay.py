@@ -1,0 +1,32 @@
+"""Step-by-step torch replay of a compiled plan -- TEST INFRASTRUCTURE ONLY (gradient oracle).
+
+The reference exposes its compiled stages so a caller can put every pair
+contraction on an autograd tape (``src/compiled.rs:7-10``: input preps, pair
+steps and finalize run in order give the same result as ``execute``).  This
+module is that caller: it replays the oracle's plan (``oracle.plan_json``)
+stage by stage with one ``torch.einsum`` per stage on CPU tensors, so
+``torch.autograd`` yields the reference-path gradient of every input.
+Only tests/ may import it.
+"""
+
+from __future__ import annotations
+
+import torch
+
+from . import oracle as O
+
+
+def replay(inputs, output, size_dict, ssa_path, tensors):
+    """Contract CPU torch tensors along the plan; differentiable with torch.autograd."""
+    plan = O.plan_json(inputs, output, size_dict, ssa_path)
+    slots = []
+    for legs, prep, t in zip(inputs, plan["preps"], tensors):
+        # trace (leg dropped) / diagonal (leg kept once), src/compiled.rs:60-75
+        slots.append(torch.einsum(t, list(legs), list(prep["legs"])) if prep["traces"] else t)
+    for st in plan["steps"]:
+        a, b = slots[st["left_slot"]], slots[st["right_slot"]]
+        slots[st["left_slot"]] = slots[st["right_slot"]] = None
+        # dangling legs are summed, the result is laid out [batch, free_a, free_b] (src/compiled.rs:155-171)
+        slots.append(torch.einsum(a, list(st["left_legs"]), b, list(st["right_legs"]), list(st["result_legs"])))
+    fin = plan["finalize"]
+    return torch.einsum(slots[fin["slot"]], list(fin["input_legs"]), list(output))

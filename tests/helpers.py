@@ -24,7 +24,7 @@ def case_arrays(case):
         arr = np.asarray(a, dtype=np.float64)
         if np.issubdtype(dt, np.complexfloating):
             arr = arr[..., 0] + 1j * arr[..., 1]
-        out.append(np.ascontiguousarray(arr.reshape(shape).astype(dt)))
+        out.append(np.array(arr.reshape(shape), dtype=dt, order="C"))
     return out
 
 
@@ -49,7 +49,7 @@ def random_arrays(inputs, size_dict, dtype, seed, scale=1.0):
             v = rng.uniform(-1, 1, shape) + 1j * rng.uniform(-1, 1, shape)
         else:
             v = rng.uniform(-1, 1, shape)
-        out.append(np.ascontiguousarray((np.asarray(v) * scale).astype(dt)))
+        out.append(np.array(np.asarray(v) * scale, dtype=dt, order="C"))
     return out
 
 

@@ -1,0 +1,96 @@
+"""GPU parity of the tcgen05 split-TF32 complex GEMM path (precision='tf32x3').
+
+Each case is a pairwise step (or a short contraction) whose dense GEMM is
+routed to the tensor-core kernel; results are compared with the FP64 product
+of the same complex64 inputs.  Tolerance: 1e-5 relative to max |C| (the c64
+bound of the workloads); the device status word must stay 0 (no bounded wait
+expired).
+"""
+
+import numpy as np
+import pytest
+
+import arctn_b200 as A
+from oracle import oracle as O
+from tests.helpers import random_arrays, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def step_network(bt, m_dims, k_dims, n_dims, seed):
+    """Two tensors whose contraction has gemm_dims (bt, prod m, prod k, prod n), legs shuffled."""
+    rng = np.random.default_rng(seed)
+    leg = iter(range(100))
+    b_legs = [next(leg)] if bt > 1 else []
+    m_legs = [next(leg) for _ in m_dims]
+    k_legs = [next(leg) for _ in k_dims]
+    n_legs = [next(leg) for _ in n_dims]
+    size = {}
+    if bt > 1:
+        size[b_legs[0]] = bt
+    size.update(zip(m_legs, m_dims))
+    size.update(zip(k_legs, k_dims))
+    size.update(zip(n_legs, n_dims))
+    a = b_legs + m_legs + k_legs
+    b = b_legs + k_legs + n_legs
+    rng.shuffle(a)
+    rng.shuffle(b)
+    out = b_legs + m_legs + n_legs
+    rng.shuffle(out)
+    return [a, b], out, size
+
+
+CASES = [
+    (1, [128], [32], [128]),
+    (1, [200], [48], [130]),
+    (2, [16, 16], [8, 8], [8, 48]),
+    (1, [384], [1000], [96]),
+    (3, [97], [33], [99]),
+    (1, [2] * 9, [2] * 10, [2] * 9),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[str(c) for c in CASES])
+def test_tc_step_matches_fp64(case):
+    bt, md, kd, nd = case
+    inputs, output, size = step_network(bt, md, kd, nd, seed=len(md) * 7 + bt)
+    arrays = random_arrays(inputs, size, np.complex64, 5)
+    prog = A.SlicedProgram(inputs, output, size, [(0, 1)], (), dtype=np.complex64, precision="tf32x3")
+    import torch
+
+    x = [torch.from_numpy(a).cuda() for a in arrays]
+    ws = torch.empty(max(prog.workspace_bytes, 1), dtype=torch.uint8, device="cuda")
+    got = prog.execute(x, workspace=ws).cpu().numpy()
+    assert prog.device_status(ws) == 0
+    want = O.naive_einsum(inputs, output, size, O.promote(arrays)) if np.prod(list(size.values())) <= 2 ** 26 \
+        else np.einsum(*sum(([a.astype(np.complex128), t] for a, t in zip(arrays, inputs)), []), output)
+    err = rel_err(got, want)
+    assert err <= 1e-5, err
+    ms, kinds, _ = prog.profile(x, workspace=ws)
+    assert 9 in kinds, "the dense step did not run on the tensor-core kernel"
+
+
+def test_tc_sliced_with_shared_operand():
+    # T0[s,i,l] . T1[l,j] . T2[s] -> [i,j], s sliced: the dense step has a per-slice A and a shared B.
+    inputs, output = [[0, 1, 2], [2, 3], [0]], [1, 3]
+    size = {0: 3, 1: 160, 2: 96, 3: 200}
+    arrays = random_arrays(inputs, size, np.complex64, 11)
+    want = O.naive_einsum(inputs, output, size, O.promote(arrays))
+    for group in (1, 2, 0):
+        got = A.SlicedProgram(inputs, output, size, [(0, 1), (2, 3)], [0], dtype=np.complex64, precision="tf32x3",
+                              max_slices_per_group=group).execute(arrays)
+        assert rel_err(got, want) <= 1e-5
+
+
+def test_tc_grid_contraction_matches_fp64_oracle():
+    # 5x5 open grid, bond 6: dense steps reach the tensor cores; whole contraction within 1e-5 of FP64.
+    from arctn_b200 import networks as N
+
+    net = N.grid_2d(5, 5, 6)
+    arrays = N.gaussian_tensors(net, np.complex64, 3, scale_base=6)
+    path = A.greedy(*net.as_tuple())
+    want = complex(O.contract_sliced(*net.as_tuple(), path, [], O.promote(arrays), threads=8))
+    got = complex(A.contract_sliced(*net.as_tuple(), arrays, [], ssa_path=path, precision="tf32x3"))
+    got32 = complex(A.contract_sliced(*net.as_tuple(), arrays, [], ssa_path=path, precision="fp32"))
+    assert abs(got - want) / abs(want) <= 1e-5
+    assert abs(got32 - want) / abs(want) <= 1e-5

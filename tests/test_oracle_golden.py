@@ -99,6 +99,21 @@ def test_oracle_sliced_matches_naive(seed):
         assert np.max(np.abs(got - want)) < 1e-9
 
 
+def test_torch_step_replay_matches_oracle_execute():
+    # The gradient oracle (per-stage einsum replay of the compiled plan) computes the same contraction.
+    import torch
+
+    from oracle.torch_replay import replay
+    from tests.helpers import SMALL_NETWORKS, random_arrays
+
+    for name, (inputs, output, size_dict) in SMALL_NETWORKS.items():
+        path = O.greedy(inputs, output, size_dict)
+        arrays = random_arrays(inputs, size_dict, np.complex128, 3)
+        got = replay(inputs, output, size_dict, path, [torch.from_numpy(a) for a in arrays]).numpy()
+        want = O.execute(inputs, output, size_dict, path, arrays)
+        assert np.max(np.abs(got - want)) <= 1e-12 * max(1.0, float(np.max(np.abs(want)))), name
+
+
 def test_oracle_rejects_invalid_slices():
     # tests/slice_output.rs:105-125, tests/slice_validation.rs:33-76
     a = [np.arange(4.0).reshape(2, 2)]
