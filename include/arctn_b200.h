@@ -234,6 +234,18 @@ int arctn_b200_program_profile(arctn_b200_program* program, const void* const* i
                                uint64_t workspace_bytes, void* cuda_stream, float* ms_out, int* kind_out,
                                double* work_out);
 
+/* No counterpart in the reference.  Batched complex64 GEMM C[b] = A[b] . B[b] (A: bt x m x k, B: bt x k x n,
+ * C: bt x m x n, row-major complex64 device buffers) on the split-TF32 tensor-core path, for callers that
+ * cannot allocate device memory (a framework holding the whole memory pool, code where an allocation
+ * would synchronise the device or break a stream capture).  It allocates nothing: its scratch is a fixed
+ * 64 MiB __device__ array that every GPU loading the library keeps until the process exits, and it
+ * returns ARCTN_B200_ERR_UNSUPPORTED for problems whose packed operands exceed it.  The first call on a
+ * device resolves the array's device address; make it before any stream capture.  All calls on a device
+ * share the array, so calls that overlap on the GPU race: order them on one stream.  Asynchronous on
+ * `cuda_stream`. */
+int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, void* c, uint64_t bt, uint64_t m, uint64_t k,
+                                    uint64_t n, void* cuda_stream);
+
 /* One-shot host-buffer call (the reference-facing e2e path of contract_sliced): copies host inputs to the
  * device, executes, copies the result back and synchronises.  Allocates its own device memory. */
 int arctn_b200_contract_sliced_host(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
