@@ -87,6 +87,7 @@ SIGNATURES = [
     ("arctn_b200_program_slices_per_group", u64, [vp]),
     ("arctn_b200_program_flops", c_double, [vp]),
     ("arctn_b200_program_launches", u64, [vp]),
+    ("arctn_b200_program_recomputed_steps", u64, [vp]),
     ("arctn_b200_program_execute", c_int, [vp, vpp, vp, vp, u64, vp]),
     ("arctn_b200_program_execute_f64out", c_int, [vp, vpp, vp, vp, u64, vp]),
     ("arctn_b200_program_execute_stripped", c_int, [vp, vpp, vp, vp, u64, vp, ctypes.POINTER(c_double)]),

@@ -247,6 +247,7 @@ class SlicedProgram:
         self.slices_per_group = int(L.arctn_b200_program_slices_per_group(h))
         self.flops = float(L.arctn_b200_program_flops(h))
         self.launches = int(L.arctn_b200_program_launches(h))
+        self.recomputed_steps = int(L.arctn_b200_program_recomputed_steps(h))
         self.output_shape = tuple(self.size_dict[l] for l in self.output)
 
     def __del__(self):

@@ -322,6 +322,9 @@ uint64_t arctn_b200_program_n_slices(const arctn_b200_program* p) { return p ? p
 uint64_t arctn_b200_program_slices_per_group(const arctn_b200_program* p) { return p ? p->p->slices_per_group() : 0; }
 double arctn_b200_program_flops(const arctn_b200_program* p) { return p ? p->p->flops() : 0.0; }
 uint64_t arctn_b200_program_launches(const arctn_b200_program* p) { return p ? p->p->launches() : 0; }
+uint64_t arctn_b200_program_recomputed_steps(const arctn_b200_program* p) {
+  return p ? p->p->recomputed_steps() : 0;
+}
 
 int arctn_b200_program_execute(arctn_b200_program* p, const void* const* inputs, void* output, void* workspace,
                                uint64_t workspace_bytes, void* cuda_stream) {

@@ -12,6 +12,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <numeric>
 #include <set>
@@ -41,6 +42,8 @@ namespace {
 
 constexpr u64 kAlign = 256;
 constexpr u64 kInf = ~0ull;
+// Tensor-core GEMMs accumulate at most this many 16-wide K tiles (K = 512) in one TMEM accumulator.
+constexpr int kSplitTiles = 32;
 inline u64 align_up(u64 x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 // Per-slice strided view of a slot.
@@ -112,6 +115,32 @@ Program::Program(const Network& net, const SsaPath& path, const std::vector<Leg>
   if (opt_.precision != PREC_FP32 && opt_.precision != PREC_TF32X3)
     throw Error(E_INVALID, "unsupported precision mode " + std::to_string(opt_.precision));
   build(net, path, sliced);
+  if (opt_.gradient && !sliced_) {
+    // Over the workspace budget: drop the largest step results from what the adjoint sweep keeps
+    // (it recomputes them) until the workspace fits, keeping the smallest layout seen.
+    const u64 budget = opt_.workspace_budget ? opt_.workspace_budget : kDefaultBudget;
+    if (ws_total_ > budget) {
+      std::vector<size_t> cand;
+      for (size_t s = 0; s < plan_.steps.size(); ++s)
+        if (plan_.steps[s].result_slot != plan_.fin.slot) cand.push_back(s);
+      std::stable_sort(cand.begin(), cand.end(), [&](size_t a, size_t b) {
+        const PairStep &x = plan_.steps[a], &y = plan_.steps[b];
+        return x.bt * x.m * x.n > y.bt * y.m * y.n;
+      });
+      std::set<size_t> best;
+      u64 best_ws = ws_total_;
+      for (size_t s : cand) {
+        drop_.insert(s);
+        build(net, path, sliced);
+        if (ws_total_ < best_ws) { best_ws = ws_total_; best = drop_; }
+        if (ws_total_ <= budget) break;
+      }
+      if (drop_ != best) {
+        drop_ = best;
+        build(net, path, sliced);
+      }
+    }
+  }
   int prev = 0;
   CK(cudaGetDevice(&prev));
   CK(cudaSetDevice(opt_.device));
@@ -131,6 +160,9 @@ Program::~Program() {
 }
 
 void Program::build(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced) {
+  ops_.clear();
+  strip_ops_.clear();
+  host_tab_.clear();
   net.validate();
   validate_slice_legs(net, sliced);
   const int dt = opt_.dtype;
@@ -187,8 +219,8 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
 
   // ---------------------------------------------------------------- buffers / ops
   std::vector<Buf> bufs;
-  std::vector<u64> saved;  // forward buffers the reverse sweep reads (step results, summed operands)
   std::vector<Op> ops1, ops2, strip1;
+  bool fwd = true;  // ops emitted while true belong to the forward sweep (and its stripped variant)
   const bool want_strip = !sliced_;
   auto new_buf = [&](bool region2, u64 bytes, u64 first) {
     bufs.push_back(Buf{bytes, first, first, region2, 0});
@@ -205,6 +237,12 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     u64 off = align_up(host_tab_.size());
     host_tab_.resize(off + v.size() * sizeof(ll));
     std::memcpy(host_tab_.data() + off, v.data(), v.size() * sizeof(ll));
+    return off;
+  };
+  auto tab_i32 = [&](const std::vector<int>& v) {
+    u64 off = align_up(host_tab_.size());
+    host_tab_.resize(off + v.size() * sizeof(int));
+    std::memcpy(host_tab_.data() + off, v.data(), v.size() * sizeof(int));
     return off;
   };
   auto emit = [&](bool phase2, const Op& op, bool also_strip) {
@@ -354,7 +392,6 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     pick(v, removed, rd, rs, 0);
     u64 numel = prod(kd);
     u64 b = new_buf(phase2, numel * eb, opidx(phase2));
-    saved.push_back(b);
     Op g{Op::GATHER};
     g.a = v.ref;
     g.sa = v.so;
@@ -364,7 +401,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     g.n_out = (ll)numel;
     g.n_red = (ll)prod(rd);
     touch(v.ref, phase2, opidx(phase2));
-    emit(phase2, g, true);
+    emit(phase2, g, fwd);
     View r;
     r.ref = g.c;
     r.shape = kd;
@@ -375,15 +412,101 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     return r;
   };
 
-  auto part = [](const std::vector<u64>& d, const std::vector<ll>& s_, size_t lo, size_t hi) {
-    return offsets(std::vector<u64>(d.begin() + lo, d.begin() + hi), std::vector<ll>(s_.begin() + lo, s_.begin() + hi));
-  };
   // A GEMM operand read through offset tables: batch, rows (M of A / N of B) and K.
   struct Operand {
     Ref ref;
     SliceOff so;
     bool variant;
     std::vector<ll> tB, tR, tK;
+    // per-leg dims and strides of the three groups, for the leg-aware pack
+    std::vector<u64> dB, dR, dK;
+    std::vector<ll> sB, sR, sK;
+  };
+  auto legs_of = [](const std::vector<u64>& d, const std::vector<ll>& s_, size_t lo, size_t hi) {
+    return std::make_pair(std::vector<u64>(d.begin() + lo, d.begin() + hi), std::vector<ll>(s_.begin() + lo, s_.begin() + hi));
+  };
+  // Operand from (dims, strides) leg lists of its batch, row and K groups.
+  auto make_operand = [&](Ref ref, SliceOff so, bool var, std::pair<std::vector<u64>, std::vector<ll>> b,
+                          std::pair<std::vector<u64>, std::vector<ll>> r, std::pair<std::vector<u64>, std::vector<ll>> k) {
+    Operand o;
+    o.ref = ref;
+    o.so = so;
+    o.variant = var;
+    o.tB = offsets(b.first, b.second);
+    o.tR = offsets(r.first, r.second);
+    o.tK = offsets(k.first, k.second);
+    o.dB = b.first; o.sB = b.second;
+    o.dR = r.first; o.sR = r.second;
+    o.dK = k.first; o.sK = k.second;
+    return o;
+  };
+  auto swap_rk = [](Operand o) {  // the same operand read with its row and K groups exchanged
+    std::swap(o.tR, o.tK);
+    std::swap(o.dR, o.dK);
+    std::swap(o.sR, o.sK);
+    return o;
+  };
+  // Leg-aware pack plan: destination strides are [z][rpad][kpad] with each group row-major.
+  auto pack_plan = [&](const Operand& X, ll rpad, ll kpad, Op& p) -> bool {
+    std::vector<u64> dims;
+    std::vector<ll> ss, ds;
+    auto add_group = [&](const std::vector<u64>& d, const std::vector<ll>& s_, ll unit) {
+      auto rm = rm_strides(d);
+      for (size_t i = 0; i < d.size(); ++i) {
+        if (d[i] <= 1) continue;
+        dims.push_back(d[i]);
+        ss.push_back(s_[i]);
+        ds.push_back(rm[i] * unit);
+      }
+    };
+    add_group(X.dB, X.sB, rpad * kpad);
+    add_group(X.dR, X.sR, kpad);
+    add_group(X.dK, X.sK, 1);
+    const size_t L = dims.size();
+    std::vector<char> in_tile(L, 0);
+    u64 T = 1;
+    auto take = [&](const std::vector<ll>& key) {
+      std::vector<size_t> order(L);
+      std::iota(order.begin(), order.end(), 0);
+      std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return key[a] < key[b]; });
+      u64 covered = 1;  // product of this side's innermost legs already in the tile
+      for (size_t i : order) {
+        if (covered >= 32) break;
+        if (in_tile[i]) { covered *= dims[i]; continue; }
+        if (T * dims[i] > (u64)tc::kPackTile) break;
+        in_tile[i] = 1;
+        T *= dims[i];
+        covered *= dims[i];
+      }
+    };
+    take(ss);
+    take(ds);
+    if (T < 32) return false;
+    std::vector<u64> td, od;
+    std::vector<ll> tss, tds, oss, ods;
+    for (size_t i = 0; i < L; ++i) {
+      if (in_tile[i]) { td.push_back(dims[i]); tss.push_back(ss[i]); tds.push_back(ds[i]); }
+      else { od.push_back(dims[i]); oss.push_back(ss[i]); ods.push_back(ds[i]); }
+    }
+    const std::vector<ll> so_ = offsets(td, tss), do_ = offsets(td, tds);
+    for (ll v : so_) if (v < 0 || v > INT32_MAX) return false;
+    for (ll v : do_) if (v < 0 || v > INT32_MAX) return false;
+    std::vector<int> rd(T), wr(T);
+    std::iota(rd.begin(), rd.end(), 0);
+    std::iota(wr.begin(), wr.end(), 0);
+    std::stable_sort(rd.begin(), rd.end(), [&](int a, int b) { return so_[a] < so_[b]; });
+    std::stable_sort(wr.begin(), wr.end(), [&](int a, int b) { return do_[a] < do_[b]; });
+    std::vector<int> rd_off(T), wr_off(T);
+    for (u64 i = 0; i < T; ++i) { rd_off[i] = (int)so_[rd[i]]; wr_off[i] = (int)do_[wr[i]]; }
+    p.tab[0] = tab_i32(rd);
+    p.tab[1] = tab_i32(rd_off);
+    p.tab[2] = tab_i32(wr);
+    p.tab[3] = tab_i32(wr_off);
+    p.tab[4] = tab_ll(offsets(od, oss));
+    p.tab[5] = tab_ll(offsets(od, ods));
+    p.tile_T = (ll)T;
+    p.n_outer = (ll)prod(od);
+    return true;
   };
   // Emits C[s,b,i,j] = sum_l A(s,b,i,l) * B(s,b,l,j) into `out`.  Dense complex64 GEMMs under tf32x3
   // go through the planar pack (permute + split, conjugating on the fly) and the tcgen05 kernel.
@@ -426,24 +549,48 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         p.a = X.ref;
         p.sa = X.so;
         p.c = Ref{Ref::WS, pbuf};
-        p.tab[0] = tab_ll(X.tB);
-        p.tab[1] = tab_ll(X.tR);
-        p.tab[2] = tab_ll(X.tK);
         p.bt = (ll)bt;
         p.rows = rows;
         p.cols = (ll)k;
         p.rpad = rpad;
         p.kpad = kpad;
         p.a_var = X.variant;
-        p.b_var = rows_contiguous(X.tR, X.tK);
         p.conj_a = conj && dtype_complex(dt);
         touch(X.ref, ph2, opidx(ph2));
-        emit(ph2, p, true);
+        if (pack_plan(X, rpad, kpad, p)) {
+          p.kind = Op::PACK_TILED;
+          if (rows < rpad || (ll)k < kpad) {  // the tiled pack writes only real elements: zero the padding
+            Op z{Op::MEMSET};
+            z.c = p.c;
+            z.bytes = 0;  // set per launch from the group size (see launch_op)
+            z.rpad = rpad;
+            z.kpad = kpad;
+            z.bt = (ll)bt;
+            z.a_var = X.variant;
+            emit(ph2, z, fwd);
+          }
+        } else {
+          p.tab[0] = tab_ll(X.tB);
+          p.tab[1] = tab_ll(X.tR);
+          p.tab[2] = tab_ll(X.tK);
+          p.b_var = rows_contiguous(X.tR, X.tK);
+        }
+        emit(ph2, p, fwd);
         return pbuf;
       };
       const u64 pa = pack(A, (ll)m, rpa, conj_a);
       const u64 pb = pack(B, (ll)n, rpb, conj_b);
       touch(Ref{Ref::WS, pa}, ph2, opidx(ph2));
+      // K longer than kSplitTiles tiles is split across CTAs (see TcArgs): partials [split][z][m][n].
+      const int kt_total = (int)(kpad / tc::BK);
+      if (kt_total > kSplitTiles) {
+        g.kt_chunk = kSplitTiles;
+        g.splits = (kt_total + kSplitTiles - 1) / kSplitTiles;
+        const u64 pbuf = new_buf(ph2, (u64)g.splits * bt * m * n * 8, opidx(ph2));
+        bufs[pbuf].fixed = ph2 && !(A.variant || B.variant);
+        g.d = Ref{Ref::WS, pbuf};
+        touch(g.d, ph2, opidx(ph2));
+      }
       g.kind = Op::GEMM_TC;
       g.a = Ref{Ref::WS, pa};
       g.b = Ref{Ref::WS, pb};
@@ -458,7 +605,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     }
     touch(A.ref, ph2, opidx(ph2));
     touch(B.ref, ph2, opidx(ph2));
-    emit(ph2, g, true);
+    emit(ph2, g, fwd);
     return g;
   };
   struct StepRec {
@@ -466,10 +613,11 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     std::vector<u64> da, db;  // their shapes in [batch, free_a, con] / [batch, con, free_b] order
   };
   std::vector<StepRec> recs;
-
-  for (size_t s = 0; s < plan_.steps.size(); ++s) {
+  // One pairwise step on the current views of its operand slots: dangling sums, then the GEMM with
+  // the step's permutes folded into its operand tables.  Returns the operands and the result view.
+  auto step_operands = [&](size_t s, View A, View B) {
     const PairStep& st = plan_.steps[s];
-    View A = view[st.left_slot], B = view[st.right_slot];
+    const Ref lref = A.ref, rref = B.ref;
     const bool ph2 = A.variant || B.variant;
     A = reduce_view(A, st.sum_a, ph2, nullptr);
     B = reduce_view(B, st.sum_b, ph2, nullptr);
@@ -478,38 +626,51 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     for (u64 p : st.a_perm) { da.push_back(A.shape[p]); sa.push_back(A.strides[p]); }
     for (u64 p : st.b_perm) { db.push_back(B.shape[p]); sb.push_back(B.strides[p]); }
     const size_t nb = st.n_batch, nfa = st.n_free_a, nc = st.n_con;
-    Operand oa{A.ref, A.so, A.variant, part(da, sa, 0, nb), part(da, sa, nb, nb + nfa), part(da, sa, nb + nfa, da.size())};
-    Operand ob{B.ref, B.so, B.variant, part(db, sb, 0, nb), part(db, sb, nb + nc, db.size()), part(db, sb, nb, nb + nc)};
+    Operand oa = make_operand(A.ref, A.so, A.variant, legs_of(da, sa, 0, nb), legs_of(da, sa, nb, nb + nfa),
+                              legs_of(da, sa, nb + nfa, da.size()));
+    Operand ob = make_operand(B.ref, B.so, B.variant, legs_of(db, sb, 0, nb), legs_of(db, sb, nb + nc, db.size()),
+                              legs_of(db, sb, nb, nb + nc));
+    touch(lref, ph2, opidx(ph2));
+    touch(rref, ph2, opidx(ph2));
+    return StepRec{oa, ob, da, db};
+  };
+  auto fwd_step = [&](size_t s, const View& A, const View& B, View& C) {
+    const PairStep& st = plan_.steps[s];
+    const bool ph2 = A.variant || B.variant;
+    StepRec rec = step_operands(s, A, B);
     const u64 cnumel = prod({st.bt, st.m, st.n});
-    u64 cb = new_buf(ph2, cnumel * eb, opidx(ph2));
-    saved.push_back(cb);
-    touch(view[st.left_slot].ref, ph2, opidx(ph2));
-    touch(view[st.right_slot].ref, ph2, opidx(ph2));
-    Op g = emit_gemm(ph2, oa, ob, st.bt, st.m, st.k, st.n, Ref{Ref::WS, cb}, false, false);
-    recs.push_back(StepRec{oa, ob, da, db});
-    if (!ph2 && want_strip) {
-      Op z{Op::MEMSET};
-      z.c = Ref{Ref::WS, (u64)strip_exp_off_};
-      z.bytes = 8;  // the max word (first 8 bytes); the exponent sits in the second 8
-      strip1.push_back(z);
-      Op mx{Op::MAXABS};
-      mx.c = g.c;
-      mx.n_out = (ll)cnumel;
-      mx.a = Ref{Ref::WS, (u64)strip_exp_off_};
-      strip1.push_back(mx);
-      Op sc{Op::STRIP};
-      sc.c = g.c;
-      sc.n_out = (ll)cnumel;
-      sc.a = Ref{Ref::WS, (u64)strip_exp_off_};
-      strip1.push_back(sc);
-    }
-    View C;
-    C.ref = g.c;
+    const u64 cb = new_buf(ph2, cnumel * eb, opidx(ph2));
+    emit_gemm(ph2, rec.a, rec.b, st.bt, st.m, st.k, st.n, Ref{Ref::WS, cb}, false, false);
+    C.ref = Ref{Ref::WS, cb};
     C.shape = st.result_shape;
     C.strides = rm_strides(st.result_shape);
     C.so.local_stride = ph2 ? (ll)cnumel : 0;
     C.so.n = 0;
     C.variant = ph2;
+    return rec;
+  };
+
+  for (size_t s = 0; s < plan_.steps.size(); ++s) {
+    const PairStep& st = plan_.steps[s];
+    View C;
+    recs.push_back(fwd_step(s, view[st.left_slot], view[st.right_slot], C));
+    const u64 cnumel = prod({st.bt, st.m, st.n});
+    if (!C.variant && want_strip) {
+      Op z{Op::MEMSET};
+      z.c = Ref{Ref::WS, (u64)strip_exp_off_};
+      z.bytes = 8;  // the max word (first 8 bytes); the exponent sits in the second 8
+      strip1.push_back(z);
+      Op mx{Op::MAXABS};
+      mx.c = C.ref;
+      mx.n_out = (ll)cnumel;
+      mx.a = Ref{Ref::WS, (u64)strip_exp_off_};
+      strip1.push_back(mx);
+      Op sc{Op::STRIP};
+      sc.c = C.ref;
+      sc.n_out = (ll)cnumel;
+      sc.a = Ref{Ref::WS, (u64)strip_exp_off_};
+      strip1.push_back(sc);
+    }
     view[st.result_slot] = C;
   }
 
@@ -553,8 +714,26 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
   // broadcast over the legs the step summed away, then through the input traces / diagonals.
   if (opt_.gradient) {
     if (sliced_) throw Error(E_UNSUPPORTED, "gradients of sliced contractions are not supported by this build");
-    for (u64 b : saved) bufs[b].last = kInf;  // forward intermediates stay alive for the sweep
+    fwd = false;
     bwd_begin_ = ops1.size();
+    // Forward values the sweep reads stay alive through the last op that reads them (touch).  Step
+    // results listed in drop_ are not read from the forward: the sweep recomputes each of them from its
+    // step's operands the first time it needs it, and the recomputed value then lives until its
+    // consumer's adjoint step, so every dropped step runs at most once more.
+    std::vector<char> have(n_slots, 0);
+    std::vector<View> cur(view);
+    for (size_t i = 0; i < n_slots; ++i) have[i] = i < plan_.n_inputs || !drop_.count(i - plan_.n_inputs);
+    std::function<View(size_t)> value = [&](size_t slot) -> View {
+      if (!have[slot]) {
+        const size_t p = slot - plan_.n_inputs;
+        const PairStep& ps = plan_.steps[p];
+        const View L = value(ps.left_slot), R = value(ps.right_slot);
+        fwd_step(p, L, R, cur[slot]);
+        have[slot] = 1;
+      }
+      return cur[slot];
+    };
+    auto dropped = [&](size_t slot) { return slot >= plan_.n_inputs && drop_.count(slot - plan_.n_inputs) > 0; };
     std::vector<View> dv(n_slots);
     auto contiguous = [&](u64 buf, const std::vector<u64>& shape) {
       View v;
@@ -616,25 +795,33 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     };
     for (size_t s = plan_.steps.size(); s-- > 0;) {
       const PairStep& st = plan_.steps[s];
-      const StepRec& rec = recs[s];
+      StepRec rec = recs[s];
+      if (dropped(st.left_slot) || dropped(st.right_slot)) {
+        const View L = value(st.left_slot), R = value(st.right_slot);
+        StepRec r2 = step_operands(s, L, R);
+        if (dropped(st.left_slot)) rec.a = r2.a;
+        if (dropped(st.right_slot)) rec.b = r2.b;
+      }
       const View dC = dv[st.result_slot];
       const size_t nb = st.n_batch, nfa = st.n_free_a;
       const auto& rsh = st.result_shape;
       const auto rst = rm_strides(rsh);
-      const std::vector<ll> dcB = part(rsh, rst, 0, nb), dcM = part(rsh, rst, nb, nb + nfa),
-                            dcN = part(rsh, rst, nb + nfa, rsh.size());
+      const auto dcB = legs_of(rsh, rst, 0, nb), dcM = legs_of(rsh, rst, nb, nb + nfa),
+                 dcN = legs_of(rsh, rst, nb + nfa, rsh.size());
       // dA' [batch, free_a, con] = dC [batch, free_a, free_b] . conj(B') [batch, con, free_b]^T
       {
-        Operand a{dC.ref, dC.so, false, dcB, dcM, dcN};
-        Operand b{rec.b.ref, rec.b.so, false, rec.b.tB, rec.b.tK, rec.b.tR};
+        Operand a = make_operand(dC.ref, dC.so, false, dcB, dcM, dcN);
+        Operand b = swap_rk(rec.b);
+        b.variant = false;
         const u64 tbuf = new_buf(false, prod({st.bt, st.m, st.k}) * eb, opidx(false));
         emit_gemm(false, a, b, st.bt, st.m, st.n, st.k, Ref{Ref::WS, tbuf}, false, true);
         dv[st.left_slot] = to_slot(tbuf, rec.da, st.a_perm, st.sum_a, st.left_shape);
       }
       // dB' [batch, con, free_b] = conj(A') [batch, free_a, con]^T . dC [batch, free_a, free_b]
       {
-        Operand a{rec.a.ref, rec.a.so, false, rec.a.tB, rec.a.tK, rec.a.tR};
-        Operand b{dC.ref, dC.so, false, dcB, dcN, dcM};
+        Operand a = swap_rk(rec.a);
+        a.variant = false;
+        Operand b = make_operand(dC.ref, dC.so, false, dcB, dcN, dcM);
         const u64 tbuf = new_buf(false, prod({st.bt, st.k, st.n}) * eb, opidx(false));
         emit_gemm(false, a, b, st.bt, st.k, st.m, st.n, Ref{Ref::WS, tbuf}, true, false);
         dv[st.right_slot] = to_slot(tbuf, rec.db, st.b_perm, st.sum_b, st.right_shape);
@@ -703,7 +890,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
   };
   region1 = layout(false, 1);
   per_slice2 = layout(true, 1);
-  const u64 budget = opt_.workspace_budget ? opt_.workspace_budget : (8ull << 30);
+  const u64 budget = opt_.workspace_budget ? opt_.workspace_budget : kDefaultBudget;
   S_ = 1;
   if (sliced_) {
     u64 room = budget > region1 ? budget - region1 : 0;
@@ -726,6 +913,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     resolve(op.a);
     resolve(op.b);
     resolve(op.c);
+    resolve(op.d);
   };
   if (want_strip) strip_exp_off_ = bufs[strip_exp_off_].offset;
   err_off_ = bufs[err_buf].offset;
@@ -902,7 +1090,7 @@ CUtensorMap plane_map(void* base, ll kpad, ll rows, ll zplanes) {
   return m;
 }
 
-void launch_tc(const Op& op, void* A, void* B, void* C, const char* tab, int* err, cudaStream_t st) {
+void launch_tc(const Op& op, void* A, void* B, void* C, void* D, const char* tab, int* err, cudaStream_t st) {
   if (op.kind == Op::PACK) {
     const ll Z = (op.a_var ? op.S : 1) * op.bt;
     const ll tiles = Z * (op.rpad / 32) * ((op.kpad + 31) / 32);
@@ -910,6 +1098,16 @@ void launch_tc(const Op& op, void* A, void* B, void* C, const char* tab, int* er
         (const cf32*)A, (float*)C, (const ll*)(tab + op.tab[0]), (const ll*)(tab + op.tab[1]),
         (const ll*)(tab + op.tab[2]), op.bt, op.rows, op.cols, op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0,
         op.conj_a ? 1 : 0);
+    return;
+  }
+  if (op.kind == Op::PACK_TILED) {
+    const ll n_slices = op.a_var ? op.S : 1;
+    const ll slice_stride = op.bt * op.rpad * op.kpad;
+    const ll plane = n_slices * slice_stride;
+    tc::k_pack_tiled<<<(int)std::min<ll>(op.n_outer * n_slices, 148 * 16), 256, 0, st>>>(
+        (const cf32*)A, (float*)C, (const int*)(tab + op.tab[0]), (const int*)(tab + op.tab[1]),
+        (const int*)(tab + op.tab[2]), (const int*)(tab + op.tab[3]), (int)op.tile_T, (const ll*)(tab + op.tab[4]),
+        (const ll*)(tab + op.tab[5]), op.n_outer, n_slices, slice_stride, plane, op.sa, op.g0, op.conj_a ? 1 : 0);
     return;
   }
   static bool attr_set[64] = {};
@@ -935,9 +1133,19 @@ void launch_tc(const Op& op, void* A, void* B, void* C, const char* tab, int* er
   args.b_var = op.b_var;
   args.err = err;
   const ll zc = s_eff * op.bt;
-  if (zc > 65535) throw Error(E_UNSUPPORTED, "tensor-core GEMM batch exceeds the grid limit");
-  dim3 grid((unsigned)((op.n + tc::BN - 1) / tc::BN), (unsigned)((op.m + tc::BM - 1) / tc::BM), (unsigned)zc);
+  if (zc * op.splits > 65535) throw Error(E_UNSUPPORTED, "tensor-core GEMM batch x K splits exceeds the grid limit");
+  if (op.splits > 1) {
+    args.kt_chunk = op.kt_chunk;
+    args.zc = (int)zc;
+    args.part = (cf32*)D;
+  }
+  dim3 grid((unsigned)((op.n + tc::BN - 1) / tc::BN), (unsigned)((op.m + tc::BM - 1) / tc::BM),
+            (unsigned)(zc * op.splits));
   tc::k_tc_cgemm_tf32x3<<<grid, 192, tc::SMEM_BYTES, st>>>(ma, mb, args);
+  if (op.splits > 1) {
+    const ll count = zc * op.m * op.n;
+    tc::k_splitk_reduce<<<grid_for(count), 256, 0, st>>>((const cf32*)D, (cf32*)C, count, op.splits);
+  }
 }
 
 }  // namespace
@@ -954,11 +1162,13 @@ void Program::launch_op(const Op& op, const void* const* inputs, void* output, c
     }
   };
   if (op.kind == Op::MEMSET) {
-    CK(cudaMemsetAsync(ptr(op.c), 0, op.bytes, st));
+    // bytes == 0: the padded planes of a tiled pack, [re|im][slices of this group][bt][rpad][kpad] fp32
+    const u64 bytes = op.bytes ? op.bytes : (u64)(2 * (op.a_var ? op.S : 1) * op.bt * op.rpad * op.kpad * 4);
+    CK(cudaMemsetAsync(ptr(op.c), 0, bytes, st));
     return;
   }
-  if (op.kind == Op::PACK || op.kind == Op::GEMM_TC) {
-    launch_tc(op, ptr(op.a), ptr(op.b), ptr(op.c), dev_tab_, (int*)(ws + err_off_), st);
+  if (op.kind == Op::PACK || op.kind == Op::PACK_TILED || op.kind == Op::GEMM_TC) {
+    launch_tc(op, ptr(op.a), ptr(op.b), ptr(op.c), ptr(op.d), dev_tab_, (int*)(ws + err_off_), st);
     CK(cudaGetLastError());
     return;
   }
@@ -1064,6 +1274,9 @@ double op_work(const Op& op, int dt) {
     case Op::GATHER: return (double)op.S * op.n_out * (op.n_red + 1) * eb;
     case Op::ACCUM: return (double)op.n_segs * op.n_e * (2.0 * wide_bytes(dt)) + (double)op.S * op.n_e * eb;
     case Op::OUTPUT: return (double)op.n_blocks * op.n_chunks * op.n_e * wide_bytes(dt);
+    case Op::PACK:
+    case Op::PACK_TILED:  // complex64 read once, two fp32 planes written (padding included)
+      return (double)(op.a_var ? op.S : 1) * op.bt * (8.0 * op.rows * op.cols + 8.0 * op.rpad * op.kpad);
     default: return (double)op.n_out * eb;
   }
 }

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <mutex>
+#include <set>
 
 #include "host.hpp"
 #include "kernels.cuh"
@@ -20,6 +21,8 @@ enum : int { PREC_FP32 = 0, PREC_TF32X3 = 1 };
 
 size_t dtype_bytes(int dt);
 inline bool dtype_complex(int dt) { return dt == DT_C64 || dt == DT_C128; }
+
+constexpr u64 kDefaultBudget = 8ull << 30;  // workspace budget when the caller gives none
 
 struct ProgramOptions {
   int dtype = DT_C64;
@@ -41,7 +44,7 @@ struct Ref {
 struct Op {
   enum Kind : int {
     GATHER = 0, GEMM_SMALL = 1, GEMM_TILE64 = 2, GEMM_TILE32 = 3, ACCUM = 4, OUTPUT = 5, MEMSET = 6, MAXABS = 7,
-    STRIP = 8, GEMM_TC = 9, GEMM_DOT = 10, PACK = 11, SCATTER = 12
+    STRIP = 8, GEMM_TC = 9, GEMM_DOT = 10, PACK = 11, SCATTER = 12, PACK_TILED = 13
   } kind;
   Ref a, b, c;
   u64 tab[6] = {0, 0, 0, 0, 0, 0};  // byte offsets of offset tables in the program's table buffer
@@ -55,6 +58,10 @@ struct Op {
   ll rows = 0, cols = 0, rpad = 0, kpad = 0, rpad_b = 0;
   bool a_var = false, b_var = false;
   bool conj_a = false, conj_b = false;  // GEMM operands read conjugated (adjoint); PACK uses conj_a
+  ll tile_T = 0, n_outer = 0;           // PACK_TILED: tile size and number of outer leg combinations
+  int splits = 1;                       // GEMM_TC: K splits (partials in `d`, summed in order into `c`)
+  int kt_chunk = 0;
+  Ref d;                                // GEMM_TC: FP32 split-K partial buffer
 };
 
 class Program {
@@ -82,6 +89,8 @@ class Program {
   void execute_gradient(int part, const void* const* inputs, const void* grad_out, void* const* grads, void* output,
                         void* ws, u64 ws_bytes, cudaStream_t st);
   bool has_gradient() const { return opt_.gradient; }
+  // Steps whose results the adjoint sweep recomputes instead of keeping (workspace over budget).
+  u64 recomputed_steps() const { return drop_.size(); }
   u64 forward_launches() const;
   u64 backward_launches() const;
 
@@ -115,6 +124,7 @@ class Program {
  private:
 
   size_t bwd_begin_ = 0;             // gradient programs: first op of the reverse sweep in ops_
+  std::set<size_t> drop_;            // gradient programs: steps recomputed by the reverse sweep
   const void* grad_out_ = nullptr;   // bound during execute_gradient
   void* const* grads_ = nullptr;
 

@@ -3,9 +3,10 @@
 // C[z] (m x n, complex64) = A[z] (m x k) . B[z] (k x n) for every batch z.
 // Operands arrive packed by k_pack_planar as K-major fp32 planes
 // [re | im][z][rows][k] (rows padded to 128, k padded to 16).  Per 16-wide K
-// slab the CTA splits every value x into hi = x with its 13 low mantissa bits
-// cleared (exactly representable in TF32) and lo = x - hi (exact in FP32), and
-// issues the 4M complex product as 12 TF32 MMAs into two TMEM accumulators:
+// slab the CTA splits every value x into hi = x rounded to the nearest TF32
+// value and lo = x - hi (exact in FP32) rounded likewise, so hi + lo carries
+// x to about 2^-23 relative with no bias, and issues the 4M complex product as
+// 12 TF32 MMAs into TMEM accumulators:
 //   Cr += Ar*Br - Ai*Bi,  Ci += Ar*Bi + Ai*Br   for (hi,hi), (hi,lo), (lo,hi),
 // the minus through the instruction's negate-A bit.  Accumulation is FP32.
 //
@@ -37,6 +38,16 @@ constexpr uint32_t TMEM_COLS = 512;
 constexpr unsigned long long kWaitNs = 1000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Nearest TF32 value of a finite FP32 bit pattern, ties away from zero: adding half of the dropped
+// 13-bit field to the sign-magnitude pattern rounds the magnitude, a carry out of the mantissa moves
+// to the next binade, and the mask clears the dropped field.  The result is exact as a TF32 operand,
+// so the tensor core's own input conversion cannot change it.
+__host__ __device__ __forceinline__ uint32_t tf32_round(uint32_t bits) { return (bits + 0x1000u) & 0xFFFFE000u; }
+// x - hi, exact in FP32 (hi is within half a TF32 unit of x, so the subtraction is Sterbenz-exact).
+__device__ __forceinline__ uint32_t tf32_residual(uint32_t x, uint32_t hi) {
+  return __float_as_uint(__uint_as_float(x) - __uint_as_float(hi));
+}
 __device__ __forceinline__ unsigned long long now_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -123,6 +134,13 @@ struct TcArgs {
   int bt;            // GEMM batch per slice
   int a_var, b_var;  // operand differs per slice (else it is shared by all slices)
   int* err;
+  // Split K: CTA blockIdx.z = split * zc + z accumulates k-tiles [split*kt_chunk, ...) in TMEM and
+  // writes its FP32 partial to part[split][z][m][n]; k_splitk_reduce sums the splits in order.  The
+  // tensor core's FP32 accumulation loses about one unit in the last place per addition, so its
+  // error grows with the number of K steps one accumulator takes; bounding that number bounds it.
+  int kt_chunk = 0;  // 0: one CTA takes all of K and writes C
+  int zc = 0;        // output batches (grid z = splits * zc)
+  cf32* part = nullptr;
 };
 
 static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_constant__ CUtensorMap tmA,
@@ -142,7 +160,11 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
   volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int tile_n = blockIdx.x, tile_m = blockIdx.y, z = blockIdx.z;
+  const int tile_n = blockIdx.x, tile_m = blockIdx.y;
+  const int split = args.kt_chunk ? (int)(blockIdx.z / args.zc) : 0;
+  const int z = args.kt_chunk ? (int)(blockIdx.z % args.zc) : (int)blockIdx.z;
+  const int kt0 = args.kt_chunk ? split * args.kt_chunk : 0;
+  const int kt1 = args.kt_chunk ? min(args.k_tiles, kt0 + args.kt_chunk) : args.k_tiles;
   const int s_idx = z / args.bt, b_idx = z % args.bt;
   const int zA = args.a_var ? z : b_idx;
   const int zB = args.b_var ? z : b_idx;
@@ -165,7 +187,7 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  const int KT = args.k_tiles;
+  const int KT = kt1 - kt0;  // pipeline iterations of this CTA; k-tile of iteration t is kt0 + t
 
   if (warp == 0) {
     // ------------------------------------------------------------ TMA producer
@@ -177,7 +199,7 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
         if (*abort_flag) break;
         unsigned char* dst = raw + s * STAGE_BYTES;
         mbar_expect_tx(&full[s], STAGE_BYTES);
-        const int k0 = t * BK;
+        const int k0 = (kt0 + t) * BK;
         tma_load_3d(&tmA, &full[s], dst + 0 * PLANE_BYTES, k0, tile_m * BM, zA);
         tma_load_3d(&tmA, &full[s], dst + 1 * PLANE_BYTES, k0, tile_m * BM, zA + args.za);
         tma_load_3d(&tmB, &full[s], dst + 2 * PLANE_BYTES, k0, tile_n * BN, zB);
@@ -240,12 +262,12 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
       uint4* lp = (uint4*)(lo + q * STAGE_BYTES);
 #pragma unroll 4
       for (int v = tid; v < STAGE_BYTES / 16; v += 128) {
-        uint4 x = rp[v];
-        uint4 h = make_uint4(x.x & 0xFFFFE000u, x.y & 0xFFFFE000u, x.z & 0xFFFFE000u, x.w & 0xFFFFE000u);
-        float4 l = make_float4(__uint_as_float(x.x) - __uint_as_float(h.x), __uint_as_float(x.y) - __uint_as_float(h.y),
-                               __uint_as_float(x.z) - __uint_as_float(h.z), __uint_as_float(x.w) - __uint_as_float(h.w));
+        const uint4 x = rp[v];
+        const uint4 h = make_uint4(tf32_round(x.x), tf32_round(x.y), tf32_round(x.z), tf32_round(x.w));
+        const uint4 l = make_uint4(tf32_round(tf32_residual(x.x, h.x)), tf32_round(tf32_residual(x.y, h.y)),
+                                   tf32_round(tf32_residual(x.z, h.z)), tf32_round(tf32_residual(x.w, h.w)));
         rp[v] = h;
-        lp[v] = *reinterpret_cast<uint4*>(&l);
+        lp[v] = l;
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       mbar_arrive(&lofull[q]);
@@ -256,7 +278,8 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int quad = warp % 4;
       const ll row = (ll)tile_m * BM + quad * 32 + lane;
-      cf32* crow = args.C + ((ll)z * args.m + row) * args.n;
+      cf32* crow = (args.part ? args.part + (ll)split * args.zc * args.m * args.n : args.C) +
+                   ((ll)z * args.m + row) * args.n;
       for (int c0 = 0; c0 < BN; c0 += 32) {
         uint32_t vr[32], vi[32], sr[32], si[32];
         const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + c0;
@@ -281,6 +304,48 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+// Leg-aware pack: the same gather as k_pack_planar, for operands whose legs are scattered (as in
+// networks of dimension-2 legs).  The host picks tile legs -- those innermost in the source plus those
+// innermost in the packed destination, at most kPackTile elements -- and lists the tile twice: in
+// source-address order (rd_*) and in destination-address order (wr_*), so both the read and the write
+// of a tile walk memory contiguously.  Remaining legs are enumerated by src_base / dst_base.
+constexpr int kPackTile = 1024;
+static __global__ void __launch_bounds__(256) k_pack_tiled(const cf32* __restrict__ src, float* __restrict__ dst,
+                                                           const int* __restrict__ rd_elem, const int* __restrict__ rd_off,
+                                                           const int* __restrict__ wr_elem, const int* __restrict__ wr_off,
+                                                           int T, const ll* __restrict__ src_base,
+                                                           const ll* __restrict__ dst_base, ll n_outer, ll n_slices,
+                                                           ll dst_slice_stride, ll plane, SliceOff so, ll g0, int conj) {
+  __shared__ cf32 tile[kPackTile];
+  const float im_sign = conj ? -1.f : 1.f;
+  for (ll blk = blockIdx.x; blk < n_outer * n_slices; blk += gridDim.x) {
+    const ll s = blk / n_outer, o = blk - s * n_outer;
+    const cf32* sb = src + slice_offset(so, g0, s) + src_base[o];
+    float* db = dst + s * dst_slice_stride + dst_base[o];
+    for (int i = threadIdx.x; i < T; i += blockDim.x) tile[rd_elem[i]] = sb[rd_off[i]];
+    __syncthreads();
+    for (int i = threadIdx.x; i < T; i += blockDim.x) {
+      const cf32 v = tile[wr_elem[i]];
+      db[wr_off[i]] = v.re;
+      db[plane + wr_off[i]] = im_sign * v.im;
+    }
+    __syncthreads();
+  }
+}
+
+// C[e] = sum over splits s = 0, 1, ... of part[s][e], added in that order in FP64 and rounded once.
+static __global__ void k_splitk_reduce(const cf32* __restrict__ part, cf32* __restrict__ C, ll count, int splits) {
+  for (ll e = (ll)blockIdx.x * blockDim.x + threadIdx.x; e < count; e += (ll)gridDim.x * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int s = 0; s < splits; ++s) {
+      const cf32 v = part[(ll)s * count + e];
+      re += v.re;
+      im += v.im;
+    }
+    C[e] = cf32{(float)re, (float)im};
   }
 }
 

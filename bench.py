@@ -379,7 +379,8 @@ def main():
                            "cross_slice_sum": "fp64", "l2": "flushed (256 MiB write) between timed iterations",
                            "parallelism": f"slice-sharded x{world}"},
                 "gpu_launches": prog.launches * args.steps, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu,
-                "clocks": clocks, "device_status": status, "result": [float(r.real), float(r.imag)]}
+                "clocks": clocks, "device_status": status, "workspace_bytes": int(prog.workspace_bytes),
+                "result": [float(r.real), float(r.imag)]}
         line.update(extras)
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -195,6 +195,10 @@ uint64_t arctn_b200_program_slices_per_group(const arctn_b200_program* program);
 double arctn_b200_program_flops(const arctn_b200_program* program);
 /* Number of kernels one execute launches. */
 uint64_t arctn_b200_program_launches(const arctn_b200_program* program);
+/* Gradient programs: how many step results the adjoint sweep recomputes instead of keeping from the
+ * forward, chosen at creation (largest results first) so that the workspace fits workspace_budget.
+ * 0 when everything fits.  No reference counterpart: the reference has no adjoint. */
+uint64_t arctn_b200_program_recomputed_steps(const arctn_b200_program* program);
 
 /* Runs on `cuda_stream` (cudaStream_t; NULL = legacy default stream).  inputs[i] are contiguous device
  * tensors in net order; output receives the full output (native dtype).  The call is asynchronous. */

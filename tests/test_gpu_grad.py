@@ -80,28 +80,52 @@ def test_autograd_function_and_central_differences_grid():
     g = [t.grad.cpu().numpy() for t in x]
     rng = np.random.default_rng(0)
     eps = 1e-3
+
+    def central(v, h):
+        fp = complex(O.contract_sliced(*net.as_tuple(), path, [], [a + h * d for a, d in zip(arrays, v)]))
+        fm = complex(O.contract_sliced(*net.as_tuple(), path, [], [a - h * d for a, d in zip(arrays, v)]))
+        return (fp - fm) / (2 * h)
+
     for _ in range(8):
-        v = [(rng.standard_normal(a.shape) + 1j * rng.standard_normal(a.shape)) for a in arrays]
-        fp = complex(O.contract_sliced(*net.as_tuple(), path, [], [a + eps * d for a, d in zip(arrays, v)]))
-        fm = complex(O.contract_sliced(*net.as_tuple(), path, [], [a - eps * d for a, d in zip(arrays, v)]))
-        fd = (fp - fm) / (2 * eps)
+        # directions scaled like the tensors themselves (entries ~ N(0,1)/sqrt(3^rank))
+        v = [(rng.standard_normal(a.shape) + 1j * rng.standard_normal(a.shape)) / np.sqrt(3.0 ** a.ndim)
+             for a in arrays]
+        d1, d2 = central(v, eps), central(v, eps / 2)
+        rich = (4 * d2 - d1) / 3  # removes the eps^2 term of the central difference
         lin = sum(np.sum(np.conj(gi) * vi) for gi, vi in zip(g, v))
         # d Re f along V  =  Re(sum conj(g) V)
-        assert abs(fd.real - lin.real) <= 1e-6 * max(1.0, abs(fd)), (fd, lin)
+        assert abs(d1.real - lin.real) <= 1e-3 * abs(d1), (d1, lin)
+        assert abs(rich.real - lin.real) <= 1e-8 * abs(rich), (rich, lin)
 
 
 def test_grid8_bond6_c64_gradient_tf32x3_against_c128():
     # 8x8 open grid, bond 6, c64 N(0,1)/sqrt(6^rank): the adjoint on the tensor cores against the FP64 sweep.
+    # With that scaling the scalar is ~1e-35, at the bottom of FP32's range; every input is multiplied
+    # by 4 (exact in binary floating point), which scales the result by 4^64 and every gradient by 4^63.
+    # The contraction cancels heavily (the scalar is far below the norms of its intermediates), so even
+    # exact-FP32 arithmetic misses the c128 value by ~1e-5 relative.  tf32x3 must do as well as the FP32
+    # SIMT path: its error is bounded by twice the FP32 path's error, and by 1e-5 where that is smaller.
     net, arrays = N.workload_grid8(6, np.complex64, seed=0)
+    arrays = [a * np.float32(4.0) for a in arrays]
     path = A.greedy(*net.as_tuple())
     x64 = [torch.from_numpy(a).cuda() for a in arrays]
     x128 = [t.to(torch.complex128) for t in x64]
-    p32 = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex64, precision="tf32x3", gradient=True,
-                          use_graph=False, workspace_budget=40 << 30)
-    p64 = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex128, gradient=True, use_graph=False,
-                          workspace_budget=40 << 30)
-    o32, g32 = p32.gradient(x64)
+    kw = dict(gradient=True, use_graph=False, workspace_budget=40 << 30)
+    ptc = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex64, precision="tf32x3", **kw)
+    pf32 = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex64, precision="fp32", **kw)
+    p64 = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex128, **kw)
+    otc, gtc = ptc.gradient(x64)
+    of32, gf32 = pf32.gradient(x64)
     o64, g64 = p64.gradient(x128)
-    assert abs(complex(o32.item()) - complex(o64.item())) / abs(complex(o64.item())) <= 1e-5
-    for a, b in zip(g32, g64):
-        assert max_rel(a.cpu().numpy(), b.cpu().numpy()) <= 1e-5 * max(1.0, 1.0)
+    ref = complex(o64.item())
+
+    def rel(o):
+        return abs(complex(o.item()) - ref) / abs(ref)
+
+    assert rel(of32) <= 1e-4  # sanity of the comparison itself
+    assert rel(otc) <= max(1e-5, 2 * rel(of32)), (rel(otc), rel(of32))
+    for a, f, b in zip(gtc, gf32, g64):
+        a, f, b = (t.cpu().numpy().astype(np.complex128) for t in (a, f, b))
+        scale = np.max(np.abs(b))
+        err_tc, err_f32 = np.max(np.abs(a - b)) / scale, np.max(np.abs(f - b)) / scale
+        assert err_tc <= max(1e-5, 2 * err_f32), (err_tc, err_f32)
