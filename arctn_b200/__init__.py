@@ -12,6 +12,7 @@ from .api import (
     Finalize,
     InputPrep,
     PairStep,
+    ProgramBatch,
     SlicedProgram,
     arctn_contract,
     contract_sliced,
@@ -31,6 +32,7 @@ __all__ = [
     "Finalize",
     "InputPrep",
     "PairStep",
+    "ProgramBatch",
     "SlicedProgram",
     "arctn_contract",
     "contract_sliced",

@@ -52,7 +52,7 @@ class FinalizeInfo(ctypes.Structure):
 class ProgramOptions(ctypes.Structure):
     _fields_ = [("dtype", c_int), ("precision", c_int), ("device", c_int), ("use_graph", c_int),
                 ("max_slices_per_group", u64), ("workspace_budget", u64), ("slice_begin", u64),
-                ("slice_end", u64), ("gradient", c_int)]
+                ("slice_end", u64), ("gradient", c_int), ("tc_k_chunk", u64)]
 
 
 # (name, restype, argtypes) for every symbol the header declares.
@@ -88,6 +88,14 @@ SIGNATURES = [
     ("arctn_b200_program_flops", c_double, [vp]),
     ("arctn_b200_program_launches", u64, [vp]),
     ("arctn_b200_program_recomputed_steps", u64, [vp]),
+    ("arctn_b200_program_describe", c_int, [vp, ctypes.c_char_p, u64, u64p]),
+    ("arctn_b200_batch_create", c_int, [ctypes.POINTER(vp), u64, c_int, ctypes.POINTER(vp)]),
+    ("arctn_b200_batch_destroy", None, [vp]),
+    ("arctn_b200_batch_workspace_size", u64, [vp]),
+    ("arctn_b200_batch_lanes", u64, [vp]),
+    ("arctn_b200_batch_execute", c_int, [vp, ctypes.POINTER(vpp), vpp, vp, u64, vp]),
+    ("arctn_b200_batch_gradient", c_int, [vp, ctypes.POINTER(vpp), vpp, ctypes.POINTER(vpp), vpp, vp, u64, vp]),
+    ("arctn_b200_batch_device_status", c_int, [vp, vp, vp, ctypes.POINTER(c_int)]),
     ("arctn_b200_program_execute", c_int, [vp, vpp, vp, vp, u64, vp]),
     ("arctn_b200_program_execute_f64out", c_int, [vp, vpp, vp, vp, u64, vp]),
     ("arctn_b200_program_execute_stripped", c_int, [vp, vpp, vp, vp, u64, vp, ctypes.POINTER(c_double)]),

@@ -211,7 +211,7 @@ class SlicedProgram:
 
     def __init__(self, inputs, output, size_dict, ssa_path, sliced_legs=(), *, dtype="complex64",
                  precision="fp32", device=None, use_graph=True, max_slices_per_group=0, workspace_budget=0,
-                 slice_begin=0, slice_end=0, gradient=False):
+                 slice_begin=0, slice_end=0, gradient=False, tc_k_chunk=0):
         torch = _torch()
         self.inputs = [[int(l) for l in t] for t in inputs]
         self.output = [int(l) for l in output]
@@ -234,7 +234,7 @@ class SlicedProgram:
         self.has_gradient = bool(gradient)
         opts = C.ProgramOptions(self.code, self.precision, self.device, 1 if use_graph else 0,
                                 int(max_slices_per_group), int(workspace_budget), int(slice_begin), int(slice_end),
-                                1 if gradient else 0)
+                                1 if gradient else 0, int(tc_k_chunk))
         h = C.vp()
         C.check(C.lib().arctn_b200_program_create(net.ptr, n, p.ctypes.data_as(C.u64p), len(self.sliced_legs),
                                                   sl.ctypes.data_as(C.u32p), ctypes.byref(opts), ctypes.byref(h)),
@@ -253,16 +253,37 @@ class SlicedProgram:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h:
-            C.lib().arctn_b200_program_destroy(h)
+            try:
+                C.lib().arctn_b200_program_destroy(h)
+            except Exception:  # interpreter shutdown: the module globals may already be gone
+                pass
             self._h = None
 
-    def execute(self, arrays, *, f64_out=False, workspace=None, stream=None):
+    def describe(self):
+        """Launch sequence and workspace layout as a dict (host-only; works without a GPU)."""
+        import json
+
+        need = C.u64(0)
+        C.check(C.lib().arctn_b200_program_describe(self._h, None, 0, ctypes.byref(need)), "describe")
+        buf = ctypes.create_string_buffer(int(need.value))
+        C.check(C.lib().arctn_b200_program_describe(self._h, buf, need.value, ctypes.byref(need)), "describe")
+        return json.loads(buf.value.decode())
+
+    def execute(self, arrays, *, f64_out=False, workspace=None, stream=None, out=None):
+        """Full output of the contraction.  ``out`` (a CUDA tensor of the output's shape and dtype -- the
+        wide dtype with ``f64_out``) receives it in place, which keeps a captured graph's pointers fixed."""
         arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "sliced contraction failed")
         if code != self.code:
             raise ValueError("sliced contraction failed: arrays dtype differs from the program's dtype")
         call = _DeviceCall(arrays, torch_mode, self.device)
         torch = _torch()
-        out = call.empty(self.output_shape, _torch_dtype(code, wide=f64_out))
+        if out is not None:
+            want = _torch_dtype(code, wide=f64_out)
+            if tuple(out.shape) != tuple(self.output_shape) or out.dtype != want or not out.is_contiguous():
+                raise ValueError(f"sliced contraction failed: out must be a contiguous {want} tensor of shape "
+                                 f"{tuple(self.output_shape)}")
+        else:
+            out = call.empty(self.output_shape, _torch_dtype(code, wide=f64_out))
         ws = workspace if workspace is not None else call.workspace(self.workspace_bytes)
         st = stream if stream is not None else call.stream
         fn = C.lib().arctn_b200_program_execute_f64out if f64_out else C.lib().arctn_b200_program_execute
@@ -345,6 +366,107 @@ class SlicedProgram:
                                                                 ws.numel(), call.stream.cuda_stream,
                                                                 ctypes.byref(e)), "compiled contraction failed")
         return _to_output(out, torch_mode), e.value
+
+
+class ProgramBatch:
+    """Many independent programs (uneven networks, mixed dtypes) run as one CUDA graph launch.
+
+    The programs are spread over up to ``max_lanes`` streams, longest first onto the least-loaded lane;
+    each lane runs its programs in turn in one workspace region and the lanes fork from and join back
+    into the caller's stream.  No reference counterpart: ArcTN contracts one network per call.
+    """
+
+    def __init__(self, programs, *, max_lanes=32):
+        self.programs = list(programs)
+        if not self.programs:
+            raise ValueError("a batch needs at least one program")
+        arr = (C.vp * len(self.programs))(*[p._h for p in self.programs])
+        h = C.vp()
+        C.check(C.lib().arctn_b200_batch_create(arr, len(self.programs), int(max_lanes), ctypes.byref(h)),
+                "batch")
+        self._h = h
+        self.workspace_bytes = int(C.lib().arctn_b200_batch_workspace_size(h))
+        self.lanes = int(C.lib().arctn_b200_batch_lanes(h))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                C.lib().arctn_b200_batch_destroy(h)
+            except Exception:  # interpreter shutdown
+                pass
+            self._h = None
+
+    def _bind(self, arrays_list, context):
+        if len(arrays_list) != len(self.programs):
+            raise ValueError(f"{context}: {len(arrays_list)} input lists for {len(self.programs)} programs")
+        calls = []
+        for j, (p, arrays) in enumerate(zip(self.programs, arrays_list)):
+            arrays, code, torch_mode = _preflight(arrays, p.inputs, p.size_dict, f"{context} (program {j})")
+            if code != p.code:
+                raise ValueError(f"{context}: program {j} arrays dtype differs from the program's dtype")
+            calls.append((_DeviceCall(arrays, torch_mode, p.device), code, torch_mode))
+        return calls
+
+    def execute(self, arrays_list, *, workspace=None, stream=None):
+        """Every program's output, in program order."""
+        calls = self._bind(arrays_list, "batch execute")
+        torch = _torch()
+        outs = [c.empty(p.output_shape, _torch_dtype(code)) for p, (c, code, _) in zip(self.programs, calls)]
+        c0 = calls[0][0]
+        ws = workspace if workspace is not None else c0.workspace(self.workspace_bytes)
+        st = stream if stream is not None else c0.stream
+        inp = (C.vpp * len(calls))(*[ctypes.cast(c.ptrs, C.vpp) for c, _, _ in calls])
+        optr = (C.vp * len(outs))(*[o.data_ptr() for o in outs])
+        with torch.cuda.device(c0.device):
+            C.check(C.lib().arctn_b200_batch_execute(self._h, inp, optr, ws.data_ptr(), ws.numel(), st.cuda_stream),
+                    "batch execute")
+        self._keep = (calls, ws, outs)
+        return [_to_output(o, tm) for o, (_, _, tm) in zip(outs, calls)]
+
+    def gradient(self, arrays_list, grad_outputs=None, *, workspace=None, stream=None):
+        """(outputs, grads) of every program (built with ``gradient=True``); grad_outputs default to ones."""
+        calls = self._bind(arrays_list, "batch gradient")
+        torch = _torch()
+        outs, gouts, grads = [], [], []
+        for j, (p, (c, code, _)) in enumerate(zip(self.programs, calls)):
+            if not p.has_gradient:
+                raise ValueError(f"batch gradient: program {j} was built without gradient=True")
+            outs.append(c.empty(p.output_shape, _torch_dtype(code)))
+            g = None if grad_outputs is None else grad_outputs[j]
+            if g is None:
+                g = torch.ones(p.output_shape, dtype=_torch_dtype(code), device=c.device)
+            elif _is_torch(g):
+                g = g.to(c.device, _torch_dtype(code)).contiguous()
+            else:
+                np_dt = {C.F32: np.float32, C.F64: np.float64, C.C64: np.complex64, C.C128: np.complex128}[code]
+                g = torch.from_numpy(np.array(g, dtype=np_dt, order="C")).to(c.device)
+            gouts.append(g)
+            grads.append([torch.empty_like(t) for t in c.tensors])
+        c0 = calls[0][0]
+        ws = workspace if workspace is not None else c0.workspace(self.workspace_bytes)
+        st = stream if stream is not None else c0.stream
+        inp = (C.vpp * len(calls))(*[ctypes.cast(c.ptrs, C.vpp) for c, _, _ in calls])
+        optr = (C.vp * len(outs))(*[o.data_ptr() for o in outs])
+        gptr = (C.vp * len(gouts))(*[g.data_ptr() for g in gouts])
+        garrs = [(C.vp * len(gl))(*[t.data_ptr() for t in gl]) for gl in grads]
+        gpp = (C.vpp * len(garrs))(*[ctypes.cast(a, C.vpp) for a in garrs])
+        with torch.cuda.device(c0.device):
+            C.check(C.lib().arctn_b200_batch_gradient(self._h, inp, gptr, gpp, optr, ws.data_ptr(), ws.numel(),
+                                                      st.cuda_stream), "batch gradient")
+        self._keep = (calls, ws, outs, gouts, grads, garrs)
+        outs_r = [_to_output(o, tm) for o, (_, _, tm) in zip(outs, calls)]
+        grads_r = [[_to_output(t, tm) for t in gl] for gl, (_, _, tm) in zip(grads, calls)]
+        return outs_r, grads_r
+
+    def device_status(self, workspace, stream=None):
+        torch = _torch()
+        st = stream if stream is not None else torch.cuda.current_stream(
+            torch.device("cuda", self.programs[0].device))
+        code = ctypes.c_int(0)
+        C.check(C.lib().arctn_b200_batch_device_status(self._h, workspace.data_ptr(), st.cuda_stream,
+                                                       ctypes.byref(code)), "batch device status")
+        return code.value
 
 
 def _is_torch_dtype(d):

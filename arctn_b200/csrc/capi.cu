@@ -5,6 +5,8 @@
 // that stage: a pair step is the contraction of its two operand leg lists
 // with the step's result legs as output, which classifies every leg the same
 // way plan_pairwise does (src/compiled.rs:481-602).
+#include <algorithm>
+#include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -12,6 +14,7 @@
 #include <tuple>
 
 #include "../../include/arctn_b200.h"
+#include "batch.hpp"
 #include "program.hpp"
 
 using namespace ab2;
@@ -33,6 +36,9 @@ struct arctn_b200_plan {
 
 struct arctn_b200_program {
   std::unique_ptr<Program> p;
+};
+struct arctn_b200_batch {
+  std::unique_ptr<ProgramBatch> b;
 };
 
 namespace {
@@ -94,6 +100,7 @@ ProgramOptions to_options(const arctn_b200_program_options* o) {
     po.slice_begin = o->slice_begin;
     po.slice_end = o->slice_end;
     po.gradient = o->gradient != 0;
+    po.tc_k_chunk = o->tc_k_chunk;
   }
   return po;
 }
@@ -360,6 +367,69 @@ int arctn_b200_program_gradient(arctn_b200_program* p, int part, const void* con
     p->p->execute_gradient(part, inputs, grad_output, grad_inputs, output, workspace, workspace_bytes,
                            (cudaStream_t)cuda_stream);
   });
+}
+
+int arctn_b200_program_describe(const arctn_b200_program* p, char* buf, uint64_t buf_bytes, uint64_t* needed) {
+  return guarded([&] {
+    if (!p) fail("program is null");
+    const std::string d = p->p->describe();
+    if (needed) *needed = d.size() + 1;
+    if (buf && buf_bytes) {
+      const size_t n = std::min<size_t>(d.size(), buf_bytes - 1);
+      std::memcpy(buf, d.data(), n);
+      buf[n] = 0;
+    }
+  });
+}
+
+int arctn_b200_batch_create(arctn_b200_program* const* programs, uint64_t n_programs, int max_lanes,
+                            arctn_b200_batch** batch_out) {
+  return guarded([&] {
+    if (!programs || !batch_out) fail("null argument");
+    std::vector<Program*> ps;
+    for (uint64_t j = 0; j < n_programs; ++j) {
+      if (!programs[j]) fail("program " + std::to_string(j) + " is null");
+      ps.push_back(programs[j]->p.get());
+    }
+    auto h = std::make_unique<arctn_b200_batch>();
+    h->b = std::make_unique<ProgramBatch>(std::move(ps), max_lanes);
+    *batch_out = h.release();
+  });
+}
+
+void arctn_b200_batch_destroy(arctn_b200_batch* batch) { delete batch; }
+uint64_t arctn_b200_batch_workspace_size(const arctn_b200_batch* b) { return b ? b->b->workspace_size() : 0; }
+uint64_t arctn_b200_batch_lanes(const arctn_b200_batch* b) { return b ? b->b->n_lanes() : 0; }
+
+int arctn_b200_batch_execute(arctn_b200_batch* batch, const void* const* const* inputs, void* const* outputs,
+                             void* workspace, uint64_t workspace_bytes, void* cuda_stream) {
+  return guarded([&] {
+    if (!batch) fail("batch is null");
+    batch->b->run(-1, inputs, nullptr, nullptr, outputs, workspace, workspace_bytes, (cudaStream_t)cuda_stream);
+  });
+}
+
+int arctn_b200_batch_gradient(arctn_b200_batch* batch, const void* const* const* inputs,
+                              const void* const* grad_outputs, void* const* const* grads, void* const* outputs,
+                              void* workspace, uint64_t workspace_bytes, void* cuda_stream) {
+  return guarded([&] {
+    if (!batch) fail("batch is null");
+    batch->b->run(0, inputs, grad_outputs, grads, outputs, workspace, workspace_bytes, (cudaStream_t)cuda_stream);
+  });
+}
+
+int arctn_b200_batch_device_status(arctn_b200_batch* batch, void* workspace, void* cuda_stream, int* code) {
+  int c = 0;
+  int rc = guarded([&] {
+    if (!batch || !workspace || !code) fail("null argument");
+    c = batch->b->device_status(workspace, (cudaStream_t)cuda_stream);
+    *code = c;
+  });
+  if (rc == ARCTN_B200_OK && c != 0) {
+    g_last_error = "a bounded device-side wait expired (code " + std::to_string(c) + ")";
+    return ARCTN_B200_ERR_DEVICE_TIMEOUT;
+  }
+  return rc;
 }
 
 int arctn_b200_program_device_status(arctn_b200_program* p, void* workspace, void* cuda_stream, int* code) {

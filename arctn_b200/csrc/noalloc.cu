@@ -35,7 +35,7 @@ std::mutex g_mu;
 void* g_scratch_ptr[kMaxDevices] = {};
 bool g_attr_set[kMaxDevices] = {};
 
-// src[b*bs + r*rs + c*cs] -> K-major planes [re|im][b][Rpad][Kpad], zero padding.
+// src[b*bs + r*rs + c*cs] -> K-major TF32-pair planes [re_hi|re_lo|im_hi|im_lo][b][Rpad][Kpad], zero padding.
 __global__ void __launch_bounds__(256) k_pack_strided(const ab2::cf32* __restrict__ src, float* __restrict__ dst,
                                                       ll Z, ll R, ll K, ll Rpad, ll Kpad, ll bs, ll rs, ll cs,
                                                       int r_major) {
@@ -62,8 +62,8 @@ __global__ void __launch_bounds__(256) k_pack_strided(const ab2::cf32* __restric
       const ll r = r0 + u, c = c0 + tx;
       if (c < Kpad) {
         const ll o = (z * Rpad + r) * Kpad + c;
-        dst[o] = tile[u][tx].re;
-        dst[plane + o] = tile[u][tx].im;
+        ab2::tc::put_split(dst, plane, o, tile[u][tx].re);
+        ab2::tc::put_split(dst + 2 * plane, plane, o, tile[u][tx].im);
       }
     }
     __syncthreads();
@@ -114,8 +114,8 @@ extern "C" int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, voi
   if (bt == 0 || m == 0 || k == 0 || n == 0) return fail_with("bt, m, k and n must be positive", ARCTN_B200_ERR_INVALID);
   const unsigned __int128 kpad = (k + tc::BK - 1) / tc::BK * tc::BK, rpa = (m + tc::BM - 1) / tc::BM * tc::BM,
                           rpb = (n + tc::BN - 1) / tc::BN * tc::BN;
-  const unsigned __int128 a_bytes = 2 * (unsigned __int128)bt * rpa * kpad * 4;
-  const unsigned __int128 b_bytes = 2 * (unsigned __int128)bt * rpb * kpad * 4;
+  const unsigned __int128 a_bytes = ab2::tc::PLANES * (unsigned __int128)bt * rpa * kpad * 4;
+  const unsigned __int128 b_bytes = ab2::tc::PLANES * (unsigned __int128)bt * rpb * kpad * 4;
   const unsigned __int128 need = ((a_bytes + 255) / 256 * 256) + ((b_bytes + 255) / 256 * 256) + 256;
   if (need > kScratchBytes)
     return fail_with("problem needs " + std::to_string((unsigned long long)need) + " scratch bytes; the fixed maximum is " +
@@ -152,7 +152,7 @@ extern "C" int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, voi
   k_pack_strided<<<tiles(Z, Ra, Kp), 256, 0, st>>>((const cf32*)a, pa, Z, (ll)m, (ll)k, Ra, Kp, (ll)(m * k), (ll)k, 1, 0);
   k_pack_strided<<<tiles(Z, Rb, Kp), 256, 0, st>>>((const cf32*)b, pb, Z, (ll)n, (ll)k, Rb, Kp, (ll)(k * n), 1, (ll)n, 1);
   CUtensorMap ma, mb;
-  if (!plane_map(&ma, pa, Kp, Ra, 2 * Z) || !plane_map(&mb, pb, Kp, Rb, 2 * Z))
+  if (!plane_map(&ma, pa, Kp, Ra, ab2::tc::PLANES * Z) || !plane_map(&mb, pb, Kp, Rb, ab2::tc::PLANES * Z))
     return fail_with("cuTensorMapEncodeTiled failed", ARCTN_B200_ERR_CUDA);
   tc::TcArgs args;
   args.C = (cf32*)c;
@@ -165,7 +165,9 @@ extern "C" int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, voi
   args.a_var = 0;
   args.b_var = 0;
   args.err = err;
-  dim3 grid((unsigned)(Rb / tc::BN), (unsigned)(Ra / tc::BM), (unsigned)Z);
+  args.m_tiles = (int)(Ra / tc::BM);
+  args.m_fast = Ra <= Rb ? 1 : 0;
+  dim3 grid((unsigned)((Ra / tc::BM) * (Rb / tc::BN)), 1u, (unsigned)Z);
   tc::k_tc_cgemm_tf32x3<<<grid, 192, tc::SMEM_BYTES, st>>>(ma, mb, args);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail_with(std::string("launch: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);

@@ -42,7 +42,10 @@ namespace {
 
 constexpr u64 kAlign = 256;
 constexpr u64 kInf = ~0ull;
-// Tensor-core GEMMs accumulate at most this many 16-wide K tiles (K = 512) in one TMEM accumulator.
+// Tensor-core GEMMs accumulate at most this many 16-wide K tiles (K = 512) in one TMEM accumulator
+// unless the options give another chunk.  The tensor core's FP32 accumulation truncates once per
+// 8-wide MMA, so its error grows with the chain length; splits are summed in FP64.  Shorter chunks
+// buy accuracy with partial traffic and per-CTA overhead (K = 256 costs about 15% on long-K steps).
 constexpr int kSplitTiles = 32;
 inline u64 align_up(u64 x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
@@ -114,6 +117,8 @@ Program::Program(const Network& net, const SsaPath& path, const std::vector<Leg>
   dtype_bytes(opt_.dtype);
   if (opt_.precision != PREC_FP32 && opt_.precision != PREC_TF32X3)
     throw Error(E_INVALID, "unsupported precision mode " + std::to_string(opt_.precision));
+  if (opt_.tc_k_chunk % tc::BK != 0 || opt_.tc_k_chunk > (1ull << 30))
+    throw Error(E_INVALID, "tc_k_chunk must be a multiple of 16 (0 for the default)");
   build(net, path, sliced);
   if (opt_.gradient && !sliced_) {
     // Over the workspace budget: drop the largest step results from what the adjoint sweep keeps
@@ -141,16 +146,43 @@ Program::Program(const Network& net, const SsaPath& path, const std::vector<Leg>
       }
     }
   }
-  int prev = 0;
-  CK(cudaGetDevice(&prev));
-  CK(cudaSetDevice(opt_.device));
+  // Upload the offset tables now when a GPU is present (so a first execute may sit inside the caller's
+  // stream capture); on a host without one the program stays inspectable (describe) and uploads on
+  // its first execute.
+  int n_dev = 0;
+  if (cudaGetDeviceCount(&n_dev) != cudaSuccess) {
+    cudaGetLastError();
+    n_dev = 0;
+  }
+  if (n_dev > 0) {
+    if (opt_.device < 0 || opt_.device >= n_dev)
+      throw Error(E_INVALID, "device " + std::to_string(opt_.device) + " is not visible");
+    int prev = 0;
+    CK(cudaGetDevice(&prev));
+    CK(cudaSetDevice(opt_.device));
+    try {
+      ensure_tables();
+    } catch (...) {
+      cudaSetDevice(prev);
+      throw;
+    }
+    cudaSetDevice(prev);
+  }
+}
+
+void Program::ensure_tables() {
+  if (dev_tab_) return;
   cudaError_t e = cudaMalloc(&dev_tab_, std::max<size_t>(host_tab_.size(), 256));
   if (e == cudaSuccess) e = cudaMemcpy(dev_tab_, host_tab_.data(), host_tab_.size(), cudaMemcpyHostToDevice);
-  cudaSetDevice(prev);
-  if (e != cudaSuccess) throw Error(E_CUDA, std::string("uploading offset tables: ") + cudaGetErrorString(e));
+  if (e != cudaSuccess) {
+    if (dev_tab_) cudaFree(dev_tab_);
+    dev_tab_ = nullptr;
+    throw Error(E_CUDA, std::string("uploading offset tables: ") + cudaGetErrorString(e));
+  }
 }
 
 Program::~Program() {
+  if (!dev_tab_ && !gexec_) return;
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(opt_.device);
@@ -465,13 +497,14 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     const size_t L = dims.size();
     std::vector<char> in_tile(L, 0);
     u64 T = 1;
-    auto take = [&](const std::vector<ll>& key) {
+    // Innermost legs of one side (by stride) until that side's contiguous run reaches `want` elements.
+    auto take = [&](const std::vector<ll>& key, u64 want) {
       std::vector<size_t> order(L);
       std::iota(order.begin(), order.end(), 0);
       std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return key[a] < key[b]; });
       u64 covered = 1;  // product of this side's innermost legs already in the tile
       for (size_t i : order) {
-        if (covered >= 32) break;
+        if (covered >= want) break;
         if (in_tile[i]) { covered *= dims[i]; continue; }
         if (T * dims[i] > (u64)tc::kPackTile) break;
         in_tile[i] = 1;
@@ -479,8 +512,9 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         covered *= dims[i];
       }
     };
-    take(ss);
-    take(ds);
+    take(ss, 32);  // a warp's read covers 32 contiguous source elements
+    take(ds, 32);  // and its write 32 contiguous floats of each plane
+    take(ss, tc::kPackTile);  // then grow along the source to a full tile: fewer, longer tiles
     if (T < 32) return false;
     std::vector<u64> td, od;
     std::vector<ll> tss, tds, oss, ods;
@@ -491,17 +525,22 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     const std::vector<ll> so_ = offsets(td, tss), do_ = offsets(td, tds);
     for (ll v : so_) if (v < 0 || v > INT32_MAX) return false;
     for (ll v : do_) if (v < 0 || v > INT32_MAX) return false;
-    std::vector<int> rd(T), wr(T);
+    // Tile elements numbered by destination offset (rank); the read list in source-offset order.
+    std::vector<int> rd(T), wr(T), rank(T);
     std::iota(rd.begin(), rd.end(), 0);
     std::iota(wr.begin(), wr.end(), 0);
     std::stable_sort(rd.begin(), rd.end(), [&](int a, int b) { return so_[a] < so_[b]; });
     std::stable_sort(wr.begin(), wr.end(), [&](int a, int b) { return do_[a] < do_[b]; });
-    std::vector<int> rd_off(T), wr_off(T);
-    for (u64 i = 0; i < T; ++i) { rd_off[i] = (int)so_[rd[i]]; wr_off[i] = (int)do_[wr[i]]; }
-    p.tab[0] = tab_i32(rd);
+    for (u64 r = 0; r < T; ++r) rank[wr[r]] = (int)r;
+    std::vector<int> rd_rank(T), rd_off(T), wr_off(T);
+    for (u64 i = 0; i < T; ++i) {
+      rd_rank[i] = rank[rd[i]];
+      rd_off[i] = (int)so_[rd[i]];
+      wr_off[i] = (int)do_[wr[i]];
+    }
+    p.tab[0] = tab_i32(rd_rank);
     p.tab[1] = tab_i32(rd_off);
-    p.tab[2] = tab_i32(wr);
-    p.tab[3] = tab_i32(wr_off);
+    p.tab[2] = tab_i32(wr_off);
     p.tab[4] = tab_ll(offsets(od, oss));
     p.tab[5] = tab_ll(offsets(od, ods));
     p.tile_T = (ll)T;
@@ -543,7 +582,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       const ll rpa = ((ll)m + tc::BM - 1) / tc::BM * tc::BM;
       const ll rpb = ((ll)n + tc::BN - 1) / tc::BN * tc::BN;
       auto pack = [&](const Operand& X, ll rows, ll rpad, bool conj) {
-        const u64 pbuf = new_buf(ph2, (u64)(2 * (ll)bt * rpad * kpad * 4), opidx(ph2));
+        const u64 pbuf = new_buf(ph2, (u64)(tc::PLANES * (ll)bt * rpad * kpad * 4), opidx(ph2));
         bufs[pbuf].fixed = ph2 && !X.variant;
         Op p{Op::PACK};
         p.a = X.ref;
@@ -583,9 +622,10 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       touch(Ref{Ref::WS, pa}, ph2, opidx(ph2));
       // K longer than kSplitTiles tiles is split across CTAs (see TcArgs): partials [split][z][m][n].
       const int kt_total = (int)(kpad / tc::BK);
-      if (kt_total > kSplitTiles) {
-        g.kt_chunk = kSplitTiles;
-        g.splits = (kt_total + kSplitTiles - 1) / kSplitTiles;
+      const int chunk = opt_.tc_k_chunk ? (int)(opt_.tc_k_chunk / tc::BK) : kSplitTiles;
+      if (kt_total > chunk) {
+        g.kt_chunk = chunk;
+        g.splits = (kt_total + chunk - 1) / chunk;
         const u64 pbuf = new_buf(ph2, (u64)g.splits * bt * m * n * 8, opidx(ph2));
         bufs[pbuf].fixed = ph2 && !(A.variant || B.variant);
         g.d = Ref{Ref::WS, pbuf};
@@ -1104,10 +1144,10 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, const char* tab
     const ll n_slices = op.a_var ? op.S : 1;
     const ll slice_stride = op.bt * op.rpad * op.kpad;
     const ll plane = n_slices * slice_stride;
-    tc::k_pack_tiled<<<(int)std::min<ll>(op.n_outer * n_slices, 148 * 16), 256, 0, st>>>(
+    tc::k_pack_tiled<<<(int)std::min<ll>(op.n_outer * n_slices, 148 * 8), tc::kPackThreads, 0, st>>>(
         (const cf32*)A, (float*)C, (const int*)(tab + op.tab[0]), (const int*)(tab + op.tab[1]),
-        (const int*)(tab + op.tab[2]), (const int*)(tab + op.tab[3]), (int)op.tile_T, (const ll*)(tab + op.tab[4]),
-        (const ll*)(tab + op.tab[5]), op.n_outer, n_slices, slice_stride, plane, op.sa, op.g0, op.conj_a ? 1 : 0);
+        (const int*)(tab + op.tab[2]), (int)op.tile_T, (const ll*)(tab + op.tab[4]), (const ll*)(tab + op.tab[5]),
+        op.n_outer, n_slices, slice_stride, plane, op.sa, op.g0, op.conj_a ? 1 : 0);
     return;
   }
   static bool attr_set[64] = {};
@@ -1119,8 +1159,8 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, const char* tab
   }
   const ll s_eff = (op.a_var || op.b_var) ? op.S : 1;
   const ll za = (op.a_var ? op.S : 1) * op.bt, zb = (op.b_var ? op.S : 1) * op.bt;
-  const CUtensorMap ma = plane_map(A, op.kpad, op.rpad, 2 * za);
-  const CUtensorMap mb = plane_map(B, op.kpad, op.rpad_b, 2 * zb);
+  const CUtensorMap ma = plane_map(A, op.kpad, op.rpad, tc::PLANES * za);
+  const CUtensorMap mb = plane_map(B, op.kpad, op.rpad_b, tc::PLANES * zb);
   tc::TcArgs args;
   args.C = (cf32*)C;
   args.m = op.m;
@@ -1139,8 +1179,12 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, const char* tab
     args.zc = (int)zc;
     args.part = (cf32*)D;
   }
-  dim3 grid((unsigned)((op.n + tc::BN - 1) / tc::BN), (unsigned)((op.m + tc::BM - 1) / tc::BM),
-            (unsigned)(zc * op.splits));
+  // The smaller operand's tiles run fastest, so it stays in L2 while the larger one streams once.
+  const ll mt = (op.m + tc::BM - 1) / tc::BM, nt = (op.n + tc::BN - 1) / tc::BN;
+  args.m_tiles = (int)mt;
+  args.m_fast = mt <= nt ? 1 : 0;
+  if (mt * nt > 0x7FFFFFFFll) throw Error(E_UNSUPPORTED, "tensor-core GEMM tile count exceeds the grid limit");
+  dim3 grid((unsigned)(mt * nt), 1u, (unsigned)(zc * op.splits));
   tc::k_tc_cgemm_tf32x3<<<grid, 192, tc::SMEM_BYTES, st>>>(ma, mb, args);
   if (op.splits > 1) {
     const ll count = zc * op.m * op.n;
@@ -1162,8 +1206,8 @@ void Program::launch_op(const Op& op, const void* const* inputs, void* output, c
     }
   };
   if (op.kind == Op::MEMSET) {
-    // bytes == 0: the padded planes of a tiled pack, [re|im][slices of this group][bt][rpad][kpad] fp32
-    const u64 bytes = op.bytes ? op.bytes : (u64)(2 * (op.a_var ? op.S : 1) * op.bt * op.rpad * op.kpad * 4);
+    // bytes == 0: the padded planes of a tiled pack, [4 planes][slices of this group][bt][rpad][kpad] fp32
+    const u64 bytes = op.bytes ? op.bytes : (u64)(tc::PLANES * (op.a_var ? op.S : 1) * op.bt * op.rpad * op.kpad * 4);
     CK(cudaMemsetAsync(ptr(op.c), 0, bytes, st));
     return;
   }
@@ -1210,6 +1254,7 @@ void Program::execute(const void* const* inputs, void* output, bool f64_out, voi
   if (ws_total_ && !ws) throw Error(E_INVALID, "workspace pointer is null");
   DeviceGuard guard(opt_.device);
   std::lock_guard<std::mutex> lk(mu_);
+  ensure_tables();
   out_f64_flag_ = f64_out;
   if (opt_.gradient) {  // plain execute of a gradient program: the forward part only
     for (size_t i = 0; i < bwd_begin_; ++i) launch_op(ops_[i], inputs, output, (char*)ws, st);
@@ -1275,8 +1320,8 @@ double op_work(const Op& op, int dt) {
     case Op::ACCUM: return (double)op.n_segs * op.n_e * (2.0 * wide_bytes(dt)) + (double)op.S * op.n_e * eb;
     case Op::OUTPUT: return (double)op.n_blocks * op.n_chunks * op.n_e * wide_bytes(dt);
     case Op::PACK:
-    case Op::PACK_TILED:  // complex64 read once, two fp32 planes written (padding included)
-      return (double)(op.a_var ? op.S : 1) * op.bt * (8.0 * op.rows * op.cols + 8.0 * op.rpad * op.kpad);
+    case Op::PACK_TILED:  // complex64 read once, four fp32 planes written (padding included)
+      return (double)(op.a_var ? op.S : 1) * op.bt * (8.0 * op.rows * op.cols + 16.0 * op.rpad * op.kpad);
     default: return (double)op.n_out * eb;
   }
 }
@@ -1287,6 +1332,7 @@ void Program::profile(const void* const* inputs, void* output, void* ws, u64 ws_
   if (ws_bytes < ws_total_) throw Error(E_WORKSPACE, "workspace is smaller than required");
   DeviceGuard guard(opt_.device);
   std::lock_guard<std::mutex> lk(mu_);
+  ensure_tables();
   out_f64_flag_ = false;
   std::vector<cudaEvent_t> ev;
   for (size_t i = 0; i <= ops_.size(); ++i) {
@@ -1347,10 +1393,83 @@ void Program::execute_gradient(int part, const void* const* inputs, const void* 
   if (ws_total_ && !ws) throw Error(E_INVALID, "workspace pointer is null");
   DeviceGuard guard(opt_.device);
   std::lock_guard<std::mutex> lk(mu_);
+  ensure_tables();
   out_f64_flag_ = false;
   grad_out_ = grad_out;
   grads_ = grads;
   const size_t lo = part == 2 ? bwd_begin_ : 0, hi = part == 1 ? bwd_begin_ : ops_.size();
+  try {
+    for (size_t i = lo; i < hi; ++i) launch_op(ops_[i], inputs, output, (char*)ws, st);
+  } catch (...) {
+    grad_out_ = nullptr;
+    grads_ = nullptr;
+    throw;
+  }
+  grad_out_ = nullptr;
+  grads_ = nullptr;
+}
+
+std::string Program::describe() const {
+  static const char* names[] = {"gather",    "gemm_small", "gemm_tile64", "gemm_tile32", "slice_accumulate",
+                                "slice_output", "memset",  "maxabs",      "strip",       "gemm_tc",
+                                "gemm_dot",  "pack",       "scatter",     "pack_tiled"};
+  std::string s = "{\"workspace_bytes\":" + std::to_string(ws_total_) + ",\"n_slices\":" + std::to_string(n_total_) +
+                  ",\"slices_per_group\":" + std::to_string(S_) + ",\"groups\":" + std::to_string(n_groups_) +
+                  ",\"launches\":" + std::to_string(launches()) + ",\"gradient\":" + (opt_.gradient ? "true" : "false") +
+                  ",\"backward_begin\":" + std::to_string(opt_.gradient ? bwd_begin_ : ops_.size()) +
+                  ",\"recomputed_steps\":[";
+  bool first = true;
+  for (size_t d : drop_) {
+    s += (first ? "" : ",") + std::to_string(d);
+    first = false;
+  }
+  s += "],\"ops\":[";
+  for (size_t i = 0; i < ops_.size(); ++i) {
+    const Op& op = ops_[i];
+    s += std::string(i ? "," : "") + "{\"kind\":\"" + names[(int)op.kind] + "\"";
+    auto f = [&](const char* k, long long v) { s += std::string(",\"") + k + "\":" + std::to_string(v); };
+    switch (op.kind) {
+      case Op::GEMM_SMALL: case Op::GEMM_TILE64: case Op::GEMM_TILE32: case Op::GEMM_DOT: case Op::GEMM_TC:
+        f("S", op.S); f("bt", op.bt); f("m", op.m); f("k", op.k); f("n", op.n);
+        f("splits", op.splits); f("conj_a", op.conj_a); f("conj_b", op.conj_b);
+        break;
+      case Op::PACK: case Op::PACK_TILED:
+        f("S", op.a_var ? op.S : 1); f("bt", op.bt); f("rows", op.rows); f("cols", op.cols); f("rpad", op.rpad);
+        f("kpad", op.kpad); f("tile", op.tile_T); f("n_outer", op.n_outer);
+        break;
+      case Op::GATHER: case Op::SCATTER: case Op::MAXABS: case Op::STRIP:
+        f("S", op.S); f("n_out", op.n_out); f("n_red", op.n_red);
+        break;
+      case Op::MEMSET: f("bytes", (long long)op.bytes); break;
+      default: f("n_e", op.n_e); break;
+    }
+    s += "}";
+  }
+  return s + "]}";
+}
+
+void Program::check_run(int part, const void* const* inputs, const void* grad_out, void* const* grads,
+                        const void* output) const {
+  if (part < -1 || part > 2) throw Error(E_INVALID, "gradient part must be 0, 1 or 2");
+  if (part >= 0 && !opt_.gradient) throw Error(E_INVALID, "the program was built without gradient support");
+  if (!inputs) throw Error(E_INVALID, "inputs pointer is null");
+  for (u64 i = 0; i < plan_.n_inputs; ++i)
+    if (!inputs[i]) throw Error(E_INVALID, "input " + std::to_string(i) + " pointer is null");
+  if (part != 2 && !output) throw Error(E_INVALID, "output pointer is null");
+  if (part == 0 || part == 2) {
+    if (!grad_out) throw Error(E_INVALID, "grad_output pointer is null");
+    for (u64 i = 0; i < plan_.n_inputs; ++i)
+      if (!grads || !grads[i]) throw Error(E_INVALID, "gradient buffer " + std::to_string(i) + " is null");
+  }
+}
+
+void Program::enqueue_part(int part, const void* const* inputs, const void* grad_out, void* const* grads,
+                           void* output, void* ws, cudaStream_t st) {
+  out_f64_flag_ = false;
+  grad_out_ = grad_out;
+  grads_ = grads;
+  const size_t fwd_end = opt_.gradient ? bwd_begin_ : ops_.size();
+  const size_t lo = part == 2 ? bwd_begin_ : 0, hi = (part == 1 || part == -1) ? fwd_end : ops_.size();
   try {
     for (size_t i = lo; i < hi; ++i) launch_op(ops_[i], inputs, output, (char*)ws, st);
   } catch (...) {
@@ -1376,6 +1495,7 @@ void Program::execute_stripped(const void* const* inputs, void* output, void* ws
   if (ws_bytes < ws_total_) throw Error(E_WORKSPACE, "workspace is smaller than required");
   DeviceGuard guard(opt_.device);
   std::lock_guard<std::mutex> lk(mu_);
+  ensure_tables();
   out_f64_flag_ = false;
   enqueue(strip_ops_, inputs, output, (char*)ws, st);
   double e = 0.0;

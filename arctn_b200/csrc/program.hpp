@@ -33,6 +33,7 @@ struct ProgramOptions {
   u64 workspace_budget = 0;
   u64 slice_begin = 0, slice_end = 0;  // both 0: every slice
   bool gradient = false;               // also build the adjoint (reverse) sweep
+  u64 tc_k_chunk = 0;                  // tf32x3: K per tensor-core accumulator (multiple of 16); 0: 512
 };
 
 // Where an operand lives at run time.
@@ -93,6 +94,24 @@ class Program {
   u64 recomputed_steps() const { return drop_.size(); }
   u64 forward_launches() const;
   u64 backward_launches() const;
+
+  // Hooks for ProgramBatch.  part: -1 plain execute (a gradient program's forward), 0 forward +
+  // reverse, 1 forward keeping intermediates, 2 reverse.  check_run validates the bindings of one run;
+  // enqueue_part launches its ops on `st` without a graph and without locking (the caller holds mutex()).
+  void check_run(int part, const void* const* inputs, const void* grad_out, void* const* grads,
+                 const void* output) const;
+  void enqueue_part(int part, const void* const* inputs, const void* grad_out, void* const* grads, void* output,
+                    void* ws, cudaStream_t st);
+  std::mutex& mutex() { return mu_; }
+  // Uploads the offset tables if the constructor could not (no GPU at build time); needs mutex() held
+  // and the program's device current, outside any stream capture.
+  void ensure_tables();
+  int device() const { return opt_.device; }
+  int dtype() const { return opt_.dtype; }
+  u64 error_offset() const { return err_off_; }
+  u64 n_inputs() const { return plan_.n_inputs; }
+  // JSON description of the launch sequence and workspace layout (host-only; no GPU needed).
+  std::string describe() const;
 
  private:
   // Workspace buffer with an op-index lifetime; region-2 sizes scale with the

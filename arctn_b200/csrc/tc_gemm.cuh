@@ -1,19 +1,20 @@
 // tcgen05 complex GEMM with split-TF32 products (sm_100a).
 //
 // C[z] (m x n, complex64) = A[z] (m x k) . B[z] (k x n) for every batch z.
-// Operands arrive packed by k_pack_planar as K-major fp32 planes
-// [re | im][z][rows][k] (rows padded to 128, k padded to 16).  Per 16-wide K
-// slab the CTA splits every value x into hi = x rounded to the nearest TF32
-// value and lo = x - hi (exact in FP32) rounded likewise, so hi + lo carries
-// x to about 2^-23 relative with no bias, and issues the 4M complex product as
-// 12 TF32 MMAs into TMEM accumulators:
+// Operands arrive packed (k_pack_tiled / k_pack_planar) as K-major fp32 planes
+// [re_hi | re_lo | im_hi | im_lo][z][rows][k] (rows padded to 128, k padded
+// to 16): every value x is stored as hi = x rounded to the nearest TF32 value
+// and lo = x - hi (exact in FP32) rounded likewise, so hi + lo carries x to
+// about 2^-23 relative with no bias.  The split happens once, in the pack, so
+// the GEMM's shared memory serves only TMA writes and tensor-core reads.  The
+// 4M complex product is 12 TF32 MMAs per 8-wide K step into TMEM accumulators:
 //   Cr += Ar*Br - Ai*Bi,  Ci += Ar*Bi + Ai*Br   for (hi,hi), (hi,lo), (lo,hi),
 // the minus through the instruction's negate-A bit.  Accumulation is FP32.
 //
 // Warp roles (192 threads, one CTA per 128x128 output tile):
-//   warp 0      TMA producer: 4 plane tiles per stage, 3-stage ring
+//   warp 0      TMA producer: 8 plane tiles per stage, 3-stage ring
 //   warp 1      TMEM allocation + single-thread MMA issue
-//   warps 2..5  hi/lo split in shared memory, then the epilogue (TMEM -> HBM)
+//   warps 2..5  epilogue (TMEM -> HBM)
 // Every mbarrier wait is bounded (about one second of global time); on expiry
 // the kernel records a code in *err, drains what it issued and returns.
 #pragma once
@@ -27,10 +28,11 @@
 namespace ab2 {
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3, LO_SLOTS = 2;
+constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3;
+constexpr int PLANES = 4;                          // re_hi, re_lo, im_hi, im_lo
 constexpr int PLANE_BYTES = BM * BK * 4;          // 8 KB: 128 rows x 64 B
-constexpr int STAGE_BYTES = 4 * PLANE_BYTES;       // Ar, Ai, Br, Bi
-constexpr int SMEM_BYTES = (STAGES + LO_SLOTS) * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*align*/;
+constexpr int STAGE_BYTES = 2 * PLANES * PLANE_BYTES;  // A planes then B planes: 64 KB
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*align*/;
 // Cr: [0,128), Ci: [128,256) take the (hi,hi) products; Cr', Ci': [256,384), [384,512) take the
 // (hi,lo) and (lo,hi) products, which are 2^-10 smaller, so the large accumulators see 4 of the 12
 // additions per K step and the rounding of each accumulation stays at the scale of its own sum.
@@ -47,6 +49,12 @@ __host__ __device__ __forceinline__ uint32_t tf32_round(uint32_t bits) { return 
 // x - hi, exact in FP32 (hi is within half a TF32 unit of x, so the subtraction is Sterbenz-exact).
 __device__ __forceinline__ uint32_t tf32_residual(uint32_t x, uint32_t hi) {
   return __float_as_uint(__uint_as_float(x) - __uint_as_float(hi));
+}
+// Stores x as its TF32 pair: hi at dst[o], lo at dst[plane + o].
+__device__ __forceinline__ void put_split(float* dst, ll plane, ll o, float x) {
+  const uint32_t b = __float_as_uint(x), h = tf32_round(b);
+  dst[o] = __uint_as_float(h);
+  dst[plane + o] = __uint_as_float(tf32_round(tf32_residual(b, h)));
 }
 __device__ __forceinline__ unsigned long long now_ns() {
   unsigned long long t;
@@ -130,7 +138,7 @@ struct TcArgs {
   cf32* C;
   ll m, n;           // logical output rows / complex columns
   int k_tiles;       // padded K / BK
-  int za, zb;        // plane batches of A and B (the imaginary plane starts at z + za / z + zb)
+  int za, zb;        // plane batches of A and B (plane p of batch z sits at z + p * za / z + p * zb)
   int bt;            // GEMM batch per slice
   int a_var, b_var;  // operand differs per slice (else it is shared by all slices)
   int* err;
@@ -141,38 +149,39 @@ struct TcArgs {
   int kt_chunk = 0;  // 0: one CTA takes all of K and writes C
   int zc = 0;        // output batches (grid z = splits * zc)
   cf32* part = nullptr;
+  // Raster: blockIdx.x enumerates the m_tiles x n_tiles output tiles with the m-tile fastest when
+  // m_fast (A's tiles stay in L2 while B streams through once), else the n-tile fastest.
+  int m_tiles = 1;
+  int m_fast = 1;
 };
 
 static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_constant__ CUtensorMap tmA,
                                                           const __grid_constant__ CUtensorMap tmB, TcArgs args) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char* raw = smem;                                   // STAGES x {Ar, Ai, Br, Bi}
-  unsigned char* lo = smem + STAGES * STAGE_BYTES;             // LO_SLOTS x {Ar, Ai, Br, Bi}
-  uint64_t* bars = (uint64_t*)(smem + (STAGES + LO_SLOTS) * STAGE_BYTES);
+  unsigned char* ring = smem;                                  // STAGES x {A planes, B planes}
+  uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
   uint64_t* full = bars;                     // TMA landed          (count 1 + tx)
   uint64_t* empty = bars + STAGES;           // MMAs done reading   (commit)
-  uint64_t* lofull = bars + 2 * STAGES;      // split done          (count 128)
-  uint64_t* loempty = lofull + LO_SLOTS;     // MMAs done with slot (commit)
-  uint64_t* accfull = loempty + LO_SLOTS;    // all MMAs done       (commit)
+  uint64_t* accfull = bars + 2 * STAGES;     // all MMAs done       (commit)
   uint64_t* drain = accfull + 1;             // abort drain         (commit)
   volatile uint32_t* tmem_slot = (volatile uint32_t*)(drain + 1);
   volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int tile_n = blockIdx.x, tile_m = blockIdx.y;
+  const int n_tiles = (int)((args.n + BN - 1) / BN);
+  const int tile_m = args.m_fast ? (int)(blockIdx.x % args.m_tiles) : (int)(blockIdx.x / n_tiles);
+  const int tile_n = args.m_fast ? (int)(blockIdx.x / args.m_tiles) : (int)(blockIdx.x % n_tiles);
   const int split = args.kt_chunk ? (int)(blockIdx.z / args.zc) : 0;
   const int z = args.kt_chunk ? (int)(blockIdx.z % args.zc) : (int)blockIdx.z;
   const int kt0 = args.kt_chunk ? split * args.kt_chunk : 0;
   const int kt1 = args.kt_chunk ? min(args.k_tiles, kt0 + args.kt_chunk) : args.k_tiles;
-  const int s_idx = z / args.bt, b_idx = z % args.bt;
+  const int b_idx = z % args.bt;
   const int zA = args.a_var ? z : b_idx;
   const int zB = args.b_var ? z : b_idx;
-  (void)s_idx;
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < STAGES; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
-    for (int i = 0; i < LO_SLOTS; ++i) { mbar_init(&lofull[i], 128); mbar_init(&loempty[i], 1); }
     mbar_init(accfull, 1);
     mbar_init(drain, 1);
     *abort_flag = 0;
@@ -197,13 +206,14 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
         const int s = t % STAGES;
         if (t >= STAGES && !mbar_wait(&empty[s], ((t / STAGES) - 1) & 1, args.err, 1)) { *abort_flag = 1; break; }
         if (*abort_flag) break;
-        unsigned char* dst = raw + s * STAGE_BYTES;
+        unsigned char* dst = ring + s * STAGE_BYTES;
         mbar_expect_tx(&full[s], STAGE_BYTES);
         const int k0 = (kt0 + t) * BK;
-        tma_load_3d(&tmA, &full[s], dst + 0 * PLANE_BYTES, k0, tile_m * BM, zA);
-        tma_load_3d(&tmA, &full[s], dst + 1 * PLANE_BYTES, k0, tile_m * BM, zA + args.za);
-        tma_load_3d(&tmB, &full[s], dst + 2 * PLANE_BYTES, k0, tile_n * BN, zB);
-        tma_load_3d(&tmB, &full[s], dst + 3 * PLANE_BYTES, k0, tile_n * BN, zB + args.zb);
+#pragma unroll
+        for (int p = 0; p < PLANES; ++p) {
+          tma_load_3d(&tmA, &full[s], dst + p * PLANE_BYTES, k0, tile_m * BM, zA + p * args.za);
+          tma_load_3d(&tmB, &full[s], dst + (PLANES + p) * PLANE_BYTES, k0, tile_n * BN, zB + p * args.zb);
+        }
         issued = t + 1;
       }
       if (*abort_flag) {  // let issued copies land before the CTA retires
@@ -218,12 +228,12 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
       const uint32_t cr = tmem, ci = tmem + BN, crs = tmem + 2 * BN, cis = tmem + 3 * BN;
       bool first = true;
       for (int t = 0; t < KT && !*abort_flag; ++t) {
-        const int s = t % STAGES, q = t % LO_SLOTS;
-        if (!mbar_wait(&lofull[q], (t / LO_SLOTS) & 1, args.err, 2)) { *abort_flag = 1; break; }
+        const int s = t % STAGES;
+        if (!mbar_wait(&full[s], (t / STAGES) & 1, args.err, 2)) { *abort_flag = 1; break; }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t rb = smem_u32(raw + s * STAGE_BYTES), lb = smem_u32(lo + q * STAGE_BYTES);
-        const uint32_t hAr = rb, hAi = rb + PLANE_BYTES, hBr = rb + 2 * PLANE_BYTES, hBi = rb + 3 * PLANE_BYTES;
-        const uint32_t lAr = lb, lAi = lb + PLANE_BYTES, lBr = lb + 2 * PLANE_BYTES, lBi = lb + 3 * PLANE_BYTES;
+        const uint32_t a0 = smem_u32(ring + s * STAGE_BYTES), b0 = a0 + PLANES * PLANE_BYTES;
+        const uint32_t hAr = a0, lAr = a0 + PLANE_BYTES, hAi = a0 + 2 * PLANE_BYTES, lAi = a0 + 3 * PLANE_BYTES;
+        const uint32_t hBr = b0, lBr = b0 + PLANE_BYTES, hBi = b0 + 2 * PLANE_BYTES, lBi = b0 + 3 * PLANE_BYTES;
 #pragma unroll
         for (int kk = 0; kk < BK / 8; ++kk) {
           const uint32_t o = kk * 32;  // 8 tf32 = 32 bytes along the swizzled row
@@ -245,35 +255,21 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
           first = false;
         }
         umma_commit(&empty[s]);
-        umma_commit(&loempty[q]);
       }
       umma_commit(*abort_flag ? drain : accfull);
       if (*abort_flag) mbar_wait(drain, 0, args.err, 8);
     }
   } else {
-    // ------------------------------------------------------------ hi/lo split (128 threads)
-    const int tid = threadIdx.x - 64;
-    for (int t = 0; t < KT; ++t) {
-      const int s = t % STAGES, q = t % LO_SLOTS;
-      bool ok = mbar_wait(&full[s], (t / STAGES) & 1, args.err, 3);
-      if (ok && t >= LO_SLOTS) ok = mbar_wait(&loempty[q], ((t / LO_SLOTS) - 1) & 1, args.err, 4);
-      if (!ok || *abort_flag) { *abort_flag = 1; break; }
-      uint4* rp = (uint4*)(raw + s * STAGE_BYTES);
-      uint4* lp = (uint4*)(lo + q * STAGE_BYTES);
-#pragma unroll 4
-      for (int v = tid; v < STAGE_BYTES / 16; v += 128) {
-        const uint4 x = rp[v];
-        const uint4 h = make_uint4(tf32_round(x.x), tf32_round(x.y), tf32_round(x.z), tf32_round(x.w));
-        const uint4 l = make_uint4(tf32_round(tf32_residual(x.x, h.x)), tf32_round(tf32_residual(x.y, h.y)),
-                                   tf32_round(tf32_residual(x.z, h.z)), tf32_round(tf32_residual(x.w, h.w)));
-        rp[v] = h;
-        lp[v] = l;
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      mbar_arrive(&lofull[q]);
+    // ------------------------------------------------------------ epilogue (128 threads)
+    // The whole main loop passes here: poll with naps, and give up early when a producer aborted.
+    bool ok = false;
+    const unsigned long long t0 = now_ns();
+    for (;;) {
+      if (mbar_try(accfull, 0)) { ok = true; break; }
+      if (*abort_flag) break;
+      if (now_ns() - t0 > kWaitNs) { atomicCAS(args.err, 0, 5); break; }
+      __nanosleep(256);
     }
-    // ------------------------------------------------------------ epilogue
-    const bool ok = !*abort_flag && mbar_wait(accfull, 0, args.err, 5);
     if (ok) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int quad = warp % 4;
@@ -309,30 +305,67 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
 
 // Leg-aware pack: the same gather as k_pack_planar, for operands whose legs are scattered (as in
 // networks of dimension-2 legs).  The host picks tile legs -- those innermost in the source plus those
-// innermost in the packed destination, at most kPackTile elements -- and lists the tile twice: in
-// source-address order (rd_*) and in destination-address order (wr_*), so both the read and the write
-// of a tile walk memory contiguously.  Remaining legs are enumerated by src_base / dst_base.
+// innermost in the packed destination, at most kPackTile elements -- and numbers the tile's elements
+// by destination address.  rd_rank[i] / rd_off[i] give the element with the i-th smallest source
+// offset (its rank and its source offset), wr_off[r] the destination offset of rank r, so the read
+// and the write of a tile both walk memory in address order.  Remaining legs are enumerated by
+// src_base / dst_base.  Each thread keeps its share of the tables in registers; the tile is held as
+// separate re / im planes with an XOR-folded index, which spreads the scattered writes over banks.
 constexpr int kPackTile = 1024;
-static __global__ void __launch_bounds__(256) k_pack_tiled(const cf32* __restrict__ src, float* __restrict__ dst,
-                                                           const int* __restrict__ rd_elem, const int* __restrict__ rd_off,
-                                                           const int* __restrict__ wr_elem, const int* __restrict__ wr_off,
-                                                           int T, const ll* __restrict__ src_base,
-                                                           const ll* __restrict__ dst_base, ll n_outer, ll n_slices,
-                                                           ll dst_slice_stride, ll plane, SliceOff so, ll g0, int conj) {
-  __shared__ cf32 tile[kPackTile];
+constexpr int kPackThreads = 256;
+__device__ __forceinline__ int pack_swz(int e) { return e ^ ((e >> 5) & 31); }
+static __global__ void __launch_bounds__(kPackThreads) k_pack_tiled(
+    const cf32* __restrict__ src, float* __restrict__ dst, const int* __restrict__ rd_rank,
+    const int* __restrict__ rd_off, const int* __restrict__ wr_off, int T, const ll* __restrict__ src_base,
+    const ll* __restrict__ dst_base, ll n_outer, ll n_slices, ll dst_slice_stride, ll plane, SliceOff so, ll g0,
+    int conj) {
+  constexpr int PER = kPackTile / kPackThreads;
+  __shared__ float t_re[kPackTile], t_im[kPackTile];
   const float im_sign = conj ? -1.f : 1.f;
-  for (ll blk = blockIdx.x; blk < n_outer * n_slices; blk += gridDim.x) {
+  int rr[PER], ro[PER], wo[PER];
+#pragma unroll
+  for (int j = 0; j < PER; ++j) {
+    const int i = threadIdx.x + j * kPackThreads;
+    rr[j] = i < T ? pack_swz(rd_rank[i]) : 0;
+    ro[j] = i < T ? rd_off[i] : 0;
+    wo[j] = i < T ? wr_off[i] : 0;
+  }
+  const ll n_blk = n_outer * n_slices;
+  // Software pipeline: the loads of the next tile are in flight while this tile is written out.
+  auto load = [&](ll blk, cf32* v) {
     const ll s = blk / n_outer, o = blk - s * n_outer;
     const cf32* sb = src + slice_offset(so, g0, s) + src_base[o];
-    float* db = dst + s * dst_slice_stride + dst_base[o];
-    for (int i = threadIdx.x; i < T; i += blockDim.x) tile[rd_elem[i]] = sb[rd_off[i]];
+#pragma unroll
+    for (int j = 0; j < PER; ++j)
+      if (threadIdx.x + j * kPackThreads < T) v[j] = sb[ro[j]];
+  };
+  cf32 v[PER], nv[PER];
+  ll blk = blockIdx.x;
+  if (blk < n_blk) load(blk, v);
+  for (; blk < n_blk; blk += gridDim.x) {
+#pragma unroll
+    for (int j = 0; j < PER; ++j)
+      if (threadIdx.x + j * kPackThreads < T) {
+        t_re[rr[j]] = v[j].re;
+        t_im[rr[j]] = v[j].im;
+      }
     __syncthreads();
-    for (int i = threadIdx.x; i < T; i += blockDim.x) {
-      const cf32 v = tile[wr_elem[i]];
-      db[wr_off[i]] = v.re;
-      db[plane + wr_off[i]] = im_sign * v.im;
+    const ll next = blk + gridDim.x;
+    if (next < n_blk) load(next, nv);
+    const ll s = blk / n_outer, o = blk - s * n_outer;
+    float* db = dst + s * dst_slice_stride + dst_base[o];
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      const int i = threadIdx.x + j * kPackThreads;
+      if (i < T) {
+        const int e = pack_swz(i);
+        put_split(db, plane, wo[j], t_re[e]);
+        put_split(db + 2 * plane, plane, wo[j], im_sign * t_im[e]);
+      }
     }
     __syncthreads();
+#pragma unroll
+    for (int j = 0; j < PER; ++j) v[j] = nv[j];
   }
 }
 
@@ -385,8 +418,8 @@ static __global__ void __launch_bounds__(256) k_pack_planar(const cf32* __restri
       const ll r = r0 + u, c = c0 + tx;
       if (c < Kpad) {
         const ll o = (zz * Rpad + r) * Kpad + c;
-        dst[o] = tile[u][tx].re;
-        dst[plane + o] = im_sign * tile[u][tx].im;
+        put_split(dst, plane, o, tile[u][tx].re);
+        put_split(dst + 2 * plane, plane, o, im_sign * tile[u][tx].im);
       }
     }
     __syncthreads();

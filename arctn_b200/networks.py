@@ -187,3 +187,18 @@ def workload_grid8(bond=6, dtype=np.complex64, seed=0):
     """8x8 open grid, bond 6, complex64 N(0,1)/sqrt(6^rank), scalar output."""
     net = grid_2d(8, 8, bond)
     return net, gaussian_tensors(net, dtype, seed, scale_base=bond)
+
+
+def workload_batch(count=256, seed=0):
+    """Many uneven networks: random 3-regular graphs with n ~ U{20, 22, ..., 50} nodes and a bond
+    dimension ~ U{2, 3, 4} per network, entries N(0,1)/sqrt(bond^3); even-numbered networks are float32,
+    odd-numbered complex64.  Returns [(net, arrays)], graph j seeded by (seed, j)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for j in range(count):
+        n = int(rng.integers(10, 26)) * 2
+        bond = int(rng.integers(2, 5))
+        net = rand_regular(n, 3, bond, seed * 100003 + j)
+        dtype = np.float32 if j % 2 == 0 else np.complex64
+        out.append((net, gaussian_tensors(net, dtype, seed * 100003 + j, scale_base=bond)))
+    return out

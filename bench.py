@@ -41,7 +41,7 @@ sys.path.insert(0, ROOT)
 METRIC = "c64 sliced TN contraction TFLOP/s"
 KIND_NAMES = {0: "k_gather_reduce", 1: "k_gemm_small", 2: "k_gemm_tile<64,64>", 3: "k_gemm_tile<32,32>",
               4: "k_slice_accumulate", 5: "k_slice_output", 7: "k_maxabs", 8: "k_strip_scale",
-              9: "k_tc_cgemm_tf32x3", 10: "k_gemm_dot", 11: "k_pack_planar"}
+              9: "k_tc_cgemm_tf32x3", 10: "k_gemm_dot", 11: "k_pack_planar", 12: "k_scatter", 13: "k_pack_tiled"}
 GEMM_KINDS = {1, 2, 3, 9, 10}
 
 
@@ -56,9 +56,13 @@ def parse():
     ap.add_argument("--target-log2", type=int, default=24)
     ap.add_argument("--group", type=int, default=0, help="slices per group (0: as many as the workspace allows)")
     ap.add_argument("--workspace-gb", type=float, default=24.0)
+    ap.add_argument("--tc-k-chunk", type=int, default=0, help="K per tensor-core accumulator (0: library default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, the FP32 comparison and the FP64 check")
+    ap.add_argument("--workload", choices=["rand3reg", "grid6", "brickwork", "grid8", "batch"], default="rand3reg",
+                    help="rand3reg: the sliced headline (default); grid6 / brickwork: latency and precision; "
+                         "grid8: forward + adjoint; batch: 256 uneven networks in one graph launch")
     return ap.parse_args()
 
 
@@ -254,11 +258,269 @@ def timed(prog, x, ws, stream, steps, warmup, dist, dev, flush, clock=None):
     return total_ms / steps, r, (sampler.summary() if sampler else None)
 
 
+# ---------------------------------------------------------------------------------------------------
+# Other measured configurations (--workload).  Each prints one JSON line with the same base keys.
+
+
+def _line(args, metric, value, unit, hib, ms, config, dtype, **extra):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+         "ms_per_step": ms, "higher_is_better": hib, "scaling": "none", "vs_baseline": None, "dtype": dtype,
+         "data": "synthetic", "config": config}
+    d.update(extra)
+    return d
+
+
+def _events_ms(stream, fn):
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _cpu_time(fn, reps):
+    fn()
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+    return statistics.median(ts)
+
+
+def run_latency(args, dev, which):
+    """grid6 (6x6 grid, bond 4, c128) or brickwork (30 wires x depth 14, c64): microseconds per contraction,
+    plus the precision study (tf32x3 / fp32 / FP64 on the GPU, the FP32 CPU executor) for brickwork."""
+    import torch
+
+    import arctn_b200 as A
+    from arctn_b200 import networks as N
+    from oracle import oracle as O
+
+    if which == "grid6":
+        net, arrays = N.workload_grid6(np.complex128, seed=0)
+        dtype, precisions = np.complex128, ["fp32"]
+    else:
+        net, arrays = N.brickwork_circuit(30, 14, seed=0)
+        arrays = [a.astype(np.complex64) for a in arrays]
+        dtype, precisions = np.complex64, ["tf32x3", "fp32"]
+    path = A.greedy(*net.as_tuple())
+    O.build()
+    ref = complex(O.contract_sliced(*net.as_tuple(), path, [], [a.astype(np.complex128) for a in arrays]))
+    cpu_native = complex(O.contract_sliced(*net.as_tuple(), path, [], arrays))
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    x = [torch.from_numpy(a).to(dev) for a in arrays]
+    res = {}
+    for prec in precisions:
+        prog = A.SlicedProgram(*net.as_tuple(), path, (), dtype=dtype, precision=prec, device=dev.index)
+        ws = torch.empty(max(prog.workspace_bytes, 1), dtype=torch.uint8, device=dev)
+        out = torch.empty(prog.output_shape, dtype=torch.complex128 if dtype == np.complex128 else torch.complex64,
+                          device=dev)
+        for _ in range(max(args.warmup, 3)):
+            prog.execute(x, workspace=ws, stream=stream, out=out)
+        torch.cuda.synchronize(dev)
+        times = []
+        sampler = ClockSampler(dev.index)
+        with sampler:
+            for _ in range(args.steps):
+                flush.fill_(1)  # L2 flush between timed contractions
+                times.append(_events_ms(stream, lambda: prog.execute(x, workspace=ws, stream=stream, out=out)))
+        got = complex(out.item())
+        res[prec] = {"us": 1e3 * statistics.mean(times), "us_p50": 1e3 * statistics.median(times),
+                     "rel_err_vs_fp64": abs(got - ref) / abs(ref), "launches": prog.launches, "flops": prog.flops,
+                     "clocks": sampler.summary()}
+    if dtype == np.complex64:
+        c128 = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex128, device=dev.index)
+        g64 = complex(c128.execute([t.to(torch.complex128) for t in x]).item())
+        res["fp64_gpu_rel_err_vs_oracle"] = abs(g64 - ref) / abs(ref)
+    head = precisions[0]
+    host_in = [np.ascontiguousarray(a) for a in arrays]
+    prog = A.SlicedProgram(*net.as_tuple(), path, (), dtype=dtype, precision=head, device=dev.index)
+    prog.execute(host_in)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r = prog.execute(host_in)
+    e2e_us = (time.perf_counter() - t0) / args.steps * 1e6
+    cpu_s = _cpu_time(lambda: O.contract_sliced(*net.as_tuple(), path, [], arrays), 5)
+    name = "grid6x6_bond4_c128" if which == "grid6" else "brickwork_30x14_c64"
+    line = _line(args, f"{name} contraction latency", res[head]["us"], "us", False, res[head]["us"] / 1e3,
+                 {"workload": name, "n_tensors": len(net.inputs), "steps_in_path": len(path),
+                  "precision": head, "l2": "flushed (256 MiB write) before each timed contraction"},
+                 "c128" if dtype == np.complex128 else "c64",
+                 gpu_launches=res[head]["launches"] * args.steps,
+                 e2e={"value": e2e_us, "unit": "us", "h2d_bytes_per_step": int(sum(a.nbytes for a in host_in)),
+                      "d2h_bytes_per_step": int(np.asarray(r).nbytes)},
+                 roofline={"bound": "latency", "note": "launch/latency-bound: a few microseconds of work per step"},
+                 cpu_baseline={"value": cpu_s * 1e6, "unit": "us", "cores": 1, "kind": "port",
+                               "sample": "one full contraction, median of 5, oracle executor in the input dtype"},
+                 clocks=res[head]["clocks"], precisions=res, fp64_oracle=[ref.real, ref.imag],
+                 cpu_native_rel_err_vs_fp64=abs(cpu_native - ref) / abs(ref))
+    print(json.dumps(line), flush=True)
+
+
+def run_grid8(args, dev):
+    """8x8 grid, bond 6, c64: forward + adjoint (gradients of all 64 inputs) on the tensor cores."""
+    import torch
+
+    import arctn_b200 as A
+    from arctn_b200 import networks as N
+
+    net, arrays = N.workload_grid8(6, np.complex64, seed=0)
+    arrays = [a * np.float32(4.0) for a in arrays]  # lifts the ~1e-35 scalar off FP32's underflow range
+    path = A.greedy(*net.as_tuple())
+    x = [torch.from_numpy(a).to(dev) for a in arrays]
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def measure(prog):
+        ws = torch.empty(max(prog.workspace_bytes, 1), dtype=torch.uint8, device=dev)
+        out = torch.empty((), dtype=torch.complex64, device=dev)
+        g_out = torch.ones((), dtype=torch.complex64, device=dev)
+        for _ in range(max(args.warmup, 3)):
+            prog.gradient(x, g_out, part=1, workspace=ws, output=out, stream=stream)
+            prog.gradient(x, g_out, part=2, workspace=ws, stream=stream)
+        torch.cuda.synchronize(dev)
+        f, b = [], []
+        sampler = ClockSampler(dev.index)
+        with sampler:
+            for _ in range(args.steps):
+                flush.fill_(1)
+                f.append(_events_ms(stream, lambda: prog.gradient(x, g_out, part=1, workspace=ws, output=out,
+                                                                  stream=stream)))
+                b.append(_events_ms(stream, lambda: prog.gradient(x, g_out, part=2, workspace=ws, stream=stream)))
+        return statistics.mean(f), statistics.mean(b), sampler.summary(), ws
+
+    kw = dict(gradient=True, use_graph=False, device=dev.index)
+    p = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex64, precision="tf32x3", workspace_budget=40 << 30,
+                        **kw)
+    fwd_ms, bwd_ms, clocks, ws = measure(p)
+    status = p.device_status(ws)
+    del ws
+    o_tc, g_tc = p.gradient(x)
+    p64 = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex128, workspace_budget=40 << 30, **kw)
+    o64, g64 = p64.gradient([t.to(torch.complex128) for t in x])
+    pf = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex64, precision="fp32", workspace_budget=40 << 30,
+                         **kw)
+    o32, g32 = pf.gradient(x)
+    ref = complex(o64.item())
+
+    def norm_err(gs):
+        return max(float(torch.linalg.norm(a.to(torch.complex128) - b) / torch.linalg.norm(b)) for a, b in zip(gs, g64))
+
+    fwd32, bwd32, _, ws32 = measure(pf)
+    del ws32
+    del p64, pf
+    # Lowered budget: half the layout that keeps every intermediate -> the sweep recomputes.
+    pr = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex64, precision="tf32x3",
+                         workspace_budget=p.workspace_bytes // 2, **kw)
+    fwd_r, bwd_r, _, wsr = measure(pr)
+    o_r, g_r = pr.gradient(x, workspace=wsr)
+    identical = bool(torch.equal(o_r, o_tc)) and all(torch.equal(a, b) for a, b in zip(g_r, g_tc))
+    del wsr
+    flops_fwd = p.flops
+    total_ms = fwd_ms + bwd_ms
+    value = 3 * flops_fwd / (total_ms * 1e-3) / 1e12  # forward F + two adjoint GEMMs per step (2F)
+    tf32_alg_peak = peaks()["bf16_tflops"] / 2 / 3  # split-TF32 4M: 3 TF32 products per real product
+    line = _line(args, "grid8 bond6 c64 forward+adjoint TFLOP/s", value, "TFLOP/s", True, total_ms,
+                 {"workload": "grid8x8_bond6_c64_adjoint", "precision": "tf32x3", "inputs_scaled_by": 4,
+                  "l2": "flushed (256 MiB write) before each timed part"}, "c64",
+                 gpu_launches=p.launches * args.steps,
+                 e2e=None,
+                 roofline={"bound": "tensor", "achieved": value, "peak": tf32_alg_peak, "unit": "TFLOP/s",
+                           "frac": value / tf32_alg_peak,
+                           "peak_source": "measured bf16 dense burst / 2 (TF32) / 3 (split-TF32 products)",
+                           "traffic": None},
+                 cpu_baseline=None, clocks=clocks, device_status=status,
+                 fwd_ms=fwd_ms, bwd_ms=bwd_ms, bwd_over_fwd=bwd_ms / fwd_ms,
+                 fp32_fwd_ms=fwd32, fp32_bwd_ms=bwd32, speedup_vs_fp32=(fwd32 + bwd32) / total_ms,
+                 rel_err_scalar_vs_c128=abs(complex(o_tc.item()) - ref) / abs(ref),
+                 fp32_rel_err_scalar_vs_c128=abs(complex(o32.item()) - ref) / abs(ref),
+                 grad_norm_rel_err_max_vs_c128=norm_err(g_tc), fp32_grad_norm_rel_err_max_vs_c128=norm_err(g32),
+                 workspace_bytes=p.workspace_bytes,
+                 recompute={"workspace_bytes": pr.workspace_bytes, "recomputed_steps": pr.recomputed_steps,
+                            "fwd_ms": fwd_r, "bwd_ms": bwd_r, "bwd_over_fwd": bwd_r / fwd_r,
+                            "bit_identical_to_kept": identical})
+    print(json.dumps(line), flush=True)
+
+
+def run_batch(args, dev):
+    """256 uneven random 3-regular networks (half float32, half complex64): forward + adjoint of all of
+    them as one graph launch; networks/s, TFLOP/s and the per-network latency distribution."""
+    import torch
+
+    import arctn_b200 as A
+    from arctn_b200 import networks as N
+
+    nets = N.workload_batch(256, seed=0)
+    progs, xs = [], []
+    for net, arrays in nets:
+        path = A.greedy(*net.as_tuple())
+        progs.append(A.SlicedProgram(*net.as_tuple(), path, (), dtype=arrays[0].dtype, precision="tf32x3",
+                                     gradient=True, use_graph=False, device=dev.index))
+        xs.append([torch.from_numpy(a).to(dev) for a in arrays])
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    batch = A.ProgramBatch(progs, max_lanes=32)
+    ws = torch.empty(max(batch.workspace_bytes, 1), dtype=torch.uint8, device=dev)
+    for _ in range(max(args.warmup, 3)):
+        batch.gradient(xs, workspace=ws, stream=stream)
+    torch.cuda.synchronize(dev)
+    times = []
+    sampler = ClockSampler(dev.index)
+    with sampler:
+        for _ in range(args.steps):
+            flush.fill_(1)
+            times.append(_events_ms(stream, lambda: batch.gradient(xs, workspace=ws, stream=stream)))
+    status = batch.device_status(ws, stream)
+    ms = statistics.mean(times)
+    flops = sum(3 * p.flops for p in progs)
+    # Per-network latency: each network's forward + adjoint alone (graph-free program launches).
+    lat = []
+    for p, x in zip(progs, xs):
+        w = torch.empty(max(p.workspace_bytes, 1), dtype=torch.uint8, device=dev)
+        p.gradient(x, workspace=w, stream=stream)
+        lat.append(_events_ms(stream, lambda: p.gradient(x, workspace=w, stream=stream)))
+    lat.sort()
+    line = _line(args, "many-network forward+adjoint throughput", len(progs) / (ms * 1e-3), "networks/s", True, ms,
+                 {"workload": "256 random 3-regular networks, n in [20,50], bond in {2,3,4}, f32/c64 alternating",
+                  "lanes": batch.lanes, "precision": "tf32x3 (c64) / fp32 (f32)",
+                  "l2": "flushed (256 MiB write) before each timed batch"}, "f32+c64",
+                 gpu_launches=sum(p.launches for p in progs) * args.steps,
+                 e2e=None, roofline={"bound": "latency", "achieved_tflops": flops / (ms * 1e-3) / 1e12},
+                 cpu_baseline=None, clocks=sampler.summary(), device_status=status,
+                 tflops=flops / (ms * 1e-3) / 1e12,
+                 single_network_ms_p50=lat[len(lat) // 2], single_network_ms_p99=lat[min(len(lat) - 1,
+                                                                                         int(0.99 * len(lat)))],
+                 sum_of_single_network_ms=sum(lat), batch_speedup_vs_serial=sum(lat) / ms)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload != "rand3reg":
+        if rank != 0:
+            return
+        import torch
+
+        torch.cuda.set_device(local)
+        dev = torch.device("cuda", local)
+        if args.workload in ("grid6", "brickwork"):
+            run_latency(args, dev, args.workload)
+        elif args.workload == "grid8":
+            run_grid8(args, dev)
+        else:
+            run_batch(args, dev)
+        return
     net, arrays, path, sliced, name = workload(args.nodes, args.target_log2)
     if args.impl == "reference":
         run_reference(args, net, arrays, path, sliced, name, rank)
@@ -278,7 +540,7 @@ def main():
     total = 2 ** len(sliced)
     begin, end = slice_range(total, world, rank)
     common = dict(dtype=np.complex64, device=local, use_graph=True, workspace_budget=int(args.workspace_gb * (1 << 30)),
-                  max_slices_per_group=args.group)
+                  max_slices_per_group=args.group, tc_k_chunk=args.tc_k_chunk)
     if world > 1:
         common.update(slice_begin=begin, slice_end=end)
     prog = A.SlicedProgram(*net.as_tuple(), path, sliced, precision=args.precision, **common)

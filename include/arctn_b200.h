@@ -179,6 +179,9 @@ typedef struct {
   uint64_t slice_begin;          /* run only global slices [slice_begin, slice_end); both 0: all slices.  A */
   uint64_t slice_end;            /* partial range sums only its slices (one rank of a sharded contraction). */
   int gradient;                  /* also build the adjoint sweep (arctn_b200_program_gradient); unsliced only */
+  uint64_t tc_k_chunk;           /* tf32x3: longest K one tensor-core accumulator sums before the FP64 split-K
+                                    reduce (multiple of 16); 0: 512.  Shorter is more accurate, longer
+                                    moves fewer partial bytes. */
 } arctn_b200_program_options;
 
 /* Builds a program that contracts `net` along `ssa_path`, summing internal sliced legs and assembling
@@ -199,6 +202,11 @@ uint64_t arctn_b200_program_launches(const arctn_b200_program* program);
  * forward, chosen at creation (largest results first) so that the workspace fits workspace_budget.
  * 0 when everything fits.  No reference counterpart: the reference has no adjoint. */
 uint64_t arctn_b200_program_recomputed_steps(const arctn_b200_program* program);
+/* JSON description of the program's launch sequence and workspace layout (op kinds with their GEMM /
+ * pack / gather geometry, group size, recomputed steps).  Host-only: a program can be created and
+ * described on a machine without a GPU (its tables are then uploaded on the first execute).  Writes at
+ * most buf_bytes bytes including the terminating NUL; *needed receives the full size. */
+int arctn_b200_program_describe(const arctn_b200_program* program, char* buf, uint64_t buf_bytes, uint64_t* needed);
 
 /* Runs on `cuda_stream` (cudaStream_t; NULL = legacy default stream).  inputs[i] are contiguous device
  * tensors in net order; output receives the full output (native dtype).  The call is asynchronous. */
@@ -249,6 +257,29 @@ int arctn_b200_program_profile(arctn_b200_program* program, const void* const* i
  * `cuda_stream`. */
 int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, void* c, uint64_t bt, uint64_t m, uint64_t k,
                                     uint64_t n, void* cuda_stream);
+
+/* ------------------------------------------------------------ batches of independent programs
+ * No counterpart in the reference (it contracts one network per call).  A batch runs many programs --
+ * uneven networks, mixed dtypes -- as one CUDA graph launch: the programs are spread over up to
+ * max_lanes streams (longest first onto the least-loaded lane), each lane runs its programs in turn in
+ * one workspace region, and the lanes fork from and join back into cuda_stream.  The programs must
+ * outlive the batch and be bound to one device; a batch locks them while it launches. */
+typedef struct arctn_b200_batch arctn_b200_batch;
+int arctn_b200_batch_create(arctn_b200_program* const* programs, uint64_t n_programs, int max_lanes,
+                            arctn_b200_batch** batch_out);
+void arctn_b200_batch_destroy(arctn_b200_batch* batch);
+uint64_t arctn_b200_batch_workspace_size(const arctn_b200_batch* batch);
+uint64_t arctn_b200_batch_lanes(const arctn_b200_batch* batch);
+/* inputs[j] is program j's array of input device pointers, outputs[j] its output buffer.  Asynchronous. */
+int arctn_b200_batch_execute(arctn_b200_batch* batch, const void* const* const* inputs, void* const* outputs,
+                             void* workspace, uint64_t workspace_bytes, void* cuda_stream);
+/* Forward + adjoint of every program (all built with options.gradient = 1): grad_outputs[j] and grads[j]
+ * as in arctn_b200_program_gradient part 0.  Asynchronous. */
+int arctn_b200_batch_gradient(arctn_b200_batch* batch, const void* const* const* inputs,
+                              const void* const* grad_outputs, void* const* const* grads, void* const* outputs,
+                              void* workspace, uint64_t workspace_bytes, void* cuda_stream);
+/* Synchronises cuda_stream; *code = the first nonzero device error word of the last run, else 0. */
+int arctn_b200_batch_device_status(arctn_b200_batch* batch, void* workspace, void* cuda_stream, int* code);
 
 /* One-shot host-buffer call (the reference-facing e2e path of contract_sliced): copies host inputs to the
  * device, executes, copies the result back and synchronises.  Allocates its own device memory. */

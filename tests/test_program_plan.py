@@ -1,0 +1,121 @@
+"""Host-side program planning, checked without a GPU through arctn_b200_program_describe.
+
+A program builds its whole launch sequence and workspace layout on the host; these tests read that
+plan back: launch counts, the tensor-core / pack geometry, the adjoint's checkpoint recompute under a
+workspace budget, and option validation.
+"""
+
+import numpy as np
+import pytest
+
+import arctn_b200 as A
+from arctn_b200 import networks as N
+
+GEMM_KINDS = {"gemm_small", "gemm_tile64", "gemm_tile32", "gemm_dot", "gemm_tc"}
+
+
+def program(net, path, sliced=(), **kw):
+    return A.SlicedProgram(*net.as_tuple(), path, sliced, device=0, **kw)
+
+
+def test_describe_matches_counters_and_plan():
+    net = N.grid_2d(4, 4, 3)
+    path = A.greedy(*net.as_tuple())
+    p = program(net, path, dtype=np.complex128)
+    d = p.describe()
+    assert d["workspace_bytes"] == p.workspace_bytes
+    assert d["launches"] == p.launches == sum(o["kind"] != "memset" for o in d["ops"])
+    assert d["groups"] == 1 and d["n_slices"] == 1
+    gemms = [o for o in d["ops"] if o["kind"] in GEMM_KINDS]
+    assert len(gemms) == len(path)  # one GEMM per pairwise step
+    cc = A.CompiledContraction.compile(*net.as_tuple(), ssa_path=path)
+    dims = sorted(tuple(s.gemm_dims()) for s in cc.pair_steps())
+    assert sorted((o["bt"], o["m"], o["k"], o["n"]) for o in gemms) == dims
+
+
+def test_sliced_program_groups_and_flops():
+    net, _ = N.workload_rand3reg(64, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 8)
+    p = program(net, path, sliced, dtype=np.complex64, max_slices_per_group=16)
+    d = p.describe()
+    assert d["n_slices"] == 2 ** len(sliced)
+    assert d["slices_per_group"] == 16
+    assert d["groups"] == -(-d["n_slices"] // 16)
+    cc = A.CompiledContraction.compile(net.inputs, net.output,
+                                       {l: (1 if l in sliced else s) for l, s in net.size_dict.items()},
+                                       ssa_path=path)
+    per_slice = 8.0 * sum(a * b * c * e for a, b, c, e in (s.gemm_dims() for s in cc.pair_steps()))
+    assert p.flops == pytest.approx(per_slice * d["n_slices"], rel=1e-12)
+
+
+def test_tf32x3_packs_use_full_tiles_and_split_long_k():
+    net, _ = N.workload_rand3reg(172, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 24)
+    p = program(net, path, sliced, dtype=np.complex64, precision="tf32x3", max_slices_per_group=4)
+    ops = p.describe()["ops"]
+    tc = [o for o in ops if o["kind"] == "gemm_tc"]
+    packs = [o for o in ops if o["kind"] == "pack_tiled"]
+    assert tc and len(packs) == 2 * len(tc)
+    for o in tc:
+        assert o["m"] >= 96 and o["n"] >= 96 and o["k"] >= 32
+        assert o["splits"] == max(1, -(-o["k"] // 512))  # one accumulator sums at most K = 512
+    for o in packs:
+        assert o["rpad"] % 128 == 0 and o["kpad"] % 16 == 0 and 32 <= o["tile"] <= 1024
+    assert all(o["tile"] == 1024 for o in packs)  # dimension-2 legs always fill a tile
+    p256 = program(net, path, sliced, dtype=np.complex64, precision="tf32x3", max_slices_per_group=4, tc_k_chunk=256)
+    for o in (o for o in p256.describe()["ops"] if o["kind"] == "gemm_tc"):
+        assert o["splits"] == max(1, -(-o["k"] // 256))
+    fp32 = program(net, path, sliced, dtype=np.complex64, precision="fp32", max_slices_per_group=4)
+    assert not any(o["kind"] in ("gemm_tc", "pack_tiled", "pack") for o in fp32.describe()["ops"])
+
+
+def test_tc_k_chunk_must_be_a_multiple_of_16():
+    net = N.grid_2d(3, 3, 2)
+    path = A.greedy(*net.as_tuple())
+    with pytest.raises(ValueError, match="multiple of 16"):
+        program(net, path, dtype=np.complex64, precision="tf32x3", tc_k_chunk=100)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64, np.float64])
+def test_adjoint_recompute_under_budget(dtype):
+    net = N.grid_2d(5, 5, 3)
+    path = A.greedy(*net.as_tuple())
+    full = program(net, path, dtype=dtype, gradient=True)
+    small = program(net, path, dtype=dtype, gradient=True, workspace_budget=1)
+    df, ds = full.describe(), small.describe()
+    assert df["recomputed_steps"] == [] and full.recomputed_steps == 0
+    assert len(ds["recomputed_steps"]) == small.recomputed_steps >= 1
+    assert small.workspace_bytes < full.workspace_bytes
+    # the forward sweeps are identical; the reverse sweep re-runs each dropped step exactly once
+    fwd_f = [o for o in df["ops"][: df["backward_begin"]]]
+    fwd_s = [o for o in ds["ops"][: ds["backward_begin"]]]
+    assert [o["kind"] for o in fwd_f] == [o["kind"] for o in fwd_s]
+    n_gemm = lambda ops: sum(o["kind"] in GEMM_KINDS for o in ops)  # noqa: E731
+    bwd_f, bwd_s = df["ops"][df["backward_begin"]:], ds["ops"][ds["backward_begin"]:]
+    assert n_gemm(bwd_f) == 2 * len(path)
+    assert n_gemm(bwd_s) == 2 * len(path) + small.recomputed_steps
+    # a budget the full layout meets recomputes nothing
+    roomy = program(net, path, dtype=dtype, gradient=True, workspace_budget=full.workspace_bytes)
+    assert roomy.recomputed_steps == 0 and roomy.workspace_bytes == full.workspace_bytes
+
+
+def test_gradient_of_sliced_program_is_rejected_before_launch():
+    net, _ = N.workload_rand3reg(64, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 8)
+    with pytest.raises(ValueError, match="sliced"):
+        program(net, path, sliced, dtype=np.complex64, gradient=True)
+
+
+def test_batch_workload_generator():
+    nets = N.workload_batch(16, seed=3)
+    assert len(nets) == 16
+    for j, (net, arrays) in enumerate(nets):
+        n = len(net.inputs)
+        assert 20 <= n <= 50 and n % 2 == 0
+        bond = next(iter(net.size_dict.values()))
+        assert bond in (2, 3, 4) and all(v == bond for v in net.size_dict.values())
+        assert arrays[0].dtype == (np.float32 if j % 2 == 0 else np.complex64)
+        assert all(len(t) == 3 for t in net.inputs)
