@@ -6,6 +6,7 @@ fallback: executing without a CUDA device raises ``ValueError``.
 """
 
 from ._capi import ArcTNB200Error
+from .execution_plan import ExecutionPlan, PlanValidationError, load_tensors_bin, save_tensors_bin
 from .api import (
     ArcTNCompiledContraction,
     CompiledContraction,
@@ -28,6 +29,8 @@ from .api import (
 __all__ = [
     "ArcTNB200Error",
     "ArcTNCompiledContraction",
+    "ExecutionPlan",
+    "PlanValidationError",
     "CompiledContraction",
     "Finalize",
     "InputPrep",
@@ -37,6 +40,8 @@ __all__ = [
     "arctn_contract",
     "contract_sliced",
     "find_slices_to_size",
+    "load_tensors_bin",
+    "save_tensors_bin",
     "greedy",
     "linear_to_ssa",
     "simulate_path",

@@ -293,6 +293,37 @@ class SlicedProgram:
         self._keep = (call, ws)  # keep device buffers alive until the next call on this stream
         return _to_output(out, torch_mode)
 
+    def bind(self, arrays, out, workspace, stream=None, *, f64_out=False):
+        """A zero-argument callable that re-runs this program on fixed CUDA buffers.
+
+        All validation and pointer marshalling happen here, once; each call is one C-ABI call
+        (graph replay when ``use_graph``), for latency-bound callers that execute the same buffers
+        repeatedly.  The caller keeps ``arrays``, ``out`` and ``workspace`` alive.
+        """
+        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "bind failed")
+        if not torch_mode:
+            raise ValueError("bind failed: arrays must be CUDA torch tensors")
+        if code != self.code:
+            raise ValueError("bind failed: arrays dtype differs from the program's dtype")
+        want = _torch_dtype(code, wide=f64_out)
+        if tuple(out.shape) != tuple(self.output_shape) or out.dtype != want or not out.is_contiguous():
+            raise ValueError(f"bind failed: out must be a contiguous {want} tensor of shape {tuple(self.output_shape)}")
+        if workspace.numel() < self.workspace_bytes:
+            raise ValueError("bind failed: workspace is smaller than workspace_bytes")
+        torch = _torch()
+        st = stream if stream is not None else torch.cuda.current_stream(arrays[0].device)
+        ptrs = (ctypes.c_void_p * len(arrays))(*[t.data_ptr() for t in arrays])
+        fn = C.lib().arctn_b200_program_execute_f64out if f64_out else C.lib().arctn_b200_program_execute
+        h, o, w, nb, s = self._h, out.data_ptr(), workspace.data_ptr(), workspace.numel(), st.cuda_stream
+
+        def launch():
+            rc = fn(h, ptrs, o, w, nb, s)
+            if rc:
+                C.check(rc, "execute failed")
+
+        launch.keep = (arrays, out, workspace, ptrs, self)
+        return launch
+
     def gradient(self, arrays, grad_output=None, *, part=0, workspace=None, output=None, stream=None):
         """Adjoint sweep (programs built with ``gradient=True``).
 

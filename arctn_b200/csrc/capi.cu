@@ -178,6 +178,24 @@ int arctn_b200_find_slices_to_size(const arctn_b200_network* net, uint64_t n_ste
   });
 }
 
+int arctn_b200_slice_plan_check(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
+                                uint64_t n_sliced, const uint32_t* sliced_legs, uint64_t target_size,
+                                double per_slice_stats_out[6], int* fits_out) {
+  return guarded([&] {
+    if (n_sliced && !sliced_legs) fail("sliced_legs is null");
+    const Network n = to_network(net);
+    const SsaPath p = to_path(n_steps, ssa_path);
+    const std::vector<Leg> sl(sliced_legs, sliced_legs + n_sliced);
+    const PathStats s = sliced_path_stats(n, p, sl);
+    if (per_slice_stats_out) {
+      const double v[6] = {s.log10_flops, s.log2_max_size, s.log2_max_contraction_size, s.log2_total_size,
+                           s.log2_read_write, s.log2_peak_size};
+      for (int i = 0; i < 6; ++i) per_slice_stats_out[i] = v[i];
+    }
+    if (fits_out) *fits_out = target_size ? (slice_result_fits_target_size(n, p, sl, target_size) ? 1 : 0) : 1;
+  });
+}
+
 uint64_t arctn_b200_slice_parallel_chunks(uint64_t n_slices, uint64_t out_numel) {
   return slice_parallel_chunks(n_slices, out_numel);
 }

@@ -432,17 +432,47 @@ void validate_slice_legs(const Network& net, const std::vector<Leg>& sliced) {
   }
 }
 
+namespace {
+// Exact "product of dims <= target" without overflow (src/slice.rs:62-75).
+bool legs_fit(const Network& cur, const std::vector<Leg>& legs, u64 target) {
+  u64 rem = target;
+  for (Leg l : legs) {
+    u64 d = cur.dim(l);
+    if (d > rem) return false;
+    rem /= d;
+  }
+  return true;
+}
+}  // namespace
+
+bool path_fits_target_size(const Network& net, const SsaPath& path, u64 target) {
+  if (target == 0) fail("target_size must be greater than 0");
+  std::vector<std::vector<Leg>> sl;
+  simulate_path(net, path, &sl);
+  if (net.n_tensors() == 1) return legs_fit(net, net.output, target);
+  for (auto& legs : sl)
+    if (!legs_fit(net, legs, target)) return false;
+  return true;
+}
+
+PathStats sliced_path_stats(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced) {
+  validate_slice_legs(net, sliced);
+  Network cur = net;
+  for (Leg l : sliced) cur.size[l] = 1;
+  return simulate_path(cur, path);
+}
+
+bool slice_result_fits_target_size(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced,
+                                   u64 target) {
+  validate_slice_legs(net, sliced);
+  Network cur = net;
+  for (Leg l : sliced) cur.size[l] = 1;
+  return path_fits_target_size(cur, path, target);
+}
+
 bool find_slices_to_size(const Network& net, const SsaPath& path, u64 target, std::vector<Leg>& out) {
   if (target == 0) return false;
-  auto fits = [&](const Network& cur, const std::vector<Leg>& legs) {  // src/slice.rs:62-75
-    u64 rem = target;
-    for (Leg l : legs) {
-      u64 d = cur.dim(l);
-      if (d > rem) return false;
-      rem /= d;
-    }
-    return true;
-  };
+  auto fits = [&](const Network& cur, const std::vector<Leg>& legs) { return legs_fit(cur, legs, target); };
   std::vector<Leg> sliced;
   for (;;) {
     Network cur = net;

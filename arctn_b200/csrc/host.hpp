@@ -64,6 +64,13 @@ bool find_slices_to_size(const Network& net, const SsaPath& path, u64 target, st
 u64 slice_parallel_chunks(u64 n_slices, u64 out_numel);
 // src/slice.rs:152-176: uniqueness, presence and no repetition inside one input.
 void validate_slice_legs(const Network& net, const std::vector<Leg>& sliced);
+// Every intermediate of `path` holds at most `target` elements (src/slice.rs:102-111).
+bool path_fits_target_size(const Network& net, const SsaPath& path, u64 target);
+// Per-slice metrics: the path on the network with every sliced leg set to 1 (src/execution_plan.rs:879-890).
+PathStats sliced_path_stats(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced);
+// The same audit with the sliced legs removed first (src/slice.rs:114-130).
+bool slice_result_fits_target_size(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced,
+                                   u64 target);
 
 // ---------------------------------------------------------------- compiled plan
 // CompiledInputPrep (src/compiled.rs:33-75)

@@ -168,7 +168,7 @@ extern "C" int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, voi
   args.m_tiles = (int)(Ra / tc::BM);
   args.m_fast = Ra <= Rb ? 1 : 0;
   dim3 grid((unsigned)((Ra / tc::BM) * (Rb / tc::BN)), 1u, (unsigned)Z);
-  tc::k_tc_cgemm_tf32x3<<<grid, 192, tc::SMEM_BYTES, st>>>(ma, mb, args);
+  tc::k_tc_cgemm_tf32x3<<<grid, tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail_with(std::string("launch: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
   ab2::set_last_error("");

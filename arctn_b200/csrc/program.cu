@@ -42,11 +42,12 @@ namespace {
 
 constexpr u64 kAlign = 256;
 constexpr u64 kInf = ~0ull;
-// Tensor-core GEMMs accumulate at most this many 16-wide K tiles (K = 512) in one TMEM accumulator
-// unless the options give another chunk.  The tensor core's FP32 accumulation truncates once per
-// 8-wide MMA, so its error grows with the chain length; splits are summed in FP64.  Shorter chunks
-// buy accuracy with partial traffic and per-CTA overhead (K = 256 costs about 15% on long-K steps).
-constexpr int kSplitTiles = 32;
+// Split-K for tensor-core GEMMs.  Accuracy needs none (the kernel keeps TMEM chains short and sums
+// them in registers), so K is split only to fill the GPU: an unsliced GEMM with fewer than two tiles
+// per SM and a long K gets up to kFillSplits-fold more CTAs, each taking at least kMinSplitTiles
+// 16-wide K tiles; the FP32 partials are summed in FP64 in split order.
+constexpr int kNumSMs = 148;
+constexpr int kMinSplitTiles = 32;
 inline u64 align_up(u64 x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 // Per-slice strided view of a slot.
@@ -620,9 +621,17 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       const u64 pa = pack(A, (ll)m, rpa, conj_a);
       const u64 pb = pack(B, (ll)n, rpb, conj_b);
       touch(Ref{Ref::WS, pa}, ph2, opidx(ph2));
-      // K longer than kSplitTiles tiles is split across CTAs (see TcArgs): partials [split][z][m][n].
+      // K split across CTAs (see TcArgs): partials [split][z][m][n].  A caller's tc_k_chunk fixes the
+      // chunk; otherwise only a one-slice GEMM with too few tiles to fill the GPU is split.
       const int kt_total = (int)(kpad / tc::BK);
-      const int chunk = opt_.tc_k_chunk ? (int)(opt_.tc_k_chunk / tc::BK) : kSplitTiles;
+      int chunk = kt_total;
+      if (opt_.tc_k_chunk) {
+        chunk = (int)(opt_.tc_k_chunk / tc::BK);
+      } else if (!ph2) {
+        const ll ctas = (rpa / tc::BM) * (rpb / tc::BN) * (ll)bt;
+        const ll want = std::min<ll>((2 * kNumSMs + ctas - 1) / ctas, kt_total / kMinSplitTiles);
+        if (want >= 2) chunk = (int)((kt_total + want - 1) / want);
+      }
       if (kt_total > chunk) {
         g.kt_chunk = chunk;
         g.splits = (kt_total + chunk - 1) / chunk;
@@ -1185,7 +1194,7 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, const char* tab
   args.m_fast = mt <= nt ? 1 : 0;
   if (mt * nt > 0x7FFFFFFFll) throw Error(E_UNSUPPORTED, "tensor-core GEMM tile count exceeds the grid limit");
   dim3 grid((unsigned)(mt * nt), 1u, (unsigned)(zc * op.splits));
-  tc::k_tc_cgemm_tf32x3<<<grid, 192, tc::SMEM_BYTES, st>>>(ma, mb, args);
+  tc::k_tc_cgemm_tf32x3<<<grid, tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
   if (op.splits > 1) {
     const ll count = zc * op.m * op.n;
     tc::k_splitk_reduce<<<grid_for(count), 256, 0, st>>>((const cf32*)D, (cf32*)C, count, op.splits);

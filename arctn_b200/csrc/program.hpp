@@ -33,7 +33,7 @@ struct ProgramOptions {
   u64 workspace_budget = 0;
   u64 slice_begin = 0, slice_end = 0;  // both 0: every slice
   bool gradient = false;               // also build the adjoint (reverse) sweep
-  u64 tc_k_chunk = 0;                  // tf32x3: K per tensor-core accumulator (multiple of 16); 0: 512
+  u64 tc_k_chunk = 0;                  // tf32x3: K per CTA before a split-K reduce (multiple of 16); 0: auto
 };
 
 // Where an operand lives at run time.

@@ -9,12 +9,14 @@
 // the GEMM's shared memory serves only TMA writes and tensor-core reads.  The
 // 4M complex product is 12 TF32 MMAs per 8-wide K step into TMEM accumulators:
 //   Cr += Ar*Br - Ai*Bi,  Ci += Ar*Bi + Ai*Br   for (hi,hi), (hi,lo), (lo,hi),
-// the minus through the instruction's negate-A bit.  Accumulation is FP32.
+// the minus through the instruction's negate-A bit.  Accumulation is FP32: short
+// chains in TMEM, summed across chains in registers.
 //
-// Warp roles (192 threads, one CTA per 128x128 output tile):
+// Warp roles (320 threads, one CTA per 128x128 output tile):
 //   warp 0      TMA producer: 8 plane tiles per stage, 3-stage ring
-//   warp 1      TMEM allocation + single-thread MMA issue
-//   warps 2..5  epilogue (TMEM -> HBM)
+//   warp 1      TMEM allocation + single-thread MMA issue into two TMEM buffers
+//   warps 2..9  drain: each finished buffer -> FP32 registers (round-to-nearest adds),
+//               then the epilogue (registers -> HBM)
 // Every mbarrier wait is bounded (about one second of global time); on expiry
 // the kernel records a code in *err, drains what it issued and returns.
 #pragma once
@@ -33,10 +35,16 @@ constexpr int PLANES = 4;                          // re_hi, re_lo, im_hi, im_lo
 constexpr int PLANE_BYTES = BM * BK * 4;          // 8 KB: 128 rows x 64 B
 constexpr int STAGE_BYTES = 2 * PLANES * PLANE_BYTES;  // A planes then B planes: 64 KB
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*align*/;
-// Cr: [0,128), Ci: [128,256) take the (hi,hi) products; Cr', Ci': [256,384), [384,512) take the
-// (hi,lo) and (lo,hi) products, which are 2^-10 smaller, so the large accumulators see 4 of the 12
-// additions per K step and the rounding of each accumulation stays at the scale of its own sum.
+// Two TMEM buffers of (Cr, Ci), 128 columns each: buffer b at columns [256 b, 256 b + 256).  The MMA
+// thread fills one buffer with kChunkTiles K tiles (all 12 products per 8-wide K step) while the drain
+// warps read the other and add it into FP32 registers with round-to-nearest.  The tensor core's FP32
+// accumulation truncates once per MMA, so keeping each TMEM chain short (24 MMAs per accumulator at
+// kChunkTiles = 2) bounds that biased error; the long sum over K happens in the drain registers.
 constexpr uint32_t TMEM_COLS = 512;
+constexpr int kChunkTiles = 2;
+constexpr int kDrainWarps = 8, kDrainThreads = kDrainWarps * 32;
+constexpr int kThreads = 64 + kDrainThreads;  // TMA warp, MMA warp, drain warps
+constexpr int kHalfCols = BN / 2;             // columns one drain thread owns
 constexpr unsigned long long kWaitNs = 1000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -155,16 +163,43 @@ struct TcArgs {
   int m_fast = 1;
 };
 
-static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_constant__ CUtensorMap tmA,
-                                                          const __grid_constant__ CUtensorMap tmB, TcArgs args) {
+#define AB2_TMEM_LD16(taddr, r)                                                                                   \
+  asm volatile(                                                                                                   \
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"    \
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),          \
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])     \
+      : "r"(taddr))
+
+// Bounded wait for the drain warps: also gives up as soon as another role aborted.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, int* err, int code,
+                                                   volatile int* abort_flag) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = now_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try(bar, parity)) return true;
+    if ((i & 63) == 0) {
+      if (*abort_flag) return false;
+      if (now_ns() - t0 > kWaitNs) {
+        atomicCAS(err, 0, code);
+        return false;
+      }
+      __nanosleep(64);
+    }
+  }
+}
+
+static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __grid_constant__ CUtensorMap tmA,
+                                                                const __grid_constant__ CUtensorMap tmB,
+                                                                TcArgs args) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* ring = smem;                                  // STAGES x {A planes, B planes}
   uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
-  uint64_t* full = bars;                     // TMA landed          (count 1 + tx)
-  uint64_t* empty = bars + STAGES;           // MMAs done reading   (commit)
-  uint64_t* accfull = bars + 2 * STAGES;     // all MMAs done       (commit)
-  uint64_t* drain = accfull + 1;             // abort drain         (commit)
+  uint64_t* full = bars;                     // TMA landed                  (count 1 + tx)
+  uint64_t* empty = bars + STAGES;           // MMAs done reading a stage   (commit)
+  uint64_t* accfull = bars + 2 * STAGES;     // [2] a TMEM buffer's chunk is complete (commit)
+  uint64_t* accempty = accfull + 2;          // [2] the drain warps have read it      (count kDrainThreads)
+  uint64_t* drain = accempty + 2;            // abort drain                 (commit)
   volatile uint32_t* tmem_slot = (volatile uint32_t*)(drain + 1);
   volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
@@ -179,10 +214,12 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
   const int b_idx = z % args.bt;
   const int zA = args.a_var ? z : b_idx;
   const int zB = args.b_var ? z : b_idx;
+  const int KT = kt1 - kt0;                           // k-tile of iteration t is kt0 + t
+  const int n_chunks = (KT + kChunkTiles - 1) / kChunkTiles;
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < STAGES; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
-    mbar_init(accfull, 1);
+    for (int i = 0; i < 2; ++i) { mbar_init(&accfull[i], 1); mbar_init(&accempty[i], kDrainThreads); }
     mbar_init(drain, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -196,7 +233,6 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  const int KT = kt1 - kt0;  // pipeline iterations of this CTA; k-tile of iteration t is kt0 + t
 
   if (warp == 0) {
     // ------------------------------------------------------------ TMA producer
@@ -225,73 +261,90 @@ static __global__ void __launch_bounds__(192, 1) k_tc_cgemm_tf32x3(const __grid_
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
       const uint32_t id_pos = idesc_tf32(false), id_neg = idesc_tf32(true);
-      const uint32_t cr = tmem, ci = tmem + BN, crs = tmem + 2 * BN, cis = tmem + 3 * BN;
-      bool first = true;
-      for (int t = 0; t < KT && !*abort_flag; ++t) {
-        const int s = t % STAGES;
-        if (!mbar_wait(&full[s], (t / STAGES) & 1, args.err, 2)) { *abort_flag = 1; break; }
+      for (int c = 0; c < n_chunks && !*abort_flag; ++c) {
+        const int b = c & 1;
+        if (c >= 2 && !mbar_wait(&accempty[b], ((c >> 1) - 1) & 1, args.err, 6)) { *abort_flag = 1; break; }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a0 = smem_u32(ring + s * STAGE_BYTES), b0 = a0 + PLANES * PLANE_BYTES;
-        const uint32_t hAr = a0, lAr = a0 + PLANE_BYTES, hAi = a0 + 2 * PLANE_BYTES, lAi = a0 + 3 * PLANE_BYTES;
-        const uint32_t hBr = b0, lBr = b0 + PLANE_BYTES, hBi = b0 + 2 * PLANE_BYTES, lBi = b0 + 3 * PLANE_BYTES;
+        const uint32_t cr = tmem + b * 2 * BN, ci = cr + BN;
+        const int t_end = min(KT, (c + 1) * kChunkTiles);
+        bool first = true;
+        for (int t = c * kChunkTiles; t < t_end; ++t) {
+          const int s = t % STAGES;
+          if (!mbar_wait(&full[s], (t / STAGES) & 1, args.err, 2)) { *abort_flag = 1; break; }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a0 = smem_u32(ring + s * STAGE_BYTES), b0 = a0 + PLANES * PLANE_BYTES;
+          const uint32_t hAr = a0, lAr = a0 + PLANE_BYTES, hAi = a0 + 2 * PLANE_BYTES, lAi = a0 + 3 * PLANE_BYTES;
+          const uint32_t hBr = b0, lBr = b0 + PLANE_BYTES, hBi = b0 + 2 * PLANE_BYTES, lBi = b0 + 3 * PLANE_BYTES;
 #pragma unroll
-        for (int kk = 0; kk < BK / 8; ++kk) {
-          const uint32_t o = kk * 32;  // 8 tf32 = 32 bytes along the swizzled row
-          const uint32_t acc = first ? 0u : 1u;
-          // correction terms (lo,hi) and (hi,lo) into Cr', Ci'
-          umma(crs, sw64_desc(lAr + o), sw64_desc(hBr + o), id_pos, acc);
-          umma(cis, sw64_desc(lAr + o), sw64_desc(hBi + o), id_pos, acc);
-          umma(crs, sw64_desc(lAi + o), sw64_desc(hBi + o), id_neg, 1);
-          umma(cis, sw64_desc(lAi + o), sw64_desc(hBr + o), id_pos, 1);
-          umma(crs, sw64_desc(hAr + o), sw64_desc(lBr + o), id_pos, 1);
-          umma(cis, sw64_desc(hAr + o), sw64_desc(lBi + o), id_pos, 1);
-          umma(crs, sw64_desc(hAi + o), sw64_desc(lBi + o), id_neg, 1);
-          umma(cis, sw64_desc(hAi + o), sw64_desc(lBr + o), id_pos, 1);
-          // leading terms (hi,hi) into Cr, Ci
-          umma(cr, sw64_desc(hAr + o), sw64_desc(hBr + o), id_pos, acc);
-          umma(ci, sw64_desc(hAr + o), sw64_desc(hBi + o), id_pos, acc);
-          umma(cr, sw64_desc(hAi + o), sw64_desc(hBi + o), id_neg, 1);
-          umma(ci, sw64_desc(hAi + o), sw64_desc(hBr + o), id_pos, 1);
-          first = false;
+          for (int kk = 0; kk < BK / 8; ++kk) {
+            const uint32_t o = kk * 32;  // 8 tf32 = 32 bytes along the swizzled row
+            const uint32_t acc = first ? 0u : 1u;
+            // leading terms (hi,hi), then the corrections (lo,hi) and (hi,lo), all into this chunk's buffer
+            umma(cr, sw64_desc(hAr + o), sw64_desc(hBr + o), id_pos, acc);
+            umma(ci, sw64_desc(hAr + o), sw64_desc(hBi + o), id_pos, acc);
+            umma(cr, sw64_desc(hAi + o), sw64_desc(hBi + o), id_neg, 1);
+            umma(ci, sw64_desc(hAi + o), sw64_desc(hBr + o), id_pos, 1);
+            umma(cr, sw64_desc(lAr + o), sw64_desc(hBr + o), id_pos, 1);
+            umma(ci, sw64_desc(lAr + o), sw64_desc(hBi + o), id_pos, 1);
+            umma(cr, sw64_desc(lAi + o), sw64_desc(hBi + o), id_neg, 1);
+            umma(ci, sw64_desc(lAi + o), sw64_desc(hBr + o), id_pos, 1);
+            umma(cr, sw64_desc(hAr + o), sw64_desc(lBr + o), id_pos, 1);
+            umma(ci, sw64_desc(hAr + o), sw64_desc(lBi + o), id_pos, 1);
+            umma(cr, sw64_desc(hAi + o), sw64_desc(lBi + o), id_neg, 1);
+            umma(ci, sw64_desc(hAi + o), sw64_desc(lBr + o), id_pos, 1);
+            first = false;
+          }
+          umma_commit(&empty[s]);
         }
-        umma_commit(&empty[s]);
+        if (*abort_flag) break;
+        umma_commit(&accfull[b]);
       }
-      umma_commit(*abort_flag ? drain : accfull);
-      if (*abort_flag) mbar_wait(drain, 0, args.err, 8);
+      if (*abort_flag) {
+        umma_commit(drain);
+        mbar_wait(drain, 0, args.err, 8);
+      }
     }
   } else {
-    // ------------------------------------------------------------ epilogue (128 threads)
-    // The whole main loop passes here: poll with naps, and give up early when a producer aborted.
-    bool ok = false;
-    const unsigned long long t0 = now_ns();
-    for (;;) {
-      if (mbar_try(accfull, 0)) { ok = true; break; }
-      if (*abort_flag) break;
-      if (now_ns() - t0 > kWaitNs) { atomicCAS(args.err, 0, 5); break; }
-      __nanosleep(256);
+    // ------------------------------------------------------------ drain + epilogue (8 warps)
+    // Warp w reads TMEM lanes 32 * (w % 4) .. +31 (its output rows) and one half of the 128 columns.
+    const int quad = warp % 4, half = (warp - 2) / 4;
+    float acc_re[kHalfCols], acc_im[kHalfCols];
+#pragma unroll
+    for (int j = 0; j < kHalfCols; ++j) acc_re[j] = acc_im[j] = 0.f;
+    bool ok = true;
+    for (int c = 0; c < n_chunks; ++c) {
+      const int b = c & 1;
+      if (!mbar_wait_or_abort(&accfull[b], (c >> 1) & 1, args.err, 5, abort_flag)) {
+        ok = false;
+        *abort_flag = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + b * 2 * BN + half * kHalfCols;
+#pragma unroll
+      for (int c0 = 0; c0 < kHalfCols; c0 += 16) {
+        uint32_t vr[16], vi[16];
+        AB2_TMEM_LD16(ta + c0, vr);
+        AB2_TMEM_LD16(ta + BN + c0, vi);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          acc_re[c0 + j] += __uint_as_float(vr[j]);
+          acc_im[c0 + j] += __uint_as_float(vi[j]);
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(&accempty[b]);
     }
     if (ok) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int quad = warp % 4;
       const ll row = (ll)tile_m * BM + quad * 32 + lane;
-      cf32* crow = (args.part ? args.part + (ll)split * args.zc * args.m * args.n : args.C) +
-                   ((ll)z * args.m + row) * args.n;
-      for (int c0 = 0; c0 < BN; c0 += 32) {
-        uint32_t vr[32], vi[32], sr[32], si[32];
-        const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + c0;
-        AB2_TMEM_LD32(ta, vr);
-        AB2_TMEM_LD32(ta + BN, vi);
-        AB2_TMEM_LD32(ta + 2 * BN, sr);
-        AB2_TMEM_LD32(ta + 3 * BN, si);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (row < args.m) {
-          const ll col0 = (ll)tile_n * BN + c0;
+      if (row < args.m) {
+        cf32* crow = (args.part ? args.part + (ll)split * args.zc * args.m * args.n : args.C) +
+                     ((ll)z * args.m + row) * args.n;
+        const ll col0 = (ll)tile_n * BN + half * kHalfCols;
 #pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (col0 + j < args.n)
-              crow[col0 + j] = cf32{__uint_as_float(vr[j]) + __uint_as_float(sr[j]),
-                                    __uint_as_float(vi[j]) + __uint_as_float(si[j])};
-        }
+        for (int j = 0; j < kHalfCols; ++j)
+          if (col0 + j < args.n) crow[col0 + j] = cf32{acc_re[j], acc_im[j]};
       }
     }
   }

@@ -94,6 +94,13 @@ int arctn_b200_greedy(const arctn_b200_network* net, uint64_t* ssa_out, uint64_t
  * reference returns None. */
 int arctn_b200_find_slices_to_size(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
                                    uint64_t target_size, uint32_t* legs_out, uint64_t* n_legs_out, int* found);
+/* Audit of a saved slice plan (src/execution_plan.rs:817-890, src/slice.rs:102-130): validates the sliced
+ * legs (validate_slice_legs, src/slice.rs:152-176), writes the per-slice path metrics (sliced legs set to
+ * dimension 1; same order as arctn_b200_simulate_path) and, for target_size > 0, *fits_out = 1 when every
+ * per-slice intermediate holds at most target_size elements (exact integer test), else 0. */
+int arctn_b200_slice_plan_check(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
+                                uint64_t n_sliced, const uint32_t* sliced_legs, uint64_t target_size,
+                                double per_slice_stats_out[6], int* fits_out);
 /* Deterministic chunk count of sliced summation (src/slice.rs:893-905). */
 uint64_t arctn_b200_slice_parallel_chunks(uint64_t n_slices, uint64_t out_numel);
 
@@ -179,9 +186,8 @@ typedef struct {
   uint64_t slice_begin;          /* run only global slices [slice_begin, slice_end); both 0: all slices.  A */
   uint64_t slice_end;            /* partial range sums only its slices (one rank of a sharded contraction). */
   int gradient;                  /* also build the adjoint sweep (arctn_b200_program_gradient); unsliced only */
-  uint64_t tc_k_chunk;           /* tf32x3: longest K one tensor-core accumulator sums before the FP64 split-K
-                                    reduce (multiple of 16); 0: 512.  Shorter is more accurate, longer
-                                    moves fewer partial bytes. */
+  uint64_t tc_k_chunk;           /* tf32x3: K per CTA before an FP64 split-K reduce (multiple of 16); 0: all of K,
+                                    except unsliced GEMMs too small to fill the GPU, which split K to do so */
 } arctn_b200_program_options;
 
 /* Builds a program that contracts `net` along `ssa_path`, summing internal sliced legs and assembling

@@ -60,7 +60,7 @@ def test_tf32x3_packs_use_full_tiles_and_split_long_k():
     assert tc and len(packs) == 2 * len(tc)
     for o in tc:
         assert o["m"] >= 96 and o["n"] >= 96 and o["k"] >= 32
-        assert o["splits"] == max(1, -(-o["k"] // 512))  # one accumulator sums at most K = 512
+        assert o["splits"] == 1  # slice-batched GEMMs fill the GPU without splitting K
     for o in packs:
         assert o["rpad"] % 128 == 0 and o["kpad"] % 16 == 0 and 32 <= o["tile"] <= 1024
     assert all(o["tile"] == 1024 for o in packs)  # dimension-2 legs always fill a tile
@@ -69,6 +69,20 @@ def test_tf32x3_packs_use_full_tiles_and_split_long_k():
         assert o["splits"] == max(1, -(-o["k"] // 256))
     fp32 = program(net, path, sliced, dtype=np.complex64, precision="fp32", max_slices_per_group=4)
     assert not any(o["kind"] in ("gemm_tc", "pack_tiled", "pack") for o in fp32.describe()["ops"])
+
+
+def test_unsliced_small_tile_gemms_split_k_to_fill_the_gpu():
+    net, _ = N.workload_grid8(6, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    p = program(net, path, dtype=np.complex64, precision="tf32x3", gradient=True)
+    tc = [o for o in p.describe()["ops"] if o["kind"] == "gemm_tc"]
+    assert tc
+    for o in tc:
+        tiles = -(-o["m"] // 128) * -(-o["n"] // 128) * o["bt"]
+        k_tiles = -(-o["k"] // 16)
+        want = min(-(-2 * 148 // tiles), k_tiles // 32)
+        assert o["splits"] == (want if want >= 2 else 1), o
+    assert any(o["splits"] > 1 for o in tc)  # the adjoint's 1296 x 1296 x 46656 GEMM
 
 
 def test_tc_k_chunk_must_be_a_multiple_of_16():
