@@ -45,6 +45,8 @@ constexpr int kChunkTiles = 2;
 constexpr int kDrainWarps = 8, kDrainThreads = kDrainWarps * 32;
 constexpr int kThreads = 64 + kDrainThreads;  // TMA warp, MMA warp, drain warps
 constexpr int kHalfCols = BN / 2;             // columns one drain thread owns
+constexpr int kTileStride = BN + 1;           // staged output tile row stride (complex elements)
+static_assert(BM * kTileStride * 8 <= STAGES * STAGE_BYTES, "the output tile is staged in the operand ring");
 constexpr unsigned long long kWaitNs = 1000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -336,15 +338,26 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(&accempty[b]);
     }
+    // Epilogue through shared memory: the last drain completed after every MMA, so the operand ring
+    // is free.  Stage the 128 x 128 complex tile row-major (rows padded by one element against bank
+    // conflicts), then write it out with consecutive threads on consecutive columns.
+    asm volatile("bar.sync 1, %0;" ::"n"(kDrainThreads) : "memory");  // every drain warp is past its loads
     if (ok) {
-      const ll row = (ll)tile_m * BM + quad * 32 + lane;
-      if (row < args.m) {
-        cf32* crow = (args.part ? args.part + (ll)split * args.zc * args.m * args.n : args.C) +
-                     ((ll)z * args.m + row) * args.n;
-        const ll col0 = (ll)tile_n * BN + half * kHalfCols;
+      cf32* tile = reinterpret_cast<cf32*>(ring) + (quad * 32 + lane) * kTileStride + half * kHalfCols;
 #pragma unroll
-        for (int j = 0; j < kHalfCols; ++j)
-          if (col0 + j < args.n) crow[col0 + j] = cf32{acc_re[j], acc_im[j]};
+      for (int j = 0; j < kHalfCols; ++j) tile[j] = cf32{acc_re[j], acc_im[j]};
+    }
+    asm volatile("bar.sync 1, %0;" ::"n"(kDrainThreads) : "memory");
+    if (ok && !*abort_flag) {
+      const cf32* tile = reinterpret_cast<const cf32*>(ring);
+      cf32* cbase = (args.part ? args.part + (ll)split * args.zc * args.m * args.n : args.C) + (ll)z * args.m * args.n;
+      const ll row0 = (ll)tile_m * BM, col0 = (ll)tile_n * BN;
+      const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
+      const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
+      cbase += row0 * args.n + col0;
+      for (int e = threadIdx.x - 64; e < rows * BN; e += kDrainThreads) {
+        const int r = e / BN, c = e % BN;
+        if (c < cols) cbase[(ll)r * args.n + c] = tile[r * kTileStride + c];
       }
     }
   }
