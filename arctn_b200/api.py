@@ -378,12 +378,23 @@ class SlicedProgram:
         ws = workspace if workspace is not None else call.workspace(self.workspace_bytes)
         n = self.launches
         ms = (ctypes.c_float * n)()
-        kind = (ctypes.c_int * n)()
+        kind = (ctypes.c_int * n)(*([-1] * n))  # one entry per op; split ops hold two kernels
         work = (ctypes.c_double * n)()
-        with _torch().cuda.device(call.device):
-            C.check(C.lib().arctn_b200_program_profile(self._h, call.ptrs, out.data_ptr(), ws.data_ptr(), ws.numel(),
-                                                       call.stream.cuda_stream, ms, kind, work), "profile failed")
-        return list(ms), list(kind), list(work)
+        torch = _torch()
+        with torch.cuda.device(call.device):
+            if self.has_gradient:  # forward + reverse sweep, with ones as the incoming gradient
+                g = torch.ones(self.output_shape, dtype=_torch_dtype(code), device=call.device)
+                grads = [torch.empty_like(t) for t in call.tensors]
+                gptr = (ctypes.c_void_p * len(grads))(*[t.data_ptr() for t in grads])
+                C.check(C.lib().arctn_b200_program_profile_gradient(
+                    self._h, call.ptrs, g.data_ptr(), gptr, out.data_ptr(), ws.data_ptr(), ws.numel(),
+                    call.stream.cuda_stream, ms, kind, work), "profile failed")
+            else:
+                C.check(C.lib().arctn_b200_program_profile(self._h, call.ptrs, out.data_ptr(), ws.data_ptr(),
+                                                           ws.numel(), call.stream.cuda_stream, ms, kind, work),
+                        "profile failed")
+        used = [i for i in range(n) if kind[i] >= 0]
+        return [ms[i] for i in used], [kind[i] for i in used], [work[i] for i in used]
 
     def execute_stripped(self, arrays):
         """Mantissa tensor and decimal exponent (src/compiled.rs:376-441); unsliced programs only."""

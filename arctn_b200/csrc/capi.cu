@@ -473,6 +473,17 @@ int arctn_b200_program_profile(arctn_b200_program* p, const void* const* inputs,
   });
 }
 
+int arctn_b200_program_profile_gradient(arctn_b200_program* p, const void* const* inputs, const void* grad_output,
+                                        void* const* grads, void* output, void* workspace, uint64_t workspace_bytes,
+                                        void* cuda_stream, float* ms_out, int* kind_out, double* work_out) {
+  return guarded([&] {
+    if (!p || !inputs || !ms_out || !kind_out || !work_out) fail("null argument");
+    if (!p->p->has_gradient()) fail("the program was built without gradient support");
+    p->p->profile(inputs, output, workspace, workspace_bytes, (cudaStream_t)cuda_stream, ms_out, kind_out, work_out,
+                  grad_output, grads);
+  });
+}
+
 int arctn_b200_contract_sliced_host(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
                                     uint64_t n_sliced, const uint32_t* sliced_legs,
                                     const arctn_b200_program_options* options, const void* const* host_inputs,

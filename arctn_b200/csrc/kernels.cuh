@@ -215,6 +215,83 @@ __global__ void __launch_bounds__(256) k_gemm_dot(GemmArgs g) {
   }
 }
 
+// Long dot products split over CTAs: CTA (output o, part p) reduces k-range [p * chunk, ...) with the
+// same fixed tree as k_gemm_dot and stores the widened partial at part[o * parts + p]; k_dot_reduce then
+// adds each output's partials in part order in the wide type and rounds once.
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm_dot_part(GemmArgs g, ll chunk, int parts,
+                                                       typename Num<T>::wide* __restrict__ part) {
+  using A = typename Num<T>::acc;
+  __shared__ A red[256];
+  const T* Ap = (const T*)g.A;
+  const T* Bp = (const T*)g.B;
+  const ll mn = g.m * g.n, per_s = g.bt * mn, total = g.S * per_s;
+  for (ll blk = blockIdx.x; blk < total * parts; blk += gridDim.x) {
+    const ll idx = blk / parts, p = blk - idx * parts;
+    const ll s = idx / per_s;
+    ll r = idx - s * per_s;
+    const ll b = r / mn;
+    r -= b * mn;
+    const ll i = r / g.n, j = r - i * g.n;
+    const T* a = Ap + slice_offset(g.sa, g.g0, s) + g.aB[b] + g.aM[i];
+    const T* bb = Bp + slice_offset(g.sb, g.g0, s) + g.bB[b] + g.bN[j];
+    const ll l0 = p * chunk, l1 = l0 + chunk < g.k ? l0 + chunk : g.k;
+    A acc = Num<T>::zero();
+    for (ll l = l0 + threadIdx.x; l < l1; l += 256) Num<T>::fma(acc, cj(a[g.aK[l]], g.conj_a), cj(bb[g.bK[l]], g.conj_b));
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (threadIdx.x < w) red[threadIdx.x] = Num<T>::add(red[threadIdx.x], red[threadIdx.x + w]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blk] = Num<T>::widen(red[0]);
+    __syncthreads();
+  }
+}
+
+template <class T>
+__global__ void k_dot_reduce(const typename Num<T>::wide* __restrict__ part, T* __restrict__ C, ll total, int parts) {
+  using W = typename Num<T>::wide;
+  for (ll o = (ll)blockIdx.x * blockDim.x + threadIdx.x; o < total; o += (ll)gridDim.x * blockDim.x) {
+    W acc = Num<W>::zero();
+    for (int p = 0; p < parts; ++p) acc = Num<W>::add(acc, part[o * parts + p]);
+    C[o] = Num<T>::narrow(acc);
+  }
+}
+
+// Warp-wide butterfly reduction in a fixed order (xor 16, 8, 4, 2, 1): deterministic, lane 0 holds it.
+__device__ __forceinline__ float shfl_xor(float v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+__device__ __forceinline__ double shfl_xor(double v, int m) { return __shfl_xor_sync(0xffffffffu, v, m); }
+__device__ __forceinline__ cf32 shfl_xor(cf32 v, int m) { return {shfl_xor(v.re, m), shfl_xor(v.im, m)}; }
+__device__ __forceinline__ cf64 shfl_xor(cf64 v, int m) { return {shfl_xor(v.re, m), shfl_xor(v.im, m)}; }
+
+// Thin steps with a moderate k (k >= 64, an output too small for a tile kernel): one warp per output,
+// lanes striding over k, then a fixed butterfly.  Eight outputs per 256-thread CTA.
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm_warp(GemmArgs g) {
+  using A = typename Num<T>::acc;
+  const T* Ap = (const T*)g.A;
+  const T* Bp = (const T*)g.B;
+  T* Cp = (T*)g.C;
+  const int lane = threadIdx.x % 32;
+  const ll mn = g.m * g.n, per_s = g.bt * mn, total = g.S * per_s;
+  const ll warps = (ll)gridDim.x * (blockDim.x / 32);
+  for (ll idx = (ll)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; idx < total; idx += warps) {
+    const ll s = idx / per_s;
+    ll r = idx - s * per_s;
+    const ll b = r / mn;
+    r -= b * mn;
+    const ll i = r / g.n, j = r - i * g.n;
+    const T* a = Ap + slice_offset(g.sa, g.g0, s) + g.aB[b] + g.aM[i];
+    const T* bb = Bp + slice_offset(g.sb, g.g0, s) + g.bB[b] + g.bN[j];
+    A acc = Num<T>::zero();
+    for (ll l = lane; l < g.k; l += 32) Num<T>::fma(acc, cj(a[g.aK[l]], g.conj_a), cj(bb[g.bK[l]], g.conj_b));
+#pragma unroll
+    for (int w = 16; w > 0; w >>= 1) acc = Num<T>::add(acc, shfl_xor(acc, w));
+    if (lane == 0) Cp[idx] = acc;
+  }
+}
+
 // Dense-enough steps on the CUDA cores: TM x TN output tile per CTA, TK-deep
 // k-slabs staged through shared memory, (TM/16) x (TN/16) outputs per thread.
 // This is the plain-FP32 (or FP64) form of the step GEMM.

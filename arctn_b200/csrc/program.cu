@@ -44,10 +44,10 @@ constexpr u64 kAlign = 256;
 constexpr u64 kInf = ~0ull;
 // Split-K for tensor-core GEMMs.  Accuracy needs none (the kernel keeps TMEM chains short and sums
 // them in registers), so K is split only to fill the GPU: an unsliced GEMM with fewer than two tiles
-// per SM and a long K gets up to kFillSplits-fold more CTAs, each taking at least kMinSplitTiles
+// per SM and a long K gets enough CTAs to cover the SMs twice, each taking at least kMinSplitTiles
 // 16-wide K tiles; the FP32 partials are summed in FP64 in split order.
 constexpr int kNumSMs = 148;
-constexpr int kMinSplitTiles = 32;
+constexpr int kMinSplitTiles = 8;
 inline u64 align_up(u64 x) { return (x + kAlign - 1) / kAlign * kAlign; }
 
 // Per-slice strided view of a slot.
@@ -574,10 +574,33 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     g.c = out;
     g.conj_a = conj_a && dtype_complex(dt);
     g.conj_b = conj_b && dtype_complex(dt);
-    if (m >= 64 && n >= 64) g.kind = Op::GEMM_TILE64;
+    // A long K over an output too small to give every SM a tile would run serially on a few SMs in the
+    // tile kernels; one warp per output spreads the K loop over all of them instead.
+    const u64 tiles32 = ((m + 31) / 32) * ((n + 31) / 32) * bt;
+    const bool long_k_few_tiles = k >= 1024 && tiles32 < 2 * (u64)kNumSMs && bt * m * n <= (1u << 17);
+    if (long_k_few_tiles && bt * m * n <= 64 && k >= 2048) g.kind = Op::GEMM_DOT;
+    else if (long_k_few_tiles) g.kind = Op::GEMM_WARP;
+    else if (m >= 64 && n >= 64) g.kind = Op::GEMM_TILE64;
     else if (m >= 24 && n >= 24) g.kind = Op::GEMM_TILE32;
     else if (k >= 2048 && bt * m * n <= 64) g.kind = Op::GEMM_DOT;
-    const bool use_tc = opt_.precision == PREC_TF32X3 && dt == DT_C64 && m >= 96 && n >= 96 && k >= 32;
+    else if (k >= 64) g.kind = Op::GEMM_WARP;  // a serial k loop per thread would dominate
+    // Tensor cores for dense c64 steps; also for a small output side with a long K, where the padded
+    // tile wastes MMA work but the K split (below) still fills the GPU.
+    if (g.kind == Op::GEMM_DOT && k >= 16384) {
+      // Too few outputs for the SMs: split each dot over CTAs (at least 2048 of k per CTA).
+      const u64 outs = bt * m * n;
+      const u64 parts = std::min<u64>((2 * kNumSMs + outs - 1) / outs, k / 2048);
+      if (parts >= 2) {
+        g.splits = (int)parts;
+        g.kt_chunk = (int)((k + parts - 1) / parts);
+        const u64 pbuf = new_buf(ph2, parts * outs * wide_bytes(dt), opidx(ph2));
+        bufs[pbuf].fixed = ph2 && !(A.variant || B.variant);
+        g.d = Ref{Ref::WS, pbuf};
+        touch(g.d, ph2, opidx(ph2));
+      }
+    }
+    const bool use_tc = opt_.precision == PREC_TF32X3 && dt == DT_C64 && k >= 32 &&
+                        ((m >= 96 && n >= 96) || (std::min(m, n) >= 16 && k >= 256));
     if (use_tc) {
       const ll kpad = ((ll)k + tc::BK - 1) / tc::BK * tc::BK;
       const ll rpa = ((ll)m + tc::BM - 1) / tc::BM * tc::BM;
@@ -1021,9 +1044,10 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
   (void)fbuf;
 }
 
-u64 Program::launches() const {
+u64 Program::launches() const {  // kernels per execute: a split GEMM adds its reduce kernel
   u64 n = 0;
-  for (auto& op : ops_) n += op.kind != Op::MEMSET;
+  for (auto& op : ops_)
+    n += (op.kind != Op::MEMSET) + ((op.kind == Op::GEMM_TC || op.kind == Op::GEMM_DOT) && op.splits > 1);
   return n;
 }
 
@@ -1036,7 +1060,8 @@ inline int grid_for(ll total, int per_block = 256, int cap = 148 * 16) {
 }
 
 template <class T>
-void launch_typed(const Op& op, const void* A, const void* B, void* C, const char* tab, bool out_f64, cudaStream_t st) {
+void launch_typed(const Op& op, const void* A, const void* B, void* C, void* D, const char* tab, bool out_f64,
+                  cudaStream_t st) {
   using W = typename Num<T>::wide;
   auto T_ = [&](int i) { return (const ll*)(tab + op.tab[i]); };
   switch (op.kind) {
@@ -1050,6 +1075,7 @@ void launch_typed(const Op& op, const void* A, const void* B, void* C, const cha
     }
     case Op::GEMM_SMALL:
     case Op::GEMM_DOT:
+    case Op::GEMM_WARP:
     case Op::GEMM_TILE64:
     case Op::GEMM_TILE32: {
       GemmArgs g;
@@ -1063,9 +1089,17 @@ void launch_typed(const Op& op, const void* A, const void* B, void* C, const cha
         const ll total = op.S * op.bt * op.m * op.n;
         const size_t smem = op.k <= 1024 ? (size_t)(2 * op.k * sizeof(ll)) : 0;
         k_gemm_small<T><<<grid_for(total, 256, 148 * 32), 256, smem, st>>>(g);
+      } else if (op.kind == Op::GEMM_DOT && op.splits > 1) {
+        const ll total = op.S * op.bt * op.m * op.n;
+        k_gemm_dot_part<T><<<(int)std::min<ll>(total * op.splits, 148 * 16), 256, 0, st>>>(g, op.kt_chunk, op.splits,
+                                                                                        (W*)D);
+        k_dot_reduce<T><<<grid_for(total), 256, 0, st>>>((const W*)D, (T*)C, total, op.splits);
       } else if (op.kind == Op::GEMM_DOT) {
         const ll total = op.S * op.bt * op.m * op.n;
         k_gemm_dot<T><<<(int)std::min<ll>(total, 148 * 16), 256, 0, st>>>(g);
+      } else if (op.kind == Op::GEMM_WARP) {
+        const ll total = op.S * op.bt * op.m * op.n;
+        k_gemm_warp<T><<<(int)std::min<ll>((total + 7) / 8, 148 * 16), 256, 0, st>>>(g);
       } else if (op.kind == Op::GEMM_TILE64) {
         const ll tiles = ((op.n + 63) / 64) * ((op.m + 63) / 64) * op.S * op.bt;
         k_gemm_tile<T, 64, 64, 16><<<(int)std::min<ll>(tiles, 148 * 8), 256, 0, st>>>(g);
@@ -1227,10 +1261,10 @@ void Program::launch_op(const Op& op, const void* const* inputs, void* output, c
   }
   const bool out_f64 = out_f64_flag_;
   switch (opt_.dtype) {
-    case DT_F32: launch_typed<float>(op, ptr(op.a), ptr(op.b), ptr(op.c), dev_tab_, out_f64, st); break;
-    case DT_F64: launch_typed<double>(op, ptr(op.a), ptr(op.b), ptr(op.c), dev_tab_, out_f64, st); break;
-    case DT_C64: launch_typed<cf32>(op, ptr(op.a), ptr(op.b), ptr(op.c), dev_tab_, out_f64, st); break;
-    case DT_C128: launch_typed<cf64>(op, ptr(op.a), ptr(op.b), ptr(op.c), dev_tab_, out_f64, st); break;
+    case DT_F32: launch_typed<float>(op, ptr(op.a), ptr(op.b), ptr(op.c), ptr(op.d), dev_tab_, out_f64, st); break;
+    case DT_F64: launch_typed<double>(op, ptr(op.a), ptr(op.b), ptr(op.c), ptr(op.d), dev_tab_, out_f64, st); break;
+    case DT_C64: launch_typed<cf32>(op, ptr(op.a), ptr(op.b), ptr(op.c), ptr(op.d), dev_tab_, out_f64, st); break;
+    case DT_C128: launch_typed<cf64>(op, ptr(op.a), ptr(op.b), ptr(op.c), ptr(op.d), dev_tab_, out_f64, st); break;
   }
   CK(cudaGetLastError());
 }
@@ -1321,6 +1355,7 @@ double op_work(const Op& op, int dt) {
   switch (op.kind) {
     case Op::GEMM_SMALL:
     case Op::GEMM_DOT:
+    case Op::GEMM_WARP:
     case Op::GEMM_TC:
     case Op::GEMM_TILE64:
     case Op::GEMM_TILE32:
@@ -1337,12 +1372,19 @@ double op_work(const Op& op, int dt) {
 }  // namespace
 
 void Program::profile(const void* const* inputs, void* output, void* ws, u64 ws_bytes, cudaStream_t st, float* ms,
-                      int* kind, double* work) {
+                      int* kind, double* work, const void* grad_out, void* const* grads) {
   if (ws_bytes < ws_total_) throw Error(E_WORKSPACE, "workspace is smaller than required");
+  if (opt_.gradient) check_run(0, inputs, grad_out, grads, output);
   DeviceGuard guard(opt_.device);
   std::lock_guard<std::mutex> lk(mu_);
   ensure_tables();
   out_f64_flag_ = false;
+  grad_out_ = grad_out;
+  grads_ = grads;
+  struct Unbind {
+    Program* p;
+    ~Unbind() { p->grad_out_ = nullptr; p->grads_ = nullptr; }
+  } unbind{this};
   std::vector<cudaEvent_t> ev;
   for (size_t i = 0; i <= ops_.size(); ++i) {
     cudaEvent_t e;
@@ -1421,7 +1463,7 @@ void Program::execute_gradient(int part, const void* const* inputs, const void* 
 std::string Program::describe() const {
   static const char* names[] = {"gather",    "gemm_small", "gemm_tile64", "gemm_tile32", "slice_accumulate",
                                 "slice_output", "memset",  "maxabs",      "strip",       "gemm_tc",
-                                "gemm_dot",  "pack",       "scatter",     "pack_tiled"};
+                                "gemm_dot",  "pack",       "scatter",     "pack_tiled", "gemm_warp"};
   std::string s = "{\"workspace_bytes\":" + std::to_string(ws_total_) + ",\"n_slices\":" + std::to_string(n_total_) +
                   ",\"slices_per_group\":" + std::to_string(S_) + ",\"groups\":" + std::to_string(n_groups_) +
                   ",\"launches\":" + std::to_string(launches()) + ",\"gradient\":" + (opt_.gradient ? "true" : "false") +
@@ -1439,6 +1481,7 @@ std::string Program::describe() const {
     auto f = [&](const char* k, long long v) { s += std::string(",\"") + k + "\":" + std::to_string(v); };
     switch (op.kind) {
       case Op::GEMM_SMALL: case Op::GEMM_TILE64: case Op::GEMM_TILE32: case Op::GEMM_DOT: case Op::GEMM_TC:
+      case Op::GEMM_WARP:
         f("S", op.S); f("bt", op.bt); f("m", op.m); f("k", op.k); f("n", op.n);
         f("splits", op.splits); f("conj_a", op.conj_a); f("conj_b", op.conj_b);
         break;

@@ -45,7 +45,7 @@ struct Ref {
 struct Op {
   enum Kind : int {
     GATHER = 0, GEMM_SMALL = 1, GEMM_TILE64 = 2, GEMM_TILE32 = 3, ACCUM = 4, OUTPUT = 5, MEMSET = 6, MAXABS = 7,
-    STRIP = 8, GEMM_TC = 9, GEMM_DOT = 10, PACK = 11, SCATTER = 12, PACK_TILED = 13
+    STRIP = 8, GEMM_TC = 9, GEMM_DOT = 10, PACK = 11, SCATTER = 12, PACK_TILED = 13, GEMM_WARP = 14
   } kind;
   Ref a, b, c;
   u64 tab[6] = {0, 0, 0, 0, 0, 0};  // byte offsets of offset tables in the program's table buffer
@@ -82,9 +82,10 @@ class Program {
   void execute(const void* const* inputs, void* output, bool f64_out, void* ws, u64 ws_bytes, cudaStream_t st);
   void execute_stripped(const void* const* inputs, void* output, void* ws, u64 ws_bytes, cudaStream_t st,
                         double* exponent);
-  // Op-by-op run with an event between launches; per launch: ms, kind, algorithmic work.
+  // Op-by-op run with an event between launches; per launch: ms, kind, algorithmic work.  Gradient
+  // programs run forward + reverse and need grad_out / grads bound.
   void profile(const void* const* inputs, void* output, void* ws, u64 ws_bytes, cudaStream_t st, float* ms,
-               int* kind, double* work);
+               int* kind, double* work, const void* grad_out = nullptr, void* const* grads = nullptr);
   // Gradient programs: part 0 = forward (keeps intermediates in ws) + reverse sweep, 1 = forward only,
   // 2 = reverse sweep only (needs the ws of a preceding part-1 run and the same inputs).
   void execute_gradient(int part, const void* const* inputs, const void* grad_out, void* const* grads, void* output,

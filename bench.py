@@ -41,8 +41,9 @@ sys.path.insert(0, ROOT)
 METRIC = "c64 sliced TN contraction TFLOP/s"
 KIND_NAMES = {0: "k_gather_reduce", 1: "k_gemm_small", 2: "k_gemm_tile<64,64>", 3: "k_gemm_tile<32,32>",
               4: "k_slice_accumulate", 5: "k_slice_output", 7: "k_maxabs", 8: "k_strip_scale",
-              9: "k_tc_cgemm_tf32x3", 10: "k_gemm_dot", 11: "k_pack_planar", 12: "k_scatter", 13: "k_pack_tiled"}
-GEMM_KINDS = {1, 2, 3, 9, 10}
+              9: "k_tc_cgemm_tf32x3", 10: "k_gemm_dot", 11: "k_pack_planar", 12: "k_scatter", 13: "k_pack_tiled",
+              14: "k_gemm_warp"}
+GEMM_KINDS = {1, 2, 3, 9, 10, 14}
 
 
 def parse():
@@ -421,6 +422,15 @@ def run_grid8(args, dev):
     fwd32, bwd32, _, ws32 = measure(pf)
     del ws32
     del p64, pf
+    # Op-by-op event profile of forward + reverse: where each sweep's time goes, per kernel kind.
+    desc = p.describe()
+    n_fwd = sum(1 for o in desc["ops"][: desc["backward_begin"]] if o["kind"] != "memset")
+    ms_ops, kinds, _ = p.profile(x)
+    sweep = {"forward": {}, "backward": {}}
+    for i, (t, k) in enumerate(zip(ms_ops, kinds)):
+        d = sweep["forward" if i < n_fwd else "backward"].setdefault(KIND_NAMES.get(int(k), str(k)), [0, 0.0])
+        d[0] += 1
+        d[1] = round(d[1] + float(t), 3)
     # Lowered budget: half the layout that keeps every intermediate -> the sweep recomputes.
     pr = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex64, precision="tf32x3",
                          workspace_budget=p.workspace_bytes // 2, **kw)
@@ -448,6 +458,7 @@ def run_grid8(args, dev):
                  fp32_rel_err_scalar_vs_c128=abs(complex(o32.item()) - ref) / abs(ref),
                  grad_norm_rel_err_max_vs_c128=norm_err(g_tc), fp32_grad_norm_rel_err_max_vs_c128=norm_err(g32),
                  workspace_bytes=p.workspace_bytes,
+                 sweep_profile_ms=sweep,
                  recompute={"workspace_bytes": pr.workspace_bytes, "recomputed_steps": pr.recomputed_steps,
                             "fwd_ms": fwd_r, "bwd_ms": bwd_r, "bwd_over_fwd": bwd_r / fwd_r,
                             "bit_identical_to_kept": identical})

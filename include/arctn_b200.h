@@ -247,10 +247,17 @@ int arctn_b200_program_device_status(arctn_b200_program* program, void* workspac
  * `cuda_stream`, synchronises, and writes per-launch duration (ms), kind and algorithmic work (real flops
  * for GEMM kinds, bytes moved for the others).  Arrays hold arctn_b200_program_launches entries.
  * Kinds: 0 gather, 1 gemm_small, 2 gemm_tile64, 3 gemm_tile32, 4 slice_accumulate, 5 slice_output,
- * 7 maxabs, 8 strip, 9 gemm_tc. */
+ * 7 maxabs, 8 strip, 9 gemm_tc, 10 gemm_dot, 11 pack, 12 scatter, 13 pack_tiled, 14 gemm_warp. */
 int arctn_b200_program_profile(arctn_b200_program* program, const void* const* inputs, void* output, void* workspace,
                                uint64_t workspace_bytes, void* cuda_stream, float* ms_out, int* kind_out,
                                double* work_out);
+
+/* The same for a gradient program: forward + reverse sweep op by op, with grad_output and grads bound as in
+ * arctn_b200_program_gradient part 0.  No reference counterpart (the reference has no adjoint). */
+int arctn_b200_program_profile_gradient(arctn_b200_program* program, const void* const* inputs,
+                                        const void* grad_output, void* const* grads, void* output, void* workspace,
+                                        uint64_t workspace_bytes, void* cuda_stream, float* ms_out, int* kind_out,
+                                        double* work_out);
 
 /* No counterpart in the reference.  Batched complex64 GEMM C[b] = A[b] . B[b] (A: bt x m x k, B: bt x k x n,
  * C: bt x m x n, row-major complex64 device buffers) on the split-TF32 tensor-core path, for callers that
