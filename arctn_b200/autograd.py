@@ -19,17 +19,25 @@ from .api import SlicedProgram, _torch_code
 class _Contract(torch.autograd.Function):
     @staticmethod
     def forward(ctx, prog, *tensors):
+        ctx.prog = prog
+        ctx.save_for_backward(*tensors)
+        if prog.sliced_legs:
+            # Sliced: each slice group's reverse sweep reuses that group's workspace, so the backward
+            # reruns the forward with it (part 0); the forward here is a plain execute.
+            ctx.ws = None
+            return prog.execute(list(tensors))
         ws = torch.empty(max(prog.workspace_bytes, 1), dtype=torch.uint8, device=tensors[0].device)
         out, _ = prog.gradient(list(tensors), part=1, workspace=ws)
-        ctx.prog = prog
         ctx.ws = ws
-        ctx.save_for_backward(*tensors)
         return out
 
     @staticmethod
     def backward(ctx, grad_out):
         tensors = ctx.saved_tensors
-        _, grads = ctx.prog.gradient(list(tensors), grad_out.contiguous(), part=2, workspace=ctx.ws)
+        if ctx.prog.sliced_legs:
+            _, grads = ctx.prog.gradient(list(tensors), grad_out.contiguous(), part=0)
+        else:
+            _, grads = ctx.prog.gradient(list(tensors), grad_out.contiguous(), part=2, workspace=ctx.ws)
         ctx.ws = None
         return (None, *grads)
 
@@ -42,16 +50,19 @@ class Contraction:
     ``tensor.grad`` for every input that requires gradients.
     """
 
-    def __init__(self, inputs, output, size_dict, ssa_path, *, precision="fp32"):
+    def __init__(self, inputs, output, size_dict, ssa_path, *, sliced_legs=(), precision="fp32", **program_kw):
         self.args = (inputs, output, size_dict, ssa_path)
+        self.sliced_legs = tuple(sliced_legs)
         self.precision = precision
+        self.program_kw = program_kw
         self._programs = {}
 
     def program(self, dtype, device):
         key = (dtype, device)
         if key not in self._programs:
-            self._programs[key] = SlicedProgram(*self.args, (), dtype=_torch_code(dtype), precision=self.precision,
-                                                device=device, use_graph=False, gradient=True)
+            self._programs[key] = SlicedProgram(*self.args, self.sliced_legs, dtype=_torch_code(dtype),
+                                                precision=self.precision, device=device, use_graph=False,
+                                                gradient=True, **self.program_kw)
         return self._programs[key]
 
     def __call__(self, *tensors):
@@ -59,9 +70,9 @@ class Contraction:
         return _Contract.apply(self.program(t0.dtype, t0.device.index), *tensors)
 
 
-def contract(inputs, output, size_dict, ssa_path, *tensors, precision="fp32"):
+def contract(inputs, output, size_dict, ssa_path, *tensors, sliced_legs=(), precision="fp32"):
     """One-shot differentiable contraction (builds the program on every call)."""
-    return Contraction(inputs, output, size_dict, ssa_path, precision=precision)(*tensors)
+    return Contraction(inputs, output, size_dict, ssa_path, sliced_legs=sliced_legs, precision=precision)(*tensors)
 
 
 __all__ = ["Contraction", "contract"]

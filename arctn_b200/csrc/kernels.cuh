@@ -141,6 +141,29 @@ __global__ void k_scatter(const T* __restrict__ in, T* __restrict__ out, const l
   }
 }
 
+// Gradient of a sliced input: acc[sliceoff(s) + offE[e]] += G[s][e] in the wide type.  One thread per
+// element e walks the group's slices in order, so slices that share a sub-block (they differ only in
+// sliced legs the input does not hold) add up deterministically without atomics; distinct (slice
+// digits, e) pairs reach distinct targets because the input's index map is injective.
+template <class T>
+__global__ void k_grad_accum(const T* __restrict__ G, typename Num<T>::wide* __restrict__ acc,
+                             const ll* __restrict__ offE, ll n_e, ll S, SliceOff so, ll g0) {
+  using W = typename Num<T>::wide;
+  for (ll e = (ll)blockIdx.x * blockDim.x + threadIdx.x; e < n_e; e += (ll)gridDim.x * blockDim.x) {
+    const ll t = offE[e];
+    for (ll s = 0; s < S; ++s) {
+      W* dst = acc + slice_offset(so, g0, s) + t;
+      *dst = Num<W>::add(*dst, Num<T>::widen(G[s * n_e + e]));
+    }
+  }
+}
+
+template <class T>
+__global__ void k_narrow(const typename Num<T>::wide* __restrict__ in, T* __restrict__ out, ll n) {
+  for (ll i = (ll)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (ll)gridDim.x * blockDim.x)
+    out[i] = Num<T>::narrow(in[i]);
+}
+
 // ---------------------------------------------------------------- GEMM tables
 struct GemmArgs {
   const void* A;

@@ -278,7 +278,10 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     std::memcpy(host_tab_.data() + off, v.data(), v.size() * sizeof(int));
     return off;
   };
-  auto emit = [&](bool phase2, const Op& op, bool also_strip) {
+  std::vector<Op> ops3;  // after every group: the sliced adjoint's input-gradient finish
+  auto emit = [&](bool phase2, const Op& op0, bool also_strip) {
+    Op op = op0;
+    op.bwd = !fwd;
     if (phase2) ops2.push_back(op);
     else {
       ops1.push_back(op);
@@ -785,7 +788,10 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
   // for C = A.B:  dA = dC . conj(B)^T,  dB = conj(A)^T . dC, mapped back through the step's permutes,
   // broadcast over the legs the step summed away, then through the input traces / diagonals.
   if (opt_.gradient) {
-    if (sliced_) throw Error(E_UNSUPPORTED, "gradients of sliced contractions are not supported by this build");
+    // Sliced programs run the reverse sweep inside every slice group, right after that group's forward
+    // (phase 2, batched over the group's slices); each input's per-slice gradients then accumulate in
+    // a wide buffer that is narrowed into the caller's gradient after the last group.
+    const bool bph = sliced_;
     fwd = false;
     bwd_begin_ = ops1.size();
     // Forward values the sweep reads stay alive through the last op that reads them (touch).  Step
@@ -807,16 +813,19 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     };
     auto dropped = [&](size_t slot) { return slot >= plan_.n_inputs && drop_.count(slot - plan_.n_inputs) > 0; };
     std::vector<View> dv(n_slots);
+    // A contiguous per-slice gradient buffer (one copy per slice of the group when sliced).
     auto contiguous = [&](u64 buf, const std::vector<u64>& shape) {
       View v;
       v.ref = Ref{Ref::WS, buf};
       v.shape = shape;
       v.strides = rm_strides(shape);
-      v.so.local_stride = 0;
+      v.so.local_stride = bph ? (ll)prod(shape) : 0;
       v.so.n = 0;
+      v.variant = bph;
       return v;
     };
     // Final slot: the incoming gradient broadcast over finalize's summed legs, permuted to slot order.
+    // A sliced program reads each slice's block of grad_output through its output-leg digits.
     {
       const auto& shp = fin.input_shape;
       auto full_st = rm_strides(full_out_shape);
@@ -829,7 +838,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         st[k2[j]] = full_st[q];
       }
       const u64 numel = prod(shp);
-      const u64 b = new_buf(false, numel * eb, opidx(false));
+      const u64 b = new_buf(bph, numel * eb, opidx(bph));
       Op g{Op::GATHER};
       g.a = Ref{Ref::GRAD_OUT, 0};
       g.c = Ref{Ref::WS, b};
@@ -837,7 +846,17 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       g.tab[1] = tab_ll({0});
       g.n_out = (ll)numel;
       g.n_red = 1;
-      emit(false, g, false);
+      if (bph) {
+        g.sa.local_stride = 0;
+        g.sa.n = 0;
+        for (size_t q = 0; q < net.output.size(); ++q) {
+          if (!sl.count(net.output[q])) continue;
+          if (g.sa.n >= kMaxSliceTerms) throw Error(E_UNSUPPORTED, "too many sliced output legs for the adjoint");
+          const auto dm = decode.at(net.output[q]);
+          g.sa.t[g.sa.n++] = SliceTerm{dm.first, dm.second, full_st[q]};
+        }
+      }
+      emit(bph, g, false);
       dv[fin.slot] = contiguous(b, shp);
     }
     // Scatter a GEMM result laid out in `order` dims (rm strides) back into a slot's own leg order,
@@ -853,7 +872,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         st[k2[j]] = src_st[p];
       }
       const u64 numel = prod(slot_shape);
-      const u64 b = new_buf(false, numel * eb, opidx(false));
+      const u64 b = new_buf(bph, numel * eb, opidx(bph));
       Op g{Op::GATHER};
       g.a = Ref{Ref::WS, src_buf};
       g.c = Ref{Ref::WS, b};
@@ -861,8 +880,10 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       g.tab[1] = tab_ll({0});
       g.n_out = (ll)numel;
       g.n_red = 1;
-      touch(g.a, false, opidx(false));
-      emit(false, g, false);
+      g.sa.local_stride = bph ? (ll)prod(order_dims) : 0;
+      g.sa.n = 0;
+      touch(g.a, bph, opidx(bph));
+      emit(bph, g, false);
       return contiguous(b, slot_shape);
     };
     for (size_t s = plan_.steps.size(); s-- > 0;) {
@@ -882,32 +903,66 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
                  dcN = legs_of(rsh, rst, nb + nfa, rsh.size());
       // dA' [batch, free_a, con] = dC [batch, free_a, free_b] . conj(B') [batch, con, free_b]^T
       {
-        Operand a = make_operand(dC.ref, dC.so, false, dcB, dcM, dcN);
+        Operand a = make_operand(dC.ref, dC.so, dC.variant, dcB, dcM, dcN);
         Operand b = swap_rk(rec.b);
-        b.variant = false;
-        const u64 tbuf = new_buf(false, prod({st.bt, st.m, st.k}) * eb, opidx(false));
-        emit_gemm(false, a, b, st.bt, st.m, st.n, st.k, Ref{Ref::WS, tbuf}, false, true);
+        const u64 tbuf = new_buf(bph, prod({st.bt, st.m, st.k}) * eb, opidx(bph));
+        emit_gemm(bph, a, b, st.bt, st.m, st.n, st.k, Ref{Ref::WS, tbuf}, false, true);
         dv[st.left_slot] = to_slot(tbuf, rec.da, st.a_perm, st.sum_a, st.left_shape);
       }
       // dB' [batch, con, free_b] = conj(A') [batch, free_a, con]^T . dC [batch, free_a, free_b]
       {
         Operand a = swap_rk(rec.a);
-        a.variant = false;
-        Operand b = make_operand(dC.ref, dC.so, false, dcB, dcN, dcM);
-        const u64 tbuf = new_buf(false, prod({st.bt, st.k, st.n}) * eb, opidx(false));
-        emit_gemm(false, a, b, st.bt, st.k, st.m, st.n, Ref{Ref::WS, tbuf}, true, false);
+        Operand b = make_operand(dC.ref, dC.so, dC.variant, dcB, dcN, dcM);
+        const u64 tbuf = new_buf(bph, prod({st.bt, st.k, st.n}) * eb, opidx(bph));
+        emit_gemm(bph, a, b, st.bt, st.k, st.m, st.n, Ref{Ref::WS, tbuf}, true, false);
         dv[st.right_slot] = to_slot(tbuf, rec.db, st.b_perm, st.sum_b, st.right_shape);
       }
     }
     // Inputs: copy to the caller's gradient buffers, or scatter through an input's traces / diagonals.
+    // Sliced: accumulate every slice's gradient of the (prepared) input into a wide buffer first.
     for (size_t i = 0; i < net.n_tensors(); ++i) {
       const View& d = dv[i];
       std::vector<u64> shape0;
       for (Leg l : net.inputs[i]) shape0.push_back(net.dim(l));
       const u64 numel0 = prod(shape0);
-      if (prep_gather[i].kind != Op::GATHER) {
+      const bool traced = prep_gather[i].kind == Op::GATHER;
+      Ref src = d.ref;  // gradient of the prepared input: per slice (sliced) or whole
+      if (bph) {
+        // Prepared full shape (sliced axes included): the input itself, or the materialised prep.
+        const u64 prep_numel = traced ? (u64)prep_gather[i].n_out : numel0;
+        const u64 acc = new_buf(false, prep_numel * wide_bytes(dt), 0);
+        bufs[acc].last = kInf;
+        Op z{Op::MEMSET};
+        z.c = Ref{Ref::WS, acc};
+        z.bytes = prep_numel * wide_bytes(dt);
+        emit(false, z, false);
+        Op ga{Op::GRAD_ACCUM};
+        ga.a = d.ref;
+        ga.c = Ref{Ref::WS, acc};
+        ga.sa = view[i].so;  // the input's slice terms over its prepared layout
+        ga.tab[0] = tab_ll(offsets(view[i].shape, view[i].strides));
+        ga.n_e = (ll)prod(view[i].shape);
+        touch(ga.a, true, opidx(true));
+        emit(true, ga, false);
+        Op nw{Op::NARROW};
+        nw.a = Ref{Ref::WS, acc};
+        nw.n_out = (ll)prep_numel;
+        if (!traced) {
+          nw.c = Ref{Ref::GRADS, i};
+          nw.bwd = true;
+          ops3.push_back(nw);
+          continue;
+        }
+        const u64 pb = new_buf(false, prep_numel * eb, 0);
+        bufs[pb].last = kInf;
+        nw.c = Ref{Ref::WS, pb};
+        nw.bwd = true;
+        ops3.push_back(nw);
+        src = Ref{Ref::WS, pb};
+      }
+      if (!traced) {
         Op g{Op::GATHER};
-        g.a = d.ref;
+        g.a = src;
         g.c = Ref{Ref::GRADS, i};
         g.tab[0] = tab_ll(offsets(shape0, rm_strides(shape0)));
         g.tab[1] = tab_ll({0});
@@ -919,13 +974,20 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         Op z{Op::MEMSET};
         z.c = Ref{Ref::GRADS, i};
         z.bytes = numel0 * eb;
-        emit(false, z, false);
+        z.bwd = true;
         Op sc = prep_gather[i];
         sc.kind = Op::SCATTER;
-        sc.a = d.ref;
+        sc.a = src;
         sc.c = Ref{Ref::GRADS, i};
-        touch(sc.a, false, opidx(false));
-        emit(false, sc, false);
+        sc.bwd = true;
+        if (bph) {
+          ops3.push_back(z);
+          ops3.push_back(sc);
+        } else {
+          emit(false, z, false);
+          touch(sc.a, false, opidx(false));
+          emit(false, sc, false);
+        }
       }
     }
   }
@@ -1040,6 +1102,10 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     out.n_chunks = (ll)n_chunks_;
     out.n_e = (ll)n_e;
     ops_.push_back(out);
+    for (Op op : ops3) {
+      finish(op);
+      ops_.push_back(op);
+    }
   }
   (void)fbuf;
 }
@@ -1124,6 +1190,12 @@ void launch_typed(const Op& op, const void* A, const void* B, void* C, void* D, 
     }
     case Op::MAXABS:
       k_maxabs<T><<<grid_for(op.n_out), 256, 0, st>>>((const T*)C, op.n_out, (unsigned long long*)A);
+      break;
+    case Op::GRAD_ACCUM:
+      k_grad_accum<T><<<grid_for(op.n_e), 256, 0, st>>>((const T*)A, (W*)C, T_(0), op.n_e, op.S, op.sa, op.g0);
+      break;
+    case Op::NARROW:
+      k_narrow<T><<<grid_for(op.n_out), 256, 0, st>>>((const W*)A, (T*)C, op.n_out);
       break;
     case Op::SCATTER:
       k_scatter<T><<<grid_for(op.n_out * op.n_red), 256, 0, st>>>((const T*)A, (T*)C, T_(0), T_(1), op.n_out, op.n_red);
@@ -1299,8 +1371,9 @@ void Program::execute(const void* const* inputs, void* output, bool f64_out, voi
   std::lock_guard<std::mutex> lk(mu_);
   ensure_tables();
   out_f64_flag_ = f64_out;
-  if (opt_.gradient) {  // plain execute of a gradient program: the forward part only
-    for (size_t i = 0; i < bwd_begin_; ++i) launch_op(ops_[i], inputs, output, (char*)ws, st);
+  if (opt_.gradient) {  // plain execute of a gradient program: the forward ops only
+    for (const Op& op : ops_)
+      if (!op.bwd) launch_op(op, inputs, output, (char*)ws, st);
     return;
   }
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -1417,13 +1490,13 @@ void Program::profile(const void* const* inputs, void* output, void* ws, u64 ws_
 
 u64 Program::forward_launches() const {
   u64 n = 0;
-  for (size_t i = 0; i < std::min(bwd_begin_, ops_.size()); ++i) n += ops_[i].kind != Op::MEMSET;
+  for (const Op& op : ops_) n += !op.bwd && op.kind != Op::MEMSET;
   return n;
 }
 
 u64 Program::backward_launches() const {
   u64 n = 0;
-  for (size_t i = bwd_begin_; i < ops_.size(); ++i) n += ops_[i].kind != Op::MEMSET;
+  for (const Op& op : ops_) n += op.bwd && op.kind != Op::MEMSET;
   return n;
 }
 
@@ -1448,9 +1521,12 @@ void Program::execute_gradient(int part, const void* const* inputs, const void* 
   out_f64_flag_ = false;
   grad_out_ = grad_out;
   grads_ = grads;
-  const size_t lo = part == 2 ? bwd_begin_ : 0, hi = part == 1 ? bwd_begin_ : ops_.size();
+  if (sliced_ && part != 0)
+    throw Error(E_UNSUPPORTED, "a sliced gradient program runs forward and reverse together (part 0): each slice "
+                               "group's reverse sweep reuses that group's workspace");
   try {
-    for (size_t i = lo; i < hi; ++i) launch_op(ops_[i], inputs, output, (char*)ws, st);
+    for (const Op& op : ops_)
+      if (part == 0 || (part == 1) == !op.bwd) launch_op(op, inputs, output, (char*)ws, st);
   } catch (...) {
     grad_out_ = nullptr;
     grads_ = nullptr;
@@ -1463,7 +1539,8 @@ void Program::execute_gradient(int part, const void* const* inputs, const void* 
 std::string Program::describe() const {
   static const char* names[] = {"gather",    "gemm_small", "gemm_tile64", "gemm_tile32", "slice_accumulate",
                                 "slice_output", "memset",  "maxabs",      "strip",       "gemm_tc",
-                                "gemm_dot",  "pack",       "scatter",     "pack_tiled", "gemm_warp"};
+                                "gemm_dot",  "pack",       "scatter",     "pack_tiled", "gemm_warp",  "grad_accum",
+                                "narrow"};
   std::string s = "{\"workspace_bytes\":" + std::to_string(ws_total_) + ",\"n_slices\":" + std::to_string(n_total_) +
                   ",\"slices_per_group\":" + std::to_string(S_) + ",\"groups\":" + std::to_string(n_groups_) +
                   ",\"launches\":" + std::to_string(launches()) + ",\"gradient\":" + (opt_.gradient ? "true" : "false") +
@@ -1477,7 +1554,7 @@ std::string Program::describe() const {
   s += "],\"ops\":[";
   for (size_t i = 0; i < ops_.size(); ++i) {
     const Op& op = ops_[i];
-    s += std::string(i ? "," : "") + "{\"kind\":\"" + names[(int)op.kind] + "\"";
+    s += std::string(i ? "," : "") + "{\"kind\":\"" + names[(int)op.kind] + "\"" + (op.bwd ? ",\"bwd\":1" : "");
     auto f = [&](const char* k, long long v) { s += std::string(",\"") + k + "\":" + std::to_string(v); };
     switch (op.kind) {
       case Op::GEMM_SMALL: case Op::GEMM_TILE64: case Op::GEMM_TILE32: case Op::GEMM_DOT: case Op::GEMM_TC:
@@ -1504,6 +1581,8 @@ void Program::check_run(int part, const void* const* inputs, const void* grad_ou
                         const void* output) const {
   if (part < -1 || part > 2) throw Error(E_INVALID, "gradient part must be 0, 1 or 2");
   if (part >= 0 && !opt_.gradient) throw Error(E_INVALID, "the program was built without gradient support");
+  if (sliced_ && (part == 1 || part == 2))
+    throw Error(E_UNSUPPORTED, "a sliced gradient program runs forward and reverse together (part 0)");
   if (!inputs) throw Error(E_INVALID, "inputs pointer is null");
   for (u64 i = 0; i < plan_.n_inputs; ++i)
     if (!inputs[i]) throw Error(E_INVALID, "input " + std::to_string(i) + " pointer is null");
@@ -1520,10 +1599,11 @@ void Program::enqueue_part(int part, const void* const* inputs, const void* grad
   out_f64_flag_ = false;
   grad_out_ = grad_out;
   grads_ = grads;
-  const size_t fwd_end = opt_.gradient ? bwd_begin_ : ops_.size();
-  const size_t lo = part == 2 ? bwd_begin_ : 0, hi = (part == 1 || part == -1) ? fwd_end : ops_.size();
   try {
-    for (size_t i = lo; i < hi; ++i) launch_op(ops_[i], inputs, output, (char*)ws, st);
+    for (const Op& op : ops_) {
+      const bool run = part == 0 || (part == 2 ? op.bwd : !op.bwd);
+      if (run) launch_op(op, inputs, output, (char*)ws, st);
+    }
   } catch (...) {
     grad_out_ = nullptr;
     grads_ = nullptr;

@@ -45,7 +45,7 @@ struct Ref {
 struct Op {
   enum Kind : int {
     GATHER = 0, GEMM_SMALL = 1, GEMM_TILE64 = 2, GEMM_TILE32 = 3, ACCUM = 4, OUTPUT = 5, MEMSET = 6, MAXABS = 7,
-    STRIP = 8, GEMM_TC = 9, GEMM_DOT = 10, PACK = 11, SCATTER = 12, PACK_TILED = 13, GEMM_WARP = 14
+    STRIP = 8, GEMM_TC = 9, GEMM_DOT = 10, PACK = 11, SCATTER = 12, PACK_TILED = 13, GEMM_WARP = 14, GRAD_ACCUM = 15, NARROW = 16
   } kind;
   Ref a, b, c;
   u64 tab[6] = {0, 0, 0, 0, 0, 0};  // byte offsets of offset tables in the program's table buffer
@@ -63,6 +63,7 @@ struct Op {
   int splits = 1;                       // GEMM_TC: K splits (partials in `d`, summed in order into `c`)
   int kt_chunk = 0;
   Ref d;                                // GEMM_TC: FP32 split-K partial buffer
+  bool bwd = false;                     // part of the adjoint sweep (skipped by a plain execute)
 };
 
 class Program {

@@ -116,12 +116,27 @@ def test_adjoint_recompute_under_budget(dtype):
     assert roomy.recomputed_steps == 0 and roomy.workspace_bytes == full.workspace_bytes
 
 
-def test_gradient_of_sliced_program_is_rejected_before_launch():
+def test_sliced_gradient_program_interleaves_reverse_sweeps_per_group():
     net, _ = N.workload_rand3reg(64, 2, 1, np.complex64, seed=0)
     path = A.greedy(*net.as_tuple())
     sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 8)
-    with pytest.raises(ValueError, match="sliced"):
-        program(net, path, sliced, dtype=np.complex64, gradient=True)
+    p = program(net, path, sliced, dtype=np.complex64, gradient=True, max_slices_per_group=32)
+    d = p.describe()
+    ops, groups, n_in = d["ops"], d["groups"], len(net.inputs)
+    assert groups == -(-d["n_slices"] // 32)
+    kinds = [o["kind"] for o in ops]
+    assert kinds.count("grad_accum") == n_in * groups  # every group folds its slices' input gradients
+    assert kinds.count("narrow") == n_in  # once, after the last group
+    assert all(o.get("bwd") for o in ops if o["kind"] in ("grad_accum", "narrow"))
+    last_output = max(i for i, k in enumerate(kinds) if k == "slice_output")
+    assert min(i for i, k in enumerate(kinds) if k == "narrow") > last_output
+    # reverse work sits inside the groups: a backward GEMM precedes the next group's forward GEMMs
+    first_bwd = min(i for i, o in enumerate(ops) if o.get("bwd") and o["kind"].startswith("gemm"))
+    assert any(o["kind"].startswith("gemm") and not o.get("bwd") for o in ops[first_bwd:])
+    # a plain execute runs only the forward ops; its GEMM count is the forward program's
+    plain = program(net, path, sliced, dtype=np.complex64, max_slices_per_group=32)
+    n_gemm = sum(o["kind"].startswith("gemm") for o in plain.describe()["ops"])
+    assert sum(o["kind"].startswith("gemm") and not o.get("bwd") for o in ops) == n_gemm
 
 
 def test_batch_workload_generator():
