@@ -579,14 +579,17 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     g.conj_b = conj_b && dtype_complex(dt);
     // A long K over an output too small to give every SM a tile would run serially on a few SMs in the
     // tile kernels; one warp per output spreads the K loop over all of them instead.
-    const u64 tiles32 = ((m + 31) / 32) * ((n + 31) / 32) * bt;
-    const bool long_k_few_tiles = k >= 1024 && tiles32 < 2 * (u64)kNumSMs && bt * m * n <= (1u << 17);
-    if (long_k_few_tiles && bt * m * n <= 64 && k >= 2048) g.kind = Op::GEMM_DOT;
+    // A one-slice GEMM (phase 1) whose tile grid would leave SMs idle spreads its outputs over warps
+    // instead: the tile kernels only win once every SM has a tile.  Phase-2 GEMMs are multiplied by
+    // the slice group, so they keep the tile kernels.
+    const u64 outs = bt * m * n;
+    const u64 tiles64 = ((m + 63) / 64) * ((n + 63) / 64) * bt, tiles32 = ((m + 31) / 32) * ((n + 31) / 32) * bt;
+    const bool long_k_few_tiles = k >= 1024 && tiles32 < 2 * (u64)kNumSMs && outs <= (1u << 17);
+    if (outs <= 64 && k >= 256) g.kind = Op::GEMM_DOT;
     else if (long_k_few_tiles) g.kind = Op::GEMM_WARP;
-    else if (m >= 64 && n >= 64) g.kind = Op::GEMM_TILE64;
-    else if (m >= 24 && n >= 24) g.kind = Op::GEMM_TILE32;
-    else if (k >= 2048 && bt * m * n <= 64) g.kind = Op::GEMM_DOT;
-    else if (k >= 64) g.kind = Op::GEMM_WARP;  // a serial k loop per thread would dominate
+    else if (m >= 64 && n >= 64 && (ph2 || tiles64 >= (u64)kNumSMs)) g.kind = Op::GEMM_TILE64;
+    else if (m >= 24 && n >= 24 && (ph2 || tiles32 >= (u64)kNumSMs)) g.kind = Op::GEMM_TILE32;
+    else if (k >= 32) g.kind = Op::GEMM_WARP;  // a serial k loop per thread would dominate
     // Tensor cores for dense c64 steps; also for a small output side with a long K, where the padded
     // tile wastes MMA work but the K split (below) still fills the GPU.
     if (g.kind == Op::GEMM_DOT && k >= 16384) {
@@ -602,15 +605,112 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         touch(g.d, ph2, opidx(ph2));
       }
     }
-    const bool use_tc = opt_.precision == PREC_TF32X3 && dt == DT_C64 && k >= 32 &&
-                        ((m >= 96 && n >= 96) || (std::min(m, n) >= 16 && k >= 256));
+    // A single 16-wide K tile (no K split possible) only pays once the slice group or the batch gives
+    // every SM an output tile; its epilogue can then write the next GEMM's packed operand directly.
+    const u64 tc_tiles = ((m + tc::BM - 1) / tc::BM) * ((n + tc::BN - 1) / tc::BN) * bt;
+    const bool use_tc = opt_.precision == PREC_TF32X3 && dt == DT_C64 &&
+                        ((k >= 32 && ((m >= 96 && n >= 96) || (std::min(m, n) >= 16 && k >= 256))) ||
+                         (k >= 16 && m >= 96 && n >= 96 && (ph2 || tc_tiles >= (u64)kNumSMs)));
     if (use_tc) {
       const ll kpad = ((ll)k + tc::BK - 1) / tc::BK * tc::BK;
       const ll rpa = ((ll)m + tc::BM - 1) / tc::BM * tc::BM;
       const ll rpb = ((ll)n + tc::BN - 1) / tc::BN * tc::BN;
+      // A phase-2 operand that is the whole unsplit output of an earlier tensor-core GEMM, read by nothing
+      // else, is packed by that GEMM's epilogue: the offsets of the packed layout separate into a row
+      // table, a column table and a batch table over the producer's row-major [bt][m][n] result.  Only
+      // layouts without padding (nothing to zero first) qualify whose tables repeat from one output tile
+      // to the next and whose packed runs inside a tile average at least 32 floats (coalesced stores).
+      auto fuse_into_producer = [&](const Operand& X, ll rows, ll rpad, bool conj, u64 pbuf) -> bool {
+        if (!ph2 || !X.variant || opt_.gradient || conj || X.ref.kind != Ref::WS || X.so.n != 0) return false;
+        if (rows != rpad || (ll)k != kpad) return false;
+        size_t pi = ops2.size();
+        for (size_t q = ops2.size(); q-- > 0;)
+          if (ops2[q].c.kind == Ref::WS && ops2[q].c.index == X.ref.index) { pi = q; break; }
+        if (pi == ops2.size()) return false;
+        auto reads_x = [&](const Ref& r) { return r.kind == Ref::WS && r.index == X.ref.index; };
+        for (size_t q = pi + 1; q < ops2.size(); ++q) {
+          const Op& o = ops2[q];
+          if (reads_x(o.a) || reads_x(o.b) || reads_x(o.c) || reads_x(o.d) || reads_x(o.pk)) return false;
+        }
+        Op& P = ops2[pi];
+        if (P.kind != Op::GEMM_TC || P.splits > 1 || P.pk.kind != Ref::NONE || P.bwd) return false;
+        const ll mp = P.m, np = P.n, btp = P.bt, mn = mp * np;
+        if (X.so.local_stride != btp * mn) return false;
+        struct L { ll d, s, t; };
+        std::vector<L> grp[3];  // producer columns, rows, batch
+        auto add = [&](const std::vector<u64>& d, const std::vector<ll>& s_, ll unit) {
+          auto rm = rm_strides(d);
+          for (size_t q = 0; q < d.size(); ++q) {
+            if (d[q] <= 1) continue;
+            const ll sv = s_[q];
+            grp[sv >= mn ? 2 : sv >= np ? 1 : 0].push_back(L{(ll)d[q], sv, rm[q] * unit});
+          }
+        };
+        add(X.dB, X.sB, rpad * kpad);
+        add(X.dR, X.sR, kpad);
+        add(X.dK, X.sK, 1);
+        const ll unit[3] = {1, np, mn}, extent[3] = {np, mn, btp * mn};
+        for (int g = 0; g < 3; ++g) {  // each group must tile its index range exactly
+          std::sort(grp[g].begin(), grp[g].end(), [](const L& x, const L& y) { return x.s < y.s; });
+          ll expect = unit[g];
+          for (const L& l : grp[g]) {
+            if (l.s != expect) return false;
+            expect *= l.d;
+          }
+          if (expect != extent[g]) return false;
+        }
+        auto table = [&](int g, ll count) {
+          std::vector<ll> t((size_t)count, 0);
+          for (ll x = 0; x < count; ++x)
+            for (const L& l : grp[g]) t[(size_t)x] += ((x * unit[g] / l.s) % l.d) * l.t;
+          return t;
+        };
+        const std::vector<ll> ti = table(1, mp), tj = table(0, np);
+        auto periodic = [](const std::vector<ll>& t, ll tile) {
+          for (size_t x = 0; x < t.size(); ++x)
+            if (t[x] != t[x / tile * tile] + t[x % tile]) return false;
+          return true;
+        };
+        if (!periodic(ti, tc::BM) || !periodic(tj, tc::BN)) return false;
+        // The tile's elements in packed order must split into chunks of 32 consecutive packed floats
+        // that share one (row, column) pattern relative to their first element.
+        const ll tr = std::min<ll>(mp, tc::BM), tcn = std::min<ll>(np, tc::BN);
+        std::vector<std::pair<ll, std::pair<ll, ll>>> walk;
+        for (ll r = 0; r < tr; ++r)
+          for (ll c = 0; c < tcn; ++c) walk.push_back({ti[r] + tj[c], {r, c}});
+        std::sort(walk.begin(), walk.end());
+        if (walk.size() % 32 || walk.back().first > INT32_MAX) return false;
+        std::vector<int> lane(32);
+        std::vector<int> chunks;  // pairs (r0 << 16 | c0, packed offset)
+        for (size_t q = 0; q < walk.size(); q += 32) {
+          const ll r0 = walk[q].second.first, c0 = walk[q].second.second;
+          for (size_t l = 0; l < 32; ++l) {
+            const ll dr = walk[q + l].second.first - r0, dc = walk[q + l].second.second - c0;
+            if (walk[q + l].first != walk[q].first + (ll)l || dr < 0 || dc < 0) return false;
+            const int pat = (int)(dr << 16 | dc);
+            if (q == 0) lane[l] = pat;
+            else if (lane[l] != pat) return false;
+          }
+          chunks.push_back((int)(r0 << 16 | c0));
+          chunks.push_back((int)walk[q].first);
+        }
+        P.pk = Ref{Ref::WS, pbuf};
+        P.pk_tab[0] = tab_ll(ti);
+        P.pk_tab[1] = tab_ll(tj);
+        P.pk_tab[2] = tab_ll(table(2, btp));
+        P.pk_tab[3] = tab_i32(chunks);
+        P.pk_tab[4] = tab_i32(lane);
+        P.pk_chunks = (int)(walk.size() / 32);
+        P.pk_slice = (ll)bt * rpad * kpad;
+        bufs[pbuf].first = std::min<u64>(bufs[pbuf].first, (u64)pi);
+        P.c = Ref{};  // the plain result is never written
+        bufs[X.ref.index].bytes = 0;
+        return true;
+      };
       auto pack = [&](const Operand& X, ll rows, ll rpad, bool conj) {
         const u64 pbuf = new_buf(ph2, (u64)(tc::PLANES * (ll)bt * rpad * kpad * 4), opidx(ph2));
         bufs[pbuf].fixed = ph2 && !X.variant;
+        if (fuse_into_producer(X, rows, rpad, conj, pbuf)) return pbuf;
         Op p{Op::PACK};
         p.a = X.ref;
         p.sa = X.so;
@@ -709,16 +809,79 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     touch(rref, ph2, opidx(ph2));
     return StepRec{oa, ob, da, db};
   };
+  // Rank of each axis of step s's result in the packed operand layout of the step that reads it
+  // ([batch][rows][K], outermost first); empty when a dangling sum or the final result reads it.
+  auto consumer_rank = [&](size_t s) {
+    const PairStep& st = plan_.steps[s];
+    std::vector<size_t> rank;
+    for (size_t c = s + 1; c < plan_.steps.size(); ++c) {
+      const PairStep& u = plan_.steps[c];
+      const bool left = u.left_slot == st.result_slot;
+      if (!left && u.right_slot != st.result_slot) continue;
+      if (!(left ? u.sum_a : u.sum_b).empty()) break;
+      std::vector<u64> order;
+      const auto& pm = left ? u.a_perm : u.b_perm;
+      const size_t nb = u.n_batch, nc = u.n_con;
+      if (left) order = pm;
+      else {  // b_perm is [batch, con, free_b]; the pack lays out [batch, free_b, con]
+        order.assign(pm.begin(), pm.begin() + nb);
+        order.insert(order.end(), pm.begin() + nb + nc, pm.end());
+        order.insert(order.end(), pm.begin() + nb, pm.begin() + nb + nc);
+      }
+      rank.assign(st.result_shape.size(), 0);
+      for (size_t q = 0; q < order.size(); ++q) rank[order[q]] = q;
+      break;
+    }
+    return rank;
+  };
+  // Each intermediate's physical leg order is free: rows and columns of a step's result are laid out
+  // in the order its consumer packs them, so the consumer's contiguous runs fall inside one output
+  // tile of the producer (the fused epilogue pack needs that; a separate pack reads longer runs).
+  // Gradient programs keep the plan's order, which the adjoint sweep's operand views assume.
+  auto reorder_result = [&](size_t s, StepRec& rec) {
+    const PairStep& st = plan_.steps[s];
+    std::vector<size_t> phys(st.result_shape.size());
+    std::iota(phys.begin(), phys.end(), 0);
+    const std::vector<size_t> rank = opt_.gradient ? std::vector<size_t>{} : consumer_rank(s);
+    if (rank.empty()) return phys;
+    const size_t nb = st.n_batch, nfa = st.n_free_a;
+    auto regroup = [&](Operand& o, size_t lo, size_t hi) {
+      std::vector<size_t> q(hi - lo);
+      std::iota(q.begin(), q.end(), 0);
+      std::stable_sort(q.begin(), q.end(), [&](size_t x, size_t y) { return rank[lo + x] < rank[lo + y]; });
+      std::vector<u64> d;
+      std::vector<ll> sv;
+      for (size_t y = 0; y < q.size(); ++y) {
+        d.push_back(o.dR[q[y]]);
+        sv.push_back(o.sR[q[y]]);
+        phys[lo + y] = lo + q[y];
+      }
+      o.dR = d;
+      o.sR = sv;
+      o.tR = offsets(d, sv);
+    };
+    regroup(rec.a, nb, nb + nfa);
+    regroup(rec.b, nb + nfa, st.result_shape.size());
+    return phys;
+  };
   auto fwd_step = [&](size_t s, const View& A, const View& B, View& C) {
     const PairStep& st = plan_.steps[s];
     const bool ph2 = A.variant || B.variant;
     StepRec rec = step_operands(s, A, B);
+    const std::vector<size_t> phys = reorder_result(s, rec);
     const u64 cnumel = prod({st.bt, st.m, st.n});
     const u64 cb = new_buf(ph2, cnumel * eb, opidx(ph2));
     emit_gemm(ph2, rec.a, rec.b, st.bt, st.m, st.k, st.n, Ref{Ref::WS, cb}, false, false);
     C.ref = Ref{Ref::WS, cb};
     C.shape = st.result_shape;
-    C.strides = rm_strides(st.result_shape);
+    C.strides.assign(phys.size(), 0);
+    {
+      ll stride = 1;
+      for (size_t q = phys.size(); q-- > 0;) {
+        C.strides[phys[q]] = stride;
+        stride *= (ll)st.result_shape[phys[q]];
+      }
+    }
     C.so.local_stride = ph2 ? (ll)cnumel : 0;
     C.so.n = 0;
     C.variant = ph2;
@@ -1048,6 +1211,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     resolve(op.b);
     resolve(op.c);
     resolve(op.d);
+    resolve(op.pk);
   };
   if (want_strip) strip_exp_off_ = bufs[strip_exp_off_].offset;
   err_off_ = bufs[err_buf].offset;
@@ -1245,7 +1409,8 @@ CUtensorMap plane_map(void* base, ll kpad, ll rows, ll zplanes) {
   return m;
 }
 
-void launch_tc(const Op& op, void* A, void* B, void* C, void* D, const char* tab, int* err, cudaStream_t st) {
+void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const char* tab, int* err,
+               cudaStream_t st) {
   if (op.kind == Op::PACK) {
     const ll Z = (op.a_var ? op.S : 1) * op.bt;
     const ll tiles = Z * (op.rpad / 32) * ((op.kpad + 31) / 32);
@@ -1259,7 +1424,7 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, const char* tab
     const ll n_slices = op.a_var ? op.S : 1;
     const ll slice_stride = op.bt * op.rpad * op.kpad;
     const ll plane = n_slices * slice_stride;
-    tc::k_pack_tiled<<<(int)std::min<ll>(op.n_outer * n_slices, 148 * 8), tc::kPackThreads, 0, st>>>(
+    tc::k_pack_tiled<<<(int)std::min<ll>(op.n_outer * n_slices, 148 * 6), tc::kPackThreads, 0, st>>>(
         (const cf32*)A, (float*)C, (const int*)(tab + op.tab[0]), (const int*)(tab + op.tab[1]),
         (const int*)(tab + op.tab[2]), (int)op.tile_T, (const ll*)(tab + op.tab[4]), (const ll*)(tab + op.tab[5]),
         op.n_outer, n_slices, slice_stride, plane, op.sa, op.g0, op.conj_a ? 1 : 0);
@@ -1287,6 +1452,17 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, const char* tab
   args.a_var = op.a_var;
   args.b_var = op.b_var;
   args.err = err;
+  if (PK) {
+    args.pk = (float*)PK;
+    args.pk_i = (const ll*)(tab + op.pk_tab[0]);
+    args.pk_j = (const ll*)(tab + op.pk_tab[1]);
+    args.pk_b = (const ll*)(tab + op.pk_tab[2]);
+    args.pk_chunk = (const int2*)(tab + op.pk_tab[3]);
+    args.pk_lane = (const int*)(tab + op.pk_tab[4]);
+    args.pk_chunks = op.pk_chunks;
+    args.pk_slice = op.pk_slice;
+    args.pk_plane = s_eff * op.pk_slice;
+  }
   const ll zc = s_eff * op.bt;
   if (zc * op.splits > 65535) throw Error(E_UNSUPPORTED, "tensor-core GEMM batch x K splits exceeds the grid limit");
   if (op.splits > 1) {
@@ -1327,7 +1503,7 @@ void Program::launch_op(const Op& op, const void* const* inputs, void* output, c
     return;
   }
   if (op.kind == Op::PACK || op.kind == Op::PACK_TILED || op.kind == Op::GEMM_TC) {
-    launch_tc(op, ptr(op.a), ptr(op.b), ptr(op.c), ptr(op.d), dev_tab_, (int*)(ws + err_off_), st);
+    launch_tc(op, ptr(op.a), ptr(op.b), ptr(op.c), ptr(op.d), ptr(op.pk), dev_tab_, (int*)(ws + err_off_), st);
     CK(cudaGetLastError());
     return;
   }
@@ -1556,11 +1732,16 @@ std::string Program::describe() const {
     const Op& op = ops_[i];
     s += std::string(i ? "," : "") + "{\"kind\":\"" + names[(int)op.kind] + "\"" + (op.bwd ? ",\"bwd\":1" : "");
     auto f = [&](const char* k, long long v) { s += std::string(",\"") + k + "\":" + std::to_string(v); };
+    // operands: reference kind (1 input, 2 workspace, 3 output, 4 grad_output, 5 grads) and index / offset
+    f("a_kind", (long long)op.a.kind); f("a", (long long)op.a.index);
+    if (op.b.kind != Ref::NONE) { f("b_kind", (long long)op.b.kind); f("b", (long long)op.b.index); }
+    f("c_kind", (long long)op.c.kind); f("c", (long long)op.c.index);
     switch (op.kind) {
       case Op::GEMM_SMALL: case Op::GEMM_TILE64: case Op::GEMM_TILE32: case Op::GEMM_DOT: case Op::GEMM_TC:
       case Op::GEMM_WARP:
         f("S", op.S); f("bt", op.bt); f("m", op.m); f("k", op.k); f("n", op.n);
         f("splits", op.splits); f("conj_a", op.conj_a); f("conj_b", op.conj_b);
+        if (op.pk.kind != Ref::NONE) f("pack_into", (long long)op.pk.index);
         break;
       case Op::PACK: case Op::PACK_TILED:
         f("S", op.a_var ? op.S : 1); f("bt", op.bt); f("rows", op.rows); f("cols", op.cols); f("rpad", op.rpad);

@@ -64,6 +64,13 @@ struct Op {
   int kt_chunk = 0;
   Ref d;                                // GEMM_TC: FP32 split-K partial buffer
   bool bwd = false;                     // part of the adjoint sweep (skipped by a plain execute)
+  // GEMM_TC whose epilogue writes the next GEMM's packed operand instead of `c`: the pack buffer, the
+  // offset tables over the output's rows, columns and batch, the tile's 32-float chunks and their lane
+  // pattern, and the packed size of one slice.
+  Ref pk;
+  u64 pk_tab[5] = {0, 0, 0, 0, 0};
+  int pk_chunks = 0;
+  ll pk_slice = 0;
 };
 
 class Program {

@@ -163,6 +163,20 @@ struct TcArgs {
   // m_fast (A's tiles stay in L2 while B streams through once), else the n-tile fastest.
   int m_tiles = 1;
   int m_fast = 1;
+  // Fused consumer pack: instead of C, write the output as the next GEMM's 4-plane operand pack.  The
+  // packed offset of element (z = slice * bt + b, i, j) is slice * pk_slice + pk_b[b] + pk_i[i] + pk_j[j];
+  // plane p sits p * pk_plane floats further.  Inside one output tile the packed offsets form chunks of
+  // 32 consecutive floats with a common shape: chunk q starts at tile position (r0, c0) = pk_chunk[q].x
+  // (r0 << 16 | c0) and packed offset pk_chunk[q].y past the tile's base, and its element l sits at
+  // (r0, c0) + pk_lane[l] (dr << 16 | dc).  A warp stores one chunk per step: 128 contiguous bytes per plane.
+  float* pk = nullptr;
+  const ll* pk_i = nullptr;
+  const ll* pk_j = nullptr;
+  const ll* pk_b = nullptr;
+  const int2* pk_chunk = nullptr;
+  const int* pk_lane = nullptr;
+  int pk_chunks = 0;
+  ll pk_plane = 0, pk_slice = 0;
 };
 
 #define AB2_TMEM_LD16(taddr, r)                                                                                   \
@@ -350,14 +364,36 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
     asm volatile("bar.sync 1, %0;" ::"n"(kDrainThreads) : "memory");
     if (ok && !*abort_flag) {
       const cf32* tile = reinterpret_cast<const cf32*>(ring);
-      cf32* cbase = (args.part ? args.part + (ll)split * args.zc * args.m * args.n : args.C) + (ll)z * args.m * args.n;
       const ll row0 = (ll)tile_m * BM, col0 = (ll)tile_n * BN;
       const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
       const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
-      cbase += row0 * args.n + col0;
-      for (int e = threadIdx.x - 64; e < rows * BN; e += kDrainThreads) {
-        const int r = e / BN, c = e % BN;
-        if (c < cols) cbase[(ll)r * args.n + c] = tile[r * kTileStride + c];
+      if (args.pk) {
+        const int lane = threadIdx.x & 31, lp = __ldg(args.pk_lane + lane);
+        const int dr = lp >> 16, dc = lp & 0xFFFF;
+        const ll plane = args.pk_plane;
+        float* tb = args.pk + (ll)(z / args.bt) * args.pk_slice + __ldg(args.pk_b + z % args.bt) +
+                    __ldg(args.pk_i + row0) + __ldg(args.pk_j + col0) + lane;
+        const int2* chunk = args.pk_chunk;
+        int q = (threadIdx.x - 64) >> 5;
+        int2 ch = q < args.pk_chunks ? __ldg(chunk + q) : make_int2(0, 0);
+        for (; q < args.pk_chunks; q += kDrainWarps) {
+          const int2 nx = q + kDrainWarps < args.pk_chunks ? __ldg(chunk + q + kDrainWarps) : ch;
+          const int r = (ch.x >> 16) + dr, c = (ch.x & 0xFFFF) + dc;
+          if (r < rows && c < cols) {
+            const cf32 v = tile[r * kTileStride + c];
+            float* d = tb + ch.y;
+            put_split(d, plane, 0, v.re);
+            put_split(d + 2 * plane, plane, 0, v.im);
+          }
+          ch = nx;
+        }
+      } else {
+        cf32* cbase = (args.part ? args.part + (ll)split * args.zc * args.m * args.n : args.C) + (ll)z * args.m * args.n;
+        cbase += row0 * args.n + col0;
+        for (int e = threadIdx.x - 64; e < rows * BN; e += kDrainThreads) {
+          const int r = e / BN, c = e % BN;
+          if (c < cols) cbase[(ll)r * args.n + c] = tile[r * kTileStride + c];
+        }
       }
     }
   }
@@ -380,7 +416,7 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
 constexpr int kPackTile = 1024;
 constexpr int kPackThreads = 256;
 __device__ __forceinline__ int pack_swz(int e) { return e ^ ((e >> 5) & 31); }
-static __global__ void __launch_bounds__(kPackThreads) k_pack_tiled(
+static __global__ void __launch_bounds__(kPackThreads, 6) k_pack_tiled(
     const cf32* __restrict__ src, float* __restrict__ dst, const int* __restrict__ rd_rank,
     const int* __restrict__ rd_off, const int* __restrict__ wr_off, int T, const ll* __restrict__ src_base,
     const ll* __restrict__ dst_base, ll n_outer, ll n_slices, ll dst_slice_stride, ll plane, SliceOff so, ll g0,

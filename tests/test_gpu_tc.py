@@ -94,3 +94,23 @@ def test_tc_grid_contraction_matches_fp64_oracle():
     got32 = complex(A.contract_sliced(*net.as_tuple(), arrays, [], ssa_path=path, precision="fp32"))
     assert abs(got - want) / abs(want) <= 1e-5
     assert abs(got32 - want) / abs(want) <= 1e-5
+
+
+def test_epilogue_packs_are_bit_identical_to_separate_packs():
+    # rand3reg n=104, 16 slices: tensor-core steps whose result feeds another tensor-core step write that
+    # step's packed operand from their epilogue, with the result's legs laid out in the consumer's order.
+    # A gradient program keeps the plan's leg order and separate packs; its forward gives the same bits.
+    from arctn_b200 import networks as N
+
+    net, arrays = N.workload_rand3reg(104, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 14)
+    kw = dict(dtype=np.complex64, precision="tf32x3", max_slices_per_group=4)
+    fused = A.SlicedProgram(*net.as_tuple(), path, sliced, **kw)
+    plain = A.SlicedProgram(*net.as_tuple(), path, sliced, gradient=True, **kw)
+    assert any("pack_into" in o for o in fused.describe()["ops"])
+    assert not any("pack_into" in o for o in plain.describe()["ops"])
+    got, ref = fused.execute(arrays), plain.execute(arrays)
+    assert np.array_equal(got, ref)
+    want = O.contract_sliced(*net.as_tuple(), path, sliced, O.promote(arrays), threads=8)
+    assert rel_err(got, want) <= 1e-5

@@ -57,9 +57,10 @@ def test_tf32x3_packs_use_full_tiles_and_split_long_k():
     ops = p.describe()["ops"]
     tc = [o for o in ops if o["kind"] == "gemm_tc"]
     packs = [o for o in ops if o["kind"] == "pack_tiled"]
-    assert tc and len(packs) == 2 * len(tc)
+    assert tc and len(packs) + sum("pack_into" in o for o in tc) == 2 * len(tc)
     for o in tc:
-        assert o["k"] >= 32 and ((o["m"] >= 96 and o["n"] >= 96) or (min(o["m"], o["n"]) >= 16 and o["k"] >= 256))
+        assert (o["k"] >= 32 and ((o["m"] >= 96 and o["n"] >= 96) or (min(o["m"], o["n"]) >= 16 and o["k"] >= 256))
+                or (o["k"] >= 16 and o["m"] >= 96 and o["n"] >= 96))
         assert o["splits"] == 1  # slice-batched GEMMs fill the GPU without splitting K
     for o in packs:
         assert o["rpad"] % 128 == 0 and o["kpad"] % 16 == 0 and 32 <= o["tile"] <= 1024
@@ -69,6 +70,29 @@ def test_tf32x3_packs_use_full_tiles_and_split_long_k():
         assert o["splits"] == max(1, -(-o["k"] // 256))
     fp32 = program(net, path, sliced, dtype=np.complex64, precision="fp32", max_slices_per_group=4)
     assert not any(o["kind"] in ("gemm_tc", "pack_tiled", "pack") for o in fp32.describe()["ops"])
+
+
+def test_tensor_core_epilogues_pack_the_next_gemm_operand():
+    # rand3reg n=172: the producer's epilogue writes the packed operand of the GEMM that reads its result,
+    # so no separate pack reads that result; gradient programs keep separate packs.
+    net, _ = N.workload_rand3reg(172, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 24)
+    p = program(net, path, sliced, dtype=np.complex64, precision="tf32x3", max_slices_per_group=4)
+    d = p.describe()
+    ops = d["ops"]
+    per_group = [i for i, o in enumerate(ops) if "pack_into" in o]
+    assert len(per_group) >= 2 * d["groups"]
+    for i in per_group:
+        prod, dst = ops[i], ops[i]["pack_into"]
+        assert prod["kind"] == "gemm_tc" and prod["splits"] == 1
+        # the next op touching the packed buffer is the consuming GEMM, reading it as an operand
+        nxt = next(o for o in ops[i + 1:] if dst in (o.get("a"), o.get("b"), o.get("c"), o.get("pack_into")))
+        assert nxt["kind"] == "gemm_tc" and dst in (nxt["a"], nxt["b"]) and nxt["c"] != dst
+    g = program(net, path, sliced, dtype=np.complex64, precision="tf32x3", max_slices_per_group=4, gradient=True)
+    assert not any("pack_into" in o for o in g.describe()["ops"])
+    fp32 = program(net, path, sliced, dtype=np.complex64, precision="fp32", max_slices_per_group=4)
+    assert not any("pack_into" in o for o in fp32.describe()["ops"])
 
 
 def test_unsliced_small_tile_gemms_split_k_to_fill_the_gpu():
