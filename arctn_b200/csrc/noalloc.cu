@@ -136,6 +136,11 @@ extern "C" int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, voi
     if (!g_attr_set[dev]) {
       cudaError_t e = cudaFuncSetAttribute(tc::k_tc_cgemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES);
       if (e != cudaSuccess) return fail_with(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
+      cudaFuncAttributes fa{};
+      e = cudaFuncGetAttributes(&fa, tc::k_tc_cgemm_tf32x3);
+      if (e != cudaSuccess) return fail_with(std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
+      if (fa.numRegs != tc::kLaunchRegs)
+        return fail_with("tensor-core GEMM register count differs from its setmaxnreg split", ARCTN_B200_ERR_UNSUPPORTED);
       g_attr_set[dev] = true;
     }
     scratch = (unsigned char*)g_scratch_ptr[dev];
@@ -167,8 +172,13 @@ extern "C" int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, voi
   args.err = err;
   args.m_tiles = (int)(Ra / tc::BM);
   args.m_fast = Ra <= Rb ? 1 : 0;
-  dim3 grid((unsigned)((Ra / tc::BM) * (Rb / tc::BN)), 1u, (unsigned)Z);
-  tc::k_tc_cgemm_tf32x3<<<grid, tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
+  args.zc = (int)Z;
+  args.tiles = (int)((Ra / tc::BM) * (Rb / tc::BN));
+  args.n_items = args.tiles * (int)Z;
+  int n_sm = 0;
+  if (cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n_sm <= 0)
+    return fail_with("cudaDeviceGetAttribute failed", ARCTN_B200_ERR_CUDA);
+  tc::k_tc_cgemm_tf32x3<<<(unsigned)std::min(args.n_items, n_sm), tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail_with(std::string("launch: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
   ab2::set_last_error("");

@@ -679,28 +679,36 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         for (ll r = 0; r < tr; ++r)
           for (ll c = 0; c < tcn; ++c) walk.push_back({ti[r] + tj[c], {r, c}});
         std::sort(walk.begin(), walk.end());
+        // The epilogue stages 32 output rows at a time, so every chunk must stay inside one such group.
         if (walk.size() % 32 || walk.back().first > INT32_MAX) return false;
         std::vector<int> lane(32);
-        std::vector<int> chunks;  // pairs (r0 << 16 | c0, packed offset)
+        std::vector<std::vector<int>> by_quad(tc::BM / tc::kStageRows);  // pairs (r0 << 16 | c0, offset)
         for (size_t q = 0; q < walk.size(); q += 32) {
           const ll r0 = walk[q].second.first, c0 = walk[q].second.second;
           for (size_t l = 0; l < 32; ++l) {
             const ll dr = walk[q + l].second.first - r0, dc = walk[q + l].second.second - c0;
             if (walk[q + l].first != walk[q].first + (ll)l || dr < 0 || dc < 0) return false;
+            if (r0 % tc::kStageRows + dr >= tc::kStageRows) return false;
             const int pat = (int)(dr << 16 | dc);
             if (q == 0) lane[l] = pat;
             else if (lane[l] != pat) return false;
           }
-          chunks.push_back((int)(r0 << 16 | c0));
-          chunks.push_back((int)walk[q].first);
+          auto& v = by_quad[(size_t)(r0 / tc::kStageRows)];
+          v.push_back((int)(r0 << 16 | c0));
+          v.push_back((int)walk[q].first);
         }
+        std::vector<int> chunks;
+        for (size_t q = 0; q < by_quad.size(); ++q) {
+          P.pk_qbeg[q] = (int)(chunks.size() / 2);
+          chunks.insert(chunks.end(), by_quad[q].begin(), by_quad[q].end());
+        }
+        P.pk_qbeg[by_quad.size()] = (int)(chunks.size() / 2);
         P.pk = Ref{Ref::WS, pbuf};
         P.pk_tab[0] = tab_ll(ti);
         P.pk_tab[1] = tab_ll(tj);
         P.pk_tab[2] = tab_ll(table(2, btp));
         P.pk_tab[3] = tab_i32(chunks);
         P.pk_tab[4] = tab_i32(lane);
-        P.pk_chunks = (int)(walk.size() / 32);
         P.pk_slice = (ll)bt * rpad * kpad;
         bufs[pbuf].first = std::min<u64>(bufs[pbuf].first, (u64)pi);
         P.c = Ref{};  // the plain result is never written
@@ -1435,6 +1443,12 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
     CK(cudaFuncSetAttribute(tc::k_tc_cgemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    // The kernel's setmaxnreg split assumes exactly kLaunchRegs registers a thread at launch.
+    cudaFuncAttributes fa{};
+    CK(cudaFuncGetAttributes(&fa, tc::k_tc_cgemm_tf32x3));
+    if (fa.numRegs != tc::kLaunchRegs)
+      throw Error(E_UNSUPPORTED, "tensor-core GEMM built with " + std::to_string(fa.numRegs) + " registers a thread, not " +
+                                     std::to_string(tc::kLaunchRegs));
     attr_set[dev] = true;
   }
   const ll s_eff = (op.a_var || op.b_var) ? op.S : 1;
@@ -1459,24 +1473,28 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
     args.pk_b = (const ll*)(tab + op.pk_tab[2]);
     args.pk_chunk = (const int2*)(tab + op.pk_tab[3]);
     args.pk_lane = (const int*)(tab + op.pk_tab[4]);
-    args.pk_chunks = op.pk_chunks;
+    for (int q = 0; q < 5; ++q) args.pk_qbeg[q] = op.pk_qbeg[q];
     args.pk_slice = op.pk_slice;
     args.pk_plane = s_eff * op.pk_slice;
   }
   const ll zc = s_eff * op.bt;
-  if (zc * op.splits > 65535) throw Error(E_UNSUPPORTED, "tensor-core GEMM batch x K splits exceeds the grid limit");
+  args.zc = (int)zc;
   if (op.splits > 1) {
     args.kt_chunk = op.kt_chunk;
-    args.zc = (int)zc;
     args.part = (cf32*)D;
   }
   // The smaller operand's tiles run fastest, so it stays in L2 while the larger one streams once.
   const ll mt = (op.m + tc::BM - 1) / tc::BM, nt = (op.n + tc::BN - 1) / tc::BN;
   args.m_tiles = (int)mt;
   args.m_fast = mt <= nt ? 1 : 0;
-  if (mt * nt > 0x7FFFFFFFll) throw Error(E_UNSUPPORTED, "tensor-core GEMM tile count exceeds the grid limit");
-  dim3 grid((unsigned)(mt * nt), 1u, (unsigned)(zc * op.splits));
-  tc::k_tc_cgemm_tf32x3<<<grid, tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
+  const ll items = mt * nt * zc * op.splits;
+  if (items > 0x7FFFFFFFll) throw Error(E_UNSUPPORTED, "tensor-core GEMM work items exceed 2^31");
+  args.tiles = (int)(mt * nt);
+  args.n_items = (int)items;
+  static int sms[64] = {};
+  if (dev < 64 && !sms[dev]) CK(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
+  const int n_sm = dev < 64 ? sms[dev] : 148;
+  tc::k_tc_cgemm_tf32x3<<<(unsigned)std::min<ll>(items, n_sm), tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
   if (op.splits > 1) {
     const ll count = zc * op.m * op.n;
     tc::k_splitk_reduce<<<grid_for(count), 256, 0, st>>>((const cf32*)D, (cf32*)C, count, op.splits);

@@ -69,7 +69,7 @@ struct Op {
   // pattern, and the packed size of one slice.
   Ref pk;
   u64 pk_tab[5] = {0, 0, 0, 0, 0};
-  int pk_chunks = 0;
+  int pk_qbeg[5] = {0, 0, 0, 0, 0};     // chunk ranges per 32-row group of the tile
   ll pk_slice = 0;
 };
 

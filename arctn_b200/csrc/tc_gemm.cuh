@@ -12,11 +12,14 @@
 // the minus through the instruction's negate-A bit.  Accumulation is FP32: short
 // chains in TMEM, summed across chains in registers.
 //
-// Warp roles (320 threads, one CTA per 128x128 output tile):
-//   warp 0      TMA producer: 8 plane tiles per stage, 3-stage ring
-//   warp 1      TMEM allocation + single-thread MMA issue into two TMEM buffers
-//   warps 2..9  drain: each finished buffer -> FP32 registers (round-to-nearest adds),
-//               then the epilogue (registers -> HBM)
+// Persistent: one CTA per SM walks a list of 128x128 output tiles (work items).
+// Warp roles (512 threads, four warpgroups):
+//   warp 0        TMA producer: 8 plane tiles per stage, 3-stage ring, across items
+//   warp 1        TMEM allocation + single-thread MMA issue into two TMEM buffers
+//   warps 4..11   drain: each finished buffer -> FP32 registers (round-to-nearest adds),
+//                 then stage the finished tile, 32 rows at a time, in shared memory
+//   warps 2..15   epilogue stores of every staged pass (staging -> HBM), while the
+//                 MMA thread already fills TMEM for the next item
 // Every mbarrier wait is bounded (about one second of global time); on expiry
 // the kernel records a code in *err, drains what it issued and returns.
 #pragma once
@@ -34,7 +37,12 @@ constexpr int BM = 128, BN = 128, BK = 16, STAGES = 3;
 constexpr int PLANES = 4;                          // re_hi, re_lo, im_hi, im_lo
 constexpr int PLANE_BYTES = BM * BK * 4;          // 8 KB: 128 rows x 64 B
 constexpr int STAGE_BYTES = 2 * PLANES * PLANE_BYTES;  // A planes then B planes: 64 KB
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*align*/;
+// The epilogue stages one TMEM lane quadrant (32 output rows of complex64, rows padded by one element)
+// in its own buffer, so the operand ring keeps feeding the next work item meanwhile.
+constexpr int kStageRows = 32;
+constexpr int STAGING_BYTES = kStageRows * BN * 8;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + STAGING_BYTES + 1024 /*barriers*/ + 1024 /*align*/;
+static_assert(SMEM_BYTES <= 232448, "shared memory above the 227 KB a block may use");
 // Two TMEM buffers of (Cr, Ci), 128 columns each: buffer b at columns [256 b, 256 b + 256).  The MMA
 // thread fills one buffer with kChunkTiles K tiles (all 12 products per 8-wide K step) while the drain
 // warps read the other and add it into FP32 registers with round-to-nearest.  The tensor core's FP32
@@ -42,11 +50,16 @@ constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*barriers*/ + 1024 /*ali
 // kChunkTiles = 2) bounds that biased error; the long sum over K happens in the drain registers.
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int kChunkTiles = 2;
+// 16 warps in four warpgroups.  Warpgroup 0: TMA producer (warp 0), TMEM owner + MMA issuer (warp 1),
+// store helpers (warps 2, 3).  Warpgroups 1 and 2: the 8 drain warps (4..11), which hold the FP32
+// accumulators in registers.  Warpgroup 3: store helpers (12..15).  The block launches at 128 registers
+// a thread; setmaxnreg then moves registers from warpgroups 0 and 3 (down to kLowRegs) to the drain
+// warpgroups (up to kDrainRegs): 2 x 128 x kLowRegs + 2 x 128 x kDrainRegs equals 512 x 128 exactly.
+constexpr int kThreads = 512, kLaunchRegs = 128, kLowRegs = 72, kDrainRegs = 184;
+static_assert(2 * 128 * kLowRegs + 2 * 128 * kDrainRegs == kThreads * kLaunchRegs, "register split must use the launch total");
 constexpr int kDrainWarps = 8, kDrainThreads = kDrainWarps * 32;
-constexpr int kThreads = 64 + kDrainThreads;  // TMA warp, MMA warp, drain warps
+constexpr int kEpiWarps = 14, kEpiThreads = kEpiWarps * 32;  // warps 2..15 share the epilogue stores
 constexpr int kHalfCols = BN / 2;             // columns one drain thread owns
-constexpr int kTileStride = BN + 1;           // staged output tile row stride (complex elements)
-static_assert(BM * kTileStride * 8 <= STAGES * STAGE_BYTES, "the output tile is staged in the operand ring");
 constexpr unsigned long long kWaitNs = 1000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -157,10 +170,13 @@ struct TcArgs {
   // tensor core's FP32 accumulation loses about one unit in the last place per addition, so its
   // error grows with the number of K steps one accumulator takes; bounding that number bounds it.
   int kt_chunk = 0;  // 0: one CTA takes all of K and writes C
-  int zc = 0;        // output batches (grid z = splits * zc)
+  int zc = 0;        // output batches
   cf32* part = nullptr;
-  // Raster: blockIdx.x enumerates the m_tiles x n_tiles output tiles with the m-tile fastest when
-  // m_fast (A's tiles stay in L2 while B streams through once), else the n-tile fastest.
+  // Persistent schedule: CTA b takes work items b, b + gridDim.x, ...; item it is output tile
+  // it % tiles of batch-and-split it / tiles (split * zc + z).  Tiles enumerate the m_tiles x n_tiles
+  // grid with the m-tile fastest when m_fast (A's tiles stay in L2 while B streams through once),
+  // else the n-tile fastest.
+  int n_items = 0, tiles = 1;
   int m_tiles = 1;
   int m_fast = 1;
   // Fused consumer pack: instead of C, write the output as the next GEMM's 4-plane operand pack.  The
@@ -173,9 +189,9 @@ struct TcArgs {
   const ll* pk_i = nullptr;
   const ll* pk_j = nullptr;
   const ll* pk_b = nullptr;
-  const int2* pk_chunk = nullptr;
+  const int2* pk_chunk = nullptr;  // grouped by lane quadrant: quadrant q owns [pk_qbeg[q], pk_qbeg[q+1])
   const int* pk_lane = nullptr;
-  int pk_chunks = 0;
+  int pk_qbeg[5] = {0, 0, 0, 0, 0};
   ll pk_plane = 0, pk_slice = 0;
 };
 
@@ -204,13 +220,82 @@ __device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parit
   }
 }
 
+// Staging layout of 32 output rows x 128 complex columns: row r, column c sits at r * BN + (c ^ g(r mod 16)),
+// g(q) = (q & 3) << 2 | q >> 2.  A stager warp (lanes = 32 rows, one column) and a row reader (lanes = 32
+// columns) both meet 16 distinct 8-byte bank pairs per half-warp, and so does a packed chunk spanning
+// 4 rows x 4 columns.
+__device__ __forceinline__ int stage_at(int r, int c) {
+  const int q = r & 15;
+  return r * BN + (c ^ (((q & 3) << 2) | (q >> 2)));
+}
+
+// One pass of the epilogue store: output rows [r_lo, r_lo + 32) of the tile, staged in `stage`, written
+// by epilogue warp ew (0..13) / thread et (0..447) either as C rows or as packed 32-float chunks.
+__device__ __forceinline__ void store_pass(const TcArgs& args, const cf32* stage, int q, int z, int split, ll row0,
+                                           ll col0, int rows, int cols, int ew, int et, int lane) {
+  const int r_lo = q * kStageRows;
+  if (r_lo >= rows) return;
+  if (args.pk) {
+    const int lp = __ldg(args.pk_lane + lane);
+    const int dr = lp >> 16, dc = lp & 0xFFFF;
+    const ll plane = args.pk_plane;
+    float* tb = args.pk + (ll)(z / args.bt) * args.pk_slice + __ldg(args.pk_b + z % args.bt) + __ldg(args.pk_i + row0) +
+                __ldg(args.pk_j + col0) + lane;
+    const int2* chunk = args.pk_chunk;
+    const int q1 = args.pk_qbeg[q + 1];
+    constexpr int U = 4;
+    for (int ci0 = args.pk_qbeg[q] + ew; ci0 < q1; ci0 += U * kEpiWarps) {
+      int2 ch[U];
+      cf32 v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int ci = ci0 + u * kEpiWarps;
+        ch[u] = ci < q1 ? __ldg(chunk + ci) : make_int2(0x7FFF0000, 0);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int r = (ch[u].x >> 16) + dr, c = (ch[u].x & 0xFFFF) + dc;
+        v[u] = (r < rows && c < cols) ? stage[stage_at(r - r_lo, c)] : cf32{0.f, 0.f};
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int r = (ch[u].x >> 16) + dr, c = (ch[u].x & 0xFFFF) + dc;
+        if (r < rows && c < cols) {
+          float* d = tb + ch[u].y;
+          put_split(d, plane, 0, v[u].re);
+          put_split(d + 2 * plane, plane, 0, v[u].im);
+        }
+      }
+    }
+  } else {
+    const int nr = rows - r_lo < kStageRows ? rows - r_lo : kStageRows;
+    cf32* cbase = (args.part ? args.part + (ll)split * args.zc * args.m * args.n : args.C) + (ll)z * args.m * args.n +
+                  (row0 + r_lo) * args.n + col0;
+    constexpr int U = 4;
+    for (int e0 = et; e0 < nr * BN; e0 += U * kEpiThreads) {
+      cf32 v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int e = e0 + u * kEpiThreads, r = e / BN, c = e % BN;
+        v[u] = (e < nr * BN && c < cols) ? stage[stage_at(r, c)] : cf32{0.f, 0.f};
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int e = e0 + u * kEpiThreads, r = e / BN, c = e % BN;
+        if (e < nr * BN && c < cols) cbase[(ll)r * args.n + c] = v[u];
+      }
+    }
+  }
+}
+
 static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __grid_constant__ CUtensorMap tmA,
                                                                 const __grid_constant__ CUtensorMap tmB,
                                                                 TcArgs args) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* ring = smem;                                  // STAGES x {A planes, B planes}
-  uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);
+  cf32* stage = reinterpret_cast<cf32*>(smem + STAGES * STAGE_BYTES);  // kStageRows x kTileStride
+  uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES + STAGING_BYTES);
   uint64_t* full = bars;                     // TMA landed                  (count 1 + tx)
   uint64_t* empty = bars + STAGES;           // MMAs done reading a stage   (commit)
   uint64_t* accfull = bars + 2 * STAGES;     // [2] a TMEM buffer's chunk is complete (commit)
@@ -221,17 +306,23 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int n_tiles = (int)((args.n + BN - 1) / BN);
-  const int tile_m = args.m_fast ? (int)(blockIdx.x % args.m_tiles) : (int)(blockIdx.x / n_tiles);
-  const int tile_n = args.m_fast ? (int)(blockIdx.x / args.m_tiles) : (int)(blockIdx.x % n_tiles);
-  const int split = args.kt_chunk ? (int)(blockIdx.z / args.zc) : 0;
-  const int z = args.kt_chunk ? (int)(blockIdx.z % args.zc) : (int)blockIdx.z;
-  const int kt0 = args.kt_chunk ? split * args.kt_chunk : 0;
-  const int kt1 = args.kt_chunk ? min(args.k_tiles, kt0 + args.kt_chunk) : args.k_tiles;
-  const int b_idx = z % args.bt;
-  const int zA = args.a_var ? z : b_idx;
-  const int zB = args.b_var ? z : b_idx;
-  const int KT = kt1 - kt0;                           // k-tile of iteration t is kt0 + t
-  const int n_chunks = (KT + kChunkTiles - 1) / kChunkTiles;
+  // Work item it: output tile it % tiles (raster as in TcArgs) of batch-and-split it / tiles.
+  struct Item { int tile_m, tile_n, z, split, kt0, KT, zA, zB; };
+  auto item_of = [&](int it) {
+    Item w;
+    const int x = it % args.tiles, zz = it / args.tiles;
+    w.tile_m = args.m_fast ? x % args.m_tiles : x / n_tiles;
+    w.tile_n = args.m_fast ? x / args.m_tiles : x % n_tiles;
+    w.split = args.kt_chunk ? zz / args.zc : 0;
+    w.z = args.kt_chunk ? zz % args.zc : zz;
+    w.kt0 = args.kt_chunk ? w.split * args.kt_chunk : 0;
+    const int kt1 = args.kt_chunk ? min(args.k_tiles, w.kt0 + args.kt_chunk) : args.k_tiles;
+    w.KT = kt1 - w.kt0;                         // k-tile of iteration t is kt0 + t
+    const int b_idx = w.z % args.bt;
+    w.zA = args.a_var ? w.z : b_idx;
+    w.zB = args.b_var ? w.z : b_idx;
+    return w;
+  };
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < STAGES; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
@@ -250,152 +341,185 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  if (warp == 0) {
-    // ------------------------------------------------------------ TMA producer
-    if (lane == 0) {
-      int issued = 0;
-      for (int t = 0; t < KT; ++t) {
-        const int s = t % STAGES;
-        if (t >= STAGES && !mbar_wait(&empty[s], ((t / STAGES) - 1) & 1, args.err, 1)) { *abort_flag = 1; break; }
-        if (*abort_flag) break;
-        unsigned char* dst = ring + s * STAGE_BYTES;
-        mbar_expect_tx(&full[s], STAGE_BYTES);
-        const int k0 = (kt0 + t) * BK;
-#pragma unroll
-        for (int p = 0; p < PLANES; ++p) {
-          tma_load_3d(&tmA, &full[s], dst + p * PLANE_BYTES, k0, tile_m * BM, zA + p * args.za);
-          tma_load_3d(&tmB, &full[s], dst + (PLANES + p) * PLANE_BYTES, k0, tile_n * BN, zB + p * args.zb);
-        }
-        issued = t + 1;
-      }
-      if (*abort_flag) {  // let issued copies land before the CTA retires
-        for (int t = (issued > STAGES ? issued - STAGES : 0); t < issued; ++t)
-          mbar_wait(&full[t % STAGES], (t / STAGES) & 1, args.err, 7);
+  // Store helpers (warps 2, 3, 12..15): they follow the drain warps' items and barriers and share the
+  // stores of every staged pass.
+  auto helpers = [&]() {
+    bool dead = false;
+    for (int it = blockIdx.x; it < args.n_items; it += gridDim.x) {
+      const Item w = item_of(it);
+      const ll row0 = (ll)w.tile_m * BM, col0 = (ll)w.tile_n * BN;
+      const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
+      const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
+#pragma unroll 1
+      for (int q = 0; q < BM / kStageRows; ++q) {
+        asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
+        asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
+        if (*abort_flag) dead = true;
+        if (!dead) store_pass(args, stage, q, w.z, w.split, row0, col0, rows, cols, warp - 2, threadIdx.x - 64, lane);
       }
     }
-  } else if (warp == 1) {
-    // ------------------------------------------------------------ MMA issuer
-    if (lane == 0) {
-      const uint32_t id_pos = idesc_tf32(false), id_neg = idesc_tf32(true);
-      for (int c = 0; c < n_chunks && !*abort_flag; ++c) {
-        const int b = c & 1;
-        if (c >= 2 && !mbar_wait(&accempty[b], ((c >> 1) - 1) & 1, args.err, 6)) { *abort_flag = 1; break; }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t cr = tmem + b * 2 * BN, ci = cr + BN;
-        const int t_end = min(KT, (c + 1) * kChunkTiles);
-        bool first = true;
-        for (int t = c * kChunkTiles; t < t_end; ++t) {
-          const int s = t % STAGES;
-          if (!mbar_wait(&full[s], (t / STAGES) & 1, args.err, 2)) { *abort_flag = 1; break; }
-          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t a0 = smem_u32(ring + s * STAGE_BYTES), b0 = a0 + PLANES * PLANE_BYTES;
-          const uint32_t hAr = a0, lAr = a0 + PLANE_BYTES, hAi = a0 + 2 * PLANE_BYTES, lAi = a0 + 3 * PLANE_BYTES;
-          const uint32_t hBr = b0, lBr = b0 + PLANE_BYTES, hBi = b0 + 2 * PLANE_BYTES, lBi = b0 + 3 * PLANE_BYTES;
-#pragma unroll
-          for (int kk = 0; kk < BK / 8; ++kk) {
-            const uint32_t o = kk * 32;  // 8 tf32 = 32 bytes along the swizzled row
-            const uint32_t acc = first ? 0u : 1u;
-            // leading terms (hi,hi), then the corrections (lo,hi) and (hi,lo), all into this chunk's buffer
-            umma(cr, sw64_desc(hAr + o), sw64_desc(hBr + o), id_pos, acc);
-            umma(ci, sw64_desc(hAr + o), sw64_desc(hBi + o), id_pos, acc);
-            umma(cr, sw64_desc(hAi + o), sw64_desc(hBi + o), id_neg, 1);
-            umma(ci, sw64_desc(hAi + o), sw64_desc(hBr + o), id_pos, 1);
-            umma(cr, sw64_desc(lAr + o), sw64_desc(hBr + o), id_pos, 1);
-            umma(ci, sw64_desc(lAr + o), sw64_desc(hBi + o), id_pos, 1);
-            umma(cr, sw64_desc(lAi + o), sw64_desc(hBi + o), id_neg, 1);
-            umma(ci, sw64_desc(lAi + o), sw64_desc(hBr + o), id_pos, 1);
-            umma(cr, sw64_desc(hAr + o), sw64_desc(lBr + o), id_pos, 1);
-            umma(ci, sw64_desc(hAr + o), sw64_desc(lBi + o), id_pos, 1);
-            umma(cr, sw64_desc(hAi + o), sw64_desc(lBi + o), id_neg, 1);
-            umma(ci, sw64_desc(hAi + o), sw64_desc(lBr + o), id_pos, 1);
-            first = false;
+  };
+  if (warp < 4) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kLowRegs));
+    if (warp == 0) {
+      // ------------------------------------------------------------ TMA producer
+      // g counts k-tiles over all of this CTA's items: stage g % STAGES, phase (g / STAGES) & 1.
+      if (lane == 0) {
+        int g = 0, issued = 0;
+        bool stop = false;
+        for (int it = blockIdx.x; it < args.n_items && !stop; it += gridDim.x) {
+          const Item w = item_of(it);
+          for (int t = 0; t < w.KT; ++t, ++g) {
+            const int s = g % STAGES;
+            if (g >= STAGES && !mbar_wait(&empty[s], ((g / STAGES) - 1) & 1, args.err, 1)) {
+              *abort_flag = 1;
+              stop = true;
+              break;
+            }
+            if (*abort_flag) { stop = true; break; }
+            unsigned char* dst = ring + s * STAGE_BYTES;
+            mbar_expect_tx(&full[s], STAGE_BYTES);
+            const int k0 = (w.kt0 + t) * BK;
+  #pragma unroll
+            for (int p = 0; p < PLANES; ++p) {
+              tma_load_3d(&tmA, &full[s], dst + p * PLANE_BYTES, k0, w.tile_m * BM, w.zA + p * args.za);
+              tma_load_3d(&tmB, &full[s], dst + (PLANES + p) * PLANE_BYTES, k0, w.tile_n * BN, w.zB + p * args.zb);
+            }
+            issued = g + 1;
           }
-          umma_commit(&empty[s]);
         }
-        if (*abort_flag) break;
-        umma_commit(&accfull[b]);
+        if (*abort_flag) {  // let issued copies land before the CTA retires
+          for (int t = (issued > STAGES ? issued - STAGES : 0); t < issued; ++t)
+            mbar_wait(&full[t % STAGES], (t / STAGES) & 1, args.err, 7);
+        }
       }
-      if (*abort_flag) {
-        umma_commit(drain);
-        mbar_wait(drain, 0, args.err, 8);
+    } else if (warp == 1) {
+      // ------------------------------------------------------------ MMA issuer
+      // gc counts chunks over all items: TMEM buffer gc & 1.  The issuer runs up to two chunks ahead
+      // of the drain warps, so the next item's first chunks overlap the previous item's epilogue.
+      if (lane == 0) {
+        const uint32_t id_pos = idesc_tf32(false), id_neg = idesc_tf32(true);
+        int g = 0, gc = 0;
+        bool stop = false;
+        for (int it = blockIdx.x; it < args.n_items && !stop; it += gridDim.x) {
+          const Item w = item_of(it);
+          const int n_chunks = (w.KT + kChunkTiles - 1) / kChunkTiles;
+          for (int c = 0; c < n_chunks; ++c, ++gc) {
+            if (*abort_flag) { stop = true; break; }
+            const int b = gc & 1;
+            if (gc >= 2 && !mbar_wait(&accempty[b], ((gc >> 1) - 1) & 1, args.err, 6)) {
+              *abort_flag = 1;
+              stop = true;
+              break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t cr = tmem + b * 2 * BN, ci = cr + BN;
+            const int t_end = min(w.KT, (c + 1) * kChunkTiles);
+            bool first = true;
+            for (int t = c * kChunkTiles; t < t_end; ++t, ++g) {
+              const int s = g % STAGES;
+              if (!mbar_wait(&full[s], (g / STAGES) & 1, args.err, 2)) {
+                *abort_flag = 1;
+                stop = true;
+                break;
+              }
+              asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+              const uint32_t a0 = smem_u32(ring + s * STAGE_BYTES), b0 = a0 + PLANES * PLANE_BYTES;
+              const uint32_t hAr = a0, lAr = a0 + PLANE_BYTES, hAi = a0 + 2 * PLANE_BYTES, lAi = a0 + 3 * PLANE_BYTES;
+              const uint32_t hBr = b0, lBr = b0 + PLANE_BYTES, hBi = b0 + 2 * PLANE_BYTES, lBi = b0 + 3 * PLANE_BYTES;
+  #pragma unroll
+              for (int kk = 0; kk < BK / 8; ++kk) {
+                const uint32_t o = kk * 32;  // 8 tf32 = 32 bytes along the swizzled row
+                const uint32_t acc = first ? 0u : 1u;
+                // leading terms (hi,hi), then the corrections (lo,hi) and (hi,lo), all into this chunk's buffer
+                umma(cr, sw64_desc(hAr + o), sw64_desc(hBr + o), id_pos, acc);
+                umma(ci, sw64_desc(hAr + o), sw64_desc(hBi + o), id_pos, acc);
+                umma(cr, sw64_desc(hAi + o), sw64_desc(hBi + o), id_neg, 1);
+                umma(ci, sw64_desc(hAi + o), sw64_desc(hBr + o), id_pos, 1);
+                umma(cr, sw64_desc(lAr + o), sw64_desc(hBr + o), id_pos, 1);
+                umma(ci, sw64_desc(lAr + o), sw64_desc(hBi + o), id_pos, 1);
+                umma(cr, sw64_desc(lAi + o), sw64_desc(hBi + o), id_neg, 1);
+                umma(ci, sw64_desc(lAi + o), sw64_desc(hBr + o), id_pos, 1);
+                umma(cr, sw64_desc(hAr + o), sw64_desc(lBr + o), id_pos, 1);
+                umma(ci, sw64_desc(hAr + o), sw64_desc(lBi + o), id_pos, 1);
+                umma(cr, sw64_desc(hAi + o), sw64_desc(lBi + o), id_neg, 1);
+                umma(ci, sw64_desc(hAi + o), sw64_desc(lBr + o), id_pos, 1);
+                first = false;
+              }
+              umma_commit(&empty[s]);
+            }
+            if (stop) break;
+            umma_commit(&accfull[b]);
+          }
+        }
+        if (*abort_flag) {
+          umma_commit(drain);
+          mbar_wait(drain, 0, args.err, 8);
+        }
+      }
+    } else {
+      helpers();
+    }
+  } else if (warp < 12) {
+    // ------------------------------------------------------------ drain + epilogue (8 warps)
+    // Warp w reads TMEM lanes 32 * (w % 4) .. +31 (its output rows) and one half of the 128 columns.
+    // Every epilogue warp walks the same items and meets the same named barriers; after an abort (dead)
+    // it skips the waits and the stores but still meets the barriers.
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kDrainRegs));
+    const int quad = warp % 4, half = (warp - 4) / 4;
+    int gc = 0;
+    bool dead = false;
+    for (int it = blockIdx.x; it < args.n_items; it += gridDim.x) {
+      const Item w = item_of(it);
+      const int n_chunks = (w.KT + kChunkTiles - 1) / kChunkTiles;
+      float acc_re[kHalfCols], acc_im[kHalfCols];
+#pragma unroll
+      for (int j = 0; j < kHalfCols; ++j) acc_re[j] = acc_im[j] = 0.f;
+      for (int c = 0; c < n_chunks; ++c, ++gc) {
+        if (dead) continue;
+        const int b = gc & 1;
+        if (!mbar_wait_or_abort(&accfull[b], (gc >> 1) & 1, args.err, 5, abort_flag)) {
+          dead = true;
+          *abort_flag = 1;
+          continue;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + b * 2 * BN + half * kHalfCols;
+#pragma unroll
+        for (int c0 = 0; c0 < kHalfCols; c0 += 16) {
+          uint32_t vr[16], vi[16];
+          AB2_TMEM_LD16(ta + c0, vr);
+          AB2_TMEM_LD16(ta + BN + c0, vi);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            acc_re[c0 + j] += __uint_as_float(vr[j]);
+            acc_im[c0 + j] += __uint_as_float(vi[j]);
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        mbar_arrive(&accempty[b]);
+      }
+      if (*abort_flag) dead = true;
+      // Epilogue, one lane quadrant (32 output rows) at a time: its two drain warps stage their rows,
+      // then all 14 epilogue warps store them.
+      const ll row0 = (ll)w.tile_m * BM, col0 = (ll)w.tile_n * BN;
+      const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
+      const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
+#pragma unroll 1
+      for (int q = 0; q < BM / kStageRows; ++q) {
+        asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");  // the previous rows are out
+        if (quad == q && !dead) {
+#pragma unroll
+          for (int j = 0; j < kHalfCols; ++j) stage[stage_at(lane, half * kHalfCols + j)] = cf32{acc_re[j], acc_im[j]};
+        }
+        asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
+        if (!dead) store_pass(args, stage, q, w.z, w.split, row0, col0, rows, cols, warp - 2, threadIdx.x - 64, lane);
       }
     }
   } else {
-    // ------------------------------------------------------------ drain + epilogue (8 warps)
-    // Warp w reads TMEM lanes 32 * (w % 4) .. +31 (its output rows) and one half of the 128 columns.
-    const int quad = warp % 4, half = (warp - 2) / 4;
-    float acc_re[kHalfCols], acc_im[kHalfCols];
-#pragma unroll
-    for (int j = 0; j < kHalfCols; ++j) acc_re[j] = acc_im[j] = 0.f;
-    bool ok = true;
-    for (int c = 0; c < n_chunks; ++c) {
-      const int b = c & 1;
-      if (!mbar_wait_or_abort(&accfull[b], (c >> 1) & 1, args.err, 5, abort_flag)) {
-        ok = false;
-        *abort_flag = 1;
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t ta = tmem + ((uint32_t)(quad * 32) << 16) + b * 2 * BN + half * kHalfCols;
-#pragma unroll
-      for (int c0 = 0; c0 < kHalfCols; c0 += 16) {
-        uint32_t vr[16], vi[16];
-        AB2_TMEM_LD16(ta + c0, vr);
-        AB2_TMEM_LD16(ta + BN + c0, vi);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          acc_re[c0 + j] += __uint_as_float(vr[j]);
-          acc_im[c0 + j] += __uint_as_float(vi[j]);
-        }
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      mbar_arrive(&accempty[b]);
-    }
-    // Epilogue through shared memory: the last drain completed after every MMA, so the operand ring
-    // is free.  Stage the 128 x 128 complex tile row-major (rows padded by one element against bank
-    // conflicts), then write it out with consecutive threads on consecutive columns.
-    asm volatile("bar.sync 1, %0;" ::"n"(kDrainThreads) : "memory");  // every drain warp is past its loads
-    if (ok) {
-      cf32* tile = reinterpret_cast<cf32*>(ring) + (quad * 32 + lane) * kTileStride + half * kHalfCols;
-#pragma unroll
-      for (int j = 0; j < kHalfCols; ++j) tile[j] = cf32{acc_re[j], acc_im[j]};
-    }
-    asm volatile("bar.sync 1, %0;" ::"n"(kDrainThreads) : "memory");
-    if (ok && !*abort_flag) {
-      const cf32* tile = reinterpret_cast<const cf32*>(ring);
-      const ll row0 = (ll)tile_m * BM, col0 = (ll)tile_n * BN;
-      const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
-      const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
-      if (args.pk) {
-        const int lane = threadIdx.x & 31, lp = __ldg(args.pk_lane + lane);
-        const int dr = lp >> 16, dc = lp & 0xFFFF;
-        const ll plane = args.pk_plane;
-        float* tb = args.pk + (ll)(z / args.bt) * args.pk_slice + __ldg(args.pk_b + z % args.bt) +
-                    __ldg(args.pk_i + row0) + __ldg(args.pk_j + col0) + lane;
-        const int2* chunk = args.pk_chunk;
-        int q = (threadIdx.x - 64) >> 5;
-        int2 ch = q < args.pk_chunks ? __ldg(chunk + q) : make_int2(0, 0);
-        for (; q < args.pk_chunks; q += kDrainWarps) {
-          const int2 nx = q + kDrainWarps < args.pk_chunks ? __ldg(chunk + q + kDrainWarps) : ch;
-          const int r = (ch.x >> 16) + dr, c = (ch.x & 0xFFFF) + dc;
-          if (r < rows && c < cols) {
-            const cf32 v = tile[r * kTileStride + c];
-            float* d = tb + ch.y;
-            put_split(d, plane, 0, v.re);
-            put_split(d + 2 * plane, plane, 0, v.im);
-          }
-          ch = nx;
-        }
-      } else {
-        cf32* cbase = (args.part ? args.part + (ll)split * args.zc * args.m * args.n : args.C) + (ll)z * args.m * args.n;
-        cbase += row0 * args.n + col0;
-        for (int e = threadIdx.x - 64; e < rows * BN; e += kDrainThreads) {
-          const int r = e / BN, c = e % BN;
-          if (c < cols) cbase[(ll)r * args.n + c] = tile[r * kTileStride + c];
-        }
-      }
-    }
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kLowRegs));
+    helpers();
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
