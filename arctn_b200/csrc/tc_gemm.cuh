@@ -55,7 +55,7 @@ constexpr int kChunkTiles = 2;
 // accumulators in registers.  Warpgroup 3: store helpers (12..15).  The block launches at 128 registers
 // a thread; setmaxnreg then moves registers from warpgroups 0 and 3 (down to kLowRegs) to the drain
 // warpgroups (up to kDrainRegs): 2 x 128 x kLowRegs + 2 x 128 x kDrainRegs equals 512 x 128 exactly.
-constexpr int kThreads = 512, kLaunchRegs = 128, kLowRegs = 72, kDrainRegs = 184;
+constexpr int kThreads = 512, kLaunchRegs = 128, kLowRegs = 56, kDrainRegs = 200;
 static_assert(2 * 128 * kLowRegs + 2 * 128 * kDrainRegs == kThreads * kLaunchRegs, "register split must use the launch total");
 constexpr int kDrainWarps = 8, kDrainThreads = kDrainWarps * 32;
 constexpr int kEpiWarps = 14, kEpiThreads = kEpiWarps * 32;  // warps 2..15 share the epilogue stores
@@ -229,48 +229,102 @@ __device__ __forceinline__ int stage_at(int r, int c) {
   return r * BN + (c ^ (((q & 3) << 2) | (q >> 2)));
 }
 
+// Per-thread epilogue state.  For the fused pack: the lane's chunk pattern (dr, dc) and this warp's
+// chunk entries, loaded once per kernel (the chunk table is the same for every tile): warp ew takes
+// chunks qbeg[q] + ew + kEpiWarps * k of quadrant q, slot s = q * kq + k, held by lane s % 32 in e0
+// (s < 32) or e1; entries past a quadrant's end hold r0 = 0x7FFF (out of every tile).
+struct EpiState {
+  int dr = 0, dc = 0, kq = 0;
+  int2 e0 = make_int2(0x7FFF0000, 0), e1 = make_int2(0x7FFF0000, 0);
+};
+__device__ __forceinline__ EpiState epi_setup(const TcArgs& args, int ew, int lane) {
+  EpiState st;
+  if (!args.pk) return st;
+  const int lp = __ldg(args.pk_lane + lane);
+  st.dr = lp >> 16;
+  st.dc = lp & 0xFFFF;
+  int most = 0;
+#pragma unroll
+  for (int q = 0; q < BM / kStageRows; ++q) most = max(most, args.pk_qbeg[q + 1] - args.pk_qbeg[q]);
+  st.kq = (most + kEpiWarps - 1) / kEpiWarps;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int slot = lane + 32 * h, q = st.kq ? slot / st.kq : 0, k = st.kq ? slot % st.kq : 0;
+    int2 e = make_int2(0x7FFF0000, 0);
+    if (q < BM / kStageRows) {
+      const int ci = args.pk_qbeg[q] + ew + kEpiWarps * k;
+      if (ci < args.pk_qbeg[q + 1]) e = __ldg(args.pk_chunk + ci);
+    }
+    if (h == 0) st.e0 = e; else st.e1 = e;
+  }
+  return st;
+}
+// Where one tile's output goes: the four packed planes (fused) or its C / split-K partial block.
+struct EpiTile {
+  float* p0;
+  float* p1;
+  float* p2;
+  float* p3;
+  cf32* cbase;
+};
+__device__ __forceinline__ EpiTile epi_tile(const TcArgs& args, int z, int split, ll row0, ll col0, int lane) {
+  EpiTile t;
+  if (args.pk) {
+    t.p0 = args.pk + (ll)(z / args.bt) * args.pk_slice + __ldg(args.pk_b + z % args.bt) + __ldg(args.pk_i + row0) +
+           __ldg(args.pk_j + col0) + lane;
+    t.p1 = t.p0 + args.pk_plane;
+    t.p2 = t.p1 + args.pk_plane;
+    t.p3 = t.p2 + args.pk_plane;
+    t.cbase = nullptr;
+  } else {
+    t.p0 = t.p1 = t.p2 = t.p3 = nullptr;
+    t.cbase = (args.part ? args.part + (ll)split * args.zc * args.m * args.n : args.C) + (ll)z * args.m * args.n +
+              row0 * args.n + col0;
+  }
+  return t;
+}
+__device__ __forceinline__ void put_pair(float* hi, float* lo, ll o, float x) {
+  const uint32_t b = __float_as_uint(x), h = tf32_round(b);
+  hi[o] = __uint_as_float(h);
+  lo[o] = __uint_as_float(tf32_round(tf32_residual(b, h)));
+}
+
 // One pass of the epilogue store: output rows [r_lo, r_lo + 32) of the tile, staged in `stage`, written
 // by epilogue warp ew (0..13) / thread et (0..447) either as C rows or as packed 32-float chunks.
-__device__ __forceinline__ void store_pass(const TcArgs& args, const cf32* stage, int q, int z, int split, ll row0,
-                                           ll col0, int rows, int cols, int ew, int et, int lane) {
+__device__ __forceinline__ void store_pass(const TcArgs& args, const EpiState& es, const EpiTile& t, const cf32* stage,
+                                           int q, int rows, int cols, int et) {
   const int r_lo = q * kStageRows;
   if (r_lo >= rows) return;
   if (args.pk) {
-    const int lp = __ldg(args.pk_lane + lane);
-    const int dr = lp >> 16, dc = lp & 0xFFFF;
-    const ll plane = args.pk_plane;
-    float* tb = args.pk + (ll)(z / args.bt) * args.pk_slice + __ldg(args.pk_b + z % args.bt) + __ldg(args.pk_i + row0) +
-                __ldg(args.pk_j + col0) + lane;
-    const int2* chunk = args.pk_chunk;
-    const int q1 = args.pk_qbeg[q + 1];
     constexpr int U = 4;
-    for (int ci0 = args.pk_qbeg[q] + ew; ci0 < q1; ci0 += U * kEpiWarps) {
+    for (int k0 = 0; k0 < es.kq; k0 += U) {
       int2 ch[U];
       cf32 v[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int ci = ci0 + u * kEpiWarps;
-        ch[u] = ci < q1 ? __ldg(chunk + ci) : make_int2(0x7FFF0000, 0);
+        const int slot = q * es.kq + k0 + u;
+        const int2 e = slot < 32 ? es.e0 : es.e1;
+        ch[u].x = __shfl_sync(0xffffffffu, e.x, slot & 31);
+        ch[u].y = __shfl_sync(0xffffffffu, e.y, slot & 31);
+        if (k0 + u >= es.kq) ch[u].x = 0x7FFF0000;
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int r = (ch[u].x >> 16) + dr, c = (ch[u].x & 0xFFFF) + dc;
+        const int r = (ch[u].x >> 16) + es.dr, c = (ch[u].x & 0xFFFF) + es.dc;
         v[u] = (r < rows && c < cols) ? stage[stage_at(r - r_lo, c)] : cf32{0.f, 0.f};
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int r = (ch[u].x >> 16) + dr, c = (ch[u].x & 0xFFFF) + dc;
+        const int r = (ch[u].x >> 16) + es.dr, c = (ch[u].x & 0xFFFF) + es.dc;
         if (r < rows && c < cols) {
-          float* d = tb + ch[u].y;
-          put_split(d, plane, 0, v[u].re);
-          put_split(d + 2 * plane, plane, 0, v[u].im);
+          put_pair(t.p0, t.p1, ch[u].y, v[u].re);
+          put_pair(t.p2, t.p3, ch[u].y, v[u].im);
         }
       }
     }
   } else {
     const int nr = rows - r_lo < kStageRows ? rows - r_lo : kStageRows;
-    cf32* cbase = (args.part ? args.part + (ll)split * args.zc * args.m * args.n : args.C) + (ll)z * args.m * args.n +
-                  (row0 + r_lo) * args.n + col0;
+    cf32* cbase = t.cbase + (ll)r_lo * args.n;
     constexpr int U = 4;
     for (int e0 = et; e0 < nr * BN; e0 += U * kEpiThreads) {
       cf32 v[U];
@@ -344,18 +398,20 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
   // Store helpers (warps 2, 3, 12..15): they follow the drain warps' items and barriers and share the
   // stores of every staged pass.
   auto helpers = [&]() {
+    const EpiState es = epi_setup(args, warp - 2, lane);
     bool dead = false;
     for (int it = blockIdx.x; it < args.n_items; it += gridDim.x) {
       const Item w = item_of(it);
       const ll row0 = (ll)w.tile_m * BM, col0 = (ll)w.tile_n * BN;
       const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
       const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
+      const EpiTile t = epi_tile(args, w.z, w.split, row0, col0, lane);
 #pragma unroll 1
       for (int q = 0; q < BM / kStageRows; ++q) {
         asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
         asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
         if (*abort_flag) dead = true;
-        if (!dead) store_pass(args, stage, q, w.z, w.split, row0, col0, rows, cols, warp - 2, threadIdx.x - 64, lane);
+        if (!dead) store_pass(args, es, t, stage, q, rows, cols, threadIdx.x - 64);
       }
     }
   };
@@ -467,11 +523,14 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
     // it skips the waits and the stores but still meets the barriers.
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kDrainRegs));
     const int quad = warp % 4, half = (warp - 4) / 4;
+    const EpiState es = epi_setup(args, warp - 2, lane);
     int gc = 0;
     bool dead = false;
     for (int it = blockIdx.x; it < args.n_items; it += gridDim.x) {
       const Item w = item_of(it);
       const int n_chunks = (w.KT + kChunkTiles - 1) / kChunkTiles;
+      const ll row0 = (ll)w.tile_m * BM, col0 = (ll)w.tile_n * BN;
+      const EpiTile t = epi_tile(args, w.z, w.split, row0, col0, lane);  // loads overlap the drain below
       float acc_re[kHalfCols], acc_im[kHalfCols];
 #pragma unroll
       for (int j = 0; j < kHalfCols; ++j) acc_re[j] = acc_im[j] = 0.f;
@@ -503,7 +562,6 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
       if (*abort_flag) dead = true;
       // Epilogue, one lane quadrant (32 output rows) at a time: its two drain warps stage their rows,
       // then all 14 epilogue warps store them.
-      const ll row0 = (ll)w.tile_m * BM, col0 = (ll)w.tile_n * BN;
       const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
       const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
 #pragma unroll 1
@@ -514,7 +572,7 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
           for (int j = 0; j < kHalfCols; ++j) stage[stage_at(lane, half * kHalfCols + j)] = cf32{acc_re[j], acc_im[j]};
         }
         asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
-        if (!dead) store_pass(args, stage, q, w.z, w.split, row0, col0, rows, cols, warp - 2, threadIdx.x - 64, lane);
+        if (!dead) store_pass(args, es, t, stage, q, rows, cols, threadIdx.x - 64);
       }
     }
   } else {
