@@ -441,7 +441,8 @@ def run_grid8(args, dev):
     flops_fwd = p.flops
     total_ms = fwd_ms + bwd_ms
     value = 3 * flops_fwd / (total_ms * 1e-3) / 1e12  # forward F + two adjoint GEMMs per step (2F)
-    tf32_alg_peak = peaks()["bf16_tflops"] / 2 / 3  # split-TF32 4M: 3 TF32 products per real product
+    pk = peaks()
+    tf32_alg_peak = pk["bf16_tflops"] / 2 / 3  # split-TF32 4M: 3 TF32 products per real product
     line = _line(args, "grid8 bond6 c64 forward+adjoint TFLOP/s", value, "TFLOP/s", True, total_ms,
                  {"workload": "grid8x8_bond6_c64_adjoint", "precision": "tf32x3", "inputs_scaled_by": 4,
                   "l2": "flushed (256 MiB write) before each timed part"}, "c64",
@@ -449,7 +450,7 @@ def run_grid8(args, dev):
                  e2e=None,
                  roofline={"bound": "tensor", "achieved": value, "peak": tf32_alg_peak, "unit": "TFLOP/s",
                            "frac": value / tf32_alg_peak,
-                           "peak_source": "measured bf16 dense burst / 2 (TF32) / 3 (split-TF32 products)",
+                           "peak_source": f"{pk['source']} bf16 dense burst / 2 (TF32) / 3 (split-TF32 products)",
                            "traffic": None},
                  cpu_baseline=None, clocks=clocks, device_status=status,
                  fwd_ms=fwd_ms, bwd_ms=bwd_ms, bwd_over_fwd=bwd_ms / fwd_ms,
