@@ -189,6 +189,73 @@ def cpu_baseline(net, arrays, path, sliced, total_slices, flops_total, threads=N
             "wall_s": dt, "host_cores": cores}
 
 
+def numpy_tensordot_baseline(net, arrays, path, sliced, total_slices, flops_total, budget_s=10.0, max_slices=16):
+    """A second CPU reference point: NumPy, one ``tensordot`` (BLAS) per pairwise step of the same plan, as the
+    reference paper's NumPy executor does.  Slices 0, 1, ... of the sliced contraction run until about
+    ``budget_s`` seconds have passed; inputs are narrowed along the sliced legs (last sliced leg fastest,
+    src/slice.rs:881-888) and each step applies its dangling sums, contracts its shared legs and permutes the
+    result to the plan's leg order (src/compiled.rs:155-171)."""
+    import arctn_b200 as A
+
+    sub = dict(net.size_dict)
+    for leg in sliced:
+        sub[leg] = 1
+    cc = A.CompiledContraction.compile(net.inputs, net.output, sub, ssa_path=path)
+    if any(not p.is_identity() for p in cc.input_preps()):  # traces / diagonals: not this executor's form
+        return None
+    dims = [net.size_dict[leg] for leg in sliced]
+
+    def one_slice(si):
+        digits = {}
+        for leg, d in zip(reversed(sliced), reversed(dims)):
+            digits[leg] = si % d
+            si //= d
+        slots = []
+        for legs, a in zip(net.inputs, arrays):
+            idx = tuple(slice(digits[l], digits[l] + 1) if l in digits else slice(None) for l in legs)
+            slots.append(a[idx])
+        for st in cc.pair_steps():
+            a, b = slots[st.left_slot()], slots[st.right_slot()]
+            wa, wb = list(st.left_legs()), list(st.right_legs())
+            for ax in st.sum_a():
+                a = a.sum(axis=ax)
+                del wa[ax]
+            for ax in st.sum_b():
+                b = b.sum(axis=ax)
+                del wb[ax]
+            out = list(st.result_legs())
+            con = [l for l in wa if l in wb and l not in out]
+            if any(l in wb and l in out for l in wa):  # batch legs: no tensordot form
+                letters = {l: chr(97 + i) for i, l in enumerate(dict.fromkeys(wa + wb))}
+                spec = "".join(letters[l] for l in wa) + "," + "".join(letters[l] for l in wb) + "->" + \
+                       "".join(letters[l] for l in out)
+                c = np.einsum(spec, a, b, optimize=True)
+            else:
+                c = np.tensordot(a, b, axes=([wa.index(l) for l in con], [wb.index(l) for l in con]))
+                got = [l for l in wa if l not in con] + [l for l in wb if l not in con]
+                c = c.transpose([got.index(l) for l in out]).copy()  # contiguous, 0-d stays 0-d
+            slots.append(c)
+        fin = cc.finalize()
+        r = slots[fin.slot()]
+        for ax in fin.sum_axes():
+            r = r.sum(axis=ax)
+        return np.transpose(r, fin.perm()).astype(np.complex128)
+
+    one_slice(0)  # warm-up: BLAS threads and page faults
+    t0 = time.perf_counter()
+    n = 0
+    acc = 0
+    while n < min(max_slices, total_slices) and (n == 0 or time.perf_counter() - t0 < budget_s):
+        acc = acc + one_slice(n)
+        n += 1
+    dt = time.perf_counter() - t0
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    return {"value": flops_total / total_slices * n / dt / 1e12, "unit": "TFLOP/s", "cores": cores,
+            "kind": "numpy", "sample": f"slices [0,{n}) of {total_slices} in sequence, {dt:.1f} s wall; NumPy "
+                                       f"{np.__version__} tensordot per step on the host BLAS threads",
+            "partial_sum": [float(np.real(acc).sum()), float(np.imag(acc).sum())]}
+
+
 def run_reference(args, net, arrays, path, sliced, name, rank):
     """--impl reference: the reference's CPU executor path (its oracle restatement) on the host cores."""
     if rank != 0:
@@ -576,8 +643,16 @@ def main():
         dist.all_reduce(f)
         flops_all = float(f.item())
     value = flops_all / (ms_per_step * 1e-3) / 1e12
+    # The reference's own unit (src/bin/tnexec.rs:4-5): Sum over steps of the product of the step's leg
+    # dimensions, a complex multiply counted as 1, per slice (sliced legs at dimension 1) times the slices.
+    sub = dict(net.size_dict)
+    for leg in sliced:
+        sub[leg] = 1
+    ref_flops = 10 ** A.simulate_path(net.inputs, net.output, sub, path)["log10_flops"] * total
+    reference_unit = {"unit": "GFLOPS (tnexec: Sum_steps prod(step leg dims), complex multiply = 1)",
+                      "value": ref_flops / (ms_per_step * 1e-3) / 1e9, "flops_per_contraction": ref_flops}
 
-    extras = {}
+    extras = {"reference_unit": reference_unit}
     e2e = None
     if world == 1 and not args.no_extras:
         # End to end through the public API: host (NumPy) inputs copied in, the scalar result copied out.
@@ -604,9 +679,9 @@ def main():
         ref = complex(prog64.execute(x64, workspace=ws64, stream=stream).item())
         del ws64, prog64
         rel = lambda v: abs(complex(v) - ref) / abs(ref)  # noqa: E731
-        extras = {"other_precision": other, "other_value": prog.flops / (ms2 * 1e-3) / 1e12,
-                  "speedup_vs_other": ms2 / ms_per_step, "rel_err_vs_fp64": rel(r.item()),
-                  "other_rel_err_vs_fp64": rel(r2.item()), "fp64_result": [ref.real, ref.imag]}
+        extras.update({"other_precision": other, "other_value": prog.flops / (ms2 * 1e-3) / 1e12,
+                       "speedup_vs_other": ms2 / ms_per_step, "rel_err_vs_fp64": rel(r.item()),
+                       "other_rel_err_vs_fp64": rel(r2.item()), "fp64_result": [ref.real, ref.imag]})
 
     roof = None
     pk = peaks()
@@ -654,6 +729,10 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(net, arrays, path, sliced, total, prog.flops)
         cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        try:
+            cpu["numpy_tensordot"] = numpy_tensordot_baseline(net, arrays, path, sliced, total, prog.flops)
+        except MemoryError:
+            cpu["numpy_tensordot"] = None
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
