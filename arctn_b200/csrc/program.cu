@@ -116,10 +116,11 @@ void pick(const View& v, const std::vector<size_t>& axes, std::vector<u64>& dims
 Program::Program(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced, const ProgramOptions& opt)
     : opt_(opt) {
   dtype_bytes(opt_.dtype);
-  if (opt_.precision != PREC_FP32 && opt_.precision != PREC_TF32X3)
+  if (opt_.precision != PREC_FP32 && opt_.precision != PREC_TF32X3 && opt_.precision != PREC_BF16X3)
     throw Error(E_INVALID, "unsupported precision mode " + std::to_string(opt_.precision));
-  if (opt_.tc_k_chunk % tc::BK != 0 || opt_.tc_k_chunk > (1ull << 30))
-    throw Error(E_INVALID, "tc_k_chunk must be a multiple of 16 (0 for the default)");
+  const u64 k_unit = opt_.precision == PREC_BF16X3 ? 2 * tc::BK : tc::BK;  // K per packed 64-byte row
+  if (opt_.tc_k_chunk % k_unit != 0 || opt_.tc_k_chunk > (1ull << 30))
+    throw Error(E_INVALID, "tc_k_chunk must be a multiple of " + std::to_string(k_unit) + " (0 for the default)");
   build(net, path, sliced);
   if (opt_.gradient && !sliced_) {
     // Over the workspace budget: drop the largest step results from what the adjoint sweep keeps
@@ -608,11 +609,14 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     // A single 16-wide K tile (no K split possible) only pays once the slice group or the batch gives
     // every SM an output tile; its epilogue can then write the next GEMM's packed operand directly.
     const u64 tc_tiles = ((m + tc::BM - 1) / tc::BM) * ((n + tc::BN - 1) / tc::BN) * bt;
-    const bool use_tc = opt_.precision == PREC_TF32X3 && dt == DT_C64 &&
+    const bool bf16 = opt_.precision == PREC_BF16X3;
+    const bool use_tc = (opt_.precision == PREC_TF32X3 || bf16) && dt == DT_C64 &&
                         ((k >= 32 && ((m >= 96 && n >= 96) || (std::min(m, n) >= 16 && k >= 256))) ||
                          (k >= 16 && m >= 96 && n >= 96 && (ph2 || tc_tiles >= (u64)kNumSMs)));
     if (use_tc) {
-      const ll kpad = ((ll)k + tc::BK - 1) / tc::BK * tc::BK;
+      const ll kt_el = bf16 ? 2 * tc::BK : tc::BK;  // K per 64-byte packed row
+      const ll el = bf16 ? 2 : 4;                  // bytes per plane element
+      const ll kpad = ((ll)k + kt_el - 1) / kt_el * kt_el;
       const ll rpa = ((ll)m + tc::BM - 1) / tc::BM * tc::BM;
       const ll rpb = ((ll)n + tc::BN - 1) / tc::BN * tc::BN;
       // A phase-2 operand that is the whole unsplit output of an earlier tensor-core GEMM, read by nothing
@@ -621,7 +625,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       // layouts without padding (nothing to zero first) qualify whose tables repeat from one output tile
       // to the next and whose packed runs inside a tile average at least 32 floats (coalesced stores).
       auto fuse_into_producer = [&](const Operand& X, ll rows, ll rpad, bool conj, u64 pbuf) -> bool {
-        if (!ph2 || !X.variant || opt_.gradient || conj || X.ref.kind != Ref::WS || X.so.n != 0) return false;
+        if (bf16 || !ph2 || !X.variant || opt_.gradient || conj || X.ref.kind != Ref::WS || X.so.n != 0) return false;
         if (rows != rpad || (ll)k != kpad) return false;
         size_t pi = ops2.size();
         for (size_t q = ops2.size(); q-- > 0;)
@@ -716,10 +720,11 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         return true;
       };
       auto pack = [&](const Operand& X, ll rows, ll rpad, bool conj) {
-        const u64 pbuf = new_buf(ph2, (u64)(tc::PLANES * (ll)bt * rpad * kpad * 4), opidx(ph2));
+        const u64 pbuf = new_buf(ph2, (u64)(tc::PLANES * (ll)bt * rpad * kpad * el), opidx(ph2));
         bufs[pbuf].fixed = ph2 && !X.variant;
         if (fuse_into_producer(X, rows, rpad, conj, pbuf)) return pbuf;
         Op p{Op::PACK};
+        p.bf16 = bf16;
         p.a = X.ref;
         p.sa = X.so;
         p.c = Ref{Ref::WS, pbuf};
@@ -741,6 +746,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
             z.kpad = kpad;
             z.bt = (ll)bt;
             z.a_var = X.variant;
+            z.bf16 = bf16;
             emit(ph2, z, fwd);
           }
         } else {
@@ -757,10 +763,10 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       touch(Ref{Ref::WS, pa}, ph2, opidx(ph2));
       // K split across CTAs (see TcArgs): partials [split][z][m][n].  A caller's tc_k_chunk fixes the
       // chunk; otherwise only a one-slice GEMM with too few tiles to fill the GPU is split.
-      const int kt_total = (int)(kpad / tc::BK);
+      const int kt_total = (int)(kpad / kt_el);
       int chunk = kt_total;
       if (opt_.tc_k_chunk) {
-        chunk = (int)(opt_.tc_k_chunk / tc::BK);
+        chunk = (int)std::max<ll>(1, (ll)opt_.tc_k_chunk / kt_el);
       } else if (!ph2) {
         const ll ctas = (rpa / tc::BM) * (rpb / tc::BN) * (ll)bt;
         const ll want = std::min<ll>((2 * kNumSMs + ctas - 1) / ctas, kt_total / kMinSplitTiles);
@@ -775,6 +781,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         touch(g.d, ph2, opidx(ph2));
       }
       g.kind = Op::GEMM_TC;
+      g.bf16 = bf16;
       g.a = Ref{Ref::WS, pa};
       g.b = Ref{Ref::WS, pb};
       g.rpad = rpa;
@@ -1404,13 +1411,16 @@ EncodeTiled encode_fn() {
 }
 
 // [re|im][z][rows][kpad] fp32 planes, boxes of 16 x 128 with 64-byte swizzle.
-CUtensorMap plane_map(void* base, ll kpad, ll rows, ll zplanes) {
+// Split-TF32 planes are fp32 (boxes of 16 x 128), split-BF16 planes bf16 (boxes of 32 x 128): 64-byte rows either way.
+CUtensorMap plane_map(void* base, ll kpad, ll rows, ll zplanes, bool bf16) {
   CUtensorMap m;
+  const ll el = bf16 ? 2 : 4;
   cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows, (cuuint64_t)zplanes};
-  cuuint64_t strides[2] = {(cuuint64_t)(kpad * 4), (cuuint64_t)(kpad * rows * 4)};
-  cuuint32_t box[3] = {(cuuint32_t)tc::BK, (cuuint32_t)tc::BM, 1};
+  cuuint64_t strides[2] = {(cuuint64_t)(kpad * el), (cuuint64_t)(kpad * rows * el)};
+  cuuint32_t box[3] = {(cuuint32_t)(bf16 ? 2 * tc::BK : tc::BK), (cuuint32_t)tc::BM, 1};
   cuuint32_t estr[3] = {1, 1, 1};
-  CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+  CUresult r = encode_fn()(&m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base,
+                           dims, strides, box, estr,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw Error(E_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
@@ -1422,44 +1432,60 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   if (op.kind == Op::PACK) {
     const ll Z = (op.a_var ? op.S : 1) * op.bt;
     const ll tiles = Z * (op.rpad / 32) * ((op.kpad + 31) / 32);
-    tc::k_pack_planar<<<(int)std::min<ll>(tiles, 148 * 16), 256, 0, st>>>(
-        (const cf32*)A, (float*)C, (const ll*)(tab + op.tab[0]), (const ll*)(tab + op.tab[1]),
-        (const ll*)(tab + op.tab[2]), op.bt, op.rows, op.cols, op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0,
-        op.conj_a ? 1 : 0);
+    const int grid = (int)std::min<ll>(tiles, 148 * 16);
+    if (op.bf16)
+      tc::k_pack_planar<__nv_bfloat16><<<grid, 256, 0, st>>>(
+          (const cf32*)A, (__nv_bfloat16*)C, (const ll*)(tab + op.tab[0]), (const ll*)(tab + op.tab[1]),
+          (const ll*)(tab + op.tab[2]), op.bt, op.rows, op.cols, op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0,
+          op.conj_a ? 1 : 0);
+    else
+      tc::k_pack_planar<float><<<grid, 256, 0, st>>>(
+          (const cf32*)A, (float*)C, (const ll*)(tab + op.tab[0]), (const ll*)(tab + op.tab[1]),
+          (const ll*)(tab + op.tab[2]), op.bt, op.rows, op.cols, op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0,
+          op.conj_a ? 1 : 0);
     return;
   }
   if (op.kind == Op::PACK_TILED) {
     const ll n_slices = op.a_var ? op.S : 1;
     const ll slice_stride = op.bt * op.rpad * op.kpad;
     const ll plane = n_slices * slice_stride;
-    tc::k_pack_tiled<<<(int)std::min<ll>(op.n_outer * n_slices, 148 * 6), tc::kPackThreads, 0, st>>>(
-        (const cf32*)A, (float*)C, (const int*)(tab + op.tab[0]), (const int*)(tab + op.tab[1]),
-        (const int*)(tab + op.tab[2]), (int)op.tile_T, (const ll*)(tab + op.tab[4]), (const ll*)(tab + op.tab[5]),
-        op.n_outer, n_slices, slice_stride, plane, op.sa, op.g0, op.conj_a ? 1 : 0);
+    const int grid = (int)std::min<ll>(op.n_outer * n_slices, 148 * 6);
+    if (op.bf16)
+      tc::k_pack_tiled<__nv_bfloat16><<<grid, tc::kPackThreads, 0, st>>>(
+          (const cf32*)A, (__nv_bfloat16*)C, (const int*)(tab + op.tab[0]), (const int*)(tab + op.tab[1]),
+          (const int*)(tab + op.tab[2]), (int)op.tile_T, (const ll*)(tab + op.tab[4]), (const ll*)(tab + op.tab[5]),
+          op.n_outer, n_slices, slice_stride, plane, op.sa, op.g0, op.conj_a ? 1 : 0);
+    else
+      tc::k_pack_tiled<float><<<grid, tc::kPackThreads, 0, st>>>(
+          (const cf32*)A, (float*)C, (const int*)(tab + op.tab[0]), (const int*)(tab + op.tab[1]),
+          (const int*)(tab + op.tab[2]), (int)op.tile_T, (const ll*)(tab + op.tab[4]), (const ll*)(tab + op.tab[5]),
+          op.n_outer, n_slices, slice_stride, plane, op.sa, op.g0, op.conj_a ? 1 : 0);
     return;
   }
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
-    CK(cudaFuncSetAttribute(tc::k_tc_cgemm_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
-    // The kernel's setmaxnreg split assumes exactly kLaunchRegs registers a thread at launch.
-    cudaFuncAttributes fa{};
-    CK(cudaFuncGetAttributes(&fa, tc::k_tc_cgemm_tf32x3));
-    if (fa.numRegs != tc::kLaunchRegs)
-      throw Error(E_UNSUPPORTED, "tensor-core GEMM built with " + std::to_string(fa.numRegs) + " registers a thread, not " +
-                                     std::to_string(tc::kLaunchRegs));
+    for (auto kern : {tc::k_tc_cgemm_tf32x3, tc::k_tc_cgemm_bf16x3}) {
+      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+      // The kernel's setmaxnreg split assumes exactly kLaunchRegs registers a thread at launch.
+      cudaFuncAttributes fa{};
+      CK(cudaFuncGetAttributes(&fa, kern));
+      if (fa.numRegs != tc::kLaunchRegs)
+        throw Error(E_UNSUPPORTED, "tensor-core GEMM built with " + std::to_string(fa.numRegs) +
+                                       " registers a thread, not " + std::to_string(tc::kLaunchRegs));
+    }
     attr_set[dev] = true;
   }
   const ll s_eff = (op.a_var || op.b_var) ? op.S : 1;
   const ll za = (op.a_var ? op.S : 1) * op.bt, zb = (op.b_var ? op.S : 1) * op.bt;
-  const CUtensorMap ma = plane_map(A, op.kpad, op.rpad, tc::PLANES * za);
-  const CUtensorMap mb = plane_map(B, op.kpad, op.rpad_b, tc::PLANES * zb);
+  const CUtensorMap ma = plane_map(A, op.kpad, op.rpad, tc::PLANES * za, op.bf16);
+  const CUtensorMap mb = plane_map(B, op.kpad, op.rpad_b, tc::PLANES * zb, op.bf16);
   tc::TcArgs args;
   args.C = (cf32*)C;
   args.m = op.m;
   args.n = op.n;
-  args.k_tiles = (int)(op.kpad / tc::BK);
+  args.k_tiles = (int)(op.kpad / (op.bf16 ? 2 * tc::BK : tc::BK));
   args.za = (int)za;
   args.zb = (int)zb;
   args.bt = (int)op.bt;
@@ -1494,7 +1520,10 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   static int sms[64] = {};
   if (dev < 64 && !sms[dev]) CK(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
   const int n_sm = dev < 64 ? sms[dev] : 148;
-  tc::k_tc_cgemm_tf32x3<<<(unsigned)std::min<ll>(items, n_sm), tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
+  if (op.bf16)
+    tc::k_tc_cgemm_bf16x3<<<(unsigned)std::min<ll>(items, n_sm), tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
+  else
+    tc::k_tc_cgemm_tf32x3<<<(unsigned)std::min<ll>(items, n_sm), tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
   if (op.splits > 1) {
     const ll count = zc * op.m * op.n;
     tc::k_splitk_reduce<<<grid_for(count), 256, 0, st>>>((const cf32*)D, (cf32*)C, count, op.splits);
@@ -1516,7 +1545,8 @@ void Program::launch_op(const Op& op, const void* const* inputs, void* output, c
   };
   if (op.kind == Op::MEMSET) {
     // bytes == 0: the padded planes of a tiled pack, [4 planes][slices of this group][bt][rpad][kpad] fp32
-    const u64 bytes = op.bytes ? op.bytes : (u64)(tc::PLANES * (op.a_var ? op.S : 1) * op.bt * op.rpad * op.kpad * 4);
+    const u64 bytes = op.bytes ? op.bytes
+                               : (u64)(tc::PLANES * (op.a_var ? op.S : 1) * op.bt * op.rpad * op.kpad * (op.bf16 ? 2 : 4));
     CK(cudaMemsetAsync(ptr(op.c), 0, bytes, st));
     return;
   }
@@ -1631,8 +1661,8 @@ double op_work(const Op& op, int dt) {
     case Op::ACCUM: return (double)op.n_segs * op.n_e * (2.0 * wide_bytes(dt)) + (double)op.S * op.n_e * eb;
     case Op::OUTPUT: return (double)op.n_blocks * op.n_chunks * op.n_e * wide_bytes(dt);
     case Op::PACK:
-    case Op::PACK_TILED:  // complex64 read once, four fp32 planes written (padding included)
-      return (double)(op.a_var ? op.S : 1) * op.bt * (8.0 * op.rows * op.cols + 16.0 * op.rpad * op.kpad);
+    case Op::PACK_TILED:  // complex64 read once, four fp32 (or bf16) planes written (padding included)
+      return (double)(op.a_var ? op.S : 1) * op.bt * (8.0 * op.rows * op.cols + (op.bf16 ? 8.0 : 16.0) * op.rpad * op.kpad);
     default: return (double)op.n_out * eb;
   }
 }
@@ -1760,10 +1790,11 @@ std::string Program::describe() const {
         f("S", op.S); f("bt", op.bt); f("m", op.m); f("k", op.k); f("n", op.n);
         f("splits", op.splits); f("conj_a", op.conj_a); f("conj_b", op.conj_b);
         if (op.pk.kind != Ref::NONE) f("pack_into", (long long)op.pk.index);
+        if (op.kind == Op::GEMM_TC) f("bf16", op.bf16);
         break;
       case Op::PACK: case Op::PACK_TILED:
         f("S", op.a_var ? op.S : 1); f("bt", op.bt); f("rows", op.rows); f("cols", op.cols); f("rpad", op.rpad);
-        f("kpad", op.kpad); f("tile", op.tile_T); f("n_outer", op.n_outer);
+        f("kpad", op.kpad); f("tile", op.tile_T); f("n_outer", op.n_outer); f("bf16", op.bf16);
         break;
       case Op::GATHER: case Op::SCATTER: case Op::MAXABS: case Op::STRIP:
         f("S", op.S); f("n_out", op.n_out); f("n_red", op.n_red);

@@ -17,7 +17,7 @@
 namespace ab2 {
 
 enum : int { DT_F32 = 0, DT_F64 = 1, DT_C64 = 2, DT_C128 = 3 };
-enum : int { PREC_FP32 = 0, PREC_TF32X3 = 1 };
+enum : int { PREC_FP32 = 0, PREC_TF32X3 = 1, PREC_BF16X3 = 2 };
 
 size_t dtype_bytes(int dt);
 inline bool dtype_complex(int dt) { return dt == DT_C64 || dt == DT_C128; }
@@ -64,6 +64,7 @@ struct Op {
   int kt_chunk = 0;
   Ref d;                                // GEMM_TC: FP32 split-K partial buffer
   bool bwd = false;                     // part of the adjoint sweep (skipped by a plain execute)
+  bool bf16 = false;                    // PACK / PACK_TILED / GEMM_TC / their MEMSET: split-BF16 planes
   // GEMM_TC whose epilogue writes the next GEMM's packed operand instead of `c`: the pack buffer, the
   // offset tables over the output's rows, columns and batch, the tile's 32-float chunks and their lane
   // pattern, and the packed size of one slice.

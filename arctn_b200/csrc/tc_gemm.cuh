@@ -25,6 +25,7 @@
 #pragma once
 
 #include <cuda.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -78,6 +79,13 @@ __device__ __forceinline__ void put_split(float* dst, ll plane, ll o, float x) {
   const uint32_t b = __float_as_uint(x), h = tf32_round(b);
   dst[o] = __uint_as_float(h);
   dst[plane + o] = __uint_as_float(tf32_round(tf32_residual(b, h)));
+}
+// Split-BF16 planes: hi = x rounded to BF16, lo = (x - hi) rounded to BF16.  x - hi is exact in FP32 (hi is
+// within half a BF16 unit of x), so hi + lo carries x to about 2^-18 relative.
+__device__ __forceinline__ void put_split(__nv_bfloat16* dst, ll plane, ll o, float x) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  dst[o] = h;
+  dst[plane + o] = __float2bfloat16_rn(x - __bfloat162float(h));
 }
 __device__ __forceinline__ unsigned long long now_ns() {
   unsigned long long t;
@@ -136,11 +144,26 @@ __host__ __device__ constexpr uint32_t idesc_tf32(bool neg_a) {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(BN >> 3) << 17) |
          ((uint32_t)(BM >> 4) << 24);
 }
+// kind::f16 with A and B both BF16 (one format code for both operands), FP32 accumulate, K-major, M = N = 128.
+__host__ __device__ constexpr uint32_t idesc_bf16(bool neg_a) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(BN >> 3) << 17) |
+         ((uint32_t)(BM >> 4) << 24);
+}
+template <bool kBF16>
+__host__ __device__ constexpr uint32_t idesc_for(bool neg_a) { return kBF16 ? idesc_bf16(neg_a) : idesc_tf32(neg_a); }
 
+// One MMA: TF32 operands cover 8 of K in the 32 bytes of each operand row it reads, BF16 operands 16.
+template <bool kBF16>
 __device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n"
-      ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+  if constexpr (kBF16) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+  } else {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n"
+        ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+  }
 }
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
@@ -342,9 +365,11 @@ __device__ __forceinline__ void store_pass(const TcArgs& args, const EpiState& e
   }
 }
 
-static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __grid_constant__ CUtensorMap tmA,
-                                                                const __grid_constant__ CUtensorMap tmB,
-                                                                TcArgs args) {
+// The GEMM body for either operand format: split-TF32 (4-byte planes, 16 of K per 64-byte operand row) or
+// split-BF16 (2-byte planes, 32 of K per row).  Shared-memory layout, swizzle, TMEM and epilogue are the same.
+template <bool kBF16>
+__device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcArgs& args) {
+  constexpr int KT_ELEMS = kBF16 ? 2 * BK : BK;  // K per 64-byte operand row
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* ring = smem;                                  // STAGES x {A planes, B planes}
@@ -435,7 +460,7 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
             if (*abort_flag) { stop = true; break; }
             unsigned char* dst = ring + s * STAGE_BYTES;
             mbar_expect_tx(&full[s], STAGE_BYTES);
-            const int k0 = (w.kt0 + t) * BK;
+            const int k0 = (w.kt0 + t) * KT_ELEMS;
   #pragma unroll
             for (int p = 0; p < PLANES; ++p) {
               tma_load_3d(&tmA, &full[s], dst + p * PLANE_BYTES, k0, w.tile_m * BM, w.zA + p * args.za);
@@ -454,7 +479,7 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
       // gc counts chunks over all items: TMEM buffer gc & 1.  The issuer runs up to two chunks ahead
       // of the drain warps, so the next item's first chunks overlap the previous item's epilogue.
       if (lane == 0) {
-        const uint32_t id_pos = idesc_tf32(false), id_neg = idesc_tf32(true);
+        const uint32_t id_pos = idesc_for<kBF16>(false), id_neg = idesc_for<kBF16>(true);
         int g = 0, gc = 0;
         bool stop = false;
         for (int it = blockIdx.x; it < args.n_items && !stop; it += gridDim.x) {
@@ -485,21 +510,21 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
               const uint32_t hBr = b0, lBr = b0 + PLANE_BYTES, hBi = b0 + 2 * PLANE_BYTES, lBi = b0 + 3 * PLANE_BYTES;
   #pragma unroll
               for (int kk = 0; kk < BK / 8; ++kk) {
-                const uint32_t o = kk * 32;  // 8 tf32 = 32 bytes along the swizzled row
+                const uint32_t o = kk * 32;  // 8 tf32 or 16 bf16 = 32 bytes along the swizzled row
                 const uint32_t acc = first ? 0u : 1u;
                 // leading terms (hi,hi), then the corrections (lo,hi) and (hi,lo), all into this chunk's buffer
-                umma(cr, sw64_desc(hAr + o), sw64_desc(hBr + o), id_pos, acc);
-                umma(ci, sw64_desc(hAr + o), sw64_desc(hBi + o), id_pos, acc);
-                umma(cr, sw64_desc(hAi + o), sw64_desc(hBi + o), id_neg, 1);
-                umma(ci, sw64_desc(hAi + o), sw64_desc(hBr + o), id_pos, 1);
-                umma(cr, sw64_desc(lAr + o), sw64_desc(hBr + o), id_pos, 1);
-                umma(ci, sw64_desc(lAr + o), sw64_desc(hBi + o), id_pos, 1);
-                umma(cr, sw64_desc(lAi + o), sw64_desc(hBi + o), id_neg, 1);
-                umma(ci, sw64_desc(lAi + o), sw64_desc(hBr + o), id_pos, 1);
-                umma(cr, sw64_desc(hAr + o), sw64_desc(lBr + o), id_pos, 1);
-                umma(ci, sw64_desc(hAr + o), sw64_desc(lBi + o), id_pos, 1);
-                umma(cr, sw64_desc(hAi + o), sw64_desc(lBi + o), id_neg, 1);
-                umma(ci, sw64_desc(hAi + o), sw64_desc(lBr + o), id_pos, 1);
+                umma<kBF16>(cr, sw64_desc(hAr + o), sw64_desc(hBr + o), id_pos, acc);
+                umma<kBF16>(ci, sw64_desc(hAr + o), sw64_desc(hBi + o), id_pos, acc);
+                umma<kBF16>(cr, sw64_desc(hAi + o), sw64_desc(hBi + o), id_neg, 1);
+                umma<kBF16>(ci, sw64_desc(hAi + o), sw64_desc(hBr + o), id_pos, 1);
+                umma<kBF16>(cr, sw64_desc(lAr + o), sw64_desc(hBr + o), id_pos, 1);
+                umma<kBF16>(ci, sw64_desc(lAr + o), sw64_desc(hBi + o), id_pos, 1);
+                umma<kBF16>(cr, sw64_desc(lAi + o), sw64_desc(hBi + o), id_neg, 1);
+                umma<kBF16>(ci, sw64_desc(lAi + o), sw64_desc(hBr + o), id_pos, 1);
+                umma<kBF16>(cr, sw64_desc(hAr + o), sw64_desc(lBr + o), id_pos, 1);
+                umma<kBF16>(ci, sw64_desc(hAr + o), sw64_desc(lBi + o), id_pos, 1);
+                umma<kBF16>(cr, sw64_desc(hAi + o), sw64_desc(lBi + o), id_neg, 1);
+                umma<kBF16>(ci, sw64_desc(hAi + o), sw64_desc(lBr + o), id_pos, 1);
                 first = false;
               }
               umma_commit(&empty[s]);
@@ -587,6 +612,18 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
   }
 }
 
+static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __grid_constant__ CUtensorMap tmA,
+                                                                const __grid_constant__ CUtensorMap tmB,
+                                                                TcArgs args) {
+  tc_cgemm_body<false>(tmA, tmB, args);
+}
+// Split-BF16: operands packed as BF16 hi/lo planes, 3 BF16 products per real product (kind::f16).
+static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_bf16x3(const __grid_constant__ CUtensorMap tmA,
+                                                                const __grid_constant__ CUtensorMap tmB,
+                                                                TcArgs args) {
+  tc_cgemm_body<true>(tmA, tmB, args);
+}
+
 // Leg-aware pack: the same gather as k_pack_planar, for operands whose legs are scattered (as in
 // networks of dimension-2 legs).  The host picks tile legs -- those innermost in the source plus those
 // innermost in the packed destination, at most kPackTile elements -- and numbers the tile's elements
@@ -598,8 +635,9 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
 constexpr int kPackTile = 1024;
 constexpr int kPackThreads = 256;
 __device__ __forceinline__ int pack_swz(int e) { return e ^ ((e >> 5) & 31); }
+template <typename PT>  // plane element: float (split-TF32) or __nv_bfloat16 (split-BF16)
 static __global__ void __launch_bounds__(kPackThreads, 6) k_pack_tiled(
-    const cf32* __restrict__ src, float* __restrict__ dst, const int* __restrict__ rd_rank,
+    const cf32* __restrict__ src, PT* __restrict__ dst, const int* __restrict__ rd_rank,
     const int* __restrict__ rd_off, const int* __restrict__ wr_off, int T, const ll* __restrict__ src_base,
     const ll* __restrict__ dst_base, ll n_outer, ll n_slices, ll dst_slice_stride, ll plane, SliceOff so, ll g0,
     int conj) {
@@ -637,7 +675,7 @@ static __global__ void __launch_bounds__(kPackThreads, 6) k_pack_tiled(
     const ll next = blk + gridDim.x;
     if (next < n_blk) load(next, nv);
     const ll s = blk / n_outer, o = blk - s * n_outer;
-    float* db = dst + s * dst_slice_stride + dst_base[o];
+    PT* db = dst + s * dst_slice_stride + dst_base[o];
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
       const int i = threadIdx.x + j * kPackThreads;
@@ -672,7 +710,8 @@ static __global__ void k_splitk_reduce(const cf32* __restrict__ part, cf32* __re
 // This is the permute of the reference step (src/tensor.rs:453-492) fused with the planar split.
 // A 32 x 32 (r, c) tile goes through shared memory: it is read along whichever index the source
 // walks with unit stride (r_major) and written along c, so both sides stay coalesced.
-static __global__ void __launch_bounds__(256) k_pack_planar(const cf32* __restrict__ src, float* __restrict__ dst,
+template <typename PT>  // plane element: float (split-TF32) or __nv_bfloat16 (split-BF16)
+static __global__ void __launch_bounds__(256) k_pack_planar(const cf32* __restrict__ src, PT* __restrict__ dst,
                                                      const ll* __restrict__ tabB, const ll* __restrict__ tabR,
                                                      const ll* __restrict__ tabC, ll bt, ll R, ll K, ll Rpad, ll Kpad,
                                                      ll Z, SliceOff so, ll g0, int r_major, int conj) {

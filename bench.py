@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--precision", choices=["fp32", "tf32x3"], default="tf32x3")
+    ap.add_argument("--precision", choices=["fp32", "tf32x3", "bf16x3"], default="tf32x3")
     ap.add_argument("--nodes", type=int, default=172)
     ap.add_argument("--target-log2", type=int, default=24)
     ap.add_argument("--group", type=int, default=0, help="slices per group (0: as many as the workspace allows)")
@@ -361,7 +361,8 @@ def _cpu_time(fn, reps):
 
 def run_latency(args, dev, which):
     """grid6 (6x6 grid, bond 4, c128) or brickwork (30 wires x depth 14, c64): microseconds per contraction,
-    plus the precision study (tf32x3 / fp32 / FP64 on the GPU, the FP32 CPU executor) for brickwork."""
+    plus the precision study (split-TF32 / FP32 / split-BF16 / FP64 on the GPU, the FP32 CPU executor) for
+    brickwork."""
     import torch
 
     import arctn_b200 as A
@@ -374,7 +375,7 @@ def run_latency(args, dev, which):
     else:
         net, arrays = N.brickwork_circuit(30, 14, seed=0)
         arrays = [a.astype(np.complex64) for a in arrays]
-        dtype, precisions = np.complex64, ["tf32x3", "fp32"]
+        dtype, precisions = np.complex64, ["tf32x3", "fp32", "bf16x3"]
     path = A.greedy(*net.as_tuple())
     O.build()
     ref = complex(O.contract_sliced(*net.as_tuple(), path, [], [a.astype(np.complex128) for a in arrays]))

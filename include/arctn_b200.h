@@ -56,9 +56,12 @@ enum {
 /* Arithmetic used for the pairwise GEMMs of f32 / c64 contractions.
  * f64 / c128 always compute in FP64. */
 enum {
-  ARCTN_B200_PREC_FP32 = 0,  /* plain FP32 FFMA on the CUDA cores */
-  ARCTN_B200_PREC_TF32X3 = 1 /* split-TF32 (3 products) on tcgen05 tensor cores, FP32 accumulate,
-                                for steps dense enough to fill a tensor-core tile; thin steps FP32 */
+  ARCTN_B200_PREC_FP32 = 0,   /* plain FP32 FFMA on the CUDA cores */
+  ARCTN_B200_PREC_TF32X3 = 1, /* split-TF32 (3 products) on tcgen05 tensor cores, FP32 accumulate,
+                                 for steps dense enough to fill a tensor-core tile; thin steps FP32 */
+  ARCTN_B200_PREC_BF16X3 = 2  /* split-BF16 (3 products, hi/lo BF16 pairs) on tcgen05 tensor cores, FP32
+                                 accumulate; each operand carried to about 2^-18, for precision studies;
+                                 the same step selection as TF32X3 */
 };
 
 /* A tensor network (TensorNetwork, src/network.rs:134-143).
@@ -186,7 +189,8 @@ typedef struct {
   uint64_t slice_begin;          /* run only global slices [slice_begin, slice_end); both 0: all slices.  A */
   uint64_t slice_end;            /* partial range sums only its slices (one rank of a sharded contraction). */
   int gradient;                  /* also build the adjoint sweep (arctn_b200_program_gradient); unsliced only */
-  uint64_t tc_k_chunk;           /* tf32x3: K per CTA before an FP64 split-K reduce (multiple of 16); 0: all of K,
+  uint64_t tc_k_chunk;           /* tf32x3 / bf16x3: K per CTA before an FP64 split-K reduce (a multiple of 16,
+                                    of 32 for bf16x3); 0: all of K,
                                     except unsliced GEMMs too small to fill the GPU, which split K to do so */
 } arctn_b200_program_options;
 

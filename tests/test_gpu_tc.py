@@ -50,12 +50,18 @@ CASES = [
 ]
 
 
+# Split-TF32 carries each operand to about 2^-22 (1e-5 on these steps); split-BF16 to about 2^-18 and drops
+# the lo x lo term, about 2^-17 of each product (1e-4).
+PRECISIONS = [("tf32x3", 1e-5), ("bf16x3", 1e-4)]
+
+
+@pytest.mark.parametrize("precision,tol", PRECISIONS, ids=[p for p, _ in PRECISIONS])
 @pytest.mark.parametrize("case", CASES, ids=[str(c) for c in CASES])
-def test_tc_step_matches_fp64(case):
+def test_tc_step_matches_fp64(case, precision, tol):
     bt, md, kd, nd = case
     inputs, output, size = step_network(bt, md, kd, nd, seed=len(md) * 7 + bt)
     arrays = random_arrays(inputs, size, np.complex64, 5)
-    prog = A.SlicedProgram(inputs, output, size, [(0, 1)], (), dtype=np.complex64, precision="tf32x3")
+    prog = A.SlicedProgram(inputs, output, size, [(0, 1)], (), dtype=np.complex64, precision=precision)
     import torch
 
     x = [torch.from_numpy(a).cuda() for a in arrays]
@@ -65,7 +71,7 @@ def test_tc_step_matches_fp64(case):
     want = O.naive_einsum(inputs, output, size, O.promote(arrays)) if np.prod(list(size.values())) <= 2 ** 26 \
         else np.einsum(*sum(([a.astype(np.complex128), t] for a, t in zip(arrays, inputs)), []), output)
     err = rel_err(got, want)
-    assert err <= 1e-5, err
+    assert err <= tol, err
     ms, kinds, _ = prog.profile(x, workspace=ws)
     assert 9 in kinds, "the dense step did not run on the tensor-core kernel"
 
@@ -76,10 +82,11 @@ def test_tc_sliced_with_shared_operand():
     size = {0: 3, 1: 160, 2: 96, 3: 200}
     arrays = random_arrays(inputs, size, np.complex64, 11)
     want = O.naive_einsum(inputs, output, size, O.promote(arrays))
-    for group in (1, 2, 0):
-        got = A.SlicedProgram(inputs, output, size, [(0, 1), (2, 3)], [0], dtype=np.complex64, precision="tf32x3",
-                              max_slices_per_group=group).execute(arrays)
-        assert rel_err(got, want) <= 1e-5
+    for precision, tol in PRECISIONS:
+        for group in (1, 2, 0):
+            got = A.SlicedProgram(inputs, output, size, [(0, 1), (2, 3)], [0], dtype=np.complex64,
+                                  precision=precision, max_slices_per_group=group).execute(arrays)
+            assert rel_err(got, want) <= tol, (precision, group)
 
 
 def test_tc_grid_contraction_matches_fp64_oracle():
@@ -92,8 +99,10 @@ def test_tc_grid_contraction_matches_fp64_oracle():
     want = complex(O.contract_sliced(*net.as_tuple(), path, [], O.promote(arrays), threads=8))
     got = complex(A.contract_sliced(*net.as_tuple(), arrays, [], ssa_path=path, precision="tf32x3"))
     got32 = complex(A.contract_sliced(*net.as_tuple(), arrays, [], ssa_path=path, precision="fp32"))
+    got_bf = complex(A.contract_sliced(*net.as_tuple(), arrays, [], ssa_path=path, precision="bf16x3"))
     assert abs(got - want) / abs(want) <= 1e-5
     assert abs(got32 - want) / abs(want) <= 1e-5
+    assert abs(got_bf - want) / abs(want) <= 1e-4
 
 
 def test_epilogue_packs_are_bit_identical_to_separate_packs():

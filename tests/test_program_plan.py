@@ -72,6 +72,25 @@ def test_tf32x3_packs_use_full_tiles_and_split_long_k():
     assert not any(o["kind"] in ("gemm_tc", "pack_tiled", "pack") for o in fp32.describe()["ops"])
 
 
+def test_bf16x3_programs_pack_bf16_planes_on_32_wide_k_rows():
+    # Split-BF16 runs the same steps on the tensor cores as split-TF32, with 2-byte planes whose packed K
+    # is a multiple of 32 (a 64-byte row), and no epilogue packs.
+    net, _ = N.workload_rand3reg(172, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 24)
+    tf = program(net, path, sliced, dtype=np.complex64, precision="tf32x3", max_slices_per_group=4).describe()["ops"]
+    bf = program(net, path, sliced, dtype=np.complex64, precision="bf16x3", max_slices_per_group=4).describe()["ops"]
+    tf_tc = [(o["bt"], o["m"], o["k"], o["n"]) for o in tf if o["kind"] == "gemm_tc"]
+    bf_tc = [(o["bt"], o["m"], o["k"], o["n"]) for o in bf if o["kind"] == "gemm_tc"]
+    assert bf_tc and sorted(bf_tc) == sorted(tf_tc)
+    assert all(o["bf16"] == 1 for o in bf if o["kind"] in ("gemm_tc", "pack", "pack_tiled"))
+    assert all(o["kpad"] % 32 == 0 for o in bf if o["kind"] in ("pack", "pack_tiled"))
+    assert not any("pack_into" in o for o in bf)
+    assert all(o["bf16"] == 0 for o in tf if o["kind"] == "gemm_tc")
+    with pytest.raises(A.ArcTNB200Error, match="multiple of 32"):
+        program(net, path, sliced, dtype=np.complex64, precision="bf16x3", tc_k_chunk=16)
+
+
 def test_tensor_core_epilogues_pack_the_next_gemm_operand():
     # rand3reg n=172: the producer's epilogue writes the packed operand of the GEMM that reads its result,
     # so no separate pack reads that result; gradient programs keep separate packs.
