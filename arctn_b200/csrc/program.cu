@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstring>
 #include <functional>
+#include <map>
 #include <mutex>
 #include <numeric>
 #include <set>
@@ -184,12 +185,19 @@ void Program::ensure_tables() {
 }
 
 Program::~Program() {
-  if (!dev_tab_ && !gexec_) return;
+  if (!dev_tab_ && !gexec_ && side_.empty()) return;
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(opt_.device);
   if (gexec_) cudaGraphExecDestroy(gexec_);
   if (dev_tab_) cudaFree(dev_tab_);
+  for (auto e : ev_)
+    if (e) cudaEventDestroy(e);
+  for (auto e : join_ev_)
+    if (e) cudaEventDestroy(e);
+  if (fork_ev_) cudaEventDestroy(fork_ev_);
+  for (auto s : side_)
+    if (s) cudaStreamDestroy(s);
   cudaSetDevice(prev);
 }
 
@@ -1230,9 +1238,32 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
   };
   if (want_strip) strip_exp_off_ = bufs[strip_exp_off_].offset;
   err_off_ = bufs[err_buf].offset;
+  // Memory footprint of an op of the main sequence, from its buffers before they are resolved to offsets.
+  foot_.clear();
+  auto note_foot = [&](const Op& op) {
+    std::vector<Foot> f;
+    auto add = [&](const Ref& r) {
+      if (r.kind == Ref::WS) {
+        const Buf& b = bufs[r.index];
+        const u64 lo = b.region2 ? align_up(region1) + b.offset : b.offset;
+        f.push_back(Foot{0, lo, lo + align_up(b.fixed ? b.bytes : b.bytes * (b.region2 ? S_ : 1))});
+      } else if (r.kind == Ref::OUTPUT) {
+        f.push_back(Foot{1, 0, ~0ull});
+      } else if (r.kind == Ref::GRADS) {
+        f.push_back(Foot{2 + (int)r.index, 0, ~0ull});
+      }  // inputs and grad_output are only read
+    };
+    add(op.a);
+    add(op.b);
+    add(op.c);
+    add(op.d);
+    add(op.pk);
+    if (op.kind == Op::GEMM_TC) f.push_back(Foot{0, err_off_, err_off_ + 8});  // its bounded waits report here
+    foot_.push_back(f);
+  };
 
   // ---------------------------------------------------------------- final op sequence
-  for (Op op : ops1) { finish(op); ops_.push_back(op); }
+  for (Op op : ops1) { note_foot(op); finish(op); ops_.push_back(op); }
   if (want_strip) {
     for (Op op : strip1) { finish(op); strip_ops_.push_back(op); }
   }
@@ -1252,6 +1283,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       }
       const u64 seg_tab = tab_ll(segs);
       for (Op op : ops2) {
+        note_foot(op);
         finish(op);
         op.S = g1 - g0;
         op.g0 = g0;
@@ -1273,8 +1305,9 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     }
     Op out{Op::OUTPUT};
     out.a = Ref{Ref::WS, part_buf};
-    finish(out);
     out.c = Ref{Ref::OUTPUT, 0};
+    note_foot(out);
+    finish(out);
     out.tab[0] = tab_ll(odims.empty() ? std::vector<ll>{0} : offsets(odims, ostr));
     out.tab[1] = tab_ll(kdims.empty() ? std::vector<ll>{0} : offsets(kdims, kstr));
     out.n_blocks = (ll)n_blocks_;
@@ -1282,11 +1315,64 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     out.n_e = (ll)n_e;
     ops_.push_back(out);
     for (Op op : ops3) {
+      note_foot(op);
       finish(op);
       ops_.push_back(op);
     }
   }
   (void)fbuf;
+  plan_dag();
+}
+
+void Program::plan_dag() {
+  const size_t n = ops_.size();
+  deps_.assign(n, {});
+  waits_.assign(n, {});
+  lane_.assign(n, 0);
+  need_ev_.assign(n, 0);
+  // Last toucher of every byte range, per space: disjoint segments lo -> (hi, op).
+  std::map<int, std::map<u64, std::pair<u64, int>>> segs;
+  for (size_t i = 0; i < n; ++i) {
+    std::set<int> d;
+    for (const Foot& f : foot_[i]) {
+      if (f.hi <= f.lo) continue;
+      auto& m = segs[f.space];
+      auto it = m.upper_bound(f.lo);
+      if (it != m.begin()) --it;
+      std::vector<std::pair<u64, std::pair<u64, int>>> keep;
+      while (it != m.end() && it->first < f.hi) {
+        const u64 a = it->first, b = it->second.first;
+        const int k = it->second.second;
+        if (b <= f.lo) { ++it; continue; }
+        if (k != (int)i) d.insert(k);
+        if (a < f.lo) keep.push_back({a, {f.lo, k}});
+        if (b > f.hi) keep.push_back({f.hi, {b, k}});
+        it = m.erase(it);
+      }
+      for (auto& kv : keep) m.insert(kv);
+      m[f.lo] = {f.hi, (int)i};
+    }
+    deps_[i].assign(d.begin(), d.end());
+  }
+  // Lanes: continue the lane whose last op is the latest dependency, else take the lane idle longest.
+  std::vector<int> last(kLanes, -1);
+  for (size_t i = 0; i < n; ++i) {
+    int lane = -1, best = -1;
+    for (int d : deps_[i])
+      if (last[lane_[d]] == d && d > best) { best = d; lane = lane_[d]; }
+    if (lane < 0) {
+      lane = 0;
+      for (int l = 1; l < kLanes; ++l)
+        if (last[l] < last[lane]) lane = l;
+    }
+    lane_[i] = lane;
+    last[lane] = (int)i;
+    for (int d : deps_[i])
+      if (lane_[d] != lane) {
+        waits_[i].push_back(d);
+        need_ev_[d] = 1;
+      }
+  }
 }
 
 u64 Program::launches() const {  // kernels per execute: a split GEMM adds its reduce kernel
@@ -1569,6 +1655,43 @@ void Program::enqueue(const std::vector<Op>& ops, const void* const* inputs, voi
   for (const Op& op : ops) launch_op(op, inputs, output, ws, st);
 }
 
+// The main sequence over kLanes streams, for capture into one graph whose edges are the op dependencies.
+// Lane 0 is st; the side lanes join the capture through fork_ev_ and are joined back into st at the end.
+void Program::ensure_lanes() {
+  if (!side_.empty()) return;  // once per program, with its device current and outside any capture
+  side_.resize(kLanes - 1, nullptr);
+  for (auto& s : side_) CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
+  join_ev_.resize(kLanes - 1, nullptr);
+  for (auto& e : join_ev_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  ev_.assign(ops_.size(), nullptr);
+  for (size_t i = 0; i < ops_.size(); ++i)
+    if (need_ev_[i]) CK(cudaEventCreateWithFlags(&ev_[i], cudaEventDisableTiming));
+}
+
+void Program::enqueue_dag(const void* const* inputs, void* output, char* ws, cudaStream_t st) {
+  auto lane_stream = [&](int l) { return l == 0 ? st : side_[(size_t)l - 1]; };
+  std::vector<char> used(kLanes, 0);
+  used[0] = 1;
+  CK(cudaEventRecord(fork_ev_, st));
+  for (size_t i = 0; i < ops_.size(); ++i) {
+    const int l = lane_[i];
+    cudaStream_t s = lane_stream(l);
+    if (!used[l]) {
+      CK(cudaStreamWaitEvent(s, fork_ev_, 0));
+      used[l] = 1;
+    }
+    for (int d : waits_[i]) CK(cudaStreamWaitEvent(s, ev_[(size_t)d], 0));
+    launch_op(ops_[i], inputs, output, ws, s);
+    if (need_ev_[i]) CK(cudaEventRecord(ev_[i], s));
+  }
+  for (int l = 1; l < kLanes; ++l)
+    if (used[l]) {
+      CK(cudaEventRecord(join_ev_[(size_t)l - 1], side_[(size_t)l - 1]));
+      CK(cudaStreamWaitEvent(st, join_ev_[(size_t)l - 1], 0));
+    }
+}
+
 namespace {
 struct DeviceGuard {
   int prev = -1;
@@ -1613,9 +1736,10 @@ void Program::execute(const void* const* inputs, void* output, bool f64_out, voi
   key.push_back((const void*)(uintptr_t)f64_out);
   if (!gexec_ || key != gkey_) {
     cudaGraph_t graph_h = nullptr;
+    ensure_lanes();
     CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     try {
-      enqueue(ops_, inputs, output, (char*)ws, st);
+      enqueue_dag(inputs, output, (char*)ws, st);
     } catch (...) {
       cudaStreamEndCapture(st, &graph_h);
       if (graph_h) cudaGraphDestroy(graph_h);
@@ -1801,6 +1925,19 @@ std::string Program::describe() const {
         break;
       case Op::MEMSET: f("bytes", (long long)op.bytes); break;
       default: f("n_e", op.n_e); break;
+    }
+    // graph DAG: lane, the ops it must follow, and its footprint [space, lo, hi) (hi = -1: unbounded)
+    if (i < lane_.size()) {
+      f("lane", lane_[i]);
+      s += ",\"deps\":[";
+      for (size_t q = 0; q < deps_[i].size(); ++q) s += (q ? "," : "") + std::to_string(deps_[i][q]);
+      s += "],\"foot\":[";
+      for (size_t q = 0; q < foot_[i].size(); ++q) {
+        const Foot& ft = foot_[i][q];
+        s += std::string(q ? "," : "") + "[" + std::to_string(ft.space) + "," + std::to_string(ft.lo) + "," +
+             (ft.hi == ~0ull ? std::string("-1") : std::to_string(ft.hi)) + "]";
+      }
+      s += "]";
     }
     s += "}";
   }

@@ -159,6 +159,25 @@ class Program {
 
   std::mutex mu_;
   bool out_f64_flag_ = false;
+
+  // Graph capture as a dependency DAG over kLanes streams (plain executes of non-gradient programs).  Op j
+  // depends on the last earlier op that touched any byte of its memory footprint (workspace ranges, the
+  // output, gradient buffers), which orders it after every earlier op touching that memory.  Ops are
+  // assigned to lanes at build time: an op continues the lane of its latest dependency where it can;
+  // waits_ lists its dependencies on other lanes (an event each).
+  static constexpr int kLanes = 8;
+  struct Foot { int space; u64 lo, hi; };  // space 0: workspace bytes, 1: output, 2 + i: gradient i
+  std::vector<std::vector<Foot>> foot_;
+  std::vector<std::vector<int>> deps_, waits_;
+  std::vector<int> lane_;
+  std::vector<char> need_ev_;
+  std::vector<cudaStream_t> side_;   // lanes 1 .. kLanes - 1 (lane 0 is the caller's stream)
+  std::vector<cudaEvent_t> ev_;      // per op with need_ev_, recorded after it
+  std::vector<cudaEvent_t> join_ev_;
+  cudaEvent_t fork_ev_ = nullptr;
+  void plan_dag();
+  void ensure_lanes();
+  void enqueue_dag(const void* const* inputs, void* output, char* ws, cudaStream_t st);
   cudaGraphExec_t gexec_ = nullptr;
   std::vector<const void*> gkey_;
 };

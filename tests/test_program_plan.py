@@ -192,3 +192,41 @@ def test_batch_workload_generator():
         assert bond in (2, 3, 4) and all(v == bond for v in net.size_dict.values())
         assert arrays[0].dtype == (np.float32 if j % 2 == 0 else np.complex64)
         assert all(len(t) == 3 for t in net.inputs)
+
+
+def _dag_orders_every_overlap(ops):
+    # anc[j]: bitset of the ops j follows through its dependency edges.
+    anc = []
+    for j, o in enumerate(ops):
+        a = 0
+        for d in o["deps"]:
+            assert d < j
+            a |= anc[d] | (1 << d)
+        anc.append(a)
+    spans = [[(sp, lo, (1 << 64) if hi == -1 else hi) for sp, lo, hi in o["foot"]] for o in ops]
+    for j in range(len(ops)):
+        for i in range(j):
+            if any(si == sj and li < hj and lj < hi_ for si, li, hi_ in spans[i] for sj, lj, hj in spans[j]):
+                assert anc[j] >> i & 1, (i, j, ops[i]["kind"], ops[j]["kind"])
+
+
+@pytest.mark.parametrize("case", ["grid6", "brickwork", "sliced_fused"])
+def test_graph_dag_orders_every_pair_of_ops_sharing_memory(case):
+    # The captured graph runs independent steps concurrently on 8 lanes; two ops whose memory footprints
+    # overlap (a step and its consumer, or two buffers the arena places on the same bytes) must stay ordered.
+    if case == "grid6":
+        net, _ = N.workload_grid6(np.complex128, seed=0)
+        p = program(net, A.greedy(*net.as_tuple()), dtype=np.complex128)
+    elif case == "brickwork":
+        net, _ = N.brickwork_circuit(30, 14, seed=0)
+        p = program(net, A.greedy(*net.as_tuple()), dtype=np.complex64, precision="tf32x3")
+    else:
+        net, _ = N.workload_rand3reg(104, 2, 1, np.complex64, seed=0)
+        path = A.greedy(*net.as_tuple())
+        sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 14)
+        p = program(net, path, sliced, dtype=np.complex64, precision="tf32x3", max_slices_per_group=4)
+    ops = p.describe()["ops"]
+    assert all("deps" in o and "foot" in o for o in ops)
+    _dag_orders_every_overlap(ops)
+    if case != "sliced_fused":
+        assert len({o["lane"] for o in ops}) > 1  # independent steps do run on several lanes
