@@ -128,10 +128,20 @@ class _DeviceCall:
             if not torch.cuda.is_available():
                 raise ValueError("the B200 executor needs a CUDA device; none is visible")
             self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
-            self.tensors = []
-            for a in arrays:
-                host = torch.from_numpy(np.array(a, order="C", copy=None)).pin_memory()
-                self.tensors.append(host.to(self.device, non_blocking=True))
+            # One pinned staging buffer and one host-to-device copy for all inputs (a network can have hundreds
+            # of small tensors); each input is a 256-byte-aligned view of the device copy.
+            arrs = [np.array(a, order="C", copy=None) for a in arrays]
+            offs, total = [], 0
+            for a in arrs:
+                offs.append(total)
+                total += (a.nbytes + 255) // 256 * 256
+            host = torch.empty(max(total, 1), dtype=torch.uint8, pin_memory=True)
+            hv = host.numpy()
+            for a, o in zip(arrs, offs):
+                hv[o:o + a.nbytes] = a.reshape(-1).view(np.uint8)
+            dev = host.to(self.device, non_blocking=True)
+            self.tensors = [dev[o:o + a.nbytes].view(torch.from_numpy(np.empty(0, a.dtype)).dtype).view(a.shape)
+                            for a, o in zip(arrs, offs)]
         self.stream = torch.cuda.current_stream(self.device)
         self.ptrs = (ctypes.c_void_p * len(self.tensors))(*[t.data_ptr() for t in self.tensors])
 
