@@ -76,7 +76,7 @@ def _expected_shapes(inputs, size_dict):
     return [tuple(int(size_dict[l]) for l in t) for t in inputs]
 
 
-def _preflight(arrays, inputs, size_dict, context):
+def _preflight(arrays, inputs, size_dict, context, shapes=None):
     """Validate count, dtype, layout and every shape before any copy (pybind/src/lib.rs:246-330)."""
     try:
         arrays = list(arrays)
@@ -86,9 +86,15 @@ def _preflight(arrays, inputs, size_dict, context):
         raise ValueError(f"{context}: {len(arrays)} arrays given for {len(inputs)} input tensors")
     if not arrays:
         raise ValueError(f"{context}: arrays is empty")
+    shapes = shapes if shapes is not None else _expected_shapes(inputs, size_dict)
     torch_mode = _is_torch(arrays[0])
+    # Fast path: NumPy arrays of one supported dtype whose shapes all match (the checks below, in one pass).
+    if not torch_mode and all(type(a) is np.ndarray for a in arrays):
+        dt = arrays[0].dtype
+        if dt in _NP_CODES and all(a.dtype == dt and a.shape == sh for a, sh in zip(arrays, shapes)):
+            return arrays, _NP_CODES[dt], False
     code = None
-    for i, (a, shape) in enumerate(zip(arrays, _expected_shapes(inputs, size_dict))):
+    for i, (a, shape) in enumerate(zip(arrays, shapes)):
         if torch_mode != _is_torch(a):
             raise ValueError(f"{context}: arrays[{i}] mixes torch tensors and NumPy arrays")
         if torch_mode:
@@ -118,18 +124,20 @@ class _DeviceCall:
 
     def __init__(self, arrays, torch_mode, device=None):
         torch = _torch()
+        self._views = None
         if torch_mode:
             self.device = arrays[0].device
             for a in arrays:
                 if a.device != self.device:
                     raise ValueError("all arrays must live on one CUDA device")
-            self.tensors = list(arrays)
+            self._views = list(arrays)
+            ptrs = [t.data_ptr() for t in arrays]
         else:
             if not torch.cuda.is_available():
                 raise ValueError("the B200 executor needs a CUDA device; none is visible")
             self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
             # One pinned staging buffer and one host-to-device copy for all inputs (a network can have hundreds
-            # of small tensors); each input is a 256-byte-aligned view of the device copy.
+            # of small tensors); input i sits 256-byte aligned at offset offs[i] of the device copy.
             arrs = [np.array(a, order="C", copy=None) for a in arrays]
             offs, total = [], 0
             for a in arrs:
@@ -139,11 +147,25 @@ class _DeviceCall:
             hv = host.numpy()
             for a, o in zip(arrs, offs):
                 hv[o:o + a.nbytes] = a.reshape(-1).view(np.uint8)
-            dev = host.to(self.device, non_blocking=True)
-            self.tensors = [dev[o:o + a.nbytes].view(torch.from_numpy(np.empty(0, a.dtype)).dtype).view(a.shape)
-                            for a, o in zip(arrs, offs)]
+            self._dev = host.to(self.device, non_blocking=True)
+            self._layout = [(o, a.nbytes, a.dtype, a.shape) for a, o in zip(arrs, offs)]
+            base = self._dev.data_ptr()
+            ptrs = [base + o for o in offs]
         self.stream = torch.cuda.current_stream(self.device)
-        self.ptrs = (ctypes.c_void_p * len(self.tensors))(*[t.data_ptr() for t in self.tensors])
+        self.ptrs = (ctypes.c_void_p * len(ptrs))(*ptrs)
+
+    @property
+    def tensors(self):
+        """The inputs as CUDA tensors (views of the staged copy for NumPy inputs), built on first use."""
+        if self._views is None:
+            torch = _torch()
+            kinds = {}
+            self._views = []
+            for o, nb, dt, shape in self._layout:
+                if dt not in kinds:
+                    kinds[dt] = torch.from_numpy(np.empty(0, dt)).dtype
+                self._views.append(self._dev[o:o + nb].view(kinds[dt]).view(shape))
+        return self._views
 
     def empty(self, shape, dtype):
         return _torch().empty(shape, dtype=dtype, device=self.device)
@@ -279,10 +301,17 @@ class SlicedProgram:
         C.check(C.lib().arctn_b200_program_describe(self._h, buf, need.value, ctypes.byref(need)), "describe")
         return json.loads(buf.value.decode())
 
+    def _shapes(self):
+        """The input shapes the network expects, computed once."""
+        if getattr(self, "_shape_cache", None) is None:
+            self._shape_cache = _expected_shapes(self.inputs, self.size_dict)
+        return self._shape_cache
+
     def execute(self, arrays, *, f64_out=False, workspace=None, stream=None, out=None):
         """Full output of the contraction.  ``out`` (a CUDA tensor of the output's shape and dtype -- the
         wide dtype with ``f64_out``) receives it in place, which keeps a captured graph's pointers fixed."""
-        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "sliced contraction failed")
+        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "sliced contraction failed",
+                                              self._shapes())
         if code != self.code:
             raise ValueError("sliced contraction failed: arrays dtype differs from the program's dtype")
         call = _DeviceCall(arrays, torch_mode, self.device)
@@ -310,7 +339,8 @@ class SlicedProgram:
         (graph replay when ``use_graph``), for latency-bound callers that execute the same buffers
         repeatedly.  The caller keeps ``arrays``, ``out`` and ``workspace`` alive.
         """
-        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "bind failed")
+        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "bind failed",
+                                              self._shapes())
         if not torch_mode:
             raise ValueError("bind failed: arrays must be CUDA torch tensors")
         if code != self.code:
@@ -343,7 +373,8 @@ class SlicedProgram:
         """
         if not self.has_gradient:
             raise ValueError("program was built without gradient=True")
-        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "gradient failed")
+        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "gradient failed",
+                                              self._shapes())
         torch = _torch()
         call = _DeviceCall(arrays, torch_mode, self.device)
         out = output if output is not None else call.empty(self.output_shape, _torch_dtype(code))
@@ -382,7 +413,8 @@ class SlicedProgram:
 
     def profile(self, arrays, *, workspace=None):
         """Op-by-op run with CUDA events between launches: (ms, kind, algorithmic work) per launch."""
-        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "profile failed")
+        arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "profile failed",
+                                              self._shapes())
         call = _DeviceCall(arrays, torch_mode, self.device)
         out = call.empty(self.output_shape, _torch_dtype(code))
         ws = workspace if workspace is not None else call.workspace(self.workspace_bytes)
