@@ -41,3 +41,22 @@ def test_graph_replay_equals_sequential_launch(name, net, arrays, sliced, precis
             got = dag.execute(x, workspace=ws, stream=st).cpu()
             assert torch.equal(got, want), name
         assert dag.device_status(ws, st) == 0
+
+
+def test_numpy_calls_reuse_buffers_and_see_new_inputs():
+    # Repeated NumPy calls on one stream reuse the staged-input buffer, workspace and output (so the graph
+    # replays); each call must still see its own inputs.  Doubling one input doubles the result exactly
+    # (a power-of-two scale is exact through every product and the TF32 split).
+    net, arrays = N.workload_rand3reg(64, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 8)
+    prog = A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex64, precision="tf32x3")
+    first = prog.execute(arrays)
+    again = prog.execute(arrays)
+    doubled = [a * 2 if i == 3 else a for i, a in enumerate(arrays)]
+    twice = prog.execute(doubled)
+    assert np.array_equal(first, again)
+    assert np.array_equal(twice, first * 2)
+    st = torch.cuda.Stream()  # an explicit stream that is not the current one: copies follow it
+    other = prog.execute(doubled, stream=st)
+    assert np.array_equal(other, twice)
