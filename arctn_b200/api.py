@@ -444,7 +444,7 @@ class SlicedProgram:
         return code.value
 
     def profile(self, arrays, *, workspace=None):
-        """Op-by-op run with CUDA events between launches: (ms, kind, algorithmic work) per launch."""
+        """Launch-by-launch run with CUDA events between launches: (ms, kind, algorithmic work) per launch."""
         arrays, code, torch_mode = _preflight(arrays, self.inputs, self.size_dict, "profile failed",
                                               self._shapes())
         call = _DeviceCall(arrays, torch_mode, self.device)
@@ -452,7 +452,7 @@ class SlicedProgram:
         ws = workspace if workspace is not None else call.workspace(self.workspace_bytes)
         n = self.launches
         ms = (ctypes.c_float * n)()
-        kind = (ctypes.c_int * n)(*([-1] * n))  # one entry per op; split ops hold two kernels
+        kind = (ctypes.c_int * n)(*([-1] * n))  # one entry per launch unit; a split op's two kernels share one
         work = (ctypes.c_double * n)()
         torch = _torch()
         with torch.cuda.device(call.device):

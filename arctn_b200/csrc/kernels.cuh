@@ -206,6 +206,58 @@ __global__ void __launch_bounds__(256) k_gemm_small(GemmArgs g) {
   }
 }
 
+// Independent one-slice thin steps of one level of the step DAG, run as one launch: each block finds its
+// problem by its first block, then loops exactly as k_gemm_small does (one thread per output element, k
+// ascending), so every element gets the same bits as in its own launch.
+constexpr int kMaxGroup = 64;
+struct SmallProb {
+  const void* A;
+  const void* B;
+  void* C;
+  const ll* aB; const ll* aM; const ll* aK;
+  const ll* bB; const ll* bK; const ll* bN;
+  ll bt, m, k, n;
+  int conj_a, conj_b;
+  int block0;  // first block of this problem in the grouped grid
+};
+struct SmallGroup {
+  int n;
+  SmallProb p[kMaxGroup];
+};
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm_small_grouped(const __grid_constant__ SmallGroup g) {
+  using A = typename Num<T>::acc;
+  int lo = 0, hi = g.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (g.p[mid].block0 <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const SmallProb& q = g.p[lo];
+  const ll nblk = (lo + 1 < g.n ? g.p[lo + 1].block0 : (int)gridDim.x) - q.block0;
+  const ll blk = (ll)blockIdx.x - q.block0;
+  const T* Ap = (const T*)q.A;
+  const T* Bp = (const T*)q.B;
+  T* Cp = (T*)q.C;
+  const ll mn = q.m * q.n, total = q.bt * mn;
+  extern __shared__ ll sh_tab[];  // aK[0..k) then bK[0..k); every grouped problem has k <= 1024
+  for (ll l = threadIdx.x; l < q.k; l += blockDim.x) { sh_tab[l] = q.aK[l]; sh_tab[q.k + l] = q.bK[l]; }
+  __syncthreads();
+  const ll* aK = sh_tab;
+  const ll* bK = sh_tab + q.k;
+  for (ll idx = blk * blockDim.x + threadIdx.x; idx < total; idx += nblk * blockDim.x) {
+    ll r = idx;
+    const ll b = r / mn;
+    r -= b * mn;
+    const ll i = r / q.n, j = r - i * q.n;
+    const T* a = Ap + q.aB[b] + q.aM[i];
+    const T* bb = Bp + q.bB[b] + q.bN[j];
+    A acc = Num<T>::zero();
+    for (ll l = 0; l < q.k; ++l) Num<T>::fma(acc, cj(a[aK[l]], q.conj_a), cj(bb[bK[l]], q.conj_b));
+    Cp[idx] = acc;
+  }
+}
+
 // Few outputs with a long contraction (a dot product per slice, k up to 2^19):
 // one CTA per output element, the k range strided over 256 threads and
 // folded by a fixed shared-memory tree, so the sum order never varies.

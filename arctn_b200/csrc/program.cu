@@ -42,6 +42,7 @@ static size_t wide_bytes(int dt) { return dtype_complex(dt) ? 16 : 8; }
 namespace {
 
 constexpr u64 kAlign = 256;
+constexpr u64 kSpreadLimit = 64ull << 20;  // regions up to this size give every buffer its own bytes
 constexpr u64 kInf = ~0ull;
 // Split-K for tensor-core GEMMs.  Accuracy needs none (the kernel keeps TMEM chains short and sums
 // them in registers), so K is split only to fill the GPU: an unsliced GEMM with fewer than two tiles
@@ -1180,10 +1181,24 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
 
   // ---------------------------------------------------------------- group size and layout
   u64 region1 = 0, per_slice2 = 0;
+  // Buffers with overlapping lifetimes never share bytes; others may.  Sharing bytes orders the ops that
+  // touch them in the graph, so a region whose buffers fit in kSpreadLimit without any sharing gets its own
+  // bytes per buffer: independent steps then stay independent.
   auto layout = [&](bool region2, u64 mult) {
     std::vector<size_t> ids;
     for (size_t b = 0; b < bufs.size(); ++b)
       if (bufs[b].region2 == region2) ids.push_back(b);
+    u64 spread = 0;
+    for (size_t id : ids) spread += align_up(bufs[id].fixed ? bufs[id].bytes : bufs[id].bytes * mult);
+    const u64 budget_cap = opt_.workspace_budget ? opt_.workspace_budget : kDefaultBudget;
+    if (spread <= kSpreadLimit && spread <= budget_cap) {
+      u64 off = 0;
+      for (size_t id : ids) {
+        bufs[id].offset = off;
+        off += align_up(bufs[id].fixed ? bufs[id].bytes : bufs[id].bytes * mult);
+      }
+      return off;
+    }
     std::sort(ids.begin(), ids.end(), [&](size_t x, size_t y) { return bufs[x].bytes > bufs[y].bytes || (bufs[x].bytes == bufs[y].bytes && x < y); });
     std::vector<size_t> placed;
     u64 top = 0;
@@ -1354,31 +1369,98 @@ void Program::plan_dag() {
     }
     deps_[i].assign(d.begin(), d.end());
   }
-  // Lanes: continue the lane whose last op is the latest dependency, else take the lane idle longest.
-  std::vector<int> last(kLanes, -1);
+  if (opt_.gradient) {  // gradient programs run op by op in program order: one unit per op, one lane
+    units_.clear();
+    unit_of_.assign(n, 0);
+    for (size_t i = 0; i < n; ++i) {
+      unit_of_[i] = (int)i;
+      units_.push_back({(int)i});
+    }
+    waits_.assign(n, {});
+    lane_.assign(n, 0);
+    need_ev_.assign(n, 0);
+    return;
+  }
+  // Levels of the op DAG; ops of one level are mutually independent.
+  std::vector<int> level(n, 0);
+  for (size_t i = 0; i < n; ++i)
+    for (int d : deps_[i]) level[i] = std::max(level[i], level[(size_t)d] + 1);
+  // Units: independent one-slice thin GEMMs of one level are grouped (same dtype for the whole program).
+  auto groupable = [&](const Op& op) {
+    return op.kind == Op::GEMM_SMALL && op.S == 1 && op.sa.n == 0 && op.sb.n == 0 && op.k <= 1024 &&
+           op.bt * op.m * op.n <= (1ll << 20);
+  };
+  units_.clear();
+  unit_of_.assign(n, -1);
+  std::map<int, int> open;  // level -> unit being filled
   for (size_t i = 0; i < n; ++i) {
+    if (groupable(ops_[i])) {
+      auto it = open.find(level[i]);
+      if (it != open.end() && units_[(size_t)it->second].size() < (size_t)kMaxGroup) {
+        units_[(size_t)it->second].push_back((int)i);
+        unit_of_[i] = it->second;
+        continue;
+      }
+      open[level[i]] = (int)units_.size();
+    }
+    unit_of_[i] = (int)units_.size();
+    units_.push_back({(int)i});
+  }
+  // Launch order: by level, then by first member (a topological order of the unit DAG).
+  std::vector<int> order(units_.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return level[(size_t)units_[(size_t)x][0]] < level[(size_t)units_[(size_t)y][0]];
+  });
+  std::vector<std::vector<int>> sorted;
+  std::vector<int> renum(units_.size());
+  for (size_t u = 0; u < order.size(); ++u) {
+    renum[(size_t)order[u]] = (int)u;
+    sorted.push_back(units_[(size_t)order[u]]);
+  }
+  units_ = sorted;
+  for (size_t i = 0; i < n; ++i) unit_of_[i] = renum[(size_t)unit_of_[i]];
+  const size_t nu = units_.size();
+  std::vector<std::vector<int>> udeps(nu);
+  for (size_t u = 0; u < nu; ++u) {
+    std::set<int> d;
+    for (int i : units_[u])
+      for (int x : deps_[(size_t)i]) d.insert(unit_of_[(size_t)x]);
+    d.erase((int)u);
+    udeps[u].assign(d.begin(), d.end());
+  }
+  // Lanes: continue the lane whose last unit is the latest dependency, else take the lane idle longest.
+  waits_.assign(nu, {});
+  lane_.assign(nu, 0);
+  need_ev_.assign(nu, 0);
+  std::vector<int> last(kLanes, -1);
+  for (size_t u = 0; u < nu; ++u) {
     int lane = -1, best = -1;
-    for (int d : deps_[i])
-      if (last[lane_[d]] == d && d > best) { best = d; lane = lane_[d]; }
+    for (int d : udeps[u])
+      if (last[lane_[(size_t)d]] == d && d > best) { best = d; lane = lane_[(size_t)d]; }
     if (lane < 0) {
       lane = 0;
       for (int l = 1; l < kLanes; ++l)
         if (last[l] < last[lane]) lane = l;
     }
-    lane_[i] = lane;
-    last[lane] = (int)i;
-    for (int d : deps_[i])
-      if (lane_[d] != lane) {
-        waits_[i].push_back(d);
-        need_ev_[d] = 1;
+    lane_[u] = lane;
+    last[lane] = (int)u;
+    for (int d : udeps[u])
+      if (lane_[(size_t)d] != lane) {
+        waits_[u].push_back(d);
+        need_ev_[(size_t)d] = 1;
       }
   }
 }
 
 u64 Program::launches() const {  // kernels per execute: a split GEMM adds its reduce kernel
   u64 n = 0;
-  for (auto& op : ops_)
+  for (size_t i = 0; i < ops_.size(); ++i) {
+    const Op& op = ops_[i];
+    // a grouped unit launches once, counted at its first member
+    if (!units_.empty() && units_[(size_t)unit_of_[i]].size() > 1 && units_[(size_t)unit_of_[i]][0] != (int)i) continue;
     n += (op.kind != Op::MEMSET) + ((op.kind == Op::GEMM_TC || op.kind == Op::GEMM_DOT) && op.splits > 1);
+  }
   return n;
 }
 
@@ -1651,6 +1733,46 @@ void Program::launch_op(const Op& op, const void* const* inputs, void* output, c
   CK(cudaGetLastError());
 }
 
+// One launch for a unit of independent one-slice thin GEMMs (k_gemm_small_grouped).
+void Program::launch_group(const std::vector<int>& members, const void* const* inputs, void* output, char* ws,
+                           cudaStream_t st) {
+  auto ptr = [&](const Ref& r) -> const void* {
+    switch (r.kind) {
+      case Ref::INPUT: return inputs[r.index];
+      case Ref::WS: return ws + r.index;
+      case Ref::OUTPUT: return output;
+      default: return nullptr;
+    }
+  };
+  SmallGroup g;
+  g.n = (int)members.size();
+  int blocks = 0;
+  ll kmax = 0;
+  for (int q = 0; q < g.n; ++q) {
+    const Op& op = ops_[(size_t)members[(size_t)q]];
+    auto T_ = [&](int i) { return (const ll*)(dev_tab_ + op.tab[i]); };
+    SmallProb& p = g.p[q];
+    p.A = ptr(op.a);
+    p.B = ptr(op.b);
+    p.C = const_cast<void*>(ptr(op.c));
+    p.aB = T_(0); p.aM = T_(1); p.aK = T_(2); p.bB = T_(3); p.bK = T_(4); p.bN = T_(5);
+    p.bt = op.bt; p.m = op.m; p.k = op.k; p.n = op.n;
+    p.conj_a = op.conj_a ? 1 : 0;
+    p.conj_b = op.conj_b ? 1 : 0;
+    p.block0 = blocks;
+    blocks += (int)std::min<ll>((op.bt * op.m * op.n + 255) / 256, 148 * 32);
+    kmax = std::max(kmax, op.k);
+  }
+  const size_t smem = (size_t)(2 * kmax * sizeof(ll));
+  switch (opt_.dtype) {
+    case DT_F32: k_gemm_small_grouped<float><<<blocks, 256, smem, st>>>(g); break;
+    case DT_F64: k_gemm_small_grouped<double><<<blocks, 256, smem, st>>>(g); break;
+    case DT_C64: k_gemm_small_grouped<cf32><<<blocks, 256, smem, st>>>(g); break;
+    case DT_C128: k_gemm_small_grouped<cf64><<<blocks, 256, smem, st>>>(g); break;
+  }
+  CK(cudaGetLastError());
+}
+
 void Program::enqueue(const std::vector<Op>& ops, const void* const* inputs, void* output, char* ws, cudaStream_t st) {
   for (const Op& op : ops) launch_op(op, inputs, output, ws, st);
 }
@@ -1664,9 +1786,9 @@ void Program::ensure_lanes() {
   CK(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
   join_ev_.resize(kLanes - 1, nullptr);
   for (auto& e : join_ev_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  ev_.assign(ops_.size(), nullptr);
-  for (size_t i = 0; i < ops_.size(); ++i)
-    if (need_ev_[i]) CK(cudaEventCreateWithFlags(&ev_[i], cudaEventDisableTiming));
+  ev_.assign(units_.size(), nullptr);
+  for (size_t u = 0; u < units_.size(); ++u)
+    if (need_ev_[u]) CK(cudaEventCreateWithFlags(&ev_[u], cudaEventDisableTiming));
 }
 
 void Program::enqueue_dag(const void* const* inputs, void* output, char* ws, cudaStream_t st) {
@@ -1674,16 +1796,17 @@ void Program::enqueue_dag(const void* const* inputs, void* output, char* ws, cud
   std::vector<char> used(kLanes, 0);
   used[0] = 1;
   CK(cudaEventRecord(fork_ev_, st));
-  for (size_t i = 0; i < ops_.size(); ++i) {
-    const int l = lane_[i];
+  for (size_t u = 0; u < units_.size(); ++u) {
+    const int l = lane_[u];
     cudaStream_t s = lane_stream(l);
     if (!used[l]) {
       CK(cudaStreamWaitEvent(s, fork_ev_, 0));
       used[l] = 1;
     }
-    for (int d : waits_[i]) CK(cudaStreamWaitEvent(s, ev_[(size_t)d], 0));
-    launch_op(ops_[i], inputs, output, ws, s);
-    if (need_ev_[i]) CK(cudaEventRecord(ev_[i], s));
+    for (int d : waits_[u]) CK(cudaStreamWaitEvent(s, ev_[(size_t)d], 0));
+    if (units_[u].size() == 1) launch_op(ops_[(size_t)units_[u][0]], inputs, output, ws, s);
+    else launch_group(units_[u], inputs, output, ws, s);
+    if (need_ev_[u]) CK(cudaEventRecord(ev_[u], s));
   }
   for (int l = 1; l < kLanes; ++l)
     if (used[l]) {
@@ -1806,27 +1929,33 @@ void Program::profile(const void* const* inputs, void* output, void* ws, u64 ws_
     Program* p;
     ~Unbind() { p->grad_out_ = nullptr; p->grads_ = nullptr; }
   } unbind{this};
+  // One entry per launch unit (a grouped unit is one launch; its work is its members' sum), in unit order.
+  const size_t nu = units_.size();
   std::vector<cudaEvent_t> ev;
-  for (size_t i = 0; i <= ops_.size(); ++i) {
+  for (size_t u = 0; u <= nu; ++u) {
     cudaEvent_t e;
     CK(cudaEventCreate(&e));
     ev.push_back(e);
   }
   try {
-    for (size_t i = 0; i < ops_.size(); ++i) {
-      CK(cudaEventRecord(ev[i], st));
-      launch_op(ops_[i], inputs, output, (char*)ws, st);
+    for (size_t u = 0; u < nu; ++u) {
+      CK(cudaEventRecord(ev[u], st));
+      if (units_[u].size() == 1) launch_op(ops_[(size_t)units_[u][0]], inputs, output, (char*)ws, st);
+      else launch_group(units_[u], inputs, output, (char*)ws, st);
     }
-    CK(cudaEventRecord(ev[ops_.size()], st));
-    CK(cudaEventSynchronize(ev[ops_.size()]));
+    CK(cudaEventRecord(ev[nu], st));
+    CK(cudaEventSynchronize(ev[nu]));
     size_t j = 0;
-    for (size_t i = 0; i < ops_.size(); ++i) {
-      if (ops_[i].kind == Op::MEMSET) continue;
+    for (size_t u = 0; u < nu; ++u) {
+      const Op& first = ops_[(size_t)units_[u][0]];
+      if (first.kind == Op::MEMSET) continue;
       float t = 0.f;
-      CK(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+      CK(cudaEventElapsedTime(&t, ev[u], ev[u + 1]));
+      double w = 0.0;
+      for (int i : units_[u]) w += op_work(ops_[(size_t)i], opt_.dtype);
       ms[j] = t;
-      kind[j] = (int)ops_[i].kind;
-      work[j] = op_work(ops_[i], opt_.dtype);
+      kind[j] = (int)first.kind;
+      work[j] = w;
       ++j;
     }
   } catch (...) {
@@ -1927,8 +2056,9 @@ std::string Program::describe() const {
       default: f("n_e", op.n_e); break;
     }
     // graph DAG: lane, the ops it must follow, and its footprint [space, lo, hi) (hi = -1: unbounded)
-    if (i < lane_.size()) {
-      f("lane", lane_[i]);
+    if (i < unit_of_.size()) {
+      f("unit", unit_of_[i]);
+      f("lane", lane_[(size_t)unit_of_[i]]);
       s += ",\"deps\":[";
       for (size_t q = 0; q < deps_[i].size(); ++q) s += (q ? "," : "") + std::to_string(deps_[i][q]);
       s += "],\"foot\":[";

@@ -168,7 +168,12 @@ class Program {
   static constexpr int kLanes = 8;
   struct Foot { int space; u64 lo, hi; };  // space 0: workspace bytes, 1: output, 2 + i: gradient i
   std::vector<std::vector<Foot>> foot_;
-  std::vector<std::vector<int>> deps_, waits_;
+  std::vector<std::vector<int>> deps_;   // per op
+  // Launch units in launch order: one op, or up to kMaxGroup independent one-slice thin GEMMs of one DAG
+  // level run as a single grouped launch.  waits_ / lane_ / need_ev_ are per unit.
+  std::vector<std::vector<int>> units_;
+  std::vector<int> unit_of_;             // op -> unit
+  std::vector<std::vector<int>> waits_;  // per unit: units on other lanes it waits for
   std::vector<int> lane_;
   std::vector<char> need_ev_;
   std::vector<cudaStream_t> side_;   // lanes 1 .. kLanes - 1 (lane 0 is the caller's stream)
@@ -177,6 +182,8 @@ class Program {
   cudaEvent_t fork_ev_ = nullptr;
   void plan_dag();
   void ensure_lanes();
+  void launch_group(const std::vector<int>& members, const void* const* inputs, void* output, char* ws,
+                    cudaStream_t st);
   void enqueue_dag(const void* const* inputs, void* output, char* ws, cudaStream_t st);
   cudaGraphExec_t gexec_ = nullptr;
   std::vector<const void*> gkey_;

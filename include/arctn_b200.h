@@ -206,7 +206,8 @@ uint64_t arctn_b200_program_n_slices(const arctn_b200_program* program);
 uint64_t arctn_b200_program_slices_per_group(const arctn_b200_program* program);
 /* Algorithmic real flops of one execution: 8 (complex) or 2 (real) x sum_steps bt*m*k*n x slices. */
 double arctn_b200_program_flops(const arctn_b200_program* program);
-/* Number of kernels one execute launches. */
+/* Number of kernels one graph-replayed execute launches (independent thin steps of one level of the step
+ * DAG count once: they share a grouped launch). */
 uint64_t arctn_b200_program_launches(const arctn_b200_program* program);
 /* Gradient programs: how many step results the adjoint sweep recomputes instead of keeping from the
  * forward, chosen at creation (largest results first) so that the workspace fits workspace_budget.
@@ -247,9 +248,10 @@ int arctn_b200_program_gradient(arctn_b200_program* program, int part, const voi
  * (the call then returns ARCTN_B200_ERR_DEVICE_TIMEOUT). */
 int arctn_b200_program_device_status(arctn_b200_program* program, void* workspace, void* cuda_stream, int* code);
 
-/* Profiled execute: launches op by op (no graph) with a CUDA event between consecutive kernels on
- * `cuda_stream`, synchronises, and writes per-launch duration (ms), kind and algorithmic work (real flops
- * for GEMM kinds, bytes moved for the others).  Arrays hold arctn_b200_program_launches entries.
+/* Profiled execute: launches unit by unit (no graph; a grouped launch of thin steps is one unit) with a CUDA
+ * event between consecutive launches on `cuda_stream`, synchronises, and writes per-launch duration (ms),
+ * kind and algorithmic work (real flops for GEMM kinds, bytes moved for the others).  Arrays hold
+ * arctn_b200_program_launches entries; unused entries keep their initial values.
  * Kinds: 0 gather, 1 gemm_small, 2 gemm_tile64, 3 gemm_tile32, 4 slice_accumulate, 5 slice_output,
  * 7 maxabs, 8 strip, 9 gemm_tc, 10 gemm_dot, 11 pack, 12 scatter, 13 pack_tiled, 14 gemm_warp. */
 int arctn_b200_program_profile(arctn_b200_program* program, const void* const* inputs, void* output, void* workspace,

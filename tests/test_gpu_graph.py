@@ -60,3 +60,21 @@ def test_numpy_calls_reuse_buffers_and_see_new_inputs():
     st = torch.cuda.Stream()  # an explicit stream that is not the current one: copies follow it
     other = prog.execute(doubled, stream=st)
     assert np.array_equal(other, twice)
+
+
+def test_profile_reports_one_entry_per_launch_unit():
+    # A grouped launch of thin steps is one profiled launch; every other kernel one entry each.
+    net, arrays = N.brickwork_circuit(30, 14, seed=0)
+    arrays = [a.astype(np.complex64) for a in arrays]
+    prog = A.SlicedProgram(*net.as_tuple(), A.greedy(*net.as_tuple()), (), dtype=np.complex64, precision="tf32x3")
+    d = prog.describe()
+    first_of_unit = {}
+    for o in d["ops"]:
+        first_of_unit.setdefault(o["unit"], o["kind"])
+    want = sum(k != "memset" for k in first_of_unit.values())
+    x = [torch.from_numpy(a).cuda() for a in arrays]
+    ms, kinds, work = prog.profile(x)
+    assert len(kinds) == len(ms) == len(work) == want < sum(o["kind"] != "memset" for o in d["ops"])
+    assert all(t > 0 for t in ms)
+    gemm = {1, 2, 3, 9, 10, 14}
+    assert sum(w for k, w in zip(kinds, work) if k in gemm) == pytest.approx(prog.flops, rel=1e-12)

@@ -24,7 +24,9 @@ def test_describe_matches_counters_and_plan():
     p = program(net, path, dtype=np.complex128)
     d = p.describe()
     assert d["workspace_bytes"] == p.workspace_bytes
-    assert d["launches"] == p.launches == sum(o["kind"] != "memset" for o in d["ops"])
+    # one launch per launch unit (independent thin GEMMs of one DAG level share one grouped launch)
+    units = {o["unit"] for o in d["ops"] if o["kind"] != "memset"}
+    assert d["launches"] == p.launches == len(units) <= sum(o["kind"] != "memset" for o in d["ops"])
     assert d["groups"] == 1 and d["n_slices"] == 1
     gemms = [o for o in d["ops"] if o["kind"] in GEMM_KINDS]
     assert len(gemms) == len(path)  # one GEMM per pairwise step
@@ -203,6 +205,14 @@ def _dag_orders_every_overlap(ops):
             assert d < j
             a |= anc[d] | (1 << d)
         anc.append(a)
+    # grouped launches: thin GEMMs only, none an ancestor of another
+    groups = {}
+    for j, o in enumerate(ops):
+        groups.setdefault(o["unit"], []).append(j)
+    for members in groups.values():
+        if len(members) > 1:
+            assert all(ops[j]["kind"] == "gemm_small" for j in members)
+            assert not any(anc[j] >> i & 1 for i in members for j in members)
     spans = [[(sp, lo, (1 << 64) if hi == -1 else hi) for sp, lo, hi in o["foot"]] for o in ops]
     for j in range(len(ops)):
         for i in range(j):
@@ -230,3 +240,4 @@ def test_graph_dag_orders_every_pair_of_ops_sharing_memory(case):
     _dag_orders_every_overlap(ops)
     if case != "sliced_fused":
         assert len({o["lane"] for o in ops}) > 1  # independent steps do run on several lanes
+        assert len({o["unit"] for o in ops}) < len(ops)  # and thin steps of one level share a launch
