@@ -92,6 +92,9 @@ SIGNATURES = [
     ("arctn_b200_program_recomputed_steps", u64, [vp]),
     ("arctn_b200_program_describe", c_int, [vp, ctypes.c_char_p, u64, u64p]),
     ("arctn_b200_batch_create", c_int, [ctypes.POINTER(vp), u64, c_int, ctypes.POINTER(vp)]),
+    ("arctn_b200_batch_create_mode", c_int, [ctypes.POINTER(vp), u64, c_int, c_int, ctypes.POINTER(vp)]),
+    ("arctn_b200_batch_describe", c_int, [vp, c_int, ctypes.c_char_p, u64, ctypes.POINTER(u64)]),
+    ("arctn_b200_batch_wait_selftest", c_int, [vp, ctypes.POINTER(c_int)]),
     ("arctn_b200_batch_destroy", None, [vp]),
     ("arctn_b200_batch_workspace_size", u64, [vp]),
     ("arctn_b200_batch_lanes", u64, [vp]),

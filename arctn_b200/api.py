@@ -487,22 +487,44 @@ class SlicedProgram:
 class ProgramBatch:
     """Many independent programs (uneven networks, mixed dtypes) run as one CUDA graph launch.
 
-    The programs are spread over up to ``max_lanes`` streams, longest first onto the least-loaded lane;
-    each lane runs its programs in turn in one workspace region and the lanes fork from and join back
-    into the caller's stream.  No reference counterpart: ArcTN contracts one network per call.
+    ``mode="persistent"`` (the default): the small programs made of SIMT steps only run inside one
+    persistent interpreter launch that follows the steps' dependencies on the device, while the others
+    (tensor-core steps, large SIMT GEMMs) run launch by launch on up to ``max_lanes`` streams alongside it.
+    ``mode="staged"``: every program inside the interpreter, tensor-core GEMMs and their operand packs
+    launched between interpreter launches.  ``mode="lanes"``: every program launch by launch, spread over
+    the streams longest first onto the least-loaded lane.  All modes give the same bits.  No reference
+    counterpart: ArcTN contracts one network per call.
     """
 
-    def __init__(self, programs, *, max_lanes=32):
+    _MODES = {"lanes": 0, "persistent": 1, "staged": 2}
+
+    def __init__(self, programs, *, max_lanes=32, mode="persistent"):
         self.programs = list(programs)
         if not self.programs:
             raise ValueError("a batch needs at least one program")
         arr = (C.vp * len(self.programs))(*[p._h for p in self.programs])
         h = C.vp()
-        C.check(C.lib().arctn_b200_batch_create(arr, len(self.programs), int(max_lanes), ctypes.byref(h)),
-                "batch")
+        if mode not in self._MODES:
+            raise ValueError(f"batch mode must be one of {sorted(self._MODES)}")
+        C.check(C.lib().arctn_b200_batch_create_mode(arr, len(self.programs), int(max_lanes), self._MODES[mode],
+                                                     ctypes.byref(h)), "batch")
         self._h = h
+        self.mode = mode
         self.workspace_bytes = int(C.lib().arctn_b200_batch_workspace_size(h))
         self.lanes = int(C.lib().arctn_b200_batch_lanes(h))
+
+    def describe(self, detail=False):
+        """Mode, lanes, workspace regions and the interpreter's stages, steps and tasks per part, as a dict
+        (host-only; works without a GPU).  ``detail=True`` adds every interpreter step and staged launch."""
+        import json
+
+        need = C.u64(0)
+        C.check(C.lib().arctn_b200_batch_describe(self._h, int(bool(detail)), None, 0, ctypes.byref(need)),
+                "batch describe")
+        buf = ctypes.create_string_buffer(int(need.value))
+        C.check(C.lib().arctn_b200_batch_describe(self._h, int(bool(detail)), buf, need.value,
+                                                  ctypes.byref(need)), "batch describe")
+        return json.loads(buf.value.decode())
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -574,6 +596,55 @@ class ProgramBatch:
         outs_r = [_to_output(o, tm) for o, (_, _, tm) in zip(outs, calls)]
         grads_r = [[_to_output(t, tm) for t in gl] for gl, (_, _, tm) in zip(grads, calls)]
         return outs_r, grads_r
+
+    def bind(self, arrays_list, *, gradient=False, grad_outputs=None, workspace=None, stream=None):
+        """A zero-argument callable that re-runs the batch on fixed CUDA buffers.
+
+        Validation, every output / gradient allocation and the pointer arrays happen here, once; each call
+        is then one C-ABI call (a graph replay on a side stream).  ``arrays_list`` holds CUDA tensors; the
+        returned callable has ``outputs``, ``grads`` (gradient runs) and ``workspace`` attributes, which
+        every call overwrites.
+        """
+        calls = self._bind(arrays_list, "batch bind")
+        torch = _torch()
+        if any(tm is False for _, _, tm in calls):
+            raise ValueError("batch bind: arrays must be CUDA torch tensors")
+        c0 = calls[0][0]
+        st = stream if stream is not None else c0.stream
+        ws = workspace if workspace is not None else c0.workspace(self.workspace_bytes)
+        outs = [c.empty(p.output_shape, _torch_dtype(code)) for p, (c, code, _) in zip(self.programs, calls)]
+        inp = (C.vpp * len(calls))(*[ctypes.cast(c.ptrs, C.vpp) for c, _, _ in calls])
+        optr = (C.vp * len(outs))(*[o.data_ptr() for o in outs])
+        lib, h, dev = C.lib(), self._h, c0.device
+        if gradient:
+            gouts, grads = [], []
+            for j, (p, (c, code, _)) in enumerate(zip(self.programs, calls)):
+                if not p.has_gradient:
+                    raise ValueError(f"batch bind: program {j} was built without gradient=True")
+                g = None if grad_outputs is None else grad_outputs[j]
+                g = torch.ones(p.output_shape, dtype=_torch_dtype(code), device=c.device) if g is None else \
+                    g.to(c.device, _torch_dtype(code)).contiguous()
+                gouts.append(g)
+                grads.append([torch.empty_like(t) for t in c.tensors])
+            gptr = (C.vp * len(gouts))(*[g.data_ptr() for g in gouts])
+            garrs = [(C.vp * len(gl))(*[t.data_ptr() for t in gl]) for gl in grads]
+            gpp = (C.vpp * len(garrs))(*[ctypes.cast(a, C.vpp) for a in garrs])
+
+            def run():
+                with torch.cuda.device(dev):
+                    C.check(lib.arctn_b200_batch_gradient(h, inp, gptr, gpp, optr, ws.data_ptr(), ws.numel(),
+                                                          st.cuda_stream), "batch gradient")
+            run.grads = grads
+            run._keep = (calls, gouts, garrs)
+        else:
+            def run():
+                with torch.cuda.device(dev):
+                    C.check(lib.arctn_b200_batch_execute(h, inp, optr, ws.data_ptr(), ws.numel(), st.cuda_stream),
+                            "batch execute")
+            run._keep = (calls,)
+        run.outputs = outs
+        run.workspace = ws
+        return run
 
     def device_status(self, workspace, stream=None):
         torch = _torch()

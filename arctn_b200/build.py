@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libarctn_b200.so")
 SOURCES = ["host.cpp", "program.cu", "batch.cu", "capi.cu", "noalloc.cu"]
-HEADERS = ["host.hpp", "program.hpp", "batch.hpp", "kernels.cuh", "tc_gemm.cuh"]
+HEADERS = ["host.hpp", "program.hpp", "batch.hpp", "kernels.cuh", "tc_gemm.cuh", "interp.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -400,8 +400,8 @@ int arctn_b200_program_describe(const arctn_b200_program* p, char* buf, uint64_t
   });
 }
 
-int arctn_b200_batch_create(arctn_b200_program* const* programs, uint64_t n_programs, int max_lanes,
-                            arctn_b200_batch** batch_out) {
+int arctn_b200_batch_create_mode(arctn_b200_program* const* programs, uint64_t n_programs, int max_lanes, int mode,
+                                 arctn_b200_batch** batch_out) {
   return guarded([&] {
     if (!programs || !batch_out) fail("null argument");
     std::vector<Program*> ps;
@@ -410,8 +410,34 @@ int arctn_b200_batch_create(arctn_b200_program* const* programs, uint64_t n_prog
       ps.push_back(programs[j]->p.get());
     }
     auto h = std::make_unique<arctn_b200_batch>();
-    h->b = std::make_unique<ProgramBatch>(std::move(ps), max_lanes);
+    h->b = std::make_unique<ProgramBatch>(std::move(ps), max_lanes, mode);
     *batch_out = h.release();
+  });
+}
+
+int arctn_b200_batch_create(arctn_b200_program* const* programs, uint64_t n_programs, int max_lanes,
+                            arctn_b200_batch** batch_out) {
+  return arctn_b200_batch_create_mode(programs, n_programs, max_lanes, ARCTN_B200_BATCH_PERSISTENT, batch_out);
+}
+
+int arctn_b200_batch_wait_selftest(void* cuda_stream, int* code) {
+  return guarded([&] {
+    if (!code) fail("null argument");
+    *code = interp_wait_selftest((cudaStream_t)cuda_stream);
+  });
+}
+
+int arctn_b200_batch_describe(const arctn_b200_batch* batch, int detail, char* buf, uint64_t buf_bytes,
+                              uint64_t* needed) {
+  return guarded([&] {
+    if (!batch) fail("batch is null");
+    const std::string d = batch->b->describe(detail);
+    if (needed) *needed = d.size() + 1;
+    if (buf && buf_bytes) {
+      const size_t n = std::min<size_t>(d.size(), (size_t)buf_bytes - 1);
+      std::memcpy(buf, d.data(), n);
+      buf[n] = 0;
+    }
   });
 }
 

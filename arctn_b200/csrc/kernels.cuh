@@ -115,11 +115,16 @@ template <class T> struct OutCast<T, T> { __device__ static T cast(T v) { return
 template <> struct OutCast<float, double> { __device__ static double cast(float v) { return v; } };
 template <> struct OutCast<cf32, cf64> { __device__ static cf64 cast(cf32 v) { return {(double)v.re, (double)v.im}; } };
 
+//
+// Every SIMT kernel below is a thin __global__ wrapper over a __device__ body that takes its block index
+// and block count (vb, nvb) as arguments: a launch passes (blockIdx.x, gridDim.x); the batch interpreter
+// (interp.cuh) runs the same bodies as tasks of one persistent launch.  An output element's arithmetic
+// never depends on (vb, nvb), so both forms give the same bits.
 template <class T, class TO>
-__global__ void k_gather_reduce(const T* __restrict__ in, TO* __restrict__ out, const ll* __restrict__ offE,
-                                const ll* __restrict__ offR, ll n_out, ll n_red, ll S, SliceOff so, ll g0) {
+__device__ __forceinline__ void gather_reduce_body(const T* in, TO* out, const ll* offE, const ll* offR, ll n_out,
+                                                   ll n_red, ll S, const SliceOff& so, ll g0, ll vb, ll nvb) {
   const ll total = S * n_out;
-  for (ll idx = (ll)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (ll)gridDim.x * blockDim.x) {
+  for (ll idx = vb * blockDim.x + threadIdx.x; idx < total; idx += nvb * blockDim.x) {
     const ll s = idx / n_out, e = idx - s * n_out;
     const T* base = in + slice_offset(so, g0, s) + offE[e];
     T acc = base[offR[0]];
@@ -127,18 +132,28 @@ __global__ void k_gather_reduce(const T* __restrict__ in, TO* __restrict__ out, 
     out[idx] = OutCast<T, TO>::cast(acc);
   }
 }
+template <class T, class TO>
+__global__ void k_gather_reduce(const T* __restrict__ in, TO* __restrict__ out, const ll* __restrict__ offE,
+                                const ll* __restrict__ offR, ll n_out, ll n_red, ll S, SliceOff so, ll g0) {
+  gather_reduce_body<T, TO>(in, out, offE, offR, n_out, n_red, S, so, g0, blockIdx.x, gridDim.x);
+}
 
 // out[offE[e] + offR[r]] = in[e] for every (e, r): the adjoint of a trace (every diagonal element
 // receives the traced gradient) or of a diagonal extraction (the diagonal receives it).  The
 // (e, r) -> position map is injective, so plain stores suffice after the output is zeroed.
 template <class T>
-__global__ void k_scatter(const T* __restrict__ in, T* __restrict__ out, const ll* __restrict__ offE,
-                          const ll* __restrict__ offR, ll n_in, ll n_red) {
+__device__ __forceinline__ void scatter_body(const T* in, T* out, const ll* offE, const ll* offR, ll n_in, ll n_red,
+                                             ll vb, ll nvb) {
   const ll total = n_in * n_red;
-  for (ll idx = (ll)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (ll)gridDim.x * blockDim.x) {
+  for (ll idx = vb * blockDim.x + threadIdx.x; idx < total; idx += nvb * blockDim.x) {
     const ll e = idx / n_red, r = idx - e * n_red;
     out[offE[e] + offR[r]] = in[e];
   }
+}
+template <class T>
+__global__ void k_scatter(const T* __restrict__ in, T* __restrict__ out, const ll* __restrict__ offE,
+                          const ll* __restrict__ offR, ll n_in, ll n_red) {
+  scatter_body<T>(in, out, offE, offR, n_in, n_red, blockIdx.x, gridDim.x);
 }
 
 // Gradient of a sliced input: acc[sliceoff(s) + offE[e]] += G[s][e] in the wide type.  One thread per
@@ -146,10 +161,10 @@ __global__ void k_scatter(const T* __restrict__ in, T* __restrict__ out, const l
 // sliced legs the input does not hold) add up deterministically without atomics; distinct (slice
 // digits, e) pairs reach distinct targets because the input's index map is injective.
 template <class T>
-__global__ void k_grad_accum(const T* __restrict__ G, typename Num<T>::wide* __restrict__ acc,
-                             const ll* __restrict__ offE, ll n_e, ll S, SliceOff so, ll g0) {
+__device__ __forceinline__ void grad_accum_body(const T* G, typename Num<T>::wide* acc, const ll* offE, ll n_e, ll S,
+                                                const SliceOff& so, ll g0, ll vb, ll nvb) {
   using W = typename Num<T>::wide;
-  for (ll e = (ll)blockIdx.x * blockDim.x + threadIdx.x; e < n_e; e += (ll)gridDim.x * blockDim.x) {
+  for (ll e = vb * blockDim.x + threadIdx.x; e < n_e; e += nvb * blockDim.x) {
     const ll t = offE[e];
     for (ll s = 0; s < S; ++s) {
       W* dst = acc + slice_offset(so, g0, s) + t;
@@ -157,11 +172,19 @@ __global__ void k_grad_accum(const T* __restrict__ G, typename Num<T>::wide* __r
     }
   }
 }
+template <class T>
+__global__ void k_grad_accum(const T* __restrict__ G, typename Num<T>::wide* __restrict__ acc,
+                             const ll* __restrict__ offE, ll n_e, ll S, SliceOff so, ll g0) {
+  grad_accum_body<T>(G, acc, offE, n_e, S, so, g0, blockIdx.x, gridDim.x);
+}
 
 template <class T>
+__device__ __forceinline__ void narrow_body(const typename Num<T>::wide* in, T* out, ll n, ll vb, ll nvb) {
+  for (ll i = vb * blockDim.x + threadIdx.x; i < n; i += nvb * blockDim.x) out[i] = Num<T>::narrow(in[i]);
+}
+template <class T>
 __global__ void k_narrow(const typename Num<T>::wide* __restrict__ in, T* __restrict__ out, ll n) {
-  for (ll i = (ll)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (ll)gridDim.x * blockDim.x)
-    out[i] = Num<T>::narrow(in[i]);
+  narrow_body<T>(in, out, n, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- GEMM tables
@@ -176,34 +199,43 @@ struct GemmArgs {
   int conj_a = 0, conj_b = 0;  // read an operand conjugated (adjoint steps)
 };
 
-// Thin steps: one thread per output element, k-loop through the tables.
+// Thin steps: one thread per output element, k-loop through the tables.  sh_tab holds 2 * k entries
+// when k <= 1024.  The bodies copy the scalar arguments to locals first: the interpreter passes `g` from
+// global memory, where every access would otherwise be reloaded after each store.
 template <class T>
-__global__ void __launch_bounds__(256) k_gemm_small(GemmArgs g) {
+__device__ __forceinline__ void gemm_small_body(const GemmArgs& g, ll* sh_tab, ll vb, ll nvb) {
   using A = typename Num<T>::acc;
   const T* Ap = (const T*)g.A;
   const T* Bp = (const T*)g.B;
   T* Cp = (T*)g.C;
-  const ll mn = g.m * g.n, per_s = g.bt * mn, total = g.S * per_s;
-  extern __shared__ ll sh_tab[];  // aK[0..k) then bK[0..k) when they fit
-  const bool tab_in_smem = g.k <= 1024;
+  const ll m = g.m, k = g.k, n = g.n, g0 = g.g0;
+  const ll *gaB = g.aB, *gaM = g.aM, *gaK = g.aK, *gbB = g.bB, *gbK = g.bK, *gbN = g.bN;
+  const int ca = g.conj_a, cb = g.conj_b;
+  const ll mn = m * n, per_s = g.bt * mn, total = g.S * per_s;
+  const bool tab_in_smem = k <= 1024;
   if (tab_in_smem) {
-    for (ll l = threadIdx.x; l < g.k; l += blockDim.x) { sh_tab[l] = g.aK[l]; sh_tab[g.k + l] = g.bK[l]; }
+    for (ll l = threadIdx.x; l < k; l += blockDim.x) { sh_tab[l] = gaK[l]; sh_tab[k + l] = gbK[l]; }
     __syncthreads();
   }
-  const ll* aK = tab_in_smem ? sh_tab : g.aK;
-  const ll* bK = tab_in_smem ? sh_tab + g.k : g.bK;
-  for (ll idx = (ll)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (ll)gridDim.x * blockDim.x) {
+  const ll* aK = tab_in_smem ? sh_tab : gaK;
+  const ll* bK = tab_in_smem ? sh_tab + k : gbK;
+  for (ll idx = vb * blockDim.x + threadIdx.x; idx < total; idx += nvb * blockDim.x) {
     const ll s = idx / per_s;
     ll r = idx - s * per_s;
     const ll b = r / mn;
     r -= b * mn;
-    const ll i = r / g.n, j = r - i * g.n;
-    const T* a = Ap + slice_offset(g.sa, g.g0, s) + g.aB[b] + g.aM[i];
-    const T* bb = Bp + slice_offset(g.sb, g.g0, s) + g.bB[b] + g.bN[j];
+    const ll i = r / n, j = r - i * n;
+    const T* a = Ap + slice_offset(g.sa, g0, s) + gaB[b] + gaM[i];
+    const T* bb = Bp + slice_offset(g.sb, g0, s) + gbB[b] + gbN[j];
     A acc = Num<T>::zero();
-    for (ll l = 0; l < g.k; ++l) Num<T>::fma(acc, cj(a[aK[l]], g.conj_a), cj(bb[bK[l]], g.conj_b));
+    for (ll l = 0; l < k; ++l) Num<T>::fma(acc, cj(a[aK[l]], ca), cj(bb[bK[l]], cb));
     Cp[idx] = acc;
   }
+}
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm_small(GemmArgs g) {
+  extern __shared__ ll sh_tab[];  // aK[0..k) then bK[0..k) when they fit
+  gemm_small_body<T>(g, sh_tab, blockIdx.x, gridDim.x);
 }
 
 // Independent one-slice thin steps of one level of the step DAG, run as one launch: each block finds its
@@ -262,23 +294,25 @@ __global__ void __launch_bounds__(256) k_gemm_small_grouped(const __grid_constan
 // one CTA per output element, the k range strided over 256 threads and
 // folded by a fixed shared-memory tree, so the sum order never varies.
 template <class T>
-__global__ void __launch_bounds__(256) k_gemm_dot(GemmArgs g) {
+__device__ __forceinline__ void gemm_dot_body(const GemmArgs& g, typename Num<T>::acc* red, ll vb, ll nvb) {
   using A = typename Num<T>::acc;
-  __shared__ A red[256];
   const T* Ap = (const T*)g.A;
   const T* Bp = (const T*)g.B;
   T* Cp = (T*)g.C;
-  const ll mn = g.m * g.n, per_s = g.bt * mn, total = g.S * per_s;
-  for (ll idx = blockIdx.x; idx < total; idx += gridDim.x) {
+  const ll m = g.m, k = g.k, n = g.n, g0 = g.g0;
+  const ll *gaB = g.aB, *gaM = g.aM, *gaK = g.aK, *gbB = g.bB, *gbK = g.bK, *gbN = g.bN;
+  const int ca = g.conj_a, cb = g.conj_b;
+  const ll mn = m * n, per_s = g.bt * mn, total = g.S * per_s;
+  for (ll idx = vb; idx < total; idx += nvb) {
     const ll s = idx / per_s;
     ll r = idx - s * per_s;
     const ll b = r / mn;
     r -= b * mn;
-    const ll i = r / g.n, j = r - i * g.n;
-    const T* a = Ap + slice_offset(g.sa, g.g0, s) + g.aB[b] + g.aM[i];
-    const T* bb = Bp + slice_offset(g.sb, g.g0, s) + g.bB[b] + g.bN[j];
+    const ll i = r / n, j = r - i * n;
+    const T* a = Ap + slice_offset(g.sa, g0, s) + gaB[b] + gaM[i];
+    const T* bb = Bp + slice_offset(g.sb, g0, s) + gbB[b] + gbN[j];
     A acc = Num<T>::zero();
-    for (ll l = threadIdx.x; l < g.k; l += 256) Num<T>::fma(acc, cj(a[g.aK[l]], g.conj_a), cj(bb[g.bK[l]], g.conj_b));
+    for (ll l = threadIdx.x; l < k; l += 256) Num<T>::fma(acc, cj(a[gaK[l]], ca), cj(bb[gbK[l]], cb));
     red[threadIdx.x] = acc;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
@@ -289,30 +323,37 @@ __global__ void __launch_bounds__(256) k_gemm_dot(GemmArgs g) {
     __syncthreads();
   }
 }
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm_dot(GemmArgs g) {
+  __shared__ typename Num<T>::acc red[256];
+  gemm_dot_body<T>(g, red, blockIdx.x, gridDim.x);
+}
 
 // Long dot products split over CTAs: CTA (output o, part p) reduces k-range [p * chunk, ...) with the
 // same fixed tree as k_gemm_dot and stores the widened partial at part[o * parts + p]; k_dot_reduce then
 // adds each output's partials in part order in the wide type and rounds once.
 template <class T>
-__global__ void __launch_bounds__(256) k_gemm_dot_part(GemmArgs g, ll chunk, int parts,
-                                                       typename Num<T>::wide* __restrict__ part) {
+__device__ __forceinline__ void gemm_dot_part_body(const GemmArgs& g, ll chunk, int parts, typename Num<T>::wide* part,
+                                                   typename Num<T>::acc* red, ll vb, ll nvb) {
   using A = typename Num<T>::acc;
-  __shared__ A red[256];
   const T* Ap = (const T*)g.A;
   const T* Bp = (const T*)g.B;
-  const ll mn = g.m * g.n, per_s = g.bt * mn, total = g.S * per_s;
-  for (ll blk = blockIdx.x; blk < total * parts; blk += gridDim.x) {
+  const ll m = g.m, k = g.k, n = g.n, g0 = g.g0;
+  const ll *gaB = g.aB, *gaM = g.aM, *gaK = g.aK, *gbB = g.bB, *gbK = g.bK, *gbN = g.bN;
+  const int ca = g.conj_a, cb = g.conj_b;
+  const ll mn = m * n, per_s = g.bt * mn, total = g.S * per_s;
+  for (ll blk = vb; blk < total * parts; blk += nvb) {
     const ll idx = blk / parts, p = blk - idx * parts;
     const ll s = idx / per_s;
     ll r = idx - s * per_s;
     const ll b = r / mn;
     r -= b * mn;
-    const ll i = r / g.n, j = r - i * g.n;
-    const T* a = Ap + slice_offset(g.sa, g.g0, s) + g.aB[b] + g.aM[i];
-    const T* bb = Bp + slice_offset(g.sb, g.g0, s) + g.bB[b] + g.bN[j];
-    const ll l0 = p * chunk, l1 = l0 + chunk < g.k ? l0 + chunk : g.k;
+    const ll i = r / n, j = r - i * n;
+    const T* a = Ap + slice_offset(g.sa, g0, s) + gaB[b] + gaM[i];
+    const T* bb = Bp + slice_offset(g.sb, g0, s) + gbB[b] + gbN[j];
+    const ll l0 = p * chunk, l1 = l0 + chunk < k ? l0 + chunk : k;
     A acc = Num<T>::zero();
-    for (ll l = l0 + threadIdx.x; l < l1; l += 256) Num<T>::fma(acc, cj(a[g.aK[l]], g.conj_a), cj(bb[g.bK[l]], g.conj_b));
+    for (ll l = l0 + threadIdx.x; l < l1; l += 256) Num<T>::fma(acc, cj(a[gaK[l]], ca), cj(bb[gbK[l]], cb));
     red[threadIdx.x] = acc;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
@@ -323,15 +364,26 @@ __global__ void __launch_bounds__(256) k_gemm_dot_part(GemmArgs g, ll chunk, int
     __syncthreads();
   }
 }
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm_dot_part(GemmArgs g, ll chunk, int parts,
+                                                       typename Num<T>::wide* __restrict__ part) {
+  __shared__ typename Num<T>::acc red[256];
+  gemm_dot_part_body<T>(g, chunk, parts, part, red, blockIdx.x, gridDim.x);
+}
 
 template <class T>
-__global__ void k_dot_reduce(const typename Num<T>::wide* __restrict__ part, T* __restrict__ C, ll total, int parts) {
+__device__ __forceinline__ void dot_reduce_body(const typename Num<T>::wide* part, T* C, ll total, int parts, ll vb,
+                                                ll nvb) {
   using W = typename Num<T>::wide;
-  for (ll o = (ll)blockIdx.x * blockDim.x + threadIdx.x; o < total; o += (ll)gridDim.x * blockDim.x) {
+  for (ll o = vb * blockDim.x + threadIdx.x; o < total; o += nvb * blockDim.x) {
     W acc = Num<W>::zero();
     for (int p = 0; p < parts; ++p) acc = Num<W>::add(acc, part[o * parts + p]);
     C[o] = Num<T>::narrow(acc);
   }
+}
+template <class T>
+__global__ void k_dot_reduce(const typename Num<T>::wide* __restrict__ part, T* __restrict__ C, ll total, int parts) {
+  dot_reduce_body<T>(part, C, total, parts, blockIdx.x, gridDim.x);
 }
 
 // Warp-wide butterfly reduction in a fixed order (xor 16, 8, 4, 2, 1): deterministic, lane 0 holds it.
@@ -343,67 +395,75 @@ __device__ __forceinline__ cf64 shfl_xor(cf64 v, int m) { return {shfl_xor(v.re,
 // Thin steps with a moderate k (k >= 64, an output too small for a tile kernel): one warp per output,
 // lanes striding over k, then a fixed butterfly.  Eight outputs per 256-thread CTA.
 template <class T>
-__global__ void __launch_bounds__(256) k_gemm_warp(GemmArgs g) {
+__device__ __forceinline__ void gemm_warp_body(const GemmArgs& g, ll vb, ll nvb) {
   using A = typename Num<T>::acc;
   const T* Ap = (const T*)g.A;
   const T* Bp = (const T*)g.B;
   T* Cp = (T*)g.C;
+  const ll m = g.m, k = g.k, n = g.n, g0 = g.g0;
+  const ll *gaB = g.aB, *gaM = g.aM, *gaK = g.aK, *gbB = g.bB, *gbK = g.bK, *gbN = g.bN;
+  const int ca = g.conj_a, cb = g.conj_b;
   const int lane = threadIdx.x % 32;
-  const ll mn = g.m * g.n, per_s = g.bt * mn, total = g.S * per_s;
-  const ll warps = (ll)gridDim.x * (blockDim.x / 32);
-  for (ll idx = (ll)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; idx < total; idx += warps) {
+  const ll mn = m * n, per_s = g.bt * mn, total = g.S * per_s;
+  const ll warps = nvb * (blockDim.x / 32);
+  for (ll idx = vb * (blockDim.x / 32) + threadIdx.x / 32; idx < total; idx += warps) {
     const ll s = idx / per_s;
     ll r = idx - s * per_s;
     const ll b = r / mn;
     r -= b * mn;
-    const ll i = r / g.n, j = r - i * g.n;
-    const T* a = Ap + slice_offset(g.sa, g.g0, s) + g.aB[b] + g.aM[i];
-    const T* bb = Bp + slice_offset(g.sb, g.g0, s) + g.bB[b] + g.bN[j];
+    const ll i = r / n, j = r - i * n;
+    const T* a = Ap + slice_offset(g.sa, g0, s) + gaB[b] + gaM[i];
+    const T* bb = Bp + slice_offset(g.sb, g0, s) + gbB[b] + gbN[j];
     A acc = Num<T>::zero();
-    for (ll l = lane; l < g.k; l += 32) Num<T>::fma(acc, cj(a[g.aK[l]], g.conj_a), cj(bb[g.bK[l]], g.conj_b));
+    for (ll l = lane; l < k; l += 32) Num<T>::fma(acc, cj(a[gaK[l]], ca), cj(bb[gbK[l]], cb));
 #pragma unroll
     for (int w = 16; w > 0; w >>= 1) acc = Num<T>::add(acc, shfl_xor(acc, w));
     if (lane == 0) Cp[idx] = acc;
   }
+}
+template <class T>
+__global__ void __launch_bounds__(256) k_gemm_warp(GemmArgs g) {
+  gemm_warp_body<T>(g, blockIdx.x, gridDim.x);
 }
 
 // Dense-enough steps on the CUDA cores: TM x TN output tile per CTA, TK-deep
 // k-slabs staged through shared memory, (TM/16) x (TN/16) outputs per thread.
 // This is the plain-FP32 (or FP64) form of the step GEMM.
 template <class T, int TM, int TN, int TK>
-__global__ void __launch_bounds__(256) k_gemm_tile(GemmArgs g) {
+__device__ __forceinline__ void gemm_tile_body(const GemmArgs& g, T (*As)[TM + 1], T (*Bs)[TN + 1], ll vb, ll nvb) {
   constexpr int RM = TM / 16, RN = TN / 16;
-  __shared__ T As[TK][TM + 1];
-  __shared__ T Bs[TK][TN + 1];
   const T* Ap = (const T*)g.A;
   const T* Bp = (const T*)g.B;
   T* Cp = (T*)g.C;
+  const ll bt = g.bt, g0 = g.g0, m = g.m, k = g.k, n = g.n;
+  const ll *gaB = g.aB, *gaM = g.aM, *gaK = g.aK, *gbB = g.bB, *gbK = g.bK, *gbN = g.bN;
+  const int ca = g.conj_a, cb = g.conj_b;
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  const ll tiles_n = (g.n + TN - 1) / TN, tiles_m = (g.m + TM - 1) / TM;
-  const ll n_tiles = tiles_n * tiles_m * g.S * g.bt;
-  for (ll t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+  const ll tiles_n = (n + TN - 1) / TN, tiles_m = (m + TM - 1) / TM;
+  const ll n_tiles = tiles_n * tiles_m * g.S * bt;
+  for (ll t = vb; t < n_tiles; t += nvb) {
     ll r = t;
     const ll tn = r % tiles_n; r /= tiles_n;
     const ll tm = r % tiles_m; r /= tiles_m;
-    const ll sb = r, s = sb / g.bt, b = sb - s * g.bt;
+    const ll sb = r, s = sb / bt, b = sb - s * bt;
     const ll i0 = tm * TM, j0 = tn * TN;
-    const T* abase = Ap + slice_offset(g.sa, g.g0, s) + g.aB[b];
-    const T* bbase = Bp + slice_offset(g.sb, g.g0, s) + g.bB[b];
+    const T* abase = Ap + slice_offset(g.sa, g0, s) + gaB[b];
+    const T* bbase = Bp + slice_offset(g.sb, g0, s) + gbB[b];
     typename Num<T>::acc acc[RM][RN];
 #pragma unroll
     for (int x = 0; x < RM; ++x)
 #pragma unroll
       for (int y = 0; y < RN; ++y) acc[x][y] = Num<T>::zero();
-    for (ll l0 = 0; l0 < g.k; l0 += TK) {
+    for (ll l0 = 0; l0 < k; l0 += TK) {
       for (int q = threadIdx.x; q < TM * TK; q += 256) {
         const int ii = q / TK, ll_ = q % TK;
         const ll i = i0 + ii, l = l0 + ll_;
-        As[ll_][ii] = (i < g.m && l < g.k) ? cj(abase[g.aM[i] + g.aK[l]], g.conj_a) : Num<T>::zero();
+        As[ll_][ii] = (i < m && l < k) ? cj(abase[gaM[i] + gaK[l]], ca) : Num<T>::zero();
       }
       for (int q = threadIdx.x; q < TN * TK; q += 256) {
         const int jj = q % TN, ll_ = q / TN;
         const ll j = j0 + jj, l = l0 + ll_;
-        Bs[ll_][jj] = (j < g.n && l < g.k) ? cj(bbase[g.bK[l] + g.bN[j]], g.conj_b) : Num<T>::zero();
+        Bs[ll_][jj] = (j < n && l < k) ? cj(bbase[gbK[l] + gbN[j]], cb) : Num<T>::zero();
       }
       __syncthreads();
 #pragma unroll 4
@@ -420,15 +480,21 @@ __global__ void __launch_bounds__(256) k_gemm_tile(GemmArgs g) {
       }
       __syncthreads();
     }
-    T* cbase = Cp + (s * g.bt + b) * g.m * g.n;
+    T* cbase = Cp + (s * bt + b) * m * n;
 #pragma unroll
     for (int x = 0; x < RM; ++x)
 #pragma unroll
       for (int y = 0; y < RN; ++y) {
         const ll i = i0 + ty + 16 * x, j = j0 + tx + 16 * y;
-        if (i < g.m && j < g.n) cbase[i * g.n + j] = acc[x][y];
+        if (i < m && j < n) cbase[i * n + j] = acc[x][y];
       }
   }
+}
+template <class T, int TM, int TN, int TK>
+__global__ void __launch_bounds__(256) k_gemm_tile(GemmArgs g) {
+  __shared__ T As[TK][TM + 1];
+  __shared__ T Bs[TK][TN + 1];
+  gemm_tile_body<T, TM, TN, TK>(g, As, Bs, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- cross-slice sum
@@ -438,11 +504,11 @@ __global__ void __launch_bounds__(256) k_gemm_tile(GemmArgs g) {
 struct Segment { ll part, lo, hi; };  // lo/hi are local slice indices in the group
 
 template <class T>
-__global__ void k_slice_accumulate(const T* __restrict__ F, typename Num<T>::wide* __restrict__ P,
-                                   const Segment* __restrict__ segs, ll n_segs, ll n_e) {
+__device__ __forceinline__ void slice_accumulate_body(const T* F, typename Num<T>::wide* P, const Segment* segs,
+                                                      ll n_segs, ll n_e, ll vb, ll nvb) {
   using W = typename Num<T>::wide;
   const ll total = n_segs * n_e;
-  for (ll idx = (ll)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (ll)gridDim.x * blockDim.x) {
+  for (ll idx = vb * blockDim.x + threadIdx.x; idx < total; idx += nvb * blockDim.x) {
     const ll sg = idx / n_e, e = idx - sg * n_e;
     const Segment seg = segs[sg];
     W acc = P[seg.part * n_e + e];
@@ -450,15 +516,20 @@ __global__ void k_slice_accumulate(const T* __restrict__ F, typename Num<T>::wid
     P[seg.part * n_e + e] = acc;
   }
 }
+template <class T>
+__global__ void k_slice_accumulate(const T* __restrict__ F, typename Num<T>::wide* __restrict__ P,
+                                   const Segment* __restrict__ segs, ll n_segs, ll n_e) {
+  slice_accumulate_body<T>(F, P, segs, n_segs, n_e, blockIdx.x, gridDim.x);
+}
 
 // out[blockbase[blk] + scatter[e]] = sum_c P[blk][c][e], chunks merged in order.
 template <class T, class TO>
-__global__ void k_slice_output(const typename Num<T>::wide* __restrict__ P, TO* __restrict__ out,
-                               const ll* __restrict__ block_base, const ll* __restrict__ scatter, ll n_blocks,
-                               ll n_chunks, ll n_e) {
+__device__ __forceinline__ void slice_output_body(const typename Num<T>::wide* P, TO* out, const ll* block_base,
+                                                  const ll* scatter, ll n_blocks, ll n_chunks, ll n_e, ll vb,
+                                                  ll nvb) {
   using W = typename Num<T>::wide;
   const ll total = n_blocks * n_e;
-  for (ll idx = (ll)blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += (ll)gridDim.x * blockDim.x) {
+  for (ll idx = vb * blockDim.x + threadIdx.x; idx < total; idx += nvb * blockDim.x) {
     const ll blk = idx / n_e, e = idx - blk * n_e;
     const W* p = P + blk * n_chunks * n_e + e;
     W acc = p[0];
@@ -468,6 +539,12 @@ __global__ void k_slice_output(const typename Num<T>::wide* __restrict__ P, TO* 
     else v = Num<T>::narrow(acc);
     out[block_base[blk] + scatter[e]] = v;
   }
+}
+template <class T, class TO>
+__global__ void k_slice_output(const typename Num<T>::wide* __restrict__ P, TO* __restrict__ out,
+                               const ll* __restrict__ block_base, const ll* __restrict__ scatter, ll n_blocks,
+                               ll n_chunks, ll n_e) {
+  slice_output_body<T, TO>(P, out, block_base, scatter, n_blocks, n_chunks, n_e, blockIdx.x, gridDim.x);
 }
 
 // ---------------------------------------------------------------- stripped execution
@@ -493,5 +570,33 @@ __global__ void k_strip_scale(T* __restrict__ c, ll n, const unsigned long long*
   for (ll i = (ll)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (ll)gridDim.x * blockDim.x) c[i] = Num<T>::scale(c[i], inv);
   if (last_block_adds && blockIdx.x == 0 && threadIdx.x == 0) *exponent += log10(f);
 }
+
+// ---------------------------------------------------------------- batch interpreter descriptors
+// One step of one program of a batch, as the persistent interpreter (interp.cuh) runs it: the kind's
+// body with every pointer resolved, split into `nvb` tasks (virtual blocks of 256 threads).  The steps
+// listed in succ[succ0 .. succ0 + nsucc) depend on it.
+enum IKind : int {
+  I_GATHER, I_SCATTER, I_GRAD_ACCUM, I_NARROW, I_GEMM_SMALL, I_GEMM_DOT, I_DOT_PART, I_DOT_REDUCE, I_GEMM_WARP,
+  I_TILE64, I_TILE32, I_ACCUM, I_OUTPUT, I_MEMSET
+};
+struct IOp {
+  int kind;      // IKind
+  int dtype;     // 0 f32, 1 f64, 2 c64, 3 c128 (DType order)
+  int nvb;       // tasks of this op
+  int out_wide;  // gather / slice output: store the FP64 (wide) type
+  int succ0, nsucc;
+  int parts;     // split dot product: number of K parts
+  int pad_;
+  ll chunk;      // split dot product: K per part
+  const void* a;  // non-GEMM kinds: source
+  void* c;        // non-GEMM kinds: destination
+  void* d;        // split dot product: the partials
+  const ll* t0;
+  const ll* t1;
+  ll n0, n1, n2, n3;  // per kind: gather (n_out, n_red, S, g0), scatter (n_in, n_red), grad_accum (n_e, -, S, g0),
+                      // narrow (n), dot_reduce (total), accumulate (n_segs, n_e), output (n_blocks, n_chunks,
+                      // n_e), memset (bytes)
+  GemmArgs g;         // GEMM kinds; g.sa is also the slice offset of gather and grad_accum
+};
 
 }  // namespace ab2

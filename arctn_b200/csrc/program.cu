@@ -1733,6 +1733,153 @@ void Program::launch_op(const Op& op, const void* const* inputs, void* output, c
   CK(cudaGetLastError());
 }
 
+bool Program::in_part(size_t i, int part) const {
+  return part == 0 || (part == 2 ? ops_[i].bwd : !ops_[i].bwd);
+}
+
+bool Program::interp_supported(size_t i) const {
+  switch (ops_[i].kind) {
+    case Op::GEMM_TC: case Op::PACK: case Op::PACK_TILED: case Op::MAXABS: case Op::STRIP: return false;
+    default: return true;
+  }
+}
+
+// The interpreter form of op i: the same body, sizes and pointers launch_op / launch_typed use.
+void Program::interp_descs(size_t i, const void* const* inputs, const void* grad_out, void* const* grads,
+                           void* output, char* ws, std::vector<IOp>& out) const {
+  const Op& op = ops_[i];
+  auto ptr = [&](const Ref& r) -> void* {
+    switch (r.kind) {
+      case Ref::INPUT: return inputs ? const_cast<void*>(inputs[r.index]) : nullptr;
+      case Ref::WS: return ws ? ws + r.index : nullptr;
+      case Ref::OUTPUT: return output;
+      case Ref::GRAD_OUT: return const_cast<void*>(grad_out);
+      case Ref::GRADS: return grads ? grads[r.index] : nullptr;
+      default: return nullptr;
+    }
+  };
+  auto T_ = [&](int q) { return dev_tab_ ? (const ll*)(dev_tab_ + op.tab[q]) : nullptr; };
+  // Tasks of a step: about 1024 elements (4 a thread) per task for the elementwise kinds, fewer outputs for
+  // the GEMMs by their K work; at most 512, which with a resident grid of ~2 CTAs an SM spreads one large
+  // step over the whole GPU.
+  auto tasks = [](ll work, ll per) { return (int)std::max<ll>(1, std::min<ll>((work + per - 1) / per, 512)); };
+  IOp d{};
+  d.dtype = opt_.dtype;
+  d.a = ptr(op.a);
+  d.c = ptr(op.c);
+  d.d = ptr(op.d);
+  auto gemm = [&]() {
+    GemmArgs& g = d.g;
+    g.A = ptr(op.a); g.B = ptr(op.b); g.C = ptr(op.c);
+    g.bt = op.bt; g.m = op.m; g.k = op.k; g.n = op.n; g.S = op.S; g.g0 = op.g0;
+    g.aB = T_(0); g.aM = T_(1); g.aK = T_(2); g.bB = T_(3); g.bK = T_(4); g.bN = T_(5);
+    g.sa = op.sa; g.sb = op.sb;
+    g.conj_a = op.conj_a ? 1 : 0;
+    g.conj_b = op.conj_b ? 1 : 0;
+  };
+  const ll outs = op.S * op.bt * op.m * op.n;
+  switch (op.kind) {
+    case Op::GATHER:
+      d.kind = I_GATHER;
+      d.out_wide = 0;  // batches write outputs in the program's dtype
+      d.t0 = T_(0); d.t1 = T_(1);
+      d.n0 = op.n_out; d.n1 = op.n_red; d.n2 = op.S; d.n3 = op.g0;
+      d.g.sa = op.sa;
+      d.nvb = tasks(op.S * op.n_out * op.n_red, 1024);
+      break;
+    case Op::SCATTER:
+      d.kind = I_SCATTER;
+      d.t0 = T_(0); d.t1 = T_(1);
+      d.n0 = op.n_out; d.n1 = op.n_red;
+      d.nvb = tasks(op.n_out * op.n_red, 1024);
+      break;
+    case Op::GRAD_ACCUM:
+      d.kind = I_GRAD_ACCUM;
+      d.t0 = T_(0);
+      d.n0 = op.n_e; d.n2 = op.S; d.n3 = op.g0;
+      d.g.sa = op.sa;
+      d.nvb = tasks(op.n_e * op.S, 1024);
+      break;
+    case Op::NARROW:
+      d.kind = I_NARROW;
+      d.n0 = op.n_out;
+      d.nvb = tasks(op.n_out, 1024);
+      break;
+    case Op::ACCUM:
+      d.kind = I_ACCUM;
+      d.t0 = dev_tab_ ? (const ll*)(dev_tab_ + op.tab[0]) : nullptr;  // Segment triples
+      d.n0 = op.n_segs; d.n1 = op.n_e;
+      d.nvb = tasks(op.n_segs * op.n_e, 1024);
+      break;
+    case Op::OUTPUT:
+      d.kind = I_OUTPUT;
+      d.out_wide = 0;
+      d.t0 = T_(0); d.t1 = T_(1);
+      d.n0 = op.n_blocks; d.n1 = op.n_chunks; d.n2 = op.n_e;
+      d.nvb = tasks(op.n_blocks * op.n_e * op.n_chunks, 1024);
+      break;
+    case Op::MEMSET:
+      d.kind = I_MEMSET;
+      d.n0 = (ll)(op.bytes ? op.bytes
+                           : (u64)(tc::PLANES * (op.a_var ? op.S : 1) * op.bt * op.rpad * op.kpad * (op.bf16 ? 2 : 4)));
+      d.nvb = tasks(d.n0, 256 * 16);
+      break;
+    case Op::GEMM_SMALL: gemm(); d.kind = I_GEMM_SMALL; d.nvb = tasks(outs * op.k, 8192); break;
+    case Op::GEMM_WARP: gemm(); d.kind = I_GEMM_WARP; d.nvb = tasks(outs * op.k, 16384); break;
+    case Op::GEMM_TILE64:
+      gemm();
+      d.kind = I_TILE64;
+      d.nvb = tasks(((op.n + 63) / 64) * ((op.m + 63) / 64) * op.S * op.bt, 1);
+      break;
+    case Op::GEMM_TILE32:
+      gemm();
+      d.kind = I_TILE32;
+      d.nvb = tasks(((op.n + 31) / 32) * ((op.m + 31) / 32) * op.S * op.bt, 1);
+      break;
+    case Op::GEMM_DOT:
+      gemm();
+      if (op.splits > 1) {
+        d.kind = I_DOT_PART;
+        d.parts = op.splits;
+        d.chunk = op.kt_chunk;
+        d.nvb = tasks(outs * op.splits, 1);
+        out.push_back(d);
+        IOp r{};
+        r.kind = I_DOT_REDUCE;
+        r.dtype = opt_.dtype;
+        r.a = ptr(op.d);
+        r.c = ptr(op.c);
+        r.n0 = outs;
+        r.parts = op.splits;
+        r.nvb = tasks(outs * op.splits, 1024);
+        out.push_back(r);
+        return;
+      }
+      d.kind = I_GEMM_DOT;
+      d.nvb = tasks(outs, 1);
+      break;
+    default:
+      throw Error(E_UNSUPPORTED, "the batch interpreter does not run this op kind");
+  }
+  out.push_back(d);
+}
+
+void Program::launch_one(size_t i, const void* const* inputs, const void* grad_out, void* const* grads,
+                         void* output, char* ws, cudaStream_t st) {
+  out_f64_flag_ = false;
+  grad_out_ = grad_out;
+  grads_ = grads;
+  try {
+    launch_op(ops_[i], inputs, output, ws, st);
+  } catch (...) {
+    grad_out_ = nullptr;
+    grads_ = nullptr;
+    throw;
+  }
+  grad_out_ = nullptr;
+  grads_ = nullptr;
+}
+
 // One launch for a unit of independent one-slice thin GEMMs (k_gemm_small_grouped).
 void Program::launch_group(const std::vector<int>& members, const void* const* inputs, void* output, char* ws,
                            cudaStream_t st) {

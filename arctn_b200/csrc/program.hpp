@@ -123,6 +123,20 @@ class Program {
   // JSON description of the launch sequence and workspace layout (host-only; no GPU needed).
   std::string describe() const;
 
+  // Hooks for the batch interpreter (interp.cuh).  Ops of the main sequence by index: whether `part`
+  // runs op i, its dependencies (earlier ops touching its memory), whether the interpreter can run it
+  // (every SIMT kind; not the tensor-core GEMM and its packs), its interpreter descriptors (two for a
+  // split dot product: partials, then their sum) with pointers resolved against one run's bindings
+  // (null bindings give the shapes and task counts only), and a standalone launch of it on `st`.
+  size_t n_ops() const { return ops_.size(); }
+  bool in_part(size_t i, int part) const;
+  const std::vector<int>& op_deps(size_t i) const { return deps_[i]; }
+  bool interp_supported(size_t i) const;
+  void interp_descs(size_t i, const void* const* inputs, const void* grad_out, void* const* grads, void* output,
+                    char* ws, std::vector<IOp>& out) const;
+  void launch_one(size_t i, const void* const* inputs, const void* grad_out, void* const* grads, void* output,
+                  char* ws, cudaStream_t st);
+
  private:
   // Workspace buffer with an op-index lifetime; region-2 sizes scale with the
   // group size unless `fixed` (operands shared by every slice of a group).

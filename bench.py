@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import argparse
 import datetime
+import contextlib
 import json
 import os
 import statistics
@@ -552,21 +553,60 @@ def run_batch(args, dev):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    batch = A.ProgramBatch(progs, max_lanes=32)
-    ws = torch.empty(max(batch.workspace_bytes, 1), dtype=torch.uint8, device=dev)
-    for _ in range(max(args.warmup, 3)):
-        batch.gradient(xs, workspace=ws, stream=stream)
-    torch.cuda.synchronize(dev)
-    times = []
+
+    def time_batch(batch, sampler=None):
+        # Device time of the whole batch on resident inputs: the bound form allocates every output and
+        # gradient once, so each timed call is one C-ABI call (a graph replay).
+        run = batch.bind(xs, gradient=True, stream=stream)
+        for _ in range(max(args.warmup, 3)):
+            run()
+        torch.cuda.synchronize(dev)
+        times = []
+        with sampler if sampler is not None else contextlib.nullcontext():
+            for _ in range(args.steps):
+                flush.fill_(1)
+                times.append(_events_ms(stream, run))
+        return statistics.mean(times), batch.device_status(run.workspace, stream)
+
+    # The lane form (every step its own launch, networks spread over 32 streams) for comparison.
+    lanes_ms, lanes_status = time_batch(A.ProgramBatch(progs, max_lanes=64, mode="lanes"))
+    batch = A.ProgramBatch(progs, max_lanes=64)
     sampler = ClockSampler(dev.index)
-    with sampler:
-        for _ in range(args.steps):
-            flush.fill_(1)
-            times.append(_events_ms(stream, lambda: batch.gradient(xs, workspace=ws, stream=stream)))
-    status = batch.device_status(ws, stream)
-    ms = statistics.mean(times)
+    ms, status = time_batch(batch, sampler)
+    status = status or lanes_status
+    # Kernels per call: one interpreter launch per stage with tasks, the staged tensor-core steps and packs
+    # (+1 for a split-K sum), every kernel of the lane programs, the status collection.
+    desc = batch.describe(detail=True)
+    part = next(p for p in desc["parts"] if p["part"] == 0)
+    ops = [p.describe()["ops"] for p in progs]
+
+    def kernels(o):
+        return (o["kind"] != "memset") + (o["kind"] in ("gemm_tc", "gemm_dot") and o.get("splits", 1) > 1)
+
+    staged = sum(kernels(ops[j][i]) for _, j, i in part["staged_launches"])
+    interpreted = set(desc["interpreted"])
+    lane_kernels = sum(kernels(o) for j in range(len(progs)) if j not in interpreted for o in ops[j])
+    launches_per_call = 1 + sum(1 for t in part["stage_tasks"] if t) + staged + lane_kernels
     flops = sum(3 * p.flops for p in progs)
     # Per-network latency: each network's forward + adjoint alone (graph-free program launches).
+    # End to end through the public API from host NumPy arrays: each call stages every network's inputs
+    # (one pinned copy per network), runs the batch and returns outputs and gradients as NumPy arrays.
+    host = [arrays for _, arrays in nets]
+    h2d = sum(a.nbytes for arrays in host for a in arrays)
+    d2h = sum(int(np.prod(p.output_shape)) * a[0].itemsize for p, a in zip(progs, host)) + h2d
+    ws_e2e = torch.empty(max(batch.workspace_bytes, 1), dtype=torch.uint8, device=dev)
+    for _ in range(2):
+        batch.gradient(host, workspace=ws_e2e, stream=stream)
+    e2e_ms = []
+    for _ in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        batch.gradient(host, workspace=ws_e2e, stream=stream)
+        torch.cuda.synchronize(dev)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e = {"value": len(progs) / (statistics.median(e2e_ms) * 1e-3), "unit": "networks/s",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": statistics.median(e2e_ms),
+           "path": "ProgramBatch.gradient on host NumPy arrays (wall clock, synchronised)"}
     lat = []
     for p, x in zip(progs, xs):
         w = torch.empty(max(p.workspace_bytes, 1), dtype=torch.uint8, device=dev)
@@ -575,10 +615,14 @@ def run_batch(args, dev):
     lat.sort()
     line = _line(args, "many-network forward+adjoint throughput", len(progs) / (ms * 1e-3), "networks/s", True, ms,
                  {"workload": "256 random 3-regular networks, n in [20,50], bond in {2,3,4}, f32/c64 alternating",
+                  "form": "persistent interpreter for the small SIMT-only networks, lane streams for the rest",
+                  "interpreted_networks": len(interpreted), "stages": part["stages"],
+                  "interpreter_tasks": part["tasks"], "lane_network_kernels": lane_kernels,
                   "lanes": batch.lanes, "precision": "tf32x3 (c64) / fp32 (f32)",
                   "l2": "flushed (256 MiB write) before each timed batch"}, "f32+c64",
-                 gpu_launches=sum(p.launches for p in progs) * args.steps,
-                 e2e=None, roofline={"bound": "latency", "achieved_tflops": flops / (ms * 1e-3) / 1e12},
+                 gpu_launches=launches_per_call * args.steps,
+                 lane_form_ms=lanes_ms, lane_form_launches_per_call=sum(p.launches for p in progs),
+                 e2e=e2e, roofline={"bound": "latency", "achieved_tflops": flops / (ms * 1e-3) / 1e12},
                  cpu_baseline=None, clocks=sampler.summary(), device_status=status,
                  tflops=flops / (ms * 1e-3) / 1e12,
                  single_network_ms_p50=lat[len(lat) // 2], single_network_ms_p99=lat[min(len(lat) - 1,

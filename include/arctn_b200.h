@@ -279,13 +279,35 @@ int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, void* c, uint6
 
 /* ------------------------------------------------------------ batches of independent programs
  * No counterpart in the reference (it contracts one network per call).  A batch runs many programs --
- * uneven networks, mixed dtypes -- as one CUDA graph launch: the programs are spread over up to
- * max_lanes streams (longest first onto the least-loaded lane), each lane runs its programs in turn in
- * one workspace region, and the lanes fork from and join back into cuda_stream.  The programs must
- * outlive the batch and be bound to one device; a batch locks them while it launches. */
+ * uneven networks, mixed dtypes -- as one CUDA graph launch, in one of three modes:
+ *   PERSISTENT (arctn_b200_batch_create's mode): the small programs made of SIMT steps only (up to 5e8
+ *     flops a forward pass) run inside one persistent interpreter launch that follows the steps'
+ *     dependencies on the device; the other programs run launch by launch on up to max_lanes streams
+ *     (longest first onto the least-loaded lane) alongside it.  Every program has its own workspace region.
+ *     A queue wait that expires (2 s) sets device error code 16.
+ *   STAGED: every program inside the interpreter; the tensor-core GEMMs and their operand packs split the
+ *     work into stages (each stage: those launches on the lane streams, then one interpreter launch).
+ *   LANES: every program launch by launch on the lane streams, each lane running its programs in turn
+ *     in one workspace region.
+ * Both fork from and join back into cuda_stream, and both use the lane form on the legacy stream or
+ * inside the caller's stream capture.  Results are the same bits in both modes.  The programs must outlive
+ * the batch and be bound to one device; a batch locks them while it launches.  Creating and describing
+ * a batch needs no GPU. */
 typedef struct arctn_b200_batch arctn_b200_batch;
+enum { ARCTN_B200_BATCH_LANES = 0, ARCTN_B200_BATCH_PERSISTENT = 1, ARCTN_B200_BATCH_STAGED = 2 };
 int arctn_b200_batch_create(arctn_b200_program* const* programs, uint64_t n_programs, int max_lanes,
                             arctn_b200_batch** batch_out);
+int arctn_b200_batch_create_mode(arctn_b200_program* const* programs, uint64_t n_programs, int max_lanes, int mode,
+                                 arctn_b200_batch** batch_out);
+/* JSON: mode, lanes, workspace, the interpreted programs, program regions and, per part (-1 execute,
+ * 0 gradient), the interpreter's
+ * stages, steps and tasks; detail = 1 adds every step [program, op, sub, stage, level, tasks, [deps]] and
+ * every staged launch [stage, program, op].  Writes at most buf_bytes (NUL-terminated); *needed = full size. */
+int arctn_b200_batch_describe(const arctn_b200_batch* batch, int detail, char* buf, uint64_t buf_bytes,
+                              uint64_t* needed);
+/* Test hook of the interpreter's bounded waits: runs it on one task whose dependency nothing completes,
+ * synchronises cuda_stream and sets *code to the error word left (16 once the 2 s wait expired). */
+int arctn_b200_batch_wait_selftest(void* cuda_stream, int* code);
 void arctn_b200_batch_destroy(arctn_b200_batch* batch);
 uint64_t arctn_b200_batch_workspace_size(const arctn_b200_batch* batch);
 uint64_t arctn_b200_batch_lanes(const arctn_b200_batch* batch);
@@ -297,7 +319,8 @@ int arctn_b200_batch_execute(arctn_b200_batch* batch, const void* const* const* 
 int arctn_b200_batch_gradient(arctn_b200_batch* batch, const void* const* const* inputs,
                               const void* const* grad_outputs, void* const* const* grads, void* const* outputs,
                               void* workspace, uint64_t workspace_bytes, void* cuda_stream);
-/* Synchronises cuda_stream; *code = the first nonzero device error word of the last run, else 0. */
+/* Synchronises cuda_stream; *code = the first nonzero device error word of the last run (the programs'
+ * in program order, then the interpreter's), else 0. */
 int arctn_b200_batch_device_status(arctn_b200_batch* batch, void* workspace, void* cuda_stream, int* code);
 
 /* One-shot host-buffer call (the reference-facing e2e path of contract_sliced): copies host inputs to the

@@ -27,15 +27,29 @@ def build(count, seed, gradient=False, precision="fp32"):
     return nets, progs, xs
 
 
+MODES = [("persistent", True), ("staged", True), ("persistent", False), ("lanes", True)]
+
+
+def run_batch(batch, fn, xs, ws, side_stream):
+    """Two calls (the second replays the captured graph) on a side stream, where the graph form and the
+    persistent interpreter run, or on the default stream, where the lane form launches directly."""
+    st = torch.cuda.Stream() if side_stream else torch.cuda.current_stream()
+    with torch.cuda.stream(st):
+        for _ in range(2):
+            res = getattr(batch, fn)(xs, workspace=ws, stream=st)
+        st.synchronize()
+        assert batch.device_status(ws, stream=st) == 0
+    return res
+
+
+@pytest.mark.parametrize("mode,side_stream", MODES)
 @pytest.mark.parametrize("precision", ["fp32", "tf32x3"])
-def test_batch_execute_equals_single_programs_and_oracle(precision):
+def test_batch_execute_equals_single_programs_and_oracle(precision, mode, side_stream):
     nets, progs, xs = build(24, 1, precision=precision)
-    batch = A.ProgramBatch(progs, max_lanes=8)
+    batch = A.ProgramBatch(progs, max_lanes=8, mode=mode)
     assert batch.lanes == 8
     ws = torch.empty(max(batch.workspace_bytes, 1), dtype=torch.uint8, device="cuda")
-    for _ in range(2):  # the second call replays the captured graph
-        outs = batch.execute(xs, workspace=ws)
-    assert batch.device_status(ws) == 0
+    outs = run_batch(batch, "execute", xs, ws, side_stream)
     for (net, arrays), p, x, o in zip(nets, progs, xs, outs):
         single = p.execute(x)
         assert torch.equal(o, single)
@@ -47,10 +61,14 @@ def test_batch_execute_equals_single_programs_and_oracle(precision):
         assert abs(got - want) <= max(1e-5 * abs(want), 8 * abs(native - want)), (got, native, want)
 
 
-def test_batch_gradient_equals_single_programs():
-    nets, progs, xs = build(12, 2, gradient=True)
-    batch = A.ProgramBatch(progs, max_lanes=4)
-    outs, grads = batch.gradient(xs)
+@pytest.mark.parametrize("mode,side_stream", MODES)
+@pytest.mark.parametrize("precision", ["fp32", "tf32x3"])
+def test_batch_gradient_equals_single_programs(precision, mode, side_stream):
+    # seed 0: networks 5 and 7 have tensor-core steps under tf32x3 (staged launches between interpreter launches)
+    nets, progs, xs = build(12, 0, gradient=True, precision=precision)
+    batch = A.ProgramBatch(progs, max_lanes=4, mode=mode)
+    ws = torch.empty(max(batch.workspace_bytes, 1), dtype=torch.uint8, device="cuda")
+    outs, grads = run_batch(batch, "gradient", xs, ws, side_stream)
     torch.cuda.synchronize()
     for p, x, o, g in zip(progs, xs, outs, grads):
         o1, g1 = p.gradient(x)
@@ -71,3 +89,22 @@ def test_batch_rejects_mismatched_inputs_before_launch():
         batch.execute(bad)
     with pytest.raises(ValueError, match="gradient"):
         batch.gradient(xs)
+
+
+def test_interpreter_wait_expires_into_status():
+    # a dependency that nothing completes: the bounded wait records code 16 and the launch drains; the
+    # context stays usable for the next batch run
+    import ctypes
+
+    from arctn_b200 import _capi as C
+
+    st = torch.cuda.Stream()
+    code = ctypes.c_int(-1)
+    C.check(C.lib().arctn_b200_batch_wait_selftest(ctypes.c_void_p(st.cuda_stream), ctypes.byref(code)), "selftest")
+    assert code.value == 16
+    nets, progs, xs = build(4, 3)
+    batch = A.ProgramBatch(progs)
+    ws = torch.empty(max(batch.workspace_bytes, 1), dtype=torch.uint8, device="cuda")
+    outs = run_batch(batch, "execute", xs, ws, True)
+    for p, x, o in zip(progs, xs, outs):
+        assert torch.equal(o, p.execute(x))
