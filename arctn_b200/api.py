@@ -540,14 +540,122 @@ class ProgramBatch:
             raise ValueError(f"{context}: {len(arrays_list)} input lists for {len(self.programs)} programs")
         calls = []
         for j, (p, arrays) in enumerate(zip(self.programs, arrays_list)):
-            arrays, code, torch_mode = _preflight(arrays, p.inputs, p.size_dict, f"{context} (program {j})")
+            arrays, code, torch_mode = _preflight(arrays, p.inputs, p.size_dict, f"{context} (program {j})",
+                                                  p._shapes())
             if code != p.code:
                 raise ValueError(f"{context}: program {j} arrays dtype differs from the program's dtype")
             calls.append((_DeviceCall(arrays, torch_mode, p.device), code, torch_mode))
         return calls
 
+    def _host_run(self, arrays_list, gradient, grad_outputs, workspace, stream, context):
+        """NumPy inputs: every program's inputs (and grad_outputs) go to the GPU through one pinned staging
+        buffer and one copy, every output and gradient comes back in one copy.  The device buffers of the
+        previous call on the same stream with the same shapes are reused, so the captured graph replays."""
+        torch = _torch()
+        if len(arrays_list) != len(self.programs):
+            raise ValueError(f"{context}: {len(arrays_list)} input lists for {len(self.programs)} programs")
+        checked = []
+        for j, (p, arrays) in enumerate(zip(self.programs, arrays_list)):
+            arrays, code, torch_mode = _preflight(arrays, p.inputs, p.size_dict, f"{context} (program {j})",
+                                                  p._shapes())
+            if torch_mode:
+                raise ValueError(f"{context}: program {j} mixes CUDA tensors with the NumPy arrays of program 0")
+            if code != p.code:
+                raise ValueError(f"{context}: program {j} arrays dtype differs from the program's dtype")
+            if gradient and not p.has_gradient:
+                raise ValueError(f"{context}: program {j} was built without gradient=True")
+            checked.append([np.array(a, order="C", copy=None) for a in arrays])
+        dev = torch.device("cuda", torch.cuda.current_device() if self.programs[0].device is None
+                           else self.programs[0].device)
+        st = stream if stream is not None else torch.cuda.current_stream(dev)
+        np_dt = {C.F32: np.float32, C.F64: np.float64, C.C64: np.complex64, C.C128: np.complex128}
+        gouts = []
+        if gradient:
+            for j, p in enumerate(self.programs):
+                g = None if grad_outputs is None else grad_outputs[j]
+                g = np.ones(p.output_shape, np_dt[p.code]) if g is None else np.array(g, np_dt[p.code], order="C")
+                if g.shape != tuple(p.output_shape):
+                    raise ValueError(f"{context}: grad_outputs[{j}] shape {g.shape} is not {tuple(p.output_shape)}")
+                gouts.append(g)
+        sig = (st.cuda_stream, gradient, tuple(tuple((a.shape, a.dtype.str) for a in arrs) for arrs in checked))
+        cache = getattr(self, "_host_cache", None)
+        if cache is None or cache["sig"] != sig or (workspace is not None and cache["ws"] is not workspace):
+            def place(tensors, total):
+                offs = []
+                for shape, dt in tensors:
+                    offs.append(total)
+                    total += (int(np.prod(shape, dtype=np.int64)) * np.dtype(dt).itemsize + 255) // 256 * 256
+                return offs, total
+            ins = [(a.shape, a.dtype) for arrs in checked for a in arrs]
+            in_offs, n_in = place(ins + [(g.shape, g.dtype) for g in gouts], 0)
+            outs = [(tuple(p.output_shape), np_dt[p.code]) for p in self.programs]
+            out_offs, n_out = place(outs + (ins if gradient else []), 0)
+            d_in = torch.empty(max(n_in, 1), dtype=torch.uint8, device=dev)
+            d_out = torch.empty(max(n_out, 1), dtype=torch.uint8, device=dev)
+            base_in, base_out = d_in.data_ptr(), d_out.data_ptr()
+            k, inp = 0, []
+            for arrs in checked:
+                inp.append((C.vp * len(arrs))(*[base_in + in_offs[k + q] for q in range(len(arrs))]))
+                k += len(arrs)
+            n_prog = len(self.programs)
+            cache = {
+                "sig": sig, "d_in": d_in, "d_out": d_out, "in_offs": in_offs, "out_offs": out_offs,
+                "h_in": torch.empty(max(n_in, 1), dtype=torch.uint8, pin_memory=True),
+                "h_out": torch.empty(max(n_out, 1), dtype=torch.uint8, pin_memory=True),
+                "ws": workspace if workspace is not None else torch.empty(
+                    max(self.workspace_bytes, 1), dtype=torch.uint8, device=dev),
+                "inp_arrays": inp, "inp": (C.vpp * n_prog)(*[ctypes.cast(a, C.vpp) for a in inp]),
+                "optr": (C.vp * n_prog)(*[base_out + out_offs[j] for j in range(n_prog)]),
+                "outs": outs, "ins": ins,
+            }
+            if gradient:
+                cache["gptr"] = (C.vp * n_prog)(*[base_in + in_offs[k + j] for j in range(n_prog)])
+                garrs, q = [], n_prog
+                for arrs in checked:
+                    garrs.append((C.vp * len(arrs))(*[base_out + out_offs[q + r] for r in range(len(arrs))]))
+                    q += len(arrs)
+                cache["garrs"] = garrs
+                cache["gpp"] = (C.vpp * n_prog)(*[ctypes.cast(a, C.vpp) for a in garrs])
+            self._host_cache = cache
+        hv = cache["h_in"].numpy()
+        for a, o in zip([a for arrs in checked for a in arrs] + gouts, cache["in_offs"]):
+            hv[o:o + a.nbytes] = a.reshape(-1).view(np.uint8)
+        ws = cache["ws"]
+        with torch.cuda.device(dev), torch.cuda.stream(st):
+            cache["d_in"].copy_(cache["h_in"], non_blocking=True)
+            if gradient:
+                C.check(C.lib().arctn_b200_batch_gradient(self._h, cache["inp"], cache["gptr"], cache["gpp"],
+                                                          cache["optr"], ws.data_ptr(), ws.numel(), st.cuda_stream),
+                        context)
+            else:
+                C.check(C.lib().arctn_b200_batch_execute(self._h, cache["inp"], cache["optr"], ws.data_ptr(),
+                                                         ws.numel(), st.cuda_stream), context)
+            cache["h_out"].copy_(cache["d_out"], non_blocking=True)
+        st.synchronize()
+        host = cache["h_out"].numpy().copy()  # one copy; the results are views of it
+        views = [host[o:o + int(np.prod(shape, dtype=np.int64)) * np.dtype(dt).itemsize].view(dt).reshape(shape)
+                 for (shape, dt), o in zip(cache["outs"] + (cache["ins"] if gradient else []), cache["out_offs"])]
+        n_prog = len(self.programs)
+        outs = views[:n_prog]
+        if not gradient:
+            return outs
+        grads, q = [], n_prog
+        for arrs in checked:
+            grads.append(views[q:q + len(arrs)])
+            q += len(arrs)
+        return outs, grads
+
+    @staticmethod
+    def _numpy_inputs(arrays_list):
+        try:
+            return len(arrays_list) > 0 and len(arrays_list[0]) > 0 and not _is_torch(arrays_list[0][0])
+        except TypeError:
+            return False
+
     def execute(self, arrays_list, *, workspace=None, stream=None):
         """Every program's output, in program order."""
+        if self._numpy_inputs(arrays_list):
+            return self._host_run(arrays_list, False, None, workspace, stream, "batch execute")
         calls = self._bind(arrays_list, "batch execute")
         torch = _torch()
         outs = [c.empty(p.output_shape, _torch_dtype(code)) for p, (c, code, _) in zip(self.programs, calls)]
@@ -564,6 +672,8 @@ class ProgramBatch:
 
     def gradient(self, arrays_list, grad_outputs=None, *, workspace=None, stream=None):
         """(outputs, grads) of every program (built with ``gradient=True``); grad_outputs default to ones."""
+        if self._numpy_inputs(arrays_list):
+            return self._host_run(arrays_list, True, grad_outputs, workspace, stream, "batch gradient")
         calls = self._bind(arrays_list, "batch gradient")
         torch = _torch()
         outs, gouts, grads = [], [], []

@@ -12,6 +12,8 @@
 // launch drains.
 #pragma once
 
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace ab2 {
@@ -68,6 +70,11 @@ __device__ __noinline__ void interp_tile(const IOp& op, unsigned char* smem, ll 
                                 reinterpret_cast<T(*)[TM + 1]>(smem + 16 * (TM + 1) * sizeof(T)), vb, op.nvb);
 }
 
+__device__ __noinline__ void interp_tile128(const IOp& op, unsigned char* smem, ll vb) {
+  gemm_tile128_body(op.g, reinterpret_cast<float(*)[kTile128 + 1]>(smem),
+                    reinterpret_cast<float(*)[kTile128 + 1]>(smem + 16 * (kTile128 + 1) * sizeof(float)), vb, op.nvb);
+}
+
 template <class T>
 __device__ __noinline__ void interp_body(const IOp& op, unsigned char* smem, ll vb) {
   using W = typename Num<T>::wide;
@@ -90,6 +97,9 @@ __device__ __noinline__ void interp_body(const IOp& op, unsigned char* smem, ll 
     case I_GEMM_WARP: gemm_warp_body<T>(op.g, vb, nvb); break;
     case I_TILE64: interp_tile<T, 64>(op, smem, vb); break;
     case I_TILE32: interp_tile<T, 32>(op, smem, vb); break;
+    case I_TILE128:  // float32 only (the planner picks it for no other dtype)
+      if constexpr (std::is_same<T, float>::value) interp_tile128(op, smem, vb);
+      break;
     case I_ACCUM: slice_accumulate_body<T>((const T*)op.a, (W*)op.c, (const Segment*)op.t0, op.n0, op.n1, vb, nvb); break;
     case I_OUTPUT:
       if (op.out_wide) slice_output_body<T, W>((const W*)op.a, (W*)op.c, op.t0, op.t1, op.n0, op.n1, op.n2, vb, nvb);

@@ -497,6 +497,91 @@ __global__ void __launch_bounds__(256) k_gemm_tile(GemmArgs g) {
   gemm_tile_body<T, TM, TN, TK>(g, As, Bs, blockIdx.x, gridDim.x);
 }
 
+// Large real FP32 steps: a 128 x 128 output tile per CTA, 8 x 8 outputs per thread (rows ty + 16 x,
+// columns tx + 16 y), K in slabs of 16 through shared memory.  Every slab, a thread loads the same eight
+// rows of A at one K column and one column of B at eight K rows, so those row and column offsets stay in
+// registers; four FMAs per shared-memory load instead of k_gemm_tile's two.  Each output accumulates its K
+// terms in increasing order with one fmaf each, slabs zero-padded to 16, exactly as k_gemm_tile does, so
+// the two give the same bits.
+constexpr int kTile128 = 128;
+__device__ __forceinline__ void gemm_tile128_body(const GemmArgs& g, float (*As)[kTile128 + 1],
+                                                  float (*Bs)[kTile128 + 1], ll vb, ll nvb) {
+  constexpr int TM = kTile128, TN = kTile128, TK = 16;
+  const float* Ap = (const float*)g.A;
+  const float* Bp = (const float*)g.B;
+  float* Cp = (float*)g.C;
+  const ll bt = g.bt, g0 = g.g0, m = g.m, k = g.k, n = g.n;
+  const ll *gaB = g.aB, *gaM = g.aM, *gaK = g.aK, *gbB = g.bB, *gbK = g.bK, *gbN = g.bN;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int a_l = threadIdx.x % TK, a_i = threadIdx.x / TK;  // A: rows a_i + 16 x, K column a_l
+  const int b_j = threadIdx.x % TN, b_l = threadIdx.x / TN;  // B: column b_j, K rows b_l + 2 x
+  const ll tiles_n = (n + TN - 1) / TN, tiles_m = (m + TM - 1) / TM;
+  const ll n_tiles = tiles_n * tiles_m * g.S * bt;
+  for (ll t = vb; t < n_tiles; t += nvb) {
+    ll r = t;
+    const ll tn = r % tiles_n; r /= tiles_n;
+    const ll tm = r % tiles_m; r /= tiles_m;
+    const ll sb = r, s = sb / bt, b = sb - s * bt;
+    const ll i0 = tm * TM, j0 = tn * TN;
+    const float* abase = Ap + slice_offset(g.sa, g0, s) + gaB[b];
+    const float* bbase = Bp + slice_offset(g.sb, g0, s) + gbB[b];
+    ll aoff[8];
+    unsigned amask = 0;
+#pragma unroll
+    for (int x = 0; x < 8; ++x) {
+      const ll i = i0 + a_i + 16 * x;
+      aoff[x] = i < m ? gaM[i] : 0;
+      amask |= (i < m ? 1u : 0u) << x;
+    }
+    const ll jb = j0 + b_j;
+    const bool bok = jb < n;
+    const ll boff = bok ? gbN[jb] : 0;
+    float acc[8][8];
+#pragma unroll
+    for (int x = 0; x < 8; ++x)
+#pragma unroll
+      for (int y = 0; y < 8; ++y) acc[x][y] = 0.f;
+    for (ll l0 = 0; l0 < k; l0 += TK) {
+      const ll la = l0 + a_l;
+      const ll ka = la < k ? gaK[la] : 0;
+#pragma unroll
+      for (int x = 0; x < 8; ++x) As[a_l][a_i + 16 * x] = (la < k && ((amask >> x) & 1u)) ? abase[aoff[x] + ka] : 0.f;
+#pragma unroll
+      for (int x = 0; x < 8; ++x) {
+        const ll lb = l0 + b_l + 2 * x;
+        Bs[b_l + 2 * x][b_j] = (bok && lb < k) ? bbase[gbK[lb] + boff] : 0.f;
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int l = 0; l < TK; ++l) {
+        float av[8], bv[8];
+#pragma unroll
+        for (int x = 0; x < 8; ++x) av[x] = As[l][ty + 16 * x];
+#pragma unroll
+        for (int y = 0; y < 8; ++y) bv[y] = Bs[l][tx + 16 * y];
+#pragma unroll
+        for (int x = 0; x < 8; ++x)
+#pragma unroll
+          for (int y = 0; y < 8; ++y) acc[x][y] = fmaf(av[x], bv[y], acc[x][y]);
+      }
+      __syncthreads();
+    }
+    float* cbase = Cp + (s * bt + b) * m * n;
+#pragma unroll
+    for (int x = 0; x < 8; ++x)
+#pragma unroll
+      for (int y = 0; y < 8; ++y) {
+        const ll i = i0 + ty + 16 * x, j = j0 + tx + 16 * y;
+        if (i < m && j < n) cbase[i * n + j] = acc[x][y];
+      }
+  }
+}
+static __global__ void __launch_bounds__(256, 2) k_gemm_tile128(GemmArgs g) {
+  __shared__ float As[16][kTile128 + 1];
+  __shared__ float Bs[16][kTile128 + 1];
+  gemm_tile128_body(g, As, Bs, blockIdx.x, gridDim.x);
+}
+
 // ---------------------------------------------------------------- cross-slice sum
 // FP64 accumulation of per-slice results into chunk partials, in slice order
 // within each chunk (src/slice.rs:1020-1064).  A segment is one (block, chunk)
@@ -577,7 +662,7 @@ __global__ void k_strip_scale(T* __restrict__ c, ll n, const unsigned long long*
 // listed in succ[succ0 .. succ0 + nsucc) depend on it.
 enum IKind : int {
   I_GATHER, I_SCATTER, I_GRAD_ACCUM, I_NARROW, I_GEMM_SMALL, I_GEMM_DOT, I_DOT_PART, I_DOT_REDUCE, I_GEMM_WARP,
-  I_TILE64, I_TILE32, I_ACCUM, I_OUTPUT, I_MEMSET
+  I_TILE64, I_TILE32, I_ACCUM, I_OUTPUT, I_MEMSET, I_TILE128
 };
 struct IOp {
   int kind;      // IKind

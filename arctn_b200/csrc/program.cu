@@ -16,6 +16,7 @@
 #include <map>
 #include <mutex>
 #include <numeric>
+#include <type_traits>
 #include <set>
 
 #include "tc_gemm.cuh"
@@ -597,6 +598,9 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     const bool long_k_few_tiles = k >= 1024 && tiles32 < 2 * (u64)kNumSMs && outs <= (1u << 17);
     if (outs <= 64 && k >= 256) g.kind = Op::GEMM_DOT;
     else if (long_k_few_tiles) g.kind = Op::GEMM_WARP;
+    else if (dt == DT_F32 && m >= 128 && n >= 128 &&
+             (ph2 || ((m + 127) / 128) * ((n + 127) / 128) * bt >= (u64)kNumSMs))
+      g.kind = Op::GEMM_TILE128;  // large real FP32 steps: the 128 x 128 tile (same bits as the 64 x 64 one)
     else if (m >= 64 && n >= 64 && (ph2 || tiles64 >= (u64)kNumSMs)) g.kind = Op::GEMM_TILE64;
     else if (m >= 24 && n >= 24 && (ph2 || tiles32 >= (u64)kNumSMs)) g.kind = Op::GEMM_TILE32;
     else if (k >= 32) g.kind = Op::GEMM_WARP;  // a serial k loop per thread would dominate
@@ -1490,7 +1494,8 @@ void launch_typed(const Op& op, const void* A, const void* B, void* C, void* D, 
     case Op::GEMM_DOT:
     case Op::GEMM_WARP:
     case Op::GEMM_TILE64:
-    case Op::GEMM_TILE32: {
+    case Op::GEMM_TILE32:
+    case Op::GEMM_TILE128: {
       GemmArgs g;
       g.A = A; g.B = B; g.C = C;
       g.bt = op.bt; g.m = op.m; g.k = op.k; g.n = op.n; g.S = op.S; g.g0 = op.g0;
@@ -1513,6 +1518,13 @@ void launch_typed(const Op& op, const void* A, const void* B, void* C, void* D, 
       } else if (op.kind == Op::GEMM_WARP) {
         const ll total = op.S * op.bt * op.m * op.n;
         k_gemm_warp<T><<<(int)std::min<ll>((total + 7) / 8, 148 * 16), 256, 0, st>>>(g);
+      } else if (op.kind == Op::GEMM_TILE128) {
+        if constexpr (std::is_same<T, float>::value) {
+          const ll tiles = ((op.n + 127) / 128) * ((op.m + 127) / 128) * op.S * op.bt;
+          k_gemm_tile128<<<(int)std::min<ll>(tiles, 148 * 2), 256, 0, st>>>(g);
+        } else {
+          throw Error(E_UNSUPPORTED, "the 128 x 128 tile GEMM is float32 only");
+        }
       } else if (op.kind == Op::GEMM_TILE64) {
         const ll tiles = ((op.n + 63) / 64) * ((op.m + 63) / 64) * op.S * op.bt;
         k_gemm_tile<T, 64, 64, 16><<<(int)std::min<ll>(tiles, 148 * 8), 256, 0, st>>>(g);
@@ -1831,6 +1843,11 @@ void Program::interp_descs(size_t i, const void* const* inputs, const void* grad
       d.kind = I_TILE64;
       d.nvb = tasks(((op.n + 63) / 64) * ((op.m + 63) / 64) * op.S * op.bt, 1);
       break;
+    case Op::GEMM_TILE128:
+      gemm();
+      d.kind = I_TILE128;
+      d.nvb = tasks(((op.n + 127) / 128) * ((op.m + 127) / 128) * op.S * op.bt, 1);
+      break;
     case Op::GEMM_TILE32:
       gemm();
       d.kind = I_TILE32;
@@ -2050,6 +2067,7 @@ double op_work(const Op& op, int dt) {
     case Op::GEMM_TC:
     case Op::GEMM_TILE64:
     case Op::GEMM_TILE32:
+    case Op::GEMM_TILE128:
       return (dtype_complex(dt) ? 8.0 : 2.0) * (double)op.S * op.bt * op.m * op.k * op.n;
     case Op::GATHER: return (double)op.S * op.n_out * (op.n_red + 1) * eb;
     case Op::ACCUM: return (double)op.n_segs * op.n_e * (2.0 * wide_bytes(dt)) + (double)op.S * op.n_e * eb;
@@ -2164,7 +2182,7 @@ std::string Program::describe() const {
   static const char* names[] = {"gather",    "gemm_small", "gemm_tile64", "gemm_tile32", "slice_accumulate",
                                 "slice_output", "memset",  "maxabs",      "strip",       "gemm_tc",
                                 "gemm_dot",  "pack",       "scatter",     "pack_tiled", "gemm_warp",  "grad_accum",
-                                "narrow"};
+                                "narrow",    "gemm_tile128"};
   std::string s = "{\"workspace_bytes\":" + std::to_string(ws_total_) + ",\"n_slices\":" + std::to_string(n_total_) +
                   ",\"slices_per_group\":" + std::to_string(S_) + ",\"groups\":" + std::to_string(n_groups_) +
                   ",\"launches\":" + std::to_string(launches()) + ",\"gradient\":" + (opt_.gradient ? "true" : "false") +
@@ -2186,7 +2204,7 @@ std::string Program::describe() const {
     f("c_kind", (long long)op.c.kind); f("c", (long long)op.c.index);
     switch (op.kind) {
       case Op::GEMM_SMALL: case Op::GEMM_TILE64: case Op::GEMM_TILE32: case Op::GEMM_DOT: case Op::GEMM_TC:
-      case Op::GEMM_WARP:
+      case Op::GEMM_WARP: case Op::GEMM_TILE128:
         f("S", op.S); f("bt", op.bt); f("m", op.m); f("k", op.k); f("n", op.n);
         f("splits", op.splits); f("conj_a", op.conj_a); f("conj_b", op.conj_b);
         if (op.pk.kind != Ref::NONE) f("pack_into", (long long)op.pk.index);

@@ -45,7 +45,8 @@ struct Ref {
 struct Op {
   enum Kind : int {
     GATHER = 0, GEMM_SMALL = 1, GEMM_TILE64 = 2, GEMM_TILE32 = 3, ACCUM = 4, OUTPUT = 5, MEMSET = 6, MAXABS = 7,
-    STRIP = 8, GEMM_TC = 9, GEMM_DOT = 10, PACK = 11, SCATTER = 12, PACK_TILED = 13, GEMM_WARP = 14, GRAD_ACCUM = 15, NARROW = 16
+    STRIP = 8, GEMM_TC = 9, GEMM_DOT = 10, PACK = 11, SCATTER = 12, PACK_TILED = 13, GEMM_WARP = 14, GRAD_ACCUM = 15, NARROW = 16,
+    GEMM_TILE128 = 17
   } kind;
   Ref a, b, c;
   u64 tab[6] = {0, 0, 0, 0, 0, 0};  // byte offsets of offset tables in the program's table buffer

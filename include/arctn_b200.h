@@ -253,7 +253,8 @@ int arctn_b200_program_device_status(arctn_b200_program* program, void* workspac
  * kind and algorithmic work (real flops for GEMM kinds, bytes moved for the others).  Arrays hold
  * arctn_b200_program_launches entries; unused entries keep their initial values.
  * Kinds: 0 gather, 1 gemm_small, 2 gemm_tile64, 3 gemm_tile32, 4 slice_accumulate, 5 slice_output,
- * 7 maxabs, 8 strip, 9 gemm_tc, 10 gemm_dot, 11 pack, 12 scatter, 13 pack_tiled, 14 gemm_warp. */
+ * 7 maxabs, 8 strip, 9 gemm_tc, 10 gemm_dot, 11 pack, 12 scatter, 13 pack_tiled, 14 gemm_warp, 15 grad_accum,
+ * 16 narrow, 17 gemm_tile128. */
 int arctn_b200_program_profile(arctn_b200_program* program, const void* const* inputs, void* output, void* workspace,
                                uint64_t workspace_bytes, void* cuda_stream, float* ms_out, int* kind_out,
                                double* work_out);

@@ -11,7 +11,7 @@ import pytest
 import arctn_b200 as A
 from arctn_b200 import networks as N
 
-GEMM_KINDS = {"gemm_small", "gemm_tile64", "gemm_tile32", "gemm_dot", "gemm_tc", "gemm_warp"}
+GEMM_KINDS = {"gemm_small", "gemm_tile64", "gemm_tile32", "gemm_tile128", "gemm_dot", "gemm_tc", "gemm_warp"}
 
 
 def program(net, path, sliced=(), **kw):
