@@ -16,6 +16,7 @@
 #include <map>
 #include <mutex>
 #include <numeric>
+#include <tuple>
 #include <type_traits>
 #include <set>
 
@@ -623,13 +624,20 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     // every SM an output tile; its epilogue can then write the next GEMM's packed operand directly.
     const u64 tc_tiles = ((m + tc::BM - 1) / tc::BM) * ((n + tc::BN - 1) / tc::BN) * bt;
     const bool bf16 = opt_.precision == PREC_BF16X3;
-    const bool use_tc = (opt_.precision == PREC_TF32X3 || bf16) && dt == DT_C64 &&
+    // Real float32 steps use the same complex kernel on half the K (Op::real): two of its four real
+    // products per complex MAC are useful, still several times the FP32 SIMT rate.  (Holding the
+    // mid-size ones back for the SIMT kernels measured slower on the many-network batch.)
+    const u64 kc = (k + 1) / 2;
+    const bool real_tc = (opt_.precision == PREC_TF32X3 || bf16) && dt == DT_F32 && kc >= 32 &&
+                         ((m >= 96 && n >= 96) || (std::min(m, n) >= 16 && kc >= 256));
+    const bool use_tc = real_tc || ((opt_.precision == PREC_TF32X3 || bf16) && dt == DT_C64 &&
                         ((k >= 32 && ((m >= 96 && n >= 96) || (std::min(m, n) >= 16 && k >= 256))) ||
-                         (k >= 16 && m >= 96 && n >= 96 && (ph2 || tc_tiles >= (u64)kNumSMs)));
+                         (k >= 16 && m >= 96 && n >= 96 && (ph2 || tc_tiles >= (u64)kNumSMs))));
     if (use_tc) {
       const ll kt_el = bf16 ? 2 * tc::BK : tc::BK;  // K per 64-byte packed row
       const ll el = bf16 ? 2 : 4;                  // bytes per plane element
-      const ll kpad = ((ll)k + kt_el - 1) / kt_el * kt_el;
+      const ll kpk = real_tc ? (ll)kc : (ll)k;     // K of the complex product
+      const ll kpad = (kpk + kt_el - 1) / kt_el * kt_el;
       const ll rpa = ((ll)m + tc::BM - 1) / tc::BM * tc::BM;
       const ll rpb = ((ll)n + tc::BN - 1) / tc::BN * tc::BN;
       // A phase-2 operand that is the whole unsplit output of an earlier tensor-core GEMM, read by nothing
@@ -638,7 +646,8 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       // layouts without padding (nothing to zero first) qualify whose tables repeat from one output tile
       // to the next and whose packed runs inside a tile average at least 32 floats (coalesced stores).
       auto fuse_into_producer = [&](const Operand& X, ll rows, ll rpad, bool conj, u64 pbuf) -> bool {
-        if (bf16 || !ph2 || !X.variant || opt_.gradient || conj || X.ref.kind != Ref::WS || X.so.n != 0) return false;
+        if (real_tc || bf16 || !ph2 || !X.variant || opt_.gradient || conj || X.ref.kind != Ref::WS || X.so.n != 0)
+          return false;
         if (rows != rpad || (ll)k != kpad) return false;
         size_t pi = ops2.size();
         for (size_t q = ops2.size(); q-- > 0;)
@@ -743,13 +752,15 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         p.c = Ref{Ref::WS, pbuf};
         p.bt = (ll)bt;
         p.rows = rows;
-        p.cols = (ll)k;
+        p.cols = kpk;
         p.rpad = rpad;
         p.kpad = kpad;
         p.a_var = X.variant;
-        p.conj_a = conj && dtype_complex(dt);
+        p.conj_a = conj && (dtype_complex(dt) || real_tc);
+        p.real = real_tc;
+        p.kfull = (ll)k;
         touch(X.ref, ph2, opidx(ph2));
-        if (pack_plan(X, rpad, kpad, p)) {
+        if (!real_tc && pack_plan(X, rpad, kpad, p)) {
           p.kind = Op::PACK_TILED;
           if (rows < rpad || (ll)k < kpad) {  // the tiled pack writes only real elements: zero the padding
             Op z{Op::MEMSET};
@@ -771,8 +782,9 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         emit(ph2, p, fwd);
         return pbuf;
       };
-      const u64 pa = pack(A, (ll)m, rpa, conj_a);
-      const u64 pb = pack(B, (ll)n, rpb, conj_b);
+      // A real step packs B conjugated: Re((A1 + i A2) . conj(B1 + i B2)) = A1 . B1 + A2 . B2.
+      const u64 pa = pack(A, (ll)m, rpa, real_tc ? false : conj_a);
+      const u64 pb = pack(B, (ll)n, rpb, real_tc ? true : conj_b);
       touch(Ref{Ref::WS, pa}, ph2, opidx(ph2));
       // K split across CTAs (see TcArgs): partials [split][z][m][n].  A caller's tc_k_chunk fixes the
       // chunk; otherwise only a one-slice GEMM with too few tiles to fill the GPU is split.
@@ -795,8 +807,11 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       }
       g.kind = Op::GEMM_TC;
       g.bf16 = bf16;
+      g.real = real_tc;
       g.a = Ref{Ref::WS, pa};
       g.b = Ref{Ref::WS, pb};
+      if (real_tc)  // the complex product lands in a scratch buffer; a gather keeps its real part
+        g.c = Ref{Ref::WS, new_buf(ph2, bt * m * n * 8, opidx(ph2))};
       g.rpad = rpa;
       g.rpad_b = rpb;
       g.kpad = kpad;
@@ -809,6 +824,21 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     touch(A.ref, ph2, opidx(ph2));
     touch(B.ref, ph2, opidx(ph2));
     emit(ph2, g, fwd);
+    if (g.real) {
+      const u64 numel = bt * m * n;
+      Op rg{Op::GATHER};  // out[s][e] = the real half of the complex result's element e
+      rg.a = g.c;
+      rg.sa.local_stride = ph2 ? (ll)(2 * numel) : 0;
+      rg.c = out;
+      std::vector<ll> re((size_t)numel);
+      for (u64 e = 0; e < numel; ++e) re[(size_t)e] = (ll)(2 * e);
+      rg.tab[0] = tab_ll(re);
+      rg.tab[1] = tab_ll(std::vector<ll>{0});
+      rg.n_out = (ll)numel;
+      rg.n_red = 1;
+      touch(g.c, ph2, opidx(ph2));
+      emit(ph2, rg, fwd);
+    }
     return g;
   };
   struct StepRec {
@@ -1613,6 +1643,19 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
     const ll Z = (op.a_var ? op.S : 1) * op.bt;
     const ll tiles = Z * (op.rpad / 32) * ((op.kpad + 31) / 32);
     const int grid = (int)std::min<ll>(tiles, 148 * 16);
+    if (op.real) {
+      auto args = std::make_tuple((const float*)A, (const ll*)(tab + op.tab[0]), (const ll*)(tab + op.tab[1]),
+                                  (const ll*)(tab + op.tab[2]));
+      if (op.bf16)
+        tc::k_pack_planar_real<__nv_bfloat16><<<grid, 256, 0, st>>>(
+            std::get<0>(args), (__nv_bfloat16*)C, std::get<1>(args), std::get<2>(args), std::get<3>(args), op.bt,
+            op.rows, op.cols, op.kfull, op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0, op.conj_a ? 1 : 0);
+      else
+        tc::k_pack_planar_real<float><<<grid, 256, 0, st>>>(
+            std::get<0>(args), (float*)C, std::get<1>(args), std::get<2>(args), std::get<3>(args), op.bt, op.rows,
+            op.cols, op.kfull, op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0, op.conj_a ? 1 : 0);
+      return;
+    }
     if (op.bf16)
       tc::k_pack_planar<__nv_bfloat16><<<grid, 256, 0, st>>>(
           (const cf32*)A, (__nv_bfloat16*)C, (const ll*)(tab + op.tab[0]), (const ll*)(tab + op.tab[1]),
@@ -2208,11 +2251,11 @@ std::string Program::describe() const {
         f("S", op.S); f("bt", op.bt); f("m", op.m); f("k", op.k); f("n", op.n);
         f("splits", op.splits); f("conj_a", op.conj_a); f("conj_b", op.conj_b);
         if (op.pk.kind != Ref::NONE) f("pack_into", (long long)op.pk.index);
-        if (op.kind == Op::GEMM_TC) f("bf16", op.bf16);
+        if (op.kind == Op::GEMM_TC) { f("bf16", op.bf16); f("real", op.real); }
         break;
       case Op::PACK: case Op::PACK_TILED:
         f("S", op.a_var ? op.S : 1); f("bt", op.bt); f("rows", op.rows); f("cols", op.cols); f("rpad", op.rpad);
-        f("kpad", op.kpad); f("tile", op.tile_T); f("n_outer", op.n_outer); f("bf16", op.bf16);
+        f("kpad", op.kpad); f("tile", op.tile_T); f("n_outer", op.n_outer); f("bf16", op.bf16); f("real", op.real);
         break;
       case Op::GATHER: case Op::SCATTER: case Op::MAXABS: case Op::STRIP:
         f("S", op.S); f("n_out", op.n_out); f("n_red", op.n_red);

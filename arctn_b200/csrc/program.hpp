@@ -66,6 +66,11 @@ struct Op {
   Ref d;                                // GEMM_TC: FP32 split-K partial buffer
   bool bwd = false;                     // part of the adjoint sweep (skipped by a plain execute)
   bool bf16 = false;                    // PACK / PACK_TILED / GEMM_TC / their MEMSET: split-BF16 planes
+  // PACK / GEMM_TC of a real float32 step on the complex tensor-core GEMM: K folds in half into the real and
+  // imaginary parts (A' = A[:, c] + i A[:, c + Kc], B' = conj(B[c, :] + i B[c + Kc, :]), Re(A'.B') = A.B);
+  // PACK: `cols` = Kc, `kfull` = K.
+  bool real = false;
+  ll kfull = 0;
   // GEMM_TC whose epilogue writes the next GEMM's packed operand instead of `c`: the pack buffer, the
   // offset tables over the output's rows, columns and batch, the tile's 32-float chunks and their lane
   // pattern, and the packed size of one slice.

@@ -749,5 +749,52 @@ static __global__ void __launch_bounds__(256) k_pack_planar(const cf32* __restri
   }
 }
 
+// A real float32 operand packed as a complex one of half the K (Kc = ceil(K / 2)): element (z, r, c) is
+// src(z, r, c) + i src(z, r, c + Kc), zero past K, conjugated for the B operand; then the same tile
+// transposition and planar split as k_pack_planar.  With both operands packed this way the complex
+// product's real part is the real product over the full K.
+template <typename PT>
+static __global__ void __launch_bounds__(256) k_pack_planar_real(const float* __restrict__ src, PT* __restrict__ dst,
+                                                          const ll* __restrict__ tabB, const ll* __restrict__ tabR,
+                                                          const ll* __restrict__ tabC, ll bt, ll R, ll Kc, ll K,
+                                                          ll Rpad, ll Kpad, ll Z, SliceOff so, ll g0, int r_major,
+                                                          int conj) {
+  const float im_sign = conj ? -1.f : 1.f;
+  __shared__ cf32 tile[32][33];
+  const int tx = threadIdx.x % 32, ty = threadIdx.x / 32;  // 32 x 8
+  const ll tiles_c = (Kpad + 31) / 32, tiles_r = Rpad / 32, per_z = tiles_c * tiles_r;
+  const ll plane = Z * Rpad * Kpad;
+  for (ll t = blockIdx.x; t < Z * per_z; t += gridDim.x) {
+    const ll zz = t / per_z, rem = t - zz * per_z;
+    const ll r0 = (rem / tiles_c) * 32, c0 = (rem % tiles_c) * 32;
+    const ll s = zz / bt, b = zz - s * bt;
+    const float* base = src + slice_offset(so, g0, s) + tabB[b];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int u = ty + 8 * j;
+      const ll r = r0 + (r_major ? tx : u), c = c0 + (r_major ? u : tx);
+      cf32 v{0.f, 0.f};
+      if (r < R && c < Kc) {
+        v.re = base[tabR[r] + tabC[c]];
+        if (c + Kc < K) v.im = base[tabR[r] + tabC[c + Kc]];
+      }
+      if (r_major) tile[tx][u] = v;
+      else tile[u][tx] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int u = ty + 8 * j;
+      const ll r = r0 + u, c = c0 + tx;
+      if (c < Kpad) {
+        const ll o = (zz * Rpad + r) * Kpad + c;
+        put_split(dst, plane, o, tile[u][tx].re);
+        put_split(dst + 2 * plane, plane, o, im_sign * tile[u][tx].im);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace tc
 }  // namespace ab2

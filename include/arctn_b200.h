@@ -58,7 +58,9 @@ enum {
 enum {
   ARCTN_B200_PREC_FP32 = 0,   /* plain FP32 FFMA on the CUDA cores */
   ARCTN_B200_PREC_TF32X3 = 1, /* split-TF32 (3 products) on tcgen05 tensor cores, FP32 accumulate,
-                                 for steps dense enough to fill a tensor-core tile; thin steps FP32 */
+                                 for steps dense enough to fill a tensor-core tile; thin steps FP32.
+                                 f32 steps run on the complex kernel with K folded in half into the
+                                 real and imaginary parts (the real part of the product is kept) */
   ARCTN_B200_PREC_BF16X3 = 2  /* split-BF16 (3 products, hi/lo BF16 pairs) on tcgen05 tensor cores, FP32
                                  accumulate; each operand carried to about 2^-18, for precision studies;
                                  the same step selection as TF32X3 */

@@ -1,8 +1,11 @@
-"""The 128 x 128 FP32 tile GEMM (k_gemm_tile128) on real float32 steps large enough to pick it.
+"""Large real float32 steps: the 128 x 128 FP32 tile GEMM (k_gemm_tile128, precision fp32) and the
+complex tensor-core GEMM on half the K (precision tf32x3: A' = A1 + i A2, B' = conj(B1 + i B2),
+Re(A'.B') = A.B).
 
 Checked against an FP64 matmul of the same operands (normwise, FP32 tolerance), with operands stored in
-both row orders (contiguous and transposed K), and against the batch interpreter's run of the same body
-(bit for bit).
+both row orders (contiguous and transposed K) and odd K, the tile GEMM also against the batch
+interpreter's run of the same body (bit for bit), and the tensor-core form's gradients against the FP32
+form's.
 """
 
 import numpy as np
@@ -53,3 +56,37 @@ def test_tile128_interpreter_equals_launch():
     assert kinds  # the small one uses the 64 x 64 tile or a thinner kernel
     for p, x, o in zip([prog, prog2], xs, outs):
         assert torch.equal(o, p.execute(x))
+
+
+@pytest.mark.parametrize("transposed", [False, True])
+@pytest.mark.parametrize("m,k,n", [(1024, 512, 768), (700, 301, 650)])
+def test_real_tensor_core_matches_fp64(m, k, n, transposed):
+    inputs, output, size = two_tensor(m, k, n, transposed)
+    prog = A.SlicedProgram(inputs, output, size, [(0, 1)], (), dtype=np.float32, precision="tf32x3")
+    ops = prog.describe()["ops"]
+    assert [o.get("real") for o in ops if o["kind"] == "gemm_tc"] == [1]
+    rng = np.random.default_rng(9)
+    arrays = [rng.standard_normal([size[l] for l in legs]).astype(np.float32) for legs in inputs]
+    got = prog.execute([torch.from_numpy(a).cuda() for a in arrays]).cpu().numpy().astype(np.float64)
+    a64, b64 = (arrays[0].T, arrays[1].T) if transposed else (arrays[0], arrays[1])
+    want = a64.astype(np.float64) @ b64.astype(np.float64)
+    assert np.linalg.norm(got - want) <= 1e-6 * np.linalg.norm(want) * np.sqrt(k)
+
+
+def test_real_tensor_core_gradient_matches_fp32():
+    inputs, output, size = two_tensor(512, 384, 640, False)
+    rng = np.random.default_rng(10)
+    arrays = [torch.from_numpy(rng.standard_normal([size[l] for l in legs]).astype(np.float32)).cuda()
+              for legs in inputs]
+    res = {}
+    for precision in ("fp32", "tf32x3"):
+        prog = A.SlicedProgram(inputs, output, size, [(0, 1)], (), dtype=np.float32, precision=precision,
+                               gradient=True)
+        kinds = [o["kind"] for o in prog.describe()["ops"]]
+        assert ("gemm_tc" in kinds) == (precision == "tf32x3")
+        out, grads = prog.gradient(arrays)
+        res[precision] = (out.double(), [g.double() for g in grads])
+    (o32, g32), (otc, gtc) = res["fp32"], res["tf32x3"]
+    assert torch.linalg.norm(otc - o32) <= 1e-5 * torch.linalg.norm(o32)
+    for a, b in zip(gtc, g32):
+        assert torch.linalg.norm(a - b) <= 1e-5 * torch.linalg.norm(b)
