@@ -581,10 +581,14 @@ class ProgramBatch:
         cache = getattr(self, "_host_cache", None)
         if cache is None or cache["sig"] != sig or (workspace is not None and cache["ws"] is not workspace):
             def place(tensors, total):
+                # element-aligned (the kernels load whole elements): tight packing lets one copy fill a run
+                # of tensors of one dtype
                 offs = []
                 for shape, dt in tensors:
+                    isz = np.dtype(dt).itemsize
+                    total = (total + isz - 1) // isz * isz
                     offs.append(total)
-                    total += (int(np.prod(shape, dtype=np.int64)) * np.dtype(dt).itemsize + 255) // 256 * 256
+                    total += int(np.prod(shape, dtype=np.int64)) * isz
                 return offs, total
             ins = [(a.shape, a.dtype) for arrs in checked for a in arrs]
             in_offs, n_in = place(ins + [(g.shape, g.dtype) for g in gouts], 0)
@@ -617,9 +621,23 @@ class ProgramBatch:
                 cache["garrs"] = garrs
                 cache["gpp"] = (C.vpp * n_prog)(*[ctypes.cast(a, C.vpp) for a in garrs])
             self._host_cache = cache
+        if "in_runs" not in cache:  # runs of consecutive tensors without alignment padding between them
+            runs, k = [], 0
+            flat = [a.nbytes for arrs in checked for a in arrs] + [g.nbytes for g in gouts]
+            offs = cache["in_offs"]
+            while k < len(flat):
+                e = k + 1
+                while e < len(flat) and offs[e] == offs[e - 1] + flat[e - 1]:
+                    e += 1
+                runs.append((k, e, offs[k]))
+                k = e
+            cache["in_runs"] = runs
         hv = cache["h_in"].numpy()
-        for a, o in zip([a for arrs in checked for a in arrs] + gouts, cache["in_offs"]):
-            hv[o:o + a.nbytes] = a.reshape(-1).view(np.uint8)
+        flat = [a for arrs in checked for a in arrs] + gouts
+        for k, e, o in cache["in_runs"]:
+            chunk = np.concatenate([a.reshape(-1).view(np.uint8) for a in flat[k:e]]) if e - k > 1 else \
+                flat[k].reshape(-1).view(np.uint8)
+            hv[o:o + chunk.nbytes] = chunk
         ws = cache["ws"]
         with torch.cuda.device(dev), torch.cuda.stream(st):
             cache["d_in"].copy_(cache["h_in"], non_blocking=True)
