@@ -568,8 +568,9 @@ def run_batch(args, dev):
                 times.append(_events_ms(stream, run))
         return statistics.mean(times), batch.device_status(run.workspace, stream)
 
-    # The lane form (every step its own launch, networks spread over 32 streams) for comparison.
-    lanes_ms, lanes_status = time_batch(A.ProgramBatch(progs, max_lanes=64, mode="lanes"))
+    # The lane form (every step its own launch, networks spread over 64 streams) for comparison.
+    lanes_ms, lanes_status = (None, 0) if args.no_extras else \
+        time_batch(A.ProgramBatch(progs, max_lanes=64, mode="lanes"))
     batch = A.ProgramBatch(progs, max_lanes=64)
     sampler = ClockSampler(dev.index)
     ms, status = time_batch(batch, sampler)
@@ -592,6 +593,13 @@ def run_batch(args, dev):
     # End to end through the public API from host NumPy arrays: each call stages every network's inputs
     # (one pinned copy per network), runs the batch and returns outputs and gradients as NumPy arrays.
     host = [arrays for _, arrays in nets]
+    if args.no_extras:  # device time only (profiling runs)
+        print(json.dumps(_line(args, "many-network forward+adjoint throughput", len(progs) / (ms * 1e-3),
+                               "networks/s", True, ms, {"workload": "256 random 3-regular networks, n in [20,50], "
+                                                        "bond in {2,3,4}, f32/c64 alternating"}, "f32+c64",
+                               gpu_launches=launches_per_call * args.steps, e2e=None, roofline=None,
+                               cpu_baseline=None, clocks=sampler.summary(), device_status=status)), flush=True)
+        return
     h2d = sum(a.nbytes for arrays in host for a in arrays)
     d2h = sum(int(np.prod(p.output_shape)) * a[0].itemsize for p, a in zip(progs, host)) + h2d
     ws_e2e = torch.empty(max(batch.workspace_bytes, 1), dtype=torch.uint8, device=dev)
