@@ -1080,10 +1080,13 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       emit(bph, g, false);
       dv[fin.slot] = contiguous(b, shp);
     }
-    // Scatter a GEMM result laid out in `order` dims (rm strides) back into a slot's own leg order,
-    // broadcasting over the legs the forward step summed away (`sum_seq`).
+    // A GEMM result laid out in `order` dims (rm strides) seen in a slot's own leg order, broadcast over the
+    // legs the forward step summed away (`sum_seq`, stride 0).  An intermediate slot's gradient stays this
+    // strided view of the GEMM result: its one consumer, the adjoint of the step that produced the slot,
+    // reads it through its operand tables.  An input's gradient is materialised contiguously when a sliced
+    // accumulation or a trace scatter reads it; otherwise the final copy reads the view.
     auto to_slot = [&](u64 src_buf, const std::vector<u64>& order_dims, const std::vector<u64>& perm,
-                       const std::vector<u64>& sum_seq, const std::vector<u64>& slot_shape) {
+                       const std::vector<u64>& sum_seq, const std::vector<u64>& slot_shape, bool materialise) {
       const auto src_st = rm_strides(order_dims);
       std::vector<size_t> k2, r2;
       split_removed(slot_shape.size(), sum_seq, k2, r2);
@@ -1091,6 +1094,16 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       for (size_t j = 0; j < k2.size(); ++j) {
         const size_t p = std::find(perm.begin(), perm.end(), (u64)j) - perm.begin();
         st[k2[j]] = src_st[p];
+      }
+      if (!materialise) {
+        View v;
+        v.ref = Ref{Ref::WS, src_buf};
+        v.shape = slot_shape;
+        v.strides = st;
+        v.so.local_stride = bph ? (ll)prod(order_dims) : 0;
+        v.so.n = 0;
+        v.variant = bph;
+        return v;
       }
       const u64 numel = prod(slot_shape);
       const u64 b = new_buf(bph, numel * eb, opidx(bph));
@@ -1107,6 +1120,10 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       emit(bph, g, false);
       return contiguous(b, slot_shape);
     };
+    // Input slots whose gradient a sliced accumulation or a trace scatter reads element by element.
+    auto keep_dense = [&](u64 slot) {
+      return slot < net.n_tensors() && (bph || prep_gather[(size_t)slot].kind == Op::GATHER);
+    };
     for (size_t s = plan_.steps.size(); s-- > 0;) {
       const PairStep& st = plan_.steps[s];
       StepRec rec = recs[s];
@@ -1119,7 +1136,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       const View dC = dv[st.result_slot];
       const size_t nb = st.n_batch, nfa = st.n_free_a;
       const auto& rsh = st.result_shape;
-      const auto rst = rm_strides(rsh);
+      const auto& rst = dC.strides;
       const auto dcB = legs_of(rsh, rst, 0, nb), dcM = legs_of(rsh, rst, nb, nb + nfa),
                  dcN = legs_of(rsh, rst, nb + nfa, rsh.size());
       // dA' [batch, free_a, con] = dC [batch, free_a, free_b] . conj(B') [batch, con, free_b]^T
@@ -1128,7 +1145,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         Operand b = swap_rk(rec.b);
         const u64 tbuf = new_buf(bph, prod({st.bt, st.m, st.k}) * eb, opidx(bph));
         emit_gemm(bph, a, b, st.bt, st.m, st.n, st.k, Ref{Ref::WS, tbuf}, false, true);
-        dv[st.left_slot] = to_slot(tbuf, rec.da, st.a_perm, st.sum_a, st.left_shape);
+        dv[st.left_slot] = to_slot(tbuf, rec.da, st.a_perm, st.sum_a, st.left_shape, keep_dense(st.left_slot));
       }
       // dB' [batch, con, free_b] = conj(A') [batch, free_a, con]^T . dC [batch, free_a, free_b]
       {
@@ -1136,7 +1153,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         Operand b = make_operand(dC.ref, dC.so, dC.variant, dcB, dcN, dcM);
         const u64 tbuf = new_buf(bph, prod({st.bt, st.k, st.n}) * eb, opidx(bph));
         emit_gemm(bph, a, b, st.bt, st.k, st.m, st.n, Ref{Ref::WS, tbuf}, true, false);
-        dv[st.right_slot] = to_slot(tbuf, rec.db, st.b_perm, st.sum_b, st.right_shape);
+        dv[st.right_slot] = to_slot(tbuf, rec.db, st.b_perm, st.sum_b, st.right_shape, keep_dense(st.right_slot));
       }
     }
     // Inputs: copy to the caller's gradient buffers, or scatter through an input's traces / diagonals.
@@ -1185,7 +1202,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         Op g{Op::GATHER};
         g.a = src;
         g.c = Ref{Ref::GRADS, i};
-        g.tab[0] = tab_ll(offsets(shape0, rm_strides(shape0)));
+        g.tab[0] = tab_ll(offsets(shape0, bph ? rm_strides(shape0) : d.strides));
         g.tab[1] = tab_ll({0});
         g.n_out = (ll)numel0;
         g.n_red = 1;
