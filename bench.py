@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, the FP32 comparison and the FP64 check")
+    ap.add_argument("--batch-size", type=int, default=256, help="networks of --workload batch (256: config 5)")
     ap.add_argument("--workload", choices=["rand3reg", "grid6", "brickwork", "grid8", "batch"], default="rand3reg",
                     help="rand3reg: the sliced headline (default); grid6 / brickwork: latency and precision; "
                          "grid8: forward + adjoint; batch: 256 uneven networks in one graph launch")
@@ -543,7 +544,7 @@ def run_batch(args, dev):
     import arctn_b200 as A
     from arctn_b200 import networks as N
 
-    nets = N.workload_batch(256, seed=0)
+    nets = N.workload_batch(args.batch_size, seed=0)
     progs, xs = [], []
     for net, arrays in nets:
         path = A.greedy(*net.as_tuple())
@@ -595,8 +596,8 @@ def run_batch(args, dev):
     host = [arrays for _, arrays in nets]
     if args.no_extras:  # device time only (profiling runs)
         print(json.dumps(_line(args, "many-network forward+adjoint throughput", len(progs) / (ms * 1e-3),
-                               "networks/s", True, ms, {"workload": "256 random 3-regular networks, n in [20,50], "
-                                                        "bond in {2,3,4}, f32/c64 alternating"}, "f32+c64",
+                               "networks/s", True, ms, {"workload": f"{len(progs)} random 3-regular networks, n in "
+                                                        "[20,50], bond in {2,3,4}, f32/c64 alternating"}, "f32+c64",
                                gpu_launches=launches_per_call * args.steps, e2e=None, roofline=None,
                                cpu_baseline=None, clocks=sampler.summary(), device_status=status)), flush=True)
         return
@@ -622,7 +623,8 @@ def run_batch(args, dev):
         lat.append(_events_ms(stream, lambda: p.gradient(x, workspace=w, stream=stream)))
     lat.sort()
     line = _line(args, "many-network forward+adjoint throughput", len(progs) / (ms * 1e-3), "networks/s", True, ms,
-                 {"workload": "256 random 3-regular networks, n in [20,50], bond in {2,3,4}, f32/c64 alternating",
+                 {"workload": f"{len(progs)} random 3-regular networks, n in [20,50], bond in {{2,3,4}}, "
+                              "f32/c64 alternating",
                   "form": "persistent interpreter for the small SIMT-only networks, lane streams for the rest",
                   "interpreted_networks": len(interpreted), "stages": part["stages"],
                   "interpreter_tasks": part["tasks"], "lane_network_kernels": lane_kernels,
