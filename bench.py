@@ -569,10 +569,10 @@ def run_batch(args, dev):
                 times.append(_events_ms(stream, run))
         return statistics.mean(times), batch.device_status(run.workspace, stream)
 
-    # The lane form (every step its own launch, networks spread over 64 streams) for comparison.
+    # The lane form (every step its own launch, networks spread over 128 streams) for comparison.
     lanes_ms, lanes_status = (None, 0) if args.no_extras else \
-        time_batch(A.ProgramBatch(progs, max_lanes=64, mode="lanes"))
-    batch = A.ProgramBatch(progs, max_lanes=64)
+        time_batch(A.ProgramBatch(progs, max_lanes=128, mode="lanes"))
+    batch = A.ProgramBatch(progs, max_lanes=128)
     sampler = ClockSampler(dev.index)
     ms, status = time_batch(batch, sampler)
     status = status or lanes_status
