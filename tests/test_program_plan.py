@@ -241,3 +241,48 @@ def test_graph_dag_orders_every_pair_of_ops_sharing_memory(case):
     if case != "sliced_fused":
         assert len({o["lane"] for o in ops}) > 1  # independent steps do run on several lanes
         assert len({o["unit"] for o in ops}) < len(ops)  # and thin steps of one level share a launch
+
+
+def _two_tensor(m, k, n):
+    return [[0, 1], [1, 2]], [0, 2], {0: m, 1: k, 2: n}
+
+
+def test_large_float32_steps_pick_the_128_tile_or_the_folded_tensor_core_gemm():
+    inputs, output, size = _two_tensor(2048, 301, 2048)
+    ops = A.SlicedProgram(inputs, output, size, [(0, 1)], (), dtype=np.float32, device=0).describe()["ops"]
+    assert [o["kind"] for o in ops if o["kind"].startswith("gemm")] == ["gemm_tile128"]
+    ops = A.SlicedProgram(inputs, output, size, [(0, 1)], (), dtype=np.float32, precision="tf32x3",
+                          device=0).describe()["ops"]
+    packs = [o for o in ops if o["kind"] == "pack"]
+    gemm = [o for o in ops if o["kind"] == "gemm_tc"]
+    assert len(packs) == 2 and len(gemm) == 1 and gemm[0]["real"] == 1
+    assert all(p["real"] == 1 and p["cols"] == 151 and p["kpad"] % 16 == 0 for p in packs)  # K = 301 folds to 151
+    # the complex product lands in scratch; one gather keeps its real part, into the output
+    last = ops[ops.index(gemm[0]) + 1]
+    assert last["kind"] == "gather" and last["a"] == gemm[0]["c"] and last["n_out"] == 2048 * 2048
+    # complex64 keeps the unfolded K
+    ops = A.SlicedProgram(inputs, output, size, [(0, 1)], (), dtype=np.complex64, precision="tf32x3",
+                          device=0).describe()["ops"]
+    assert [o["real"] for o in ops if o["kind"] == "gemm_tc"] == [0]
+
+
+def test_adjoint_reads_gradients_through_strides_without_permute_copies():
+    # each intermediate's gradient is the adjoint GEMM's output seen through strides: the reverse sweep
+    # copies only into the callers' gradient buffers (one gather per input) besides the incoming gradient
+    net = N.grid_2d(4, 4, 3)
+    p = program(net, A.greedy(*net.as_tuple()), dtype=np.float32, gradient=True)
+    bwd = [o for o in p.describe()["ops"] if o.get("bwd")]
+    gathers = sum(o["kind"] == "gather" for o in bwd)
+    gemms = sum(o["kind"].startswith("gemm") for o in bwd)
+    assert gemms == 2 * (len(net.inputs) - 1)
+    assert gathers <= len(net.inputs) + 1
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32x3"])
+def test_gradient_program_dag_orders_every_pair_of_ops_sharing_memory(precision):
+    # the batch interpreter runs a gradient program's steps from these dependencies
+    nets = N.workload_batch(8, seed=0)
+    for j in (5, 6):
+        net, arrays = nets[j]
+        p = program(net, A.greedy(*net.as_tuple()), dtype=arrays[0].dtype, precision=precision, gradient=True)
+        _dag_orders_every_overlap(p.describe()["ops"])
