@@ -112,6 +112,7 @@ SIGNATURES = [
                                                     ctypes.POINTER(ctypes.c_float), ctypes.POINTER(c_int),
                                                     ctypes.POINTER(c_double)]),
     ("arctn_b200_cgemm_tf32x3_noalloc", c_int, [vp, vp, vp, u64, u64, u64, u64, vp]),
+    ("arctn_b200_cgemm_noalloc_status", c_int, [vp, ctypes.POINTER(c_int)]),
     ("arctn_b200_contract_sliced_host", c_int, [NETP, u64, u64p, u64, u32p, ctypes.POINTER(ProgramOptions), vpp,
                                                 vp]),
 ]

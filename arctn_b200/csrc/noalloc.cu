@@ -16,6 +16,10 @@
 // pointer); make that first call before any stream capture.  Every call on a
 // device shares the one array and leaves its contents behind, so calls whose
 // work overlaps on the GPU (different streams, no ordering) race: order them.
+//
+// The array's first 256 bytes hold the kernel's status word (the code of a
+// bounded wait that expired, 0 otherwise), cleared by every call and read back
+// by arctn_b200_cgemm_noalloc_status; the operand planes follow it.
 #include <algorithm>
 #include <mutex>
 #include <string>
@@ -28,6 +32,7 @@ namespace {
 using ab2::ll;
 
 constexpr size_t kScratchBytes = 64u << 20;  // 64 MiB per device
+constexpr size_t kStatusBytes = 256;          // status word at the start, then the operand planes
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
@@ -116,7 +121,7 @@ extern "C" int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, voi
                           rpb = (n + tc::BN - 1) / tc::BN * tc::BN;
   const unsigned __int128 a_bytes = ab2::tc::PLANES * (unsigned __int128)bt * rpa * kpad * 4;
   const unsigned __int128 b_bytes = ab2::tc::PLANES * (unsigned __int128)bt * rpb * kpad * 4;
-  const unsigned __int128 need = ((a_bytes + 255) / 256 * 256) + ((b_bytes + 255) / 256 * 256) + 256;
+  const unsigned __int128 need = kStatusBytes + ((a_bytes + 255) / 256 * 256) + ((b_bytes + 255) / 256 * 256);
   if (need > kScratchBytes)
     return fail_with("problem needs " + std::to_string((unsigned long long)need) + " scratch bytes; the fixed maximum is " +
                          std::to_string(kScratchBytes) + " (reduce bt, m, n or k)",
@@ -146,9 +151,9 @@ extern "C" int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, voi
     scratch = (unsigned char*)g_scratch_ptr[dev];
   }
   cudaStream_t st = (cudaStream_t)cuda_stream;
-  float* pa = (float*)scratch;
-  float* pb = (float*)(scratch + (size_t)((a_bytes + 255) / 256 * 256));
-  int* err = (int*)(scratch + (size_t)((a_bytes + 255) / 256 * 256) + (size_t)((b_bytes + 255) / 256 * 256));
+  int* err = (int*)scratch;
+  float* pa = (float*)(scratch + kStatusBytes);
+  float* pb = (float*)(scratch + kStatusBytes + (size_t)((a_bytes + 255) / 256 * 256));
   // The status word must start at zero; the planes are fully rewritten (padding included) by the packs.
   if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return fail_with("cudaMemsetAsync failed", ARCTN_B200_ERR_CUDA);
   const ll Kp = (ll)kpad, Ra = (ll)rpa, Rb = (ll)rpb, Z = (ll)bt;
@@ -181,6 +186,33 @@ extern "C" int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, voi
   tc::k_tc_cgemm_tf32x3<<<(unsigned)std::min(args.n_items, n_sm), tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail_with(std::string("launch: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
+  ab2::set_last_error("");
+  return ARCTN_B200_OK;
+}
+
+// Waits for cuda_stream, then copies the status word of the last call on the current device into *code
+// (0: every bounded wait of the kernel completed; nonzero: the code of the wait that expired, and C is
+// incomplete).  One device-to-host copy of 4 bytes into the caller's host memory; nothing is allocated.
+extern "C" int arctn_b200_cgemm_noalloc_status(void* cuda_stream, int* code) {
+  if (!code) return fail_with("code must point to host memory", ARCTN_B200_ERR_INVALID);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev >= kMaxDevices) return fail_with("no usable current device", ARCTN_B200_ERR_CUDA);
+  void* p = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    p = g_scratch_ptr[dev];
+  }
+  if (!p) {  // no call on this device yet: nothing can have failed
+    *code = 0;
+    ab2::set_last_error("");
+    return ARCTN_B200_OK;
+  }
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)cuda_stream);
+  if (e != cudaSuccess) return fail_with(std::string("cudaStreamSynchronize: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
+  int v = 0;
+  e = cudaMemcpy(&v, p, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return fail_with(std::string("cudaMemcpy: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
+  *code = v;
   ab2::set_last_error("");
   return ARCTN_B200_OK;
 }

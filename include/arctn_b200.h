@@ -279,6 +279,11 @@ int arctn_b200_program_profile_gradient(arctn_b200_program* program, const void*
  * `cuda_stream`. */
 int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, void* c, uint64_t bt, uint64_t m, uint64_t k,
                                     uint64_t n, void* cuda_stream);
+/* No counterpart in the reference.  Status of the last arctn_b200_cgemm_tf32x3_noalloc call on the current
+ * device: waits for cuda_stream, then sets *code to its kernel's status word (0: complete; nonzero: a bounded
+ * wait expired, C is incomplete; the codes are those of arctn_b200_program_device_status).  Allocates
+ * nothing: a 4-byte copy into the caller's host memory.  *code = 0 when no call has run on the device. */
+int arctn_b200_cgemm_noalloc_status(void* cuda_stream, int* code);
 
 /* ------------------------------------------------------------ batches of independent programs
  * No counterpart in the reference (it contracts one network per call).  A batch runs many programs --

@@ -51,8 +51,38 @@ def test_noalloc_cgemm_matches_existing_entry_point_twice():
         stream.synchronize()
         C.check(rc, "no-alloc GEMM")
         got = out.cpu().numpy()
+        assert _status(stream) == 0
         assert np.all(np.isfinite(got))
         assert rel_err(got, want.cpu().numpy()) <= 1e-5
+        assert rel_err(got, exact) <= 1e-5
+
+
+def _status(stream):
+    code = ctypes.c_int(-1)
+    C.check(C.lib().arctn_b200_cgemm_noalloc_status(stream.cuda_stream, ctypes.byref(code)), "no-alloc status")
+    return code.value
+
+
+# Ragged shapes: K not a multiple of the 16-wide K tile (zero padding of the packs), m and n below one
+# 32-row pack tile, n not a multiple of 32 on the strided B pack.
+SMALL = [(1, 5, 7, 3), (2, 130, 17, 33), (4, 64, 1, 129)]
+
+
+@pytest.mark.parametrize("shape", SMALL, ids=[str(s) for s in SMALL])
+def test_noalloc_cgemm_ragged_shapes(shape):
+    import torch
+
+    bt, m, k, n = shape
+    a, b, ta, tb = _operands(bt, m, k, n, 29 + m)
+    exact = np.einsum("bik,bkj->bij", a.astype(np.complex128), b.astype(np.complex128))
+    fn = C.lib().arctn_b200_cgemm_tf32x3_noalloc
+    stream = torch.cuda.current_stream()
+    for _ in range(2):
+        out = torch.full((bt, m, n), float("nan"), dtype=torch.complex64, device="cuda")
+        C.check(fn(ta.data_ptr(), tb.data_ptr(), out.data_ptr(), bt, m, k, n, stream.cuda_stream), "no-alloc GEMM")
+        assert _status(stream) == 0
+        got = out.cpu().numpy()
+        assert np.all(np.isfinite(got))
         assert rel_err(got, exact) <= 1e-5
 
 
