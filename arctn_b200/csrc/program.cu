@@ -2244,6 +2244,7 @@ std::string Program::describe() const {
                                 "gemm_dot",  "pack",       "scatter",     "pack_tiled", "gemm_warp",  "grad_accum",
                                 "narrow",    "gemm_tile128"};
   std::string s = "{\"workspace_bytes\":" + std::to_string(ws_total_) + ",\"n_slices\":" + std::to_string(n_total_) +
+                  ",\"slice_begin\":" + std::to_string(range_begin_) + ",\"slice_end\":" + std::to_string(range_end_) +
                   ",\"slices_per_group\":" + std::to_string(S_) + ",\"groups\":" + std::to_string(n_groups_) +
                   ",\"launches\":" + std::to_string(launches()) + ",\"gradient\":" + (opt_.gradient ? "true" : "false") +
                   ",\"backward_begin\":" + std::to_string(opt_.gradient ? bwd_begin_ : ops_.size()) +

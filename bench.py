@@ -32,6 +32,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -118,12 +119,12 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = None
 
     def __enter__(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.f = open(self.path, "w")
+            fd, self.path = tempfile.mkstemp(prefix="arctn_b200_clocks_", suffix=".csv")
+            self.f = os.fdopen(fd, "w")
             q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -144,7 +145,7 @@ class ClockSampler:
             self.f.close()
 
     def summary(self):
-        if not self.proc or not os.path.exists(self.path):
+        if not self.proc or not self.path or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -160,6 +161,11 @@ class ClockSampler:
             for name, v in zip(names, parts[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(name)
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
+        self.path = None
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
                 "samples": len(sm)}
 
@@ -174,21 +180,56 @@ def per_slice_flops(net, path, sliced):
     return 8.0 * sum(a * b * c * d for a, b, c, d in (s.gemm_dims() for s in cc.pair_steps()))
 
 
+def load_networks():
+    """The synthetic network generators (pure NumPy) loaded from their file, without importing the
+    arctn_b200 package: the reference arm must not load the product library."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("_bench_networks", os.path.join(ROOT, "arctn_b200", "networks.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # dataclasses resolve annotations through sys.modules
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def oracle_workload(n_nodes, target_log2):
+    """The headline workload planned by the oracle alone: its greedy path, slice search and flop count."""
+    from oracle import oracle as O
+
+    N = load_networks()
+    net, arrays = N.workload_rand3reg(n_nodes, 2, 1, np.complex64, seed=0)
+    path = O.greedy(*net.as_tuple())
+    sliced = O.find_slices_to_size(*net.as_tuple(), path, 2 ** target_log2)
+    if sliced is None:
+        raise SystemExit("no slicing meets the target")
+    sub = dict(net.size_dict)
+    for leg in sliced:
+        sub[leg] = 1
+    plan = O.plan_json(net.inputs, net.output, sub, path)
+    flops = 8.0 * sum(a * b * c * d for a, b, c, d in (st["gemm_dims"] for st in plan["steps"]))
+    name = f"rand3reg_n{n_nodes}_bond2_seed1_c64_greedy_target2^{target_log2}_{2 ** len(sliced)}slices"
+    return net, arrays, path, sliced, name, flops
+
+
+def host_threads():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+
 def cpu_baseline(net, arrays, path, sliced, total_slices, flops_total, threads=None):
     """The oracle (CPU restatement of the reference executor) on a bounded sample of slices."""
     from oracle import oracle as O
 
     O.build()
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    threads = threads or max(1, min(cores, 32, total_slices))
+    cores = host_threads()
+    threads = threads or max(1, min(cores, 64, total_slices))
     t0 = time.perf_counter()
-    O.contract_slice_range(*net.as_tuple(), path, sliced, 0, threads, arrays, threads=threads)
+    part = O.contract_slice_range(*net.as_tuple(), path, sliced, 0, threads, arrays, threads=threads)
     dt = time.perf_counter() - t0
     flops = flops_total / total_slices * threads
     return {"value": flops / dt / 1e12, "unit": "TFLOP/s", "cores": threads, "kind": "port",
             "sample": f"slices [0,{threads}) of {total_slices}, one slice per host thread, {dt:.1f} s wall; "
-                      "oracle complex64 executor (reference step algorithm, k-ascending row-panel GEMM)",
-            "wall_s": dt, "host_cores": cores}
+                      "oracle complex64 executor (reference step algorithm, register-blocked k-ascending GEMM)",
+            "wall_s": dt, "host_cores": cores, "partial": complex(np.asarray(part).sum())}
 
 
 def numpy_tensordot_baseline(net, arrays, path, sliced, total_slices, flops_total, budget_s=10.0, max_slices=16):
@@ -258,15 +299,21 @@ def numpy_tensordot_baseline(net, arrays, path, sliced, total_slices, flops_tota
             "partial_sum": [float(np.real(acc).sum()), float(np.imag(acc).sum())]}
 
 
-def run_reference(args, net, arrays, path, sliced, name, rank):
-    """--impl reference: the reference's CPU executor path (its oracle restatement) on the host cores."""
+def run_reference(args, rank):
+    """--impl reference: the reference's CPU executor path (its oracle restatement) on the host cores.
+
+    Planning (greedy path, slice search), the flop count and the contraction all come from the oracle;
+    the product library is never loaded in this process.  Each step contracts a bounded sample of the
+    slices (one per host thread) and the rate is that sample's flops over its wall time."""
     if rank != 0:
         return
-    total = 2 ** len(sliced)
-    flops_total = per_slice_flops(net, path, sliced) * total
     from oracle import oracle as O
-    from arctn_b200 import networks as N
 
+    O.build()
+    net, arrays, path, sliced, name, per_slice = oracle_workload(args.nodes, args.target_log2)
+    total = 2 ** len(sliced)
+    flops_total = per_slice * total
+    N = load_networks()
     small, small_arrays = N.workload_rand3reg(64, 2, 1, np.complex64, seed=0)
     spath = O.greedy(*small.as_tuple())
     for _ in range(args.warmup):  # warm-up: load the library and touch the allocator on a small contraction
@@ -278,12 +325,15 @@ def run_reference(args, net, arrays, path, sliced, name, rank):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "TFLOP/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "c64", "data": "synthetic",
-            "config": {"workload": name, "sample": cb["sample"]},
+            "config": {"workload": name, "n_nodes": args.nodes, "bond": 2, "graph_seed": 1,
+                       "target_size": 2 ** args.target_log2, "n_slices": total, "precision": "fp32 (CPU)",
+                       "cross_slice_sum": "in the input dtype, the reference's chunk order",
+                       "sample": cb["sample"], "planned_by": "oracle greedy + find_slices_to_size"},
             "cpu_baseline": {"value": v, "unit": "TFLOP/s", "cores": cb["cores"], "kind": "port",
                              "sample": cb["sample"]},
             "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference Rust executor cannot be built in this image (no cargo/rustc, crates not "
-                    "vendored); its CPU restatement (oracle/) is timed instead"}
+                    "vendored); its CPU restatement (oracle/) is timed instead, on a sample of slices"}
     print(json.dumps(line), flush=True)
 
 
@@ -660,10 +710,10 @@ def main():
         else:
             run_batch(args, dev)
         return
-    net, arrays, path, sliced, name = workload(args.nodes, args.target_log2)
     if args.impl == "reference":
-        run_reference(args, net, arrays, path, sliced, name, rank)
+        run_reference(args, rank)
         return
+    net, arrays, path, sliced, name = workload(args.nodes, args.target_log2)
 
     import torch
 
@@ -737,6 +787,24 @@ def main():
         extras.update({"other_precision": other, "other_value": prog.flops / (ms2 * 1e-3) / 1e12,
                        "speedup_vs_other": ms2 / ms_per_step, "rel_err_vs_fp64": rel(r.item()),
                        "other_rel_err_vs_fp64": rel(r2.item()), "fp64_result": [ref.real, ref.imag]})
+        # The oracle (complex128 inputs, the reference's executor) on a sample of slices, against the same
+        # slices on the GPU through a slice-range program of the benchmarked precision.
+        from oracle import oracle as O
+
+        O.build()
+        samp = max(1, min(total, host_threads(), 32))
+        t0 = time.perf_counter()
+        want = complex(np.asarray(O.contract_slice_range(*net.as_tuple(), path, sliced, 0, samp, O.promote(arrays),
+                                                         threads=samp)))
+        t_or = time.perf_counter() - t0
+        rs = dict(common)
+        rs.update(slice_begin=0, slice_end=samp)
+        ps = A.SlicedProgram(*net.as_tuple(), path, sliced, precision=args.precision, **rs)
+        got = complex(ps.execute(x, f64_out=True, stream=stream).item())
+        del ps
+        extras["oracle_sample"] = {"slices": [0, samp], "rel_err": abs(got - want) / abs(want),
+                                   "oracle": [want.real, want.imag], "gpu": [got.real, got.imag],
+                                   "oracle_wall_s": t_or, "oracle_threads": samp}
 
     roof = None
     pk = peaks()

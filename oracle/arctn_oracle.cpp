@@ -628,21 +628,65 @@ static Tensor<T> select_axis(const Tensor<T>& t, usize ax, usize i) {
   return out;
 }
 
-// src/contract.rs:102-181 with the GEMM backend restated as a k-ascending loop
-// (each output element accumulates l = 0..k-1 in order), blocked over columns
-// so a row panel of C stays in cache.  Built for AVX2 where the host has it.
+// src/contract.rs:102-181 with the GEMM backend (matrixmultiply 0.3.10, not vendored) restated as a
+// k-ascending loop: every output element starts at zero and adds its products for l = 0, 1, ..., k-1 in
+// that order, each product formed as num-complex does ((ar*br - ai*bi), (ar*bi + ai*br)).  The loop is
+// register-blocked (MR rows x NR columns of C held in registers across a KC-long slice of K, a packed
+// KC x NR panel of B split into real and imaginary parts) so it runs near the host's vector rate; the
+// blocking changes which values sit in registers, never the order of any output's additions, so the bits
+// equal the plain triple loop's.  Built for AVX2 where the host has it.
+template <class T> struct GemmParts { using R = T; static constexpr bool cx = false; };
+template <class R_> struct GemmParts<Cx<R_>> { using R = R_; static constexpr bool cx = true; };
+
 template <class T>
 __attribute__((target_clones("avx2", "default"))) static void gemm_rows(const T* A, const T* B, T* C, usize m,
                                                                            usize k, usize n) {
-  const usize JB = 512;
-  for (usize j0 = 0; j0 < n; j0 += JB) {
-    const usize j1 = std::min(n, j0 + JB);
-    for (usize i = 0; i < m; ++i) {
-      T* crow = C + i * n;
-      for (usize l = 0; l < k; ++l) {
-        const T av = A[i * k + l];
-        const T* brow = B + l * n;
-        for (usize j = j0; j < j1; ++j) crow[j] += av * brow[j];
+  using R = typename GemmParts<T>::R;
+  constexpr bool cx = GemmParts<T>::cx;
+  constexpr usize MR = 4, NR = cx ? 8 : 16, KC = 256;
+  alignas(64) R bre[KC * NR], bim[cx ? KC * NR : 1];
+  for (usize j0 = 0; j0 < n; j0 += NR) {
+    const usize nr = std::min<usize>(NR, n - j0);
+    for (usize k0 = 0; k0 < k; k0 += KC) {
+      const usize kc = std::min<usize>(KC, k - k0);
+      for (usize l = 0; l < kc; ++l)
+        for (usize c = 0; c < NR; ++c) {
+          const T v = c < nr ? B[(k0 + l) * n + j0 + c] : S<T>::zero();
+          if constexpr (cx) { bre[l * NR + c] = v.re; bim[l * NR + c] = v.im; }
+          else bre[l * NR + c] = v;
+        }
+      for (usize i0 = 0; i0 < m; i0 += MR) {
+        const usize mr = std::min<usize>(MR, m - i0);
+        R ar_[MR][NR], ai_[MR][cx ? NR : 1];
+        for (usize r = 0; r < MR; ++r)
+          for (usize c = 0; c < NR; ++c) {
+            const T v = (r < mr && c < nr) ? C[(i0 + r) * n + j0 + c] : S<T>::zero();
+            if constexpr (cx) { ar_[r][c] = v.re; ai_[r][c] = v.im; }
+            else ar_[r][c] = v;
+          }
+        for (usize l = 0; l < kc; ++l) {
+          const R* br = bre + l * NR;
+          const R* bi = bim + (cx ? l * NR : 0);
+          for (usize r = 0; r < MR; ++r) {
+            const T a = r < mr ? A[(i0 + r) * k + k0 + l] : S<T>::zero();
+            if constexpr (cx) {
+              const R xr = a.re, xi = a.im;
+              for (usize c = 0; c < NR; ++c) {
+                const R tr = xr * br[c] - xi * bi[c];
+                const R ti = xr * bi[c] + xi * br[c];
+                ar_[r][c] += tr;
+                ai_[r][c] += ti;
+              }
+            } else {
+              for (usize c = 0; c < NR; ++c) ar_[r][c] += a * br[c];
+            }
+          }
+        }
+        for (usize r = 0; r < mr; ++r)
+          for (usize c = 0; c < nr; ++c) {
+            if constexpr (cx) C[(i0 + r) * n + j0 + c] = T{ar_[r][c], ai_[r][c]};
+            else C[(i0 + r) * n + j0 + c] = ar_[r][c];
+          }
       }
     }
   }

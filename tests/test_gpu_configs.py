@@ -1,0 +1,179 @@
+"""GPU parity at the benchmarked configurations, against the oracle.
+
+- Headline (rand3reg n=172, bond 2, target 2^24 -> 256 slices, complex64): two samples of slices run
+  through slice-range programs at the benchmarked precisions, against the oracle's complex128 executor on
+  the same slices (``contract_slice_range``); 1e-5 relative.  The tensor-core kernel must carry the work.
+- Brickwork circuit (30 wires, depth 14, complex64): every precision against the complex128 oracle;
+  1e-5 for split-TF32 and FP32, 1e-12 for complex128, and split-BF16 (3 products) within 1e-4.
+- Grid 8x8, bond 6 (forward + adjoint of all 64 inputs, split-TF32): gradients within 1e-5 normwise of
+  the step-by-step complex128 autograd replay, directional derivatives against FP64 central differences
+  (tests/golden/grid8_bond6.json), and the scalar no further from complex128 than the reference's own
+  complex64 executor.
+- The product's slice-range partition (tnmpi's contract_slice_range split over k ranks) summed on the
+  host agrees with the full program and the oracle to 1e-12 (complex128).
+"""
+
+import json
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import arctn_b200 as A
+from arctn_b200 import networks as N
+from oracle import oracle as O
+from oracle.torch_replay import replay
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def host_threads():
+    return max(1, min(16, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()))
+
+
+def rel(got, want):
+    return abs(complex(got) - complex(want)) / abs(complex(want))
+
+
+# ------------------------------------------------------------------------------------------- headline
+HEADLINE_SAMPLES = [(0, 4), (165, 169)]
+
+
+@pytest.fixture(scope="module")
+def headline():
+    net, arrays = N.workload_rand3reg(172, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 24)
+    assert 2 ** len(sliced) == 256
+    want = {}
+    for lo, hi in HEADLINE_SAMPLES:
+        want[(lo, hi)] = complex(np.asarray(O.contract_slice_range(
+            *net.as_tuple(), path, sliced, lo, hi, O.promote(arrays), threads=min(hi - lo, host_threads()))))
+    return net, arrays, path, sliced, want
+
+
+@pytest.mark.parametrize("precision", ["tf32x3", "fp32"])
+def test_headline_slice_samples_match_oracle(headline, precision):
+    net, arrays, path, sliced, want = headline
+    x = [torch.from_numpy(a).cuda() for a in arrays]
+    for lo, hi in HEADLINE_SAMPLES:
+        prog = A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex64, precision=precision,
+                               slice_begin=lo, slice_end=hi, workspace_budget=8 << 30)
+        ws = torch.empty(max(prog.workspace_bytes, 1), dtype=torch.uint8, device="cuda")
+        got = prog.execute(x, f64_out=True, workspace=ws)
+        assert prog.device_status(ws) == 0
+        err = rel(got.item(), want[(lo, hi)])
+        assert err <= 1e-5, (lo, hi, precision, err)
+        if precision == "tf32x3":
+            ms, kinds, work = prog.profile(x, workspace=ws)
+            tc = sum(w for k, w in zip(kinds, work) if int(k) == 9)
+            assert tc >= 0.95 * prog.flops, "the tensor-core kernel does not carry the headline's flops"
+        del ws, prog
+
+
+# ------------------------------------------------------------------------------------------- brickwork
+@pytest.fixture(scope="module")
+def brickwork():
+    net, arrays = N.brickwork_circuit(30, 14, seed=0)
+    a64 = [a.astype(np.complex64) for a in arrays]
+    path = A.greedy(*net.as_tuple())
+    assert A.find_slices_to_size(*net.as_tuple(), path, 2 ** 27) == []  # the configuration needs no slicing
+    want = complex(O.contract_sliced(*net.as_tuple(), path, [], O.promote(a64)))
+    ref_c64 = complex(O.contract_sliced(*net.as_tuple(), path, [], a64))
+    return net, a64, path, want, ref_c64
+
+
+# Split-BF16 with three products carries each operand to about 2^-18 and drops the lo x lo term.
+@pytest.mark.parametrize("precision,tol", [("tf32x3", 1e-5), ("fp32", 1e-5), ("bf16x3", 1e-4)])
+def test_brickwork_precisions_match_c128_oracle(brickwork, precision, tol):
+    net, a64, path, want, ref_c64 = brickwork
+    assert rel(ref_c64, want) <= 1e-5  # the reference's own complex64 executor on these inputs
+    prog = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex64, precision=precision)
+    x = [torch.from_numpy(a).cuda() for a in a64]
+    ws = torch.empty(max(prog.workspace_bytes, 1), dtype=torch.uint8, device="cuda")
+    got = prog.execute(x, workspace=ws)
+    assert prog.device_status(ws) == 0
+    err = rel(got.item(), want)
+    print(f"brickwork {precision}: rel err {err:.3e} (reference c64 executor {rel(ref_c64, want):.3e})")
+    assert err <= tol, err
+
+
+def test_brickwork_c128_matches_oracle(brickwork):
+    net, a64, path, want, _ = brickwork
+    prog = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex128)
+    got = prog.execute([torch.from_numpy(a.astype(np.complex128)).cuda() for a in a64])
+    assert rel(got.item(), want) <= 1e-12
+
+
+# ------------------------------------------------------------------------------------------- grid8
+def test_grid8_bond6_adjoint_against_replay_and_central_differences():
+    fx = json.load(open(os.path.join(HERE, "golden", "grid8_bond6.json")))
+    net, arrays = N.workload_grid8(6, np.complex64, seed=0)
+    arrays = [a * np.float32(4.0) for a in arrays]  # as the fixture: lifts the scalar off FP32's underflow
+    path = A.greedy(*net.as_tuple())
+    assert path == O.greedy(*net.as_tuple()) and len(path) == fx["path_len"]
+    # The step-by-step autograd replay in complex128 (the reference's documented gradient route).
+    ts = [torch.from_numpy(a.astype(np.complex128)).requires_grad_() for a in arrays]
+    out = replay(*net.as_tuple(), path, ts)
+    out.backward(torch.ones((), dtype=torch.complex128))
+    want_g = [t.grad.numpy() for t in ts]
+    c128 = complex(*fx["c128"])
+    assert rel(out.item(), c128) <= 1e-12
+    prog = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex64, precision="tf32x3", gradient=True,
+                           use_graph=False, workspace_budget=40 << 30)
+    x = [torch.from_numpy(a).cuda() for a in arrays]
+    o, grads = prog.gradient(x)
+    g = [t.cpu().numpy().astype(np.complex128) for t in grads]
+    # Gradients: every input's gradient within 1e-5 normwise of the replay.
+    worst = max(float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(g, want_g))
+    print(f"grid8 adjoint: worst normwise gradient error {worst:.3e}")
+    assert worst <= 1e-5, worst
+    # Directional derivatives sum_i <conj(g_i), V_i> against FP64 central differences.  A sum of 64 terms
+    # carries each term's error, so the bound is relative to the sum of the terms' magnitudes.
+    rng = np.random.default_rng(0)
+    for fd in fx["directional"]:
+        v = [(rng.standard_normal(a.shape) + 1j * rng.standard_normal(a.shape)) / np.sqrt(6.0 ** a.ndim)
+             for a in arrays]
+        terms = [np.sum(np.conj(gi) * vi) for gi, vi in zip(g, v)]
+        ref_terms = [np.sum(np.conj(gi) * vi) for gi, vi in zip(want_g, v)]
+        fdv = complex(*fd)
+        assert abs(sum(ref_terms) - fdv) <= 1e-8 * abs(fdv)  # the replay gradient itself, at this size
+        scale = sum(abs(t) for t in ref_terms)
+        assert abs(sum(terms) - fdv) <= 1e-5 * scale, (sum(terms), fdv, scale)
+    # The scalar cancels (its condition number is in the tens to hundreds), so no FP32 executor reaches
+    # 1e-5 on it: the reference's own complex64 executor misses by ~7e-5.  The tensor-core path must do
+    # no worse than that.
+    err_tc = rel(o.item(), c128)
+    err_ref = rel(complex(*fx["oracle_c64"]), c128)
+    print(f"grid8 scalar: tf32x3 {err_tc:.3e}, reference c64 executor {err_ref:.3e}")
+    assert err_tc <= err_ref, (err_tc, err_ref)
+
+
+# ------------------------------------------------------------------------------------------- ranks
+@pytest.mark.parametrize("ranks", [2, 3, 5])
+def test_slice_range_partition_matches_full_program(ranks):
+    # tnmpi's slice_range (src/bin/tnmpi.rs:279-284): each "rank" runs the product's slice-range program
+    # for its contiguous share; the FP64 partials summed on the host match the full program and the oracle.
+    net, arrays = N.workload_rand3reg(64, 2, 1, np.complex128, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 8)
+    total = 2 ** len(sliced)
+    x = [torch.from_numpy(a).cuda() for a in arrays]
+    full = complex(A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex128).execute(x, f64_out=True).item())
+    acc = 0j
+    covered = []
+    for r in range(ranks):
+        lo, hi = A.slice_range(total, ranks, r)
+        covered.append((lo, hi))
+        p = A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex128, slice_begin=lo, slice_end=hi)
+        assert p.flops == pytest.approx(A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex128).flops
+                                        * (hi - lo) / total)
+        acc += complex(p.execute(x, f64_out=True).item())
+    assert covered[0][0] == 0 and covered[-1][1] == total
+    assert all(a[1] == b[0] for a, b in zip(covered, covered[1:]))
+    want = complex(O.contract_sliced(*net.as_tuple(), path, sliced, arrays, threads=4))
+    assert rel(acc, full) <= 1e-12
+    assert rel(acc, want) <= 1e-12

@@ -3,7 +3,10 @@
 Mirrors the reference's MPI path (src/bin/tnmpi.rs): each rank takes the contiguous
 slice range slice_range(n, ranks, rank), contracts it into a zeroed full output
 (the oracle's contract_slice_range), and one all-reduce(SUM) assembles the result.
-The GPU path does the same with a program's slice_begin/slice_end and NCCL; here the
+Each rank also builds the product's slice-range program (SlicedProgram with
+slice_begin/slice_end, host-only) for its range: the ranges it reports, gathered over
+the group, tile [0, n) in rank order, and its flops add up to the full program's.  The
+GPU path runs those programs and all-reduces their FP64 partials over NCCL; here the
 partition and the collective are exercised without a GPU.  Also covers more ranks
 than slices (empty ranges) and output-leg slicing.
 """
@@ -53,8 +56,19 @@ def _worker(rank, world, port, name, q):
             else np.zeros(shape)
         t = torch.from_numpy(np.array(part, dtype=np.float64, order="C")).reshape(-1)
         dist.all_reduce(t)
+        # The product's program for this rank's range (built and described on the host).
+        rng_flops = torch.zeros(3, dtype=torch.float64)
+        if b < e:
+            prog = A.SlicedProgram(inputs, output, size_dict, path, sliced, dtype=np.float64, slice_begin=b,
+                                   slice_end=e)
+            d = prog.describe()
+            rng_flops[:] = torch.tensor([d["slice_begin"], d["slice_end"], prog.flops], dtype=torch.float64)
+        else:
+            rng_flops[:] = torch.tensor([b, e, 0.0], dtype=torch.float64)
+        gathered = [torch.zeros(3, dtype=torch.float64) for _ in range(world)]
+        dist.all_gather(gathered, rng_flops)
         if rank == 0:
-            q.put(t.numpy().reshape(shape))
+            q.put((t.numpy().reshape(shape), [g.tolist() for g in gathered]))
     finally:
         dist.destroy_process_group()
 
@@ -68,8 +82,16 @@ def test_slice_sharded_allreduce_matches_single_rank(name, world):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     mp.start_processes(_worker, args=(world, _free_port(), name, q), nprocs=world, join=True, start_method="spawn")
-    got = q.get(timeout=30)
+    got, ranges = q.get(timeout=30)
     assert np.max(np.abs(got - want)) < 1e-12
+    n = int(np.prod([size_dict[l] for l in sliced]))
+    full = A.SlicedProgram(inputs, output, size_dict, path, sliced, dtype=np.float64)
+    covered = 0
+    for lo, hi, _ in ranges:
+        assert int(lo) == covered and hi >= lo
+        covered = int(hi)
+    assert covered == n
+    assert sum(f for _, _, f in ranges) == pytest.approx(full.flops)
 
 
 def test_slice_range_partition():
