@@ -24,6 +24,7 @@ from .api import (
     slice_parallel_chunks,
     slice_range,
     ssa_to_linear,
+    tensor_pipe_peak,
 )
 
 __all__ = [
@@ -48,4 +49,5 @@ __all__ = [
     "slice_parallel_chunks",
     "slice_range",
     "ssa_to_linear",
+    "tensor_pipe_peak",
 ]

@@ -113,6 +113,7 @@ SIGNATURES = [
                                                     ctypes.POINTER(c_double)]),
     ("arctn_b200_cgemm_tf32x3_noalloc", c_int, [vp, vp, vp, u64, u64, u64, u64, vp]),
     ("arctn_b200_cgemm_noalloc_status", c_int, [vp, ctypes.POINTER(c_int)]),
+    ("arctn_b200_tc_peak", c_int, [c_int, c_int, u64, vp, vp, ctypes.POINTER(c_double)]),
     ("arctn_b200_contract_sliced_host", c_int, [NETP, u64, u64p, u64, u32p, ctypes.POINTER(ProgramOptions), vpp,
                                                 vp]),
 ]

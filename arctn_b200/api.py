@@ -245,6 +245,28 @@ def slice_parallel_chunks(n_slices, out_numel):
 # ---------------------------------------------------------------------------- programs
 
 
+def tensor_pipe_peak(kind="tf32", n=256, iters=1 << 16, device=None, repeats=3):
+    """Measured dense tensor-pipe rate of a GPU in TFLOP/s (``arctn_b200_tc_peak``): tcgen05 MMAs with M = 128,
+    N = ``n`` (128 or 256) over operands resident in shared memory, ``kind`` "tf32" or "bf16"; best of
+    ``repeats`` launches after one warm-up."""
+    torch = _torch()
+    code = {"tf32": 0, "bf16": 1}[kind]
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    with torch.cuda.device(dev):
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        stream = torch.cuda.current_stream(dev)
+        best = 0.0
+        for r in range(repeats + 1):
+            out = ctypes.c_double(0.0)
+            C.check(C.lib().arctn_b200_tc_peak(code, int(n), int(iters), status.data_ptr(), stream.cuda_stream,
+                                               ctypes.byref(out)), "tensor-pipe peak")
+            if r:
+                best = max(best, out.value)
+        if int(status.item()) != 0:
+            raise C.ArcTNB200Error(C.ERR_DEVICE_TIMEOUT, "tensor-pipe peak probe: a bounded wait expired")
+    return best
+
+
 class SlicedProgram:
     """A network + SSA path + sliced legs bound to a dtype, precision and GPU.
 

@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libarctn_b200.so")
-SOURCES = ["host.cpp", "program.cu", "batch.cu", "capi.cu", "noalloc.cu"]
+SOURCES = ["host.cpp", "program.cu", "batch.cu", "capi.cu", "noalloc.cu", "peak.cu"]
 HEADERS = ["host.hpp", "program.hpp", "batch.hpp", "kernels.cuh", "tc_gemm.cuh", "interp.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

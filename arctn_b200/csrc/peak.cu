@@ -1,0 +1,121 @@
+// Tensor-pipe peak probe: the dense MMA rate of this GPU for the operand kinds the GEMMs use.
+//
+// Every SM runs one CTA whose single issuing thread streams `iters` tcgen05.mma instructions (M = 128,
+// N = 128 or 256, K = 8 for kind::tf32 / 16 for kind::f16 with BF16 operands) over operands that stay
+// resident in shared memory, accumulating into TMEM.  There is no TMA traffic and no epilogue, so the
+// rate is the tensor pipe's own, limited only by how fast it can read its operands from shared memory:
+// an M = 128, N = 128 TF32 MMA reads 8 KB for 131072 MACs, an N = 256 one 12 KB for twice the MACs.
+// The host times the launch with CUDA events; flops = 2 * 128 * N * K * iters * CTAs.  The only wait (the
+// final commit) is bounded and reports expiry in the caller's status word.
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "../../include/arctn_b200.h"
+#include "tc_gemm.cuh"
+
+namespace ab2 {
+void set_last_error(const std::string& m);  // capi.cu
+}
+
+namespace {
+
+using namespace ab2;
+
+__host__ __device__ constexpr uint32_t peak_idesc(bool bf16, int n) {
+  return (1u << 4) | ((bf16 ? 1u : 2u) << 7) | ((bf16 ? 1u : 2u) << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(128 >> 4) << 24);
+}
+
+template <bool kBF16, int N>
+__global__ void __launch_bounds__(128, 1) k_tc_peak(long long iters, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  constexpr int kRows = 128 + N;  // A rows then B rows, 64 bytes each (64-byte swizzle atoms)
+  uint32_t* words = (uint32_t*)smem;
+  // Operand values: 1.0 (TF32) or a pair of BF16 1.0; the sums stay finite for every allowed iters.
+  const uint32_t one = kBF16 ? 0x3F803F80u : 0x3F800000u;
+  for (int i = threadIdx.x; i < kRows * 16; i += blockDim.x) words[i] = one;
+  uint64_t* bar = (uint64_t*)(smem + kRows * 64);
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(bar + 1);
+  const int warp = threadIdx.x / 32;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // operand writes visible to the tensor core
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tc::smem_u32((const void*)tmem_slot)),
+                 "r"((uint32_t)N));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  if (threadIdx.x == 32) {
+    const uint32_t a0 = tc::smem_u32(smem), b0 = a0 + 128 * 64;
+    const uint32_t idesc = peak_idesc(kBF16, N);
+    for (long long i = 0; i < iters; ++i) {
+      const uint32_t o = (uint32_t)(i & 1) * 32;  // the two 32-byte K halves of the 64-byte rows
+      tc::umma<kBF16>(tmem, tc::sw64_desc(a0 + o), tc::sw64_desc(b0 + o), idesc, i > 0 ? 1u : 0u);
+    }
+    tc::umma_commit(bar);
+    tc::mbar_wait(bar, 0, err, 9);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)N));
+  }
+}
+
+template <bool kBF16, int N>
+cudaError_t launch_peak(int ctas, long long iters, int* err, cudaStream_t st) {
+  constexpr int smem = (128 + N) * 64 + 64 + 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_tc_peak<kBF16, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  k_tc_peak<kBF16, N><<<ctas, 128, smem, st>>>(iters, err);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status, void* cuda_stream,
+                                  double* tflops_out) {
+  auto fail = [](const std::string& m, int code) {
+    ab2::set_last_error(m);
+    return code;
+  };
+  if (kind != 0 && kind != 1) return fail("kind must be 0 (tf32) or 1 (bf16)", ARCTN_B200_ERR_INVALID);
+  if (n != 128 && n != 256) return fail("n must be 128 or 256", ARCTN_B200_ERR_INVALID);
+  if (iters < 2 || iters > (1ull << 22)) return fail("iters must lie in [2, 2^22]", ARCTN_B200_ERR_INVALID);
+  if (!status || !tflops_out) return fail("status and tflops_out must not be null", ARCTN_B200_ERR_INVALID);
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return fail("no usable current device", ARCTN_B200_ERR_CUDA);
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+    return fail("cudaEventCreate failed", ARCTN_B200_ERR_CUDA);
+  cudaError_t e = cudaEventRecord(e0, st);
+  const long long it = (long long)iters;
+  int* err = (int*)status;
+  if (e == cudaSuccess) {
+    if (kind == 0) e = n == 128 ? launch_peak<false, 128>(sms, it, err, st) : launch_peak<false, 256>(sms, it, err, st);
+    else e = n == 128 ? launch_peak<true, 128>(sms, it, err, st) : launch_peak<true, 256>(sms, it, err, st);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+  float ms = 0.f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return fail(std::string("tensor-core peak probe: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
+  const double k = kind == 0 ? 8.0 : 16.0;
+  *tflops_out = 2.0 * 128.0 * n * k * (double)iters * sms / (ms * 1e-3) / 1e12;
+  ab2::set_last_error("");
+  return ARCTN_B200_OK;
+}

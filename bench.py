@@ -824,21 +824,30 @@ def main():
             # full clock, so the denominator is the burst bf16 rate; the sustained one is reported beside it.
             achieved = tw / (tms * 1e-3) / 1e12
             peak = pk["bf16_tflops"]
-            traffic = profiled_traffic()
+            traffic = profiled_traffic()  # scaled from an ncu capture of a smaller slice group
             roof = {"bound": "tensor", "kernel": KIND_NAMES.get(top, str(top)), "achieved": achieved,
                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                     "frac_of_sustained": achieved / pk["bf16_tflops_sustained"],
                     "peak_source": f"{pk['source']} bf16 dense burst (MEASURED_PEAKS.json)",
-                    "traffic": traffic, "launches": tn, "avg_launch_ms": tms / tn,
+                    "traffic": traffic, "traffic_source": "ncu capture of a slice group of 4, scaled by slices "
+                    "(profiles/k_tc_cgemm_tf32x3_rand3reg_n172.md)" if traffic else None,
+                    "launches": tn, "avg_launch_ms": tms / tn,
                     "share_of_profiled_time": tms / tot}
             if traffic:
                 roof["traffic_gbs"] = traffic / (tms / tn * 1e-3) / 1e9  # far below HBM: not memory-bound
             if top == 9:
-                # split-TF32 4M: 12 TF32 MMAs per complex MAC step = 24 pipe flops per 8 algorithmic flops;
-                # TF32 dense rate taken as half the measured bf16 rate.
-                tf32_peak = peak / 2
+                # split-TF32 4M: 12 TF32 MMAs per complex MAC step = 24 pipe flops per 8 algorithmic flops.
+                # The TF32 denominator is measured on this GPU by the library's own tcgen05 probe (MMAs over
+                # shared-memory-resident operands, no TMA, no epilogue); N = 128 is the MMA shape the GEMM
+                # issues, N = 256 the pipe's best.
+                pk_tc = {f"{kind}_n{n}": A.tensor_pipe_peak(kind, n, device=local)
+                         for kind in ("tf32", "bf16") for n in (128, 256)}
+                tf32_peak = max(pk_tc["tf32_n128"], pk_tc["tf32_n256"])
+                roof["tensor_pipe_measured_tflops"] = pk_tc
                 roof["pipe_tflops"] = achieved * 3
                 roof["pipe_frac_of_tf32_peak"] = achieved * 3 / tf32_peak
+                roof["pipe_frac_of_tf32_n128"] = achieved * 3 / pk_tc["tf32_n128"]
+                roof["tf32_peak_source"] = "measured: arctn_b200_tc_peak (tcgen05 kind::tf32, M=128, best N)"
         else:
             achieved = tw / (tms * 1e-3) / 1e9
             roof = {"bound": "hbm", "kernel": KIND_NAMES.get(top, str(top)), "achieved": achieved,

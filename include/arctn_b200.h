@@ -285,6 +285,13 @@ int arctn_b200_cgemm_tf32x3_noalloc(const void* a, const void* b, void* c, uint6
  * nothing: a 4-byte copy into the caller's host memory.  *code = 0 when no call has run on the device. */
 int arctn_b200_cgemm_noalloc_status(void* cuda_stream, int* code);
 
+/* No counterpart in the reference (a measurement aid).  The dense tensor-pipe rate of the current GPU:
+ * one CTA per SM streams `iters` tcgen05.mma instructions (M = 128, N = n in {128, 256}; kind 0: TF32,
+ * K = 8; kind 1: BF16, K = 16) over operands resident in shared memory, with no TMA and no epilogue.
+ * Synchronises cuda_stream and sets *tflops_out to 2*128*n*K*iters*SMs / elapsed.  `status` is a device
+ * int the caller zeroed: nonzero afterwards means the final bounded wait expired.  iters in [2, 2^22]. */
+int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status, void* cuda_stream, double* tflops_out);
+
 /* ------------------------------------------------------------ batches of independent programs
  * No counterpart in the reference (it contracts one network per call).  A batch runs many programs --
  * uneven networks, mixed dtypes -- as one CUDA graph launch, in one of three modes:

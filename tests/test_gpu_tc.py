@@ -123,3 +123,14 @@ def test_epilogue_packs_are_bit_identical_to_separate_packs():
     assert np.array_equal(got, ref)
     want = O.contract_sliced(*net.as_tuple(), path, sliced, O.promote(arrays), threads=8)
     assert rel_err(got, want) <= 1e-5
+
+
+@pytest.mark.parametrize("kind", ["tf32", "bf16"])
+def test_tensor_pipe_peak_probe(kind):
+    # The probe's MMAs complete (no expired wait) and give a plausible dense rate: above 100 TFLOP/s for
+    # either kind, and BF16 (K = 16 per MMA) faster than TF32 (K = 8) at the same N.
+    rates = {n: A.tensor_pipe_peak(kind, n, iters=1 << 14, repeats=1) for n in (128, 256)}
+    print(kind, rates)
+    assert all(100.0 < r < 5000.0 for r in rates.values()), rates
+    if kind == "bf16":
+        assert rates[256] > A.tensor_pipe_peak("tf32", 256, iters=1 << 14, repeats=1)
