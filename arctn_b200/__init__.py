@@ -26,6 +26,7 @@ from .api import (
     ssa_to_linear,
     tensor_pipe_peak,
 )
+from .tuning import TuneTable, autotune
 
 __all__ = [
     "ArcTNB200Error",
@@ -38,6 +39,8 @@ __all__ = [
     "PairStep",
     "ProgramBatch",
     "SlicedProgram",
+    "TuneTable",
+    "autotune",
     "arctn_contract",
     "contract_sliced",
     "find_slices_to_size",

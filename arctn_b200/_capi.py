@@ -55,6 +55,11 @@ class ProgramOptions(ctypes.Structure):
                 ("slice_end", u64), ("gradient", c_int), ("tc_k_chunk", u64)]
 
 
+class GemmChoice(ctypes.Structure):
+    _fields_ = [("dtype", c_int), ("precision", c_int), ("phase", c_int), ("a_var", c_int), ("b_var", c_int),
+                ("variant", c_int), ("bt", u64), ("m", u64), ("k", u64), ("n", u64)]
+
+
 # (name, restype, argtypes) for every symbol the header declares.
 NETP = ctypes.POINTER(Network)
 SIGNATURES = [
@@ -83,6 +88,9 @@ SIGNATURES = [
     ("arctn_b200_plan_finalize_execute", c_int, [vp, c_int, vp, vp, vp, u64, vp]),
     ("arctn_b200_program_create", c_int, [NETP, u64, u64p, u64, u32p, ctypes.POINTER(ProgramOptions),
                                           ctypes.POINTER(vp)]),
+    ("arctn_b200_program_create_tuned", c_int, [NETP, u64, u64p, u64, u32p, ctypes.POINTER(ProgramOptions),
+                                                ctypes.POINTER(GemmChoice), u64, ctypes.POINTER(vp)]),
+    ("arctn_b200_program_gemms", c_int, [vp, ctypes.POINTER(GemmChoice), ctypes.POINTER(c_int), u64, u64p]),
     ("arctn_b200_program_destroy", None, [vp]),
     ("arctn_b200_program_workspace_size", u64, [vp]),
     ("arctn_b200_program_n_slices", u64, [vp]),

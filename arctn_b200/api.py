@@ -277,7 +277,7 @@ class SlicedProgram:
 
     def __init__(self, inputs, output, size_dict, ssa_path, sliced_legs=(), *, dtype="complex64",
                  precision="fp32", device=None, use_graph=True, max_slices_per_group=0, workspace_budget=0,
-                 slice_begin=0, slice_end=0, gradient=False, tc_k_chunk=0):
+                 slice_begin=0, slice_end=0, gradient=False, tc_k_chunk=0, tuning=None):
         torch = _torch()
         self.inputs = [[int(l) for l in t] for t in inputs]
         self.output = [int(l) for l in output]
@@ -302,9 +302,18 @@ class SlicedProgram:
                                 int(max_slices_per_group), int(workspace_budget), int(slice_begin), int(slice_end),
                                 1 if gradient else 0, int(tc_k_chunk))
         h = C.vp()
-        C.check(C.lib().arctn_b200_program_create(net.ptr, n, p.ctypes.data_as(C.u64p), len(self.sliced_legs),
-                                                  sl.ctypes.data_as(C.u32p), ctypes.byref(opts), ctypes.byref(h)),
-                "sliced contraction failed")
+        entries = tuning.entries_for(self.code, self.precision) if tuning is not None else []
+        self.tuning = tuning
+        if entries:
+            table = (C.GemmChoice * len(entries))(*[C.GemmChoice(*e) for e in entries])
+            C.check(C.lib().arctn_b200_program_create_tuned(net.ptr, n, p.ctypes.data_as(C.u64p),
+                                                            len(self.sliced_legs), sl.ctypes.data_as(C.u32p),
+                                                            ctypes.byref(opts), table, len(entries),
+                                                            ctypes.byref(h)), "sliced contraction failed")
+        else:
+            C.check(C.lib().arctn_b200_program_create(net.ptr, n, p.ctypes.data_as(C.u64p), len(self.sliced_legs),
+                                                      sl.ctypes.data_as(C.u32p), ctypes.byref(opts),
+                                                      ctypes.byref(h)), "sliced contraction failed")
         self._h = h
         self._lock = threading.Lock()
         L = C.lib()
@@ -334,6 +343,21 @@ class SlicedProgram:
         buf = ctypes.create_string_buffer(int(need.value))
         C.check(C.lib().arctn_b200_program_describe(self._h, buf, need.value, ctypes.byref(need)), "describe")
         return json.loads(buf.value.decode())
+
+    def gemms(self):
+        """The program's GEMMs in launch order (a per-slice GEMM once per slice group), as dicts: the shape key
+        (dtype, precision, phase, a_var, b_var, bt, m, k, n), the variant that runs and whether a tuning
+        table chose it.  Host-only."""
+        from .tuning import VARIANT_NAMES
+
+        n = C.u64(0)
+        C.check(C.lib().arctn_b200_program_gemms(self._h, None, None, 0, ctypes.byref(n)), "gemms")
+        out = (C.GemmChoice * max(1, n.value))()
+        tuned = (ctypes.c_int * max(1, n.value))()
+        C.check(C.lib().arctn_b200_program_gemms(self._h, out, tuned, n.value, ctypes.byref(n)), "gemms")
+        return [dict(dtype=e.dtype, precision=e.precision, phase=e.phase, a_var=e.a_var, b_var=e.b_var, bt=e.bt,
+                     m=e.m, k=e.k, n=e.n, variant=VARIANT_NAMES[e.variant], tuned=bool(tuned[i]))
+                for i, e in enumerate(out[:n.value])]
 
     def _shapes(self):
         """The input shapes the network expects, computed once."""

@@ -340,6 +340,46 @@ int arctn_b200_program_create(const arctn_b200_network* net, uint64_t n_steps, c
   });
 }
 
+int arctn_b200_program_create_tuned(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
+                                    uint64_t n_sliced, const uint32_t* sliced_legs,
+                                    const arctn_b200_program_options* options, const arctn_b200_gemm_choice* table,
+                                    uint64_t n_table, arctn_b200_program** program_out) {
+  return guarded([&] {
+    if (!program_out) fail("program_out is null");
+    if (n_sliced && !sliced_legs) fail("sliced_legs is null");
+    if (n_table && !table) fail("table is null");
+    std::vector<Leg> sl(sliced_legs, sliced_legs + n_sliced);
+    ProgramOptions po = to_options(options);
+    for (u64 i = 0; i < n_table; ++i) {
+      const arctn_b200_gemm_choice& e = table[i];
+      if (e.variant < ARCTN_B200_GEMM_AUTO || e.variant > ARCTN_B200_GEMM_TC_SPLITK)
+        fail("tuning entry " + std::to_string(i) + ": unknown variant " + std::to_string(e.variant));
+      if (e.phase != 1 && e.phase != 2) fail("tuning entry " + std::to_string(i) + ": phase must be 1 or 2");
+      GemmKey k{e.dtype, e.precision, e.phase, e.a_var ? 1 : 0, e.b_var ? 1 : 0, e.bt, e.m, e.k, e.n};
+      po.tuning[k] = e.variant;
+    }
+    auto h = std::make_unique<arctn_b200_program>();
+    h->p = std::make_unique<Program>(to_network(net), to_path(n_steps, ssa_path), sl, po);
+    *program_out = h.release();
+  });
+}
+
+int arctn_b200_program_gemms(const arctn_b200_program* p, arctn_b200_gemm_choice* out, int* tuned_out, uint64_t cap,
+                             uint64_t* n_out) {
+  return guarded([&] {
+    if (!p || !n_out) fail("null argument");
+    const auto v = p->p->gemm_choices();
+    *n_out = v.size();
+    if (cap && !out) fail("out is null");
+    for (size_t i = 0; i < v.size() && i < cap; ++i) {
+      const GemmKey& k = v[i].key;
+      out[i] = arctn_b200_gemm_choice{k.dtype, k.precision, k.phase, k.a_var, k.b_var, v[i].variant,
+                                      k.bt, k.m, k.k, k.n};
+      if (tuned_out) tuned_out[i] = v[i].tuned ? 1 : 0;
+    }
+  });
+}
+
 void arctn_b200_program_destroy(arctn_b200_program* program) { delete program; }
 
 uint64_t arctn_b200_program_workspace_size(const arctn_b200_program* p) { return p ? p->p->workspace_size() : 0; }

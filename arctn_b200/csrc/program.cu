@@ -291,9 +291,11 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     return off;
   };
   std::vector<Op> ops3;  // after every group: the sliced adjoint's input-gradient finish
+  int cur_gemm = -1, n_gemms = 0;  // ops emitted while a GEMM is being emitted serve it (packs, gathers)
   auto emit = [&](bool phase2, const Op& op0, bool also_strip) {
     Op op = op0;
     op.bwd = !fwd;
+    op.gemm = cur_gemm;
     if (phase2) ops2.push_back(op);
     else {
       ops1.push_back(op);
@@ -567,6 +569,8 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
   // go through the planar pack (permute + split, conjugating on the fly) and the tcgen05 kernel.
   auto emit_gemm = [&](bool ph2, const Operand& A, const Operand& B, u64 bt, u64 m, u64 k, u64 n, Ref out,
                        bool conj_a, bool conj_b) {
+    cur_gemm = n_gemms++;
+    struct Done { int& c; ~Done() { c = -1; } } done{cur_gemm};
     auto rows_contiguous = [](const std::vector<ll>& r, const std::vector<ll>& c) {
       const bool r1 = r.size() > 1 && r[1] - r[0] == 1, c1 = c.size() > 1 && c[1] - c[0] == 1;
       return r1 && !c1;  // the pack then reads the source along rows
@@ -605,6 +609,29 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     else if (m >= 64 && n >= 64 && (ph2 || tiles64 >= (u64)kNumSMs)) g.kind = Op::GEMM_TILE64;
     else if (m >= 24 && n >= 24 && (ph2 || tiles32 >= (u64)kNumSMs)) g.kind = Op::GEMM_TILE32;
     else if (k >= 32) g.kind = Op::GEMM_WARP;  // a serial k loop per thread would dominate
+    // A tuning table entry for this shape replaces the heuristic choice (SIMT kind, or the tensor core with
+    // a given tile order / K split); the entry must name a variant this dtype and precision can run.
+    g.key = GemmKey{dt, opt_.precision, ph2 ? 2 : 1, A.variant ? 1 : 0, B.variant ? 1 : 0, bt, m, k, n};
+    const bool tc_allowed = (opt_.precision == PREC_TF32X3 || opt_.precision == PREC_BF16X3) &&
+                            (dt == DT_C64 || dt == DT_F32);
+    int forced = GV_AUTO;
+    if (auto it = opt_.tuning.find(g.key); it != opt_.tuning.end()) forced = it->second;
+    const bool forced_tc = forced == GV_TC_MFAST || forced == GV_TC_NFAST || forced == GV_TC_SPLITK;
+    if (forced_tc && !tc_allowed)
+      throw Error(E_INVALID, "tuning entry asks for the tensor-core GEMM, which needs precision tf32x3 or bf16x3 "
+                             "and a float32 or complex64 network");
+    if (forced == GV_TILE128 && dt != DT_F32) throw Error(E_INVALID, "tuning entry asks for the 128 x 128 tile, "
+                                                                     "which is float32 only");
+    switch (forced) {
+      case GV_SMALL: g.kind = Op::GEMM_SMALL; break;
+      case GV_TILE64: g.kind = Op::GEMM_TILE64; break;
+      case GV_TILE32: g.kind = Op::GEMM_TILE32; break;
+      case GV_WARP: g.kind = Op::GEMM_WARP; break;
+      case GV_TILE128: g.kind = Op::GEMM_TILE128; break;
+      case GV_DOT: g.kind = Op::GEMM_DOT; break;
+      default: break;
+    }
+    g.tuned = forced != GV_AUTO;
     // Tensor cores for dense c64 steps; also for a small output side with a long K, where the padded
     // tile wastes MMA work but the K split (below) still fills the GPU.
     if (g.kind == Op::GEMM_DOT && k >= 16384) {
@@ -628,11 +655,26 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     // products per complex MAC are useful, still several times the FP32 SIMT rate.  (Holding the
     // mid-size ones back for the SIMT kernels measured slower on the many-network batch.)
     const u64 kc = (k + 1) / 2;
-    const bool real_tc = (opt_.precision == PREC_TF32X3 || bf16) && dt == DT_F32 && kc >= 32 &&
-                         ((m >= 96 && n >= 96) || (std::min(m, n) >= 16 && kc >= 256));
-    const bool use_tc = real_tc || ((opt_.precision == PREC_TF32X3 || bf16) && dt == DT_C64 &&
-                        ((k >= 32 && ((m >= 96 && n >= 96) || (std::min(m, n) >= 16 && k >= 256))) ||
-                         (k >= 16 && m >= 96 && n >= 96 && (ph2 || tc_tiles >= (u64)kNumSMs))));
+    bool real_tc = (opt_.precision == PREC_TF32X3 || bf16) && dt == DT_F32 && kc >= 32 &&
+                   ((m >= 96 && n >= 96) || (std::min(m, n) >= 16 && kc >= 256));
+    if (forced != GV_AUTO) real_tc = false;  // set again below when the pinned variant is a tensor-core one
+    const bool heuristic_tc = real_tc || ((opt_.precision == PREC_TF32X3 || bf16) && dt == DT_C64 &&
+                              ((k >= 32 && ((m >= 96 && n >= 96) || (std::min(m, n) >= 16 && k >= 256))) ||
+                               (k >= 16 && m >= 96 && n >= 96 && (ph2 || tc_tiles >= (u64)kNumSMs))));
+    const bool use_tc = forced == GV_AUTO ? heuristic_tc : forced_tc;
+    if (forced_tc && dt == DT_F32) real_tc = true;  // a pinned tensor-core variant of a float32 step folds K
+    g.variant = forced != GV_AUTO ? forced : GV_AUTO;
+    if (!use_tc && g.variant == GV_AUTO) {
+      switch (g.kind) {
+        case Op::GEMM_SMALL: g.variant = GV_SMALL; break;
+        case Op::GEMM_TILE64: g.variant = GV_TILE64; break;
+        case Op::GEMM_TILE32: g.variant = GV_TILE32; break;
+        case Op::GEMM_WARP: g.variant = GV_WARP; break;
+        case Op::GEMM_TILE128: g.variant = GV_TILE128; break;
+        case Op::GEMM_DOT: g.variant = GV_DOT; break;
+        default: break;
+      }
+    }
     if (use_tc) {
       const ll kt_el = bf16 ? 2 * tc::BK : tc::BK;  // K per 64-byte packed row
       const ll el = bf16 ? 2 : 4;                  // bytes per plane element
@@ -736,6 +778,17 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         P.pk_tab[3] = tab_i32(chunks);
         P.pk_tab[4] = tab_i32(lane);
         P.pk_slice = (ll)bt * rpad * kpad;
+        // 16-byte stores need every chunk start 4-float aligned: tile bases (row / column tables at tile
+        // starts, batch table), chunk offsets inside a tile, and the slice stride (the plane stride is a
+        // multiple of it and the pack buffer is 256-byte aligned).
+        {
+          bool vec = P.pk_slice % 4 == 0;
+          for (ll r = 0; r < mp && vec; r += tc::BM) vec = ti[(size_t)r] % 4 == 0;
+          for (ll c = 0; c < np && vec; c += tc::BN) vec = tj[(size_t)c] % 4 == 0;
+          for (ll v : table(2, btp)) vec = vec && v % 4 == 0;
+          for (size_t q = 1; q < chunks.size() && vec; q += 2) vec = chunks[q] % 4 == 0;
+          P.pk_vec = vec;
+        }
         bufs[pbuf].first = std::min<u64>(bufs[pbuf].first, (u64)pi);
         P.c = Ref{};  // the plain result is never written
         bufs[X.ref.index].bytes = 0;
@@ -792,7 +845,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       int chunk = kt_total;
       if (opt_.tc_k_chunk) {
         chunk = (int)std::max<ll>(1, (ll)opt_.tc_k_chunk / kt_el);
-      } else if (!ph2) {
+      } else if ((forced == GV_AUTO && !ph2) || forced == GV_TC_SPLITK) {
         const ll ctas = (rpa / tc::BM) * (rpb / tc::BN) * (ll)bt;
         const ll want = std::min<ll>((2 * kNumSMs + ctas - 1) / ctas, kt_total / kMinSplitTiles);
         if (want >= 2) chunk = (int)((kt_total + want - 1) / want);
@@ -808,6 +861,9 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       g.kind = Op::GEMM_TC;
       g.bf16 = bf16;
       g.real = real_tc;
+      const ll mt = (ll)(m + tc::BM - 1) / tc::BM, nt = (ll)(n + tc::BN - 1) / tc::BN;
+      g.raster = forced == GV_TC_MFAST ? 1 : forced == GV_TC_NFAST ? 0 : -1;
+      if (g.variant == GV_AUTO) g.variant = g.splits > 1 ? GV_TC_SPLITK : (mt <= nt ? GV_TC_MFAST : GV_TC_NFAST);
       g.a = Ref{Ref::WS, pa};
       g.b = Ref{Ref::WS, pb};
       if (real_tc)  // the complex product lands in a scratch buffer; a gather keeps its real part
@@ -1742,6 +1798,7 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
     for (int q = 0; q < 5; ++q) args.pk_qbeg[q] = op.pk_qbeg[q];
     args.pk_slice = op.pk_slice;
     args.pk_plane = s_eff * op.pk_slice;
+    args.pk_vec = op.pk_vec && ((uintptr_t)PK & 15) == 0 ? 1 : 0;
   }
   const ll zc = s_eff * op.bt;
   args.zc = (int)zc;
@@ -1752,7 +1809,7 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   // The smaller operand's tiles run fastest, so it stays in L2 while the larger one streams once.
   const ll mt = (op.m + tc::BM - 1) / tc::BM, nt = (op.n + tc::BN - 1) / tc::BN;
   args.m_tiles = (int)mt;
-  args.m_fast = mt <= nt ? 1 : 0;
+  args.m_fast = op.raster >= 0 ? op.raster : (mt <= nt ? 1 : 0);
   const ll items = mt * nt * zc * op.splits;
   if (items > 0x7FFFFFFFll) throw Error(E_UNSUPPORTED, "tensor-core GEMM work items exceed 2^31");
   args.tiles = (int)(mt * nt);
@@ -2238,6 +2295,27 @@ void Program::execute_gradient(int part, const void* const* inputs, const void* 
   grads_ = nullptr;
 }
 
+const char* gemm_variant_name(int v) {
+  static const char* names[GV_COUNT] = {"auto", "simt_small", "simt_tile64", "simt_tile32", "simt_warp",
+                                        "simt_tile128", "simt_dot", "tc_mfast", "tc_nfast", "tc_splitk"};
+  return v >= 0 && v < GV_COUNT ? names[v] : "?";
+}
+
+std::vector<Program::GemmChoice> Program::gemm_choices() const {
+  std::vector<GemmChoice> out;
+  for (size_t i = 0; i < ops_.size(); ++i) {
+    const Op& op = ops_[i];
+    switch (op.kind) {
+      case Op::GEMM_SMALL: case Op::GEMM_TILE64: case Op::GEMM_TILE32: case Op::GEMM_DOT: case Op::GEMM_TC:
+      case Op::GEMM_WARP: case Op::GEMM_TILE128:
+        out.push_back(GemmChoice{op.key, op.variant, op.tuned, i});
+        break;
+      default: break;
+    }
+  }
+  return out;
+}
+
 std::string Program::describe() const {
   static const char* names[] = {"gather",    "gemm_small", "gemm_tile64", "gemm_tile32", "slice_accumulate",
                                 "slice_output", "memset",  "maxabs",      "strip",       "gemm_tc",
@@ -2259,6 +2337,7 @@ std::string Program::describe() const {
     const Op& op = ops_[i];
     s += std::string(i ? "," : "") + "{\"kind\":\"" + names[(int)op.kind] + "\"" + (op.bwd ? ",\"bwd\":1" : "");
     auto f = [&](const char* k, long long v) { s += std::string(",\"") + k + "\":" + std::to_string(v); };
+    if (op.gemm >= 0) f("gemm", op.gemm);  // the GEMM (numbered in emit order) this op runs or serves
     // operands: reference kind (1 input, 2 workspace, 3 output, 4 grad_output, 5 grads) and index / offset
     f("a_kind", (long long)op.a.kind); f("a", (long long)op.a.index);
     if (op.b.kind != Ref::NONE) { f("b_kind", (long long)op.b.kind); f("b", (long long)op.b.index); }
@@ -2268,8 +2347,11 @@ std::string Program::describe() const {
       case Op::GEMM_WARP: case Op::GEMM_TILE128:
         f("S", op.S); f("bt", op.bt); f("m", op.m); f("k", op.k); f("n", op.n);
         f("splits", op.splits); f("conj_a", op.conj_a); f("conj_b", op.conj_b);
-        if (op.pk.kind != Ref::NONE) f("pack_into", (long long)op.pk.index);
+        if (op.pk.kind != Ref::NONE) { f("pack_into", (long long)op.pk.index); f("pack_vec", op.pk_vec ? 1 : 0); }
         if (op.kind == Op::GEMM_TC) { f("bf16", op.bf16); f("real", op.real); }
+        s += std::string(",\"variant\":\"") + gemm_variant_name(op.variant) + "\"";
+        f("tuned", op.tuned ? 1 : 0);
+        f("phase", op.key.phase); f("a_var", op.key.a_var); f("b_var", op.key.b_var);
         break;
       case Op::PACK: case Op::PACK_TILED:
         f("S", op.a_var ? op.S : 1); f("bt", op.bt); f("rows", op.rows); f("cols", op.cols); f("rpad", op.rpad);

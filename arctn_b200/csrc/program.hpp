@@ -8,8 +8,10 @@
 
 #include <cuda_runtime.h>
 
+#include <map>
 #include <mutex>
 #include <set>
+#include <tuple>
 
 #include "host.hpp"
 #include "kernels.cuh"
@@ -19,7 +21,24 @@ namespace ab2 {
 enum : int { DT_F32 = 0, DT_F64 = 1, DT_C64 = 2, DT_C128 = 3 };
 enum : int { PREC_FP32 = 0, PREC_TF32X3 = 1, PREC_BF16X3 = 2 };
 
+// GEMM kernel variants a tuning table can pin per GEMM shape (the values of ARCTN_B200_GEMM_*).
+enum : int {
+  GV_AUTO = 0, GV_SMALL = 1, GV_TILE64 = 2, GV_TILE32 = 3, GV_WARP = 4, GV_TILE128 = 5, GV_DOT = 6,
+  GV_TC_MFAST = 7, GV_TC_NFAST = 8, GV_TC_SPLITK = 9, GV_COUNT = 10
+};
+// A GEMM's shape key: element type, precision, phase (1: slice-invariant, run once; 2: run per slice group),
+// which operands vary per slice, and gemm_dims (bt, m, k, n) of one slice.
+struct GemmKey {
+  int dtype = 0, precision = 0, phase = 1, a_var = 0, b_var = 0;
+  u64 bt = 1, m = 1, k = 1, n = 1;
+  bool operator<(const GemmKey& o) const {
+    return std::tie(dtype, precision, phase, a_var, b_var, bt, m, k, n) <
+           std::tie(o.dtype, o.precision, o.phase, o.a_var, o.b_var, o.bt, o.m, o.k, o.n);
+  }
+};
+
 size_t dtype_bytes(int dt);
+const char* gemm_variant_name(int v);  // "simt_tile64", "tc_mfast", ...
 inline bool dtype_complex(int dt) { return dt == DT_C64 || dt == DT_C128; }
 
 constexpr u64 kDefaultBudget = 8ull << 30;  // workspace budget when the caller gives none
@@ -34,6 +53,7 @@ struct ProgramOptions {
   u64 slice_begin = 0, slice_end = 0;  // both 0: every slice
   bool gradient = false;               // also build the adjoint (reverse) sweep
   u64 tc_k_chunk = 0;                  // tf32x3: K per CTA before a split-K reduce (multiple of 16); 0: auto
+  std::map<GemmKey, int> tuning;       // GEMM shape -> GV_* variant (an autotuner's table); others: heuristics
 };
 
 // Where an operand lives at run time.
@@ -63,6 +83,12 @@ struct Op {
   ll tile_T = 0, n_outer = 0;           // PACK_TILED: tile size and number of outer leg combinations
   int splits = 1;                       // GEMM_TC: K splits (partials in `d`, summed in order into `c`)
   int kt_chunk = 0;
+  int raster = -1;                      // GEMM_TC tile order: 1 m-tiles fastest, 0 n-tiles fastest, -1 smaller side fastest
+  // GEMM kinds: the shape key, the variant that runs (never GV_AUTO) and whether a tuning table chose it.
+  GemmKey key;
+  int variant = GV_AUTO;
+  bool tuned = false;
+  int gemm = -1;                        // the GEMM (numbered in emit order) this op runs or serves; -1: none
   Ref d;                                // GEMM_TC: FP32 split-K partial buffer
   bool bwd = false;                     // part of the adjoint sweep (skipped by a plain execute)
   bool bf16 = false;                    // PACK / PACK_TILED / GEMM_TC / their MEMSET: split-BF16 planes
@@ -78,6 +104,7 @@ struct Op {
   u64 pk_tab[5] = {0, 0, 0, 0, 0};
   int pk_qbeg[5] = {0, 0, 0, 0, 0};     // chunk ranges per 32-row group of the tile
   ll pk_slice = 0;
+  bool pk_vec = false;                  // every packed chunk start is 16-byte aligned (vector stores)
 };
 
 class Program {
@@ -128,6 +155,9 @@ class Program {
   u64 n_inputs() const { return plan_.n_inputs; }
   // JSON description of the launch sequence and workspace layout (host-only; no GPU needed).
   std::string describe() const;
+  // Every GEMM op in launch order: its shape key, the variant it runs and whether the tuning table chose it.
+  struct GemmChoice { GemmKey key; int variant; bool tuned; size_t op; };
+  std::vector<GemmChoice> gemm_choices() const;
 
   // Hooks for the batch interpreter (interp.cuh).  Ops of the main sequence by index: whether `part`
   // runs op i, its dependencies (earlier ops touching its memory), whether the interpreter can run it

@@ -216,6 +216,10 @@ struct TcArgs {
   const int* pk_lane = nullptr;
   int pk_qbeg[5] = {0, 0, 0, 0, 0};
   ll pk_plane = 0, pk_slice = 0;
+  // Every packed offset a tile's chunks start at, the tile bases, the slice and plane strides and the pack's
+  // address are multiples of 4 floats: a quarter-warp then stores one chunk with 16-byte stores (4 chunks
+  // per warp step, 4 stores per element quadruple instead of 16).
+  int pk_vec = 0;
 };
 
 #define AB2_TMEM_LD16(taddr, r)                                                                                   \
@@ -266,6 +270,7 @@ __device__ __forceinline__ EpiState epi_setup(const TcArgs& args, int ew, int la
   const int lp = __ldg(args.pk_lane + lane);
   st.dr = lp >> 16;
   st.dc = lp & 0xFFFF;
+
   int most = 0;
 #pragma unroll
   for (int q = 0; q < BM / kStageRows; ++q) most = max(most, args.pk_qbeg[q + 1] - args.pk_qbeg[q]);
@@ -294,7 +299,7 @@ __device__ __forceinline__ EpiTile epi_tile(const TcArgs& args, int z, int split
   EpiTile t;
   if (args.pk) {
     t.p0 = args.pk + (ll)(z / args.bt) * args.pk_slice + __ldg(args.pk_b + z % args.bt) + __ldg(args.pk_i + row0) +
-           __ldg(args.pk_j + col0) + lane;
+           __ldg(args.pk_j + col0) + (args.pk_vec ? (lane & 7) * 4 : lane);
     t.p1 = t.p0 + args.pk_plane;
     t.p2 = t.p1 + args.pk_plane;
     t.p3 = t.p2 + args.pk_plane;
@@ -318,7 +323,57 @@ __device__ __forceinline__ void store_pass(const TcArgs& args, const EpiState& e
                                            int q, int rows, int cols, int et) {
   const int r_lo = q * kStageRows;
   if (r_lo >= rows) return;
-  if (args.pk) {
+  if (args.pk && args.pk_vec) {
+    // Quarter-warp g = lane / 8 takes chunk k0 + g of this warp's list; its lane stores floats 4 (lane % 8) ..
+    // + 3 of the chunk: the four elements are read from staging, split, and written as one float4 per plane.
+    const int lane = threadIdx.x & 31, g = lane >> 3;
+    // (dr << 16 | dc) of chunk elements 4 (lane % 8) .. + 3, read per pass (L1-resident) so that the drain
+    // warps, which hold a tile of accumulators meanwhile, keep no extra registers across passes
+    const int4 vq = __ldg(reinterpret_cast<const int4*>(args.pk_lane) + (lane & 7));
+    const int vp[4] = {vq.x, vq.y, vq.z, vq.w};
+    for (int k0 = 0; k0 < es.kq; k0 += 4) {
+      const int kk = k0 + g, slot = q * es.kq + kk;
+      const int x0 = __shfl_sync(0xffffffffu, es.e0.x, slot & 31), y0 = __shfl_sync(0xffffffffu, es.e0.y, slot & 31);
+      const int x1 = __shfl_sync(0xffffffffu, es.e1.x, slot & 31), y1 = __shfl_sync(0xffffffffu, es.e1.y, slot & 31);
+      int cx = slot < 32 ? x0 : x1;
+      const int cy = slot < 32 ? y0 : y1;
+      if (kk >= es.kq) cx = 0x7FFF0000;
+      const int rb = cx >> 16, cb = cx & 0xFFFF;
+      cf32 v[4];
+      bool in[4], all = true, any = false;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int r = rb + (vp[i] >> 16), c = cb + (vp[i] & 0xFFFF);
+        in[i] = r < rows && c < cols;
+        all = all && in[i];
+        any = any || in[i];
+        v[i] = in[i] ? stage[stage_at(r - r_lo, c)] : cf32{0.f, 0.f};
+      }
+      if (all) {
+#pragma unroll
+        for (int part = 0; part < 2; ++part) {  // real parts to planes 0 / 1, then imaginary parts to 2 / 3
+          float4 h, l;
+          float* hp = &h.x;
+          float* lp = &l.x;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const uint32_t b = __float_as_uint(part ? v[i].im : v[i].re), th = tf32_round(b);
+            hp[i] = __uint_as_float(th);
+            lp[i] = __uint_as_float(tf32_round(tf32_residual(b, th)));
+          }
+          *reinterpret_cast<float4*>((part ? t.p2 : t.p0) + cy) = h;
+          *reinterpret_cast<float4*>((part ? t.p3 : t.p1) + cy) = l;
+        }
+      } else if (any) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if (!in[i]) continue;
+          put_pair(t.p0, t.p1, cy + i, v[i].re);
+          put_pair(t.p2, t.p3, cy + i, v[i].im);
+        }
+      }
+    }
+  } else if (args.pk) {
     constexpr int U = 4;
     for (int k0 = 0; k0 < es.kq; k0 += U) {
       int2 ch[U];

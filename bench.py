@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--group", type=int, default=0, help="slices per group (0: as many as the workspace allows)")
     ap.add_argument("--workspace-gb", type=float, default=24.0)
     ap.add_argument("--tc-k-chunk", type=int, default=0, help="K per tensor-core accumulator (0: library default)")
+    ap.add_argument("--no-tune", action="store_true", help="keep the built-in GEMM heuristics (skip the autotuner)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, the FP32 comparison and the FP64 check")
@@ -732,7 +733,32 @@ def main():
                   max_slices_per_group=args.group, tc_k_chunk=args.tc_k_chunk)
     if world > 1:
         common.update(slice_begin=begin, slice_end=end)
-    prog = A.SlicedProgram(*net.as_tuple(), path, sliced, precision=args.precision, **common)
+    # The GEMM autotuner times every kernel variant on every GEMM shape of the program (standalone, before
+    # anything is timed) and pins the fastest; the table also serves the FP32 form below.
+    tuning, tune_info = None, None
+    if not args.no_tune:
+        t0 = time.perf_counter()
+        tuning = A.autotune(*net.as_tuple(), path, sliced, precision=args.precision, **common)
+        tune_info = {"tune_s": round(time.perf_counter() - t0, 1), "gemm_shapes": len(tuning)}
+    prog = A.SlicedProgram(*net.as_tuple(), path, sliced, precision=args.precision, tuning=tuning, **common)
+    if tuning is not None:
+        from arctn_b200 import tuning as T
+
+        changed = [k for k in tuning.keys() if tuning.get(k) != tuning.timings(k).get("heuristic")]
+        tune_info["changed_from_heuristic"] = len(changed)
+        seen, picks = set(), []
+        for g in prog.gemms():
+            k = T.key_of(g)
+            if k not in seen and g["bt"] * g["m"] * g["k"] * g["n"] >= 1 << 24:
+                seen.add(k)
+                picks.append({"bt_m_k_n": [g["bt"], g["m"], g["k"], g["n"]], "variant": g["variant"],
+                              "heuristic": tuning.timings(k).get("heuristic"),
+                              "ms": {v: (round(t, 4) if t is not None else None)
+                                     for v, t in tuning.timings(k).items() if v in T.VARIANT_CODES},
+                              "whole_program_ms": tuning.timings(k).get("whole_program_ms")})
+        tune_info["program_ms"] = {"heuristics": tuning.meta.get("program_ms_before"),
+                                   "tuned": tuning.meta.get("program_ms_after")}
+        tune_info["large_gemms"] = picks
     x = [torch.from_numpy(a).to(dev) for a in arrays]
     ws = torch.empty(max(prog.workspace_bytes, 1), dtype=torch.uint8, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -772,7 +798,9 @@ def main():
                "h2d_bytes_per_step": int(sum(a.nbytes for a in host_in)), "d2h_bytes_per_step": int(res.nbytes)}
         # The plain FP32 GPU form on the same workload, and both results against an FP64 contraction.
         other = "fp32" if args.precision == "tf32x3" else "tf32x3"
-        prog2 = A.SlicedProgram(*net.as_tuple(), path, sliced, precision=other, **common)
+        t2 = A.autotune(*net.as_tuple(), path, sliced, precision=other, table=tuning, **common) \
+            if tuning is not None else None
+        prog2 = A.SlicedProgram(*net.as_tuple(), path, sliced, precision=other, tuning=t2, **common)
         ws2 = torch.empty(max(prog2.workspace_bytes, 1), dtype=torch.uint8, device=dev)
         ms2, r2, _ = timed(prog2, x, ws2, stream, max(1, min(args.steps, 2)), 1, None, dev, flush)
         del ws2, prog2
@@ -799,7 +827,7 @@ def main():
         t_or = time.perf_counter() - t0
         rs = dict(common)
         rs.update(slice_begin=0, slice_end=samp)
-        ps = A.SlicedProgram(*net.as_tuple(), path, sliced, precision=args.precision, **rs)
+        ps = A.SlicedProgram(*net.as_tuple(), path, sliced, precision=args.precision, tuning=tuning, **rs)
         got = complex(ps.execute(x, f64_out=True, stream=stream).item())
         del ps
         extras["oracle_sample"] = {"slices": [0, samp], "rel_err": abs(got - want) / abs(want),
@@ -874,7 +902,7 @@ def main():
                            "target_size": 2 ** args.target_log2, "n_slices": total,
                            "slices_per_group": prog.slices_per_group, "precision": args.precision,
                            "cross_slice_sum": "fp64", "l2": "flushed (256 MiB write) between timed iterations",
-                           "parallelism": f"slice-sharded x{world}"},
+                           "parallelism": f"slice-sharded x{world}", "tuning": tune_info},
                 "gpu_launches": prog.launches * args.steps, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu,
                 "clocks": clocks, "device_status": status, "workspace_bytes": int(prog.workspace_bytes),
                 "result": [float(r.real), float(r.imag)]}

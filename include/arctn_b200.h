@@ -202,6 +202,43 @@ typedef struct {
 int arctn_b200_program_create(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
                               uint64_t n_sliced, const uint32_t* sliced_legs,
                               const arctn_b200_program_options* options, arctn_b200_program** program_out);
+/* GEMM kernel variants.  A program picks one per GEMM from its shape with built-in heuristics; a tuning
+ * table (arctn_b200_program_create_tuned) pins the variant per shape instead.  The reference runs every GEMM
+ * through matrixmultiply's cgemm/zgemm/sgemm/dgemm (src/tensor.rs:49-64,193-231,270-308); it has no
+ * variants and no tuner. */
+enum {
+  ARCTN_B200_GEMM_AUTO = 0,        /* the built-in heuristics */
+  ARCTN_B200_GEMM_SIMT_SMALL = 1,  /* one thread per output, serial K (CUDA cores) */
+  ARCTN_B200_GEMM_SIMT_TILE64 = 2, /* 64 x 64 output tile per CTA (CUDA cores) */
+  ARCTN_B200_GEMM_SIMT_TILE32 = 3, /* 32 x 32 output tile per CTA (CUDA cores) */
+  ARCTN_B200_GEMM_SIMT_WARP = 4,   /* one warp per output, lanes split K (CUDA cores) */
+  ARCTN_B200_GEMM_SIMT_TILE128 = 5,/* 128 x 128 output tile per CTA, float32 only (CUDA cores) */
+  ARCTN_B200_GEMM_SIMT_DOT = 6,    /* one CTA per output (split over CTAs when K >= 16384) */
+  ARCTN_B200_GEMM_TC_MFAST = 7,    /* tcgen05 tensor-core GEMM, output tiles walked with m fastest, K unsplit */
+  ARCTN_B200_GEMM_TC_NFAST = 8,    /* the same, n fastest */
+  ARCTN_B200_GEMM_TC_SPLITK = 9    /* the same, K split across CTAs to cover the SMs twice (FP64 split sum) */
+};
+/* One GEMM shape and its variant.  phase: 1 for a slice-invariant GEMM (run once per execute), 2 for one run
+ * per slice group; a_var / b_var: whether that operand differs per slice; bt, m, k, n: gemm_dims() of one
+ * slice (src/compiled.rs:138-141).  The tensor-core variants need precision TF32X3 or BF16X3 and a C64 or
+ * F32 network; SIMT_TILE128 needs F32. */
+typedef struct {
+  int dtype, precision, phase, a_var, b_var, variant;
+  uint64_t bt, m, k, n;
+} arctn_b200_gemm_choice;
+
+/* arctn_b200_program_create with a tuning table: every GEMM whose shape key (all fields but variant) matches
+ * an entry runs that entry's variant; the others keep the heuristics.  An entry naming a variant the
+ * program's dtype or precision cannot run is rejected (ARCTN_B200_ERR_INVALID).  No reference counterpart. */
+int arctn_b200_program_create_tuned(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
+                                    uint64_t n_sliced, const uint32_t* sliced_legs,
+                                    const arctn_b200_program_options* options, const arctn_b200_gemm_choice* table,
+                                    uint64_t n_table, arctn_b200_program** program_out);
+/* The program's GEMMs in launch order (a per-slice GEMM once per slice group): shape key and the variant it
+ * runs (never AUTO); tuned_out[i] = 1 where a table entry chose it.  Writes at most cap entries (tuned_out
+ * may be null); *n_out = the full count.  Host-only.  No reference counterpart. */
+int arctn_b200_program_gemms(const arctn_b200_program* program, arctn_b200_gemm_choice* out, int* tuned_out,
+                             uint64_t cap, uint64_t* n_out);
 void arctn_b200_program_destroy(arctn_b200_program* program);
 uint64_t arctn_b200_program_workspace_size(const arctn_b200_program* program);
 uint64_t arctn_b200_program_n_slices(const arctn_b200_program* program);
