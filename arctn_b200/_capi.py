@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libarctn_b200.so")
 
 OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED, ERR_DEVICE_TIMEOUT, ERR_WORKSPACE = range(6)
 F32, F64, C64, C128 = range(4)
-PREC_FP32, PREC_TF32X3, PREC_BF16X3 = 0, 1, 2
+PREC_FP32, PREC_TF32X3, PREC_BF16X3, PREC_BF16X6 = 0, 1, 2, 3
 
 u64 = ctypes.c_uint64
 u32 = ctypes.c_uint32

@@ -32,7 +32,7 @@ from . import _capi as C
 
 _NP_CODES = {np.dtype(np.float32): C.F32, np.dtype(np.float64): C.F64, np.dtype(np.complex64): C.C64,
              np.dtype(np.complex128): C.C128}
-_PRECISIONS = {"fp32": C.PREC_FP32, "tf32x3": C.PREC_TF32X3, "bf16x3": C.PREC_BF16X3}
+_PRECISIONS = {"fp32": C.PREC_FP32, "tf32x3": C.PREC_TF32X3, "bf16x3": C.PREC_BF16X3, "bf16x6": C.PREC_BF16X6}
 
 
 def _torch():

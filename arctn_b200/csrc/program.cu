@@ -120,9 +120,10 @@ void pick(const View& v, const std::vector<size_t>& axes, std::vector<u64>& dims
 Program::Program(const Network& net, const SsaPath& path, const std::vector<Leg>& sliced, const ProgramOptions& opt)
     : opt_(opt) {
   dtype_bytes(opt_.dtype);
-  if (opt_.precision != PREC_FP32 && opt_.precision != PREC_TF32X3 && opt_.precision != PREC_BF16X3)
+  if (opt_.precision != PREC_FP32 && opt_.precision != PREC_TF32X3 && opt_.precision != PREC_BF16X3 &&
+      opt_.precision != PREC_BF16X6)
     throw Error(E_INVALID, "unsupported precision mode " + std::to_string(opt_.precision));
-  const u64 k_unit = opt_.precision == PREC_BF16X3 ? 2 * tc::BK : tc::BK;  // K per packed 64-byte row
+  const u64 k_unit = opt_.precision == PREC_BF16X3 || opt_.precision == PREC_BF16X6 ? 2 * tc::BK : tc::BK;
   if (opt_.tc_k_chunk % k_unit != 0 || opt_.tc_k_chunk > (1ull << 30))
     throw Error(E_INVALID, "tc_k_chunk must be a multiple of " + std::to_string(k_unit) + " (0 for the default)");
   build(net, path, sliced);
@@ -612,14 +613,14 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     // A tuning table entry for this shape replaces the heuristic choice (SIMT kind, or the tensor core with
     // a given tile order / K split); the entry must name a variant this dtype and precision can run.
     g.key = GemmKey{dt, opt_.precision, ph2 ? 2 : 1, A.variant ? 1 : 0, B.variant ? 1 : 0, bt, m, k, n};
-    const bool tc_allowed = (opt_.precision == PREC_TF32X3 || opt_.precision == PREC_BF16X3) &&
-                            (dt == DT_C64 || dt == DT_F32);
+    const bool tc_allowed = (opt_.precision == PREC_TF32X3 || opt_.precision == PREC_BF16X3 ||
+                             opt_.precision == PREC_BF16X6) && (dt == DT_C64 || dt == DT_F32);
     int forced = GV_AUTO;
     if (auto it = opt_.tuning.find(g.key); it != opt_.tuning.end()) forced = it->second;
     const bool forced_tc = forced == GV_TC_MFAST || forced == GV_TC_NFAST || forced == GV_TC_SPLITK;
     if (forced_tc && !tc_allowed)
-      throw Error(E_INVALID, "tuning entry asks for the tensor-core GEMM, which needs precision tf32x3 or bf16x3 "
-                             "and a float32 or complex64 network");
+      throw Error(E_INVALID, "tuning entry asks for the tensor-core GEMM, which needs precision tf32x3, bf16x3 or "
+                             "bf16x6 and a float32 or complex64 network");
     if (forced == GV_TILE128 && dt != DT_F32) throw Error(E_INVALID, "tuning entry asks for the 128 x 128 tile, "
                                                                      "which is float32 only");
     switch (forced) {
@@ -650,7 +651,9 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     // A single 16-wide K tile (no K split possible) only pays once the slice group or the batch gives
     // every SM an output tile; its epilogue can then write the next GEMM's packed operand directly.
     const u64 tc_tiles = ((m + tc::BM - 1) / tc::BM) * ((n + tc::BN - 1) / tc::BN) * bt;
-    const bool bf16 = opt_.precision == PREC_BF16X3;
+    const bool six = opt_.precision == PREC_BF16X6;
+    const bool bf16 = opt_.precision == PREC_BF16X3 || six;
+    const ll planes = six ? 6 : tc::PLANES;  // planes per packed operand
     // Real float32 steps use the same complex kernel on half the K (Op::real): two of its four real
     // products per complex MAC are useful, still several times the FP32 SIMT rate.  (Holding the
     // mid-size ones back for the SIMT kernels measured slower on the many-network batch.)
@@ -795,11 +798,12 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         return true;
       };
       auto pack = [&](const Operand& X, ll rows, ll rpad, bool conj) {
-        const u64 pbuf = new_buf(ph2, (u64)(tc::PLANES * (ll)bt * rpad * kpad * el), opidx(ph2));
+        const u64 pbuf = new_buf(ph2, (u64)(planes * (ll)bt * rpad * kpad * el), opidx(ph2));
         bufs[pbuf].fixed = ph2 && !X.variant;
         if (fuse_into_producer(X, rows, rpad, conj, pbuf)) return pbuf;
         Op p{Op::PACK};
         p.bf16 = bf16;
+        p.six = six;
         p.a = X.ref;
         p.sa = X.so;
         p.c = Ref{Ref::WS, pbuf};
@@ -824,6 +828,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
             z.bt = (ll)bt;
             z.a_var = X.variant;
             z.bf16 = bf16;
+            z.six = six;
             emit(ph2, z, fwd);
           }
         } else {
@@ -860,6 +865,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       }
       g.kind = Op::GEMM_TC;
       g.bf16 = bf16;
+      g.six = six;
       g.real = real_tc;
       const ll mt = (ll)(m + tc::BM - 1) / tc::BM, nt = (ll)(n + tc::BN - 1) / tc::BN;
       g.raster = forced == GV_TC_MFAST ? 1 : forced == GV_TC_NFAST ? 0 : -1;
@@ -1710,35 +1716,35 @@ CUtensorMap plane_map(void* base, ll kpad, ll rows, ll zplanes, bool bf16) {
   return m;
 }
 
+// Calls f with a value of the plane element type of op's packs: float (split-TF32), __nv_bfloat16 (split-BF16)
+// or tc::bf16p3 (three BF16 pieces).
+template <class Fn>
+void with_plane_type(const Op& op, Fn&& f) {
+  if (op.six) f(tc::bf16p3{});
+  else if (op.bf16) f(__nv_bfloat16{});
+  else f(0.f);
+}
+
 void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const char* tab, int* err,
                cudaStream_t st) {
   if (op.kind == Op::PACK) {
     const ll Z = (op.a_var ? op.S : 1) * op.bt;
     const ll tiles = Z * (op.rpad / 32) * ((op.kpad + 31) / 32);
     const int grid = (int)std::min<ll>(tiles, 148 * 16);
-    if (op.real) {
-      auto args = std::make_tuple((const float*)A, (const ll*)(tab + op.tab[0]), (const ll*)(tab + op.tab[1]),
-                                  (const ll*)(tab + op.tab[2]));
-      if (op.bf16)
-        tc::k_pack_planar_real<__nv_bfloat16><<<grid, 256, 0, st>>>(
-            std::get<0>(args), (__nv_bfloat16*)C, std::get<1>(args), std::get<2>(args), std::get<3>(args), op.bt,
-            op.rows, op.cols, op.kfull, op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0, op.conj_a ? 1 : 0);
+    const ll* t0 = (const ll*)(tab + op.tab[0]);
+    const ll* t1 = (const ll*)(tab + op.tab[1]);
+    const ll* t2 = (const ll*)(tab + op.tab[2]);
+    with_plane_type(op, [&](auto tag) {
+      using PT = decltype(tag);
+      if (op.real)
+        tc::k_pack_planar_real<PT><<<grid, 256, 0, st>>>((const float*)A, (PT*)C, t0, t1, t2, op.bt, op.rows, op.cols,
+                                                         op.kfull, op.rpad, op.kpad, Z, op.sa, op.g0,
+                                                         op.b_var ? 1 : 0, op.conj_a ? 1 : 0);
       else
-        tc::k_pack_planar_real<float><<<grid, 256, 0, st>>>(
-            std::get<0>(args), (float*)C, std::get<1>(args), std::get<2>(args), std::get<3>(args), op.bt, op.rows,
-            op.cols, op.kfull, op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0, op.conj_a ? 1 : 0);
-      return;
-    }
-    if (op.bf16)
-      tc::k_pack_planar<__nv_bfloat16><<<grid, 256, 0, st>>>(
-          (const cf32*)A, (__nv_bfloat16*)C, (const ll*)(tab + op.tab[0]), (const ll*)(tab + op.tab[1]),
-          (const ll*)(tab + op.tab[2]), op.bt, op.rows, op.cols, op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0,
-          op.conj_a ? 1 : 0);
-    else
-      tc::k_pack_planar<float><<<grid, 256, 0, st>>>(
-          (const cf32*)A, (float*)C, (const ll*)(tab + op.tab[0]), (const ll*)(tab + op.tab[1]),
-          (const ll*)(tab + op.tab[2]), op.bt, op.rows, op.cols, op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0,
-          op.conj_a ? 1 : 0);
+        tc::k_pack_planar<PT><<<grid, 256, 0, st>>>((const cf32*)A, (PT*)C, t0, t1, t2, op.bt, op.rows, op.cols,
+                                                    op.rpad, op.kpad, Z, op.sa, op.g0, op.b_var ? 1 : 0,
+                                                    op.conj_a ? 1 : 0);
+    });
     return;
   }
   if (op.kind == Op::PACK_TILED) {
@@ -1746,24 +1752,25 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
     const ll slice_stride = op.bt * op.rpad * op.kpad;
     const ll plane = n_slices * slice_stride;
     const int grid = (int)std::min<ll>(op.n_outer * n_slices, 148 * 6);
-    if (op.bf16)
-      tc::k_pack_tiled<__nv_bfloat16><<<grid, tc::kPackThreads, 0, st>>>(
-          (const cf32*)A, (__nv_bfloat16*)C, (const int*)(tab + op.tab[0]), (const int*)(tab + op.tab[1]),
+    with_plane_type(op, [&](auto tag) {
+      using PT = decltype(tag);
+      tc::k_pack_tiled<PT><<<grid, tc::kPackThreads, 0, st>>>(
+          (const cf32*)A, (PT*)C, (const int*)(tab + op.tab[0]), (const int*)(tab + op.tab[1]),
           (const int*)(tab + op.tab[2]), (int)op.tile_T, (const ll*)(tab + op.tab[4]), (const ll*)(tab + op.tab[5]),
           op.n_outer, n_slices, slice_stride, plane, op.sa, op.g0, op.conj_a ? 1 : 0);
-    else
-      tc::k_pack_tiled<float><<<grid, tc::kPackThreads, 0, st>>>(
-          (const cf32*)A, (float*)C, (const int*)(tab + op.tab[0]), (const int*)(tab + op.tab[1]),
-          (const int*)(tab + op.tab[2]), (int)op.tile_T, (const ll*)(tab + op.tab[4]), (const ll*)(tab + op.tab[5]),
-          op.n_outer, n_slices, slice_stride, plane, op.sa, op.g0, op.conj_a ? 1 : 0);
+    });
     return;
   }
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
-    for (auto kern : {tc::k_tc_cgemm_tf32x3, tc::k_tc_cgemm_bf16x3}) {
-      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    const std::pair<decltype(&tc::k_tc_cgemm_tf32x3), int> kerns[3] = {
+        {tc::k_tc_cgemm_tf32x3, tc::Fmt<tc::FMT_TF32X3>::kSmemBytes},
+        {tc::k_tc_cgemm_bf16x3, tc::Fmt<tc::FMT_BF16X3>::kSmemBytes},
+        {tc::k_tc_cgemm_bf16x6, tc::Fmt<tc::FMT_BF16X6>::kSmemBytes}};
+    for (auto [kern, smem] : kerns) {
+      CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       // The kernel's setmaxnreg split assumes exactly kLaunchRegs registers a thread at launch.
       cudaFuncAttributes fa{};
       CK(cudaFuncGetAttributes(&fa, kern));
@@ -1775,8 +1782,9 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   }
   const ll s_eff = (op.a_var || op.b_var) ? op.S : 1;
   const ll za = (op.a_var ? op.S : 1) * op.bt, zb = (op.b_var ? op.S : 1) * op.bt;
-  const CUtensorMap ma = plane_map(A, op.kpad, op.rpad, tc::PLANES * za, op.bf16);
-  const CUtensorMap mb = plane_map(B, op.kpad, op.rpad_b, tc::PLANES * zb, op.bf16);
+  const ll planes = op.six ? 6 : tc::PLANES;
+  const CUtensorMap ma = plane_map(A, op.kpad, op.rpad, planes * za, op.bf16);
+  const CUtensorMap mb = plane_map(B, op.kpad, op.rpad_b, planes * zb, op.bf16);
   tc::TcArgs args;
   args.C = (cf32*)C;
   args.m = op.m;
@@ -1817,10 +1825,13 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   static int sms[64] = {};
   if (dev < 64 && !sms[dev]) CK(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
   const int n_sm = dev < 64 ? sms[dev] : 148;
-  if (op.bf16)
-    tc::k_tc_cgemm_bf16x3<<<(unsigned)std::min<ll>(items, n_sm), tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
+  const unsigned grid = (unsigned)std::min<ll>(items, n_sm);
+  if (op.six)
+    tc::k_tc_cgemm_bf16x6<<<grid, tc::kThreads, tc::Fmt<tc::FMT_BF16X6>::kSmemBytes, st>>>(ma, mb, args);
+  else if (op.bf16)
+    tc::k_tc_cgemm_bf16x3<<<grid, tc::kThreads, tc::Fmt<tc::FMT_BF16X3>::kSmemBytes, st>>>(ma, mb, args);
   else
-    tc::k_tc_cgemm_tf32x3<<<(unsigned)std::min<ll>(items, n_sm), tc::kThreads, tc::SMEM_BYTES, st>>>(ma, mb, args);
+    tc::k_tc_cgemm_tf32x3<<<grid, tc::kThreads, tc::Fmt<tc::FMT_TF32X3>::kSmemBytes, st>>>(ma, mb, args);
   if (op.splits > 1) {
     const ll count = zc * op.m * op.n;
     tc::k_splitk_reduce<<<grid_for(count), 256, 0, st>>>((const cf32*)D, (cf32*)C, count, op.splits);
@@ -1843,7 +1854,7 @@ void Program::launch_op(const Op& op, const void* const* inputs, void* output, c
   if (op.kind == Op::MEMSET) {
     // bytes == 0: the padded planes of a tiled pack, [4 planes][slices of this group][bt][rpad][kpad] fp32
     const u64 bytes = op.bytes ? op.bytes
-                               : (u64)(tc::PLANES * (op.a_var ? op.S : 1) * op.bt * op.rpad * op.kpad * (op.bf16 ? 2 : 4));
+                               : (u64)((op.six ? 6 : tc::PLANES) * (op.a_var ? op.S : 1) * op.bt * op.rpad * op.kpad * (op.bf16 ? 2 : 4));
     CK(cudaMemsetAsync(ptr(op.c), 0, bytes, st));
     return;
   }
@@ -1950,7 +1961,7 @@ void Program::interp_descs(size_t i, const void* const* inputs, const void* grad
     case Op::MEMSET:
       d.kind = I_MEMSET;
       d.n0 = (ll)(op.bytes ? op.bytes
-                           : (u64)(tc::PLANES * (op.a_var ? op.S : 1) * op.bt * op.rpad * op.kpad * (op.bf16 ? 2 : 4)));
+                           : (u64)((op.six ? 6 : tc::PLANES) * (op.a_var ? op.S : 1) * op.bt * op.rpad * op.kpad * (op.bf16 ? 2 : 4)));
       d.nvb = tasks(d.n0, 256 * 16);
       break;
     case Op::GEMM_SMALL: gemm(); d.kind = I_GEMM_SMALL; d.nvb = tasks(outs * op.k, 8192); break;
@@ -2191,7 +2202,8 @@ double op_work(const Op& op, int dt) {
     case Op::OUTPUT: return (double)op.n_blocks * op.n_chunks * op.n_e * wide_bytes(dt);
     case Op::PACK:
     case Op::PACK_TILED:  // complex64 read once, four fp32 (or bf16) planes written (padding included)
-      return (double)(op.a_var ? op.S : 1) * op.bt * (8.0 * op.rows * op.cols + (op.bf16 ? 8.0 : 16.0) * op.rpad * op.kpad);
+      return (double)(op.a_var ? op.S : 1) * op.bt *
+             (8.0 * op.rows * op.cols + (op.six ? 12.0 : op.bf16 ? 8.0 : 16.0) * op.rpad * op.kpad);
     default: return (double)op.n_out * eb;
   }
 }
@@ -2348,14 +2360,15 @@ std::string Program::describe() const {
         f("S", op.S); f("bt", op.bt); f("m", op.m); f("k", op.k); f("n", op.n);
         f("splits", op.splits); f("conj_a", op.conj_a); f("conj_b", op.conj_b);
         if (op.pk.kind != Ref::NONE) { f("pack_into", (long long)op.pk.index); f("pack_vec", op.pk_vec ? 1 : 0); }
-        if (op.kind == Op::GEMM_TC) { f("bf16", op.bf16); f("real", op.real); }
+        if (op.kind == Op::GEMM_TC) { f("bf16", op.bf16); f("bf16x6", op.six); f("real", op.real); }
         s += std::string(",\"variant\":\"") + gemm_variant_name(op.variant) + "\"";
         f("tuned", op.tuned ? 1 : 0);
         f("phase", op.key.phase); f("a_var", op.key.a_var); f("b_var", op.key.b_var);
         break;
       case Op::PACK: case Op::PACK_TILED:
         f("S", op.a_var ? op.S : 1); f("bt", op.bt); f("rows", op.rows); f("cols", op.cols); f("rpad", op.rpad);
-        f("kpad", op.kpad); f("tile", op.tile_T); f("n_outer", op.n_outer); f("bf16", op.bf16); f("real", op.real);
+        f("kpad", op.kpad); f("tile", op.tile_T); f("n_outer", op.n_outer); f("bf16", op.bf16); f("bf16x6", op.six);
+        f("real", op.real);
         break;
       case Op::GATHER: case Op::SCATTER: case Op::MAXABS: case Op::STRIP:
         f("S", op.S); f("n_out", op.n_out); f("n_red", op.n_red);

@@ -19,7 +19,7 @@
 namespace ab2 {
 
 enum : int { DT_F32 = 0, DT_F64 = 1, DT_C64 = 2, DT_C128 = 3 };
-enum : int { PREC_FP32 = 0, PREC_TF32X3 = 1, PREC_BF16X3 = 2 };
+enum : int { PREC_FP32 = 0, PREC_TF32X3 = 1, PREC_BF16X3 = 2, PREC_BF16X6 = 3 };
 
 // GEMM kernel variants a tuning table can pin per GEMM shape (the values of ARCTN_B200_GEMM_*).
 enum : int {
@@ -92,6 +92,7 @@ struct Op {
   Ref d;                                // GEMM_TC: FP32 split-K partial buffer
   bool bwd = false;                     // part of the adjoint sweep (skipped by a plain execute)
   bool bf16 = false;                    // PACK / PACK_TILED / GEMM_TC / their MEMSET: split-BF16 planes
+  bool six = false;                     // ... with three BF16 pieces per value (6 planes per operand)
   // PACK / GEMM_TC of a real float32 step on the complex tensor-core GEMM: K folds in half into the real and
   // imaginary parts (A' = A[:, c] + i A[:, c + Kc], B' = conj(B[c, :] + i B[c + Kc, :]), Re(A'.B') = A.B);
   // PACK: `cols` = Kc, `kfull` = K.

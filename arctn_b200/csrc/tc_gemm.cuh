@@ -51,6 +51,26 @@ static_assert(SMEM_BYTES <= 232448, "shared memory above the 227 KB a block may 
 // kChunkTiles = 2) bounds that biased error; the long sum over K happens in the drain registers.
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int kChunkTiles = 2;
+
+// Operand formats of the kernel body.  FMT_TF32X3: each value as a TF32 pair (hi, lo) in 4-byte planes,
+// 3 products per real product.  FMT_BF16X3: a BF16 pair, 3 products.  FMT_BF16X6: three BF16 pieces
+// x = h + m + l (h = bf16(x), m = bf16(x - h), l = bf16(x - h - m); each difference is exact in FP32), which
+// carry x to about 2^-26, and the 6 products hh, hm, mh, hl, lh, mm -- every dropped term (ml, lm, ll) is at
+// most about 2^-24 of the product, so the result matches FP32 arithmetic; at the BF16 rate, 6 BF16 MMAs of
+// K = 16 take as long as 3 TF32 MMAs of K = 8 over the same K.  Its 6 planes per operand fill a 96 KB stage,
+// so the ring holds 2 stages, and one stage (32 of K) per TMEM chunk keeps 24 MMAs per accumulator chain.
+enum : int { FMT_TF32X3 = 0, FMT_BF16X3 = 1, FMT_BF16X6 = 2 };
+template <int F>
+struct Fmt {
+  static constexpr bool kBF16 = F != FMT_TF32X3;
+  static constexpr int kPieces = F == FMT_BF16X6 ? 3 : 2;
+  static constexpr int kPlanes = 2 * kPieces;  // re pieces, then im pieces
+  static constexpr int kStages = F == FMT_BF16X6 ? 2 : STAGES;
+  static constexpr int kStageBytes = 2 * kPlanes * PLANE_BYTES;
+  static constexpr int kChunkTiles = F == FMT_BF16X6 ? 1 : tc::kChunkTiles;
+  static constexpr int kSmemBytes = kStages * kStageBytes + STAGING_BYTES + 1024 + 1024;
+  static_assert(kSmemBytes <= 232448, "shared memory above the 227 KB a block may use");
+};
 // 16 warps in four warpgroups.  Warpgroup 0: TMA producer (warp 0), TMEM owner + MMA issuer (warp 1),
 // store helpers (warps 2, 3).  Warpgroups 1 and 2: the 8 drain warps (4..11), which hold the FP32
 // accumulators in registers.  Warpgroup 3: store helpers (12..15).  The block launches at 128 registers
@@ -87,6 +107,24 @@ __device__ __forceinline__ void put_split(__nv_bfloat16* dst, ll plane, ll o, fl
   dst[o] = h;
   dst[plane + o] = __float2bfloat16_rn(x - __bfloat162float(h));
 }
+// Split-BF16 with three pieces: the plane element of FMT_BF16X6 packs (2 bytes, like __nv_bfloat16).  put_split
+// writes h, m, l to planes 0, 1, 2 (plane floats apart).
+struct __align__(2) bf16p3 {
+  __nv_bfloat16 v;
+};
+__device__ __forceinline__ void put_split(bf16p3* dst, ll plane, ll o, float x) {
+  const __nv_bfloat16 h = __float2bfloat16_rn(x);
+  const float r1 = x - __bfloat162float(h);  // exact: h is within half a BF16 unit of x
+  const __nv_bfloat16 m = __float2bfloat16_rn(r1);
+  const float r2 = r1 - __bfloat162float(m);  // exact likewise
+  dst[o].v = h;
+  dst[plane + o].v = m;
+  dst[2 * plane + o].v = __float2bfloat16_rn(r2);
+}
+// Pieces per value of a plane element type (the imaginary part's planes start this many planes later).
+template <typename PT> __host__ __device__ constexpr int pieces_of() { return 2; }
+template <> __host__ __device__ constexpr int pieces_of<bf16p3>() { return 3; }
+
 __device__ __forceinline__ unsigned long long now_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -422,8 +460,12 @@ __device__ __forceinline__ void store_pass(const TcArgs& args, const EpiState& e
 
 // The GEMM body for either operand format: split-TF32 (4-byte planes, 16 of K per 64-byte operand row) or
 // split-BF16 (2-byte planes, 32 of K per row).  Shared-memory layout, swizzle, TMEM and epilogue are the same.
-template <bool kBF16>
+template <int F>
 __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcArgs& args) {
+  using FM = Fmt<F>;
+  constexpr bool kBF16 = FM::kBF16;
+  constexpr int STAGES = FM::kStages, STAGE_BYTES = FM::kStageBytes, PLANES = FM::kPlanes;
+  constexpr int kChunkTiles = FM::kChunkTiles;
   constexpr int KT_ELEMS = kBF16 ? 2 * BK : BK;  // K per 64-byte operand row
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -561,6 +603,27 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
               }
               asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
               const uint32_t a0 = smem_u32(ring + s * STAGE_BYTES), b0 = a0 + PLANES * PLANE_BYTES;
+              if constexpr (F == FMT_BF16X6) {
+                // planes re_h, re_m, re_l, im_h, im_m, im_l; products (h,h), (h,m), (m,h), (h,l), (l,h), (m,m)
+                constexpr int px[6] = {0, 0, 1, 0, 2, 1}, py[6] = {0, 1, 0, 2, 0, 1};
+  #pragma unroll
+                for (int kk = 0; kk < BK / 8; ++kk) {
+                  const uint32_t o = kk * 32;
+  #pragma unroll
+                  for (int q = 0; q < 6; ++q) {
+                    const uint32_t Ar = a0 + px[q] * PLANE_BYTES + o, Ai = Ar + 3 * PLANE_BYTES;
+                    const uint32_t Br = b0 + py[q] * PLANE_BYTES + o, Bi = Br + 3 * PLANE_BYTES;
+                    const uint32_t acc = (first && q == 0) ? 0u : 1u;
+                    umma<true>(cr, sw64_desc(Ar), sw64_desc(Br), id_pos, acc);
+                    umma<true>(ci, sw64_desc(Ar), sw64_desc(Bi), id_pos, acc);
+                    umma<true>(cr, sw64_desc(Ai), sw64_desc(Bi), id_neg, 1);
+                    umma<true>(ci, sw64_desc(Ai), sw64_desc(Br), id_pos, 1);
+                  }
+                  first = false;
+                }
+                umma_commit(&empty[s]);
+                continue;
+              }
               const uint32_t hAr = a0, lAr = a0 + PLANE_BYTES, hAi = a0 + 2 * PLANE_BYTES, lAi = a0 + 3 * PLANE_BYTES;
               const uint32_t hBr = b0, lBr = b0 + PLANE_BYTES, hBi = b0 + 2 * PLANE_BYTES, lBi = b0 + 3 * PLANE_BYTES;
   #pragma unroll
@@ -670,13 +733,19 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
 static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __grid_constant__ CUtensorMap tmA,
                                                                 const __grid_constant__ CUtensorMap tmB,
                                                                 TcArgs args) {
-  tc_cgemm_body<false>(tmA, tmB, args);
+  tc_cgemm_body<FMT_TF32X3>(tmA, tmB, args);
 }
 // Split-BF16: operands packed as BF16 hi/lo planes, 3 BF16 products per real product (kind::f16).
 static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_bf16x3(const __grid_constant__ CUtensorMap tmA,
                                                                 const __grid_constant__ CUtensorMap tmB,
                                                                 TcArgs args) {
-  tc_cgemm_body<true>(tmA, tmB, args);
+  tc_cgemm_body<FMT_BF16X3>(tmA, tmB, args);
+}
+// Three-piece split-BF16: 6 BF16 products per real product (kind::f16), FP32-level accuracy.
+static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_bf16x6(const __grid_constant__ CUtensorMap tmA,
+                                                                const __grid_constant__ CUtensorMap tmB,
+                                                                TcArgs args) {
+  tc_cgemm_body<FMT_BF16X6>(tmA, tmB, args);
 }
 
 // Leg-aware pack: the same gather as k_pack_planar, for operands whose legs are scattered (as in
@@ -690,7 +759,7 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_bf16x3(const __
 constexpr int kPackTile = 1024;
 constexpr int kPackThreads = 256;
 __device__ __forceinline__ int pack_swz(int e) { return e ^ ((e >> 5) & 31); }
-template <typename PT>  // plane element: float (split-TF32) or __nv_bfloat16 (split-BF16)
+template <typename PT>  // plane element: float (split-TF32), __nv_bfloat16 (split-BF16) or bf16p3 (three pieces)
 static __global__ void __launch_bounds__(kPackThreads, 6) k_pack_tiled(
     const cf32* __restrict__ src, PT* __restrict__ dst, const int* __restrict__ rd_rank,
     const int* __restrict__ rd_off, const int* __restrict__ wr_off, int T, const ll* __restrict__ src_base,
@@ -737,7 +806,7 @@ static __global__ void __launch_bounds__(kPackThreads, 6) k_pack_tiled(
       if (i < T) {
         const int e = pack_swz(i);
         put_split(db, plane, wo[j], t_re[e]);
-        put_split(db + 2 * plane, plane, wo[j], im_sign * t_im[e]);
+        put_split(db + pieces_of<PT>() * plane, plane, wo[j], im_sign * t_im[e]);
       }
     }
     __syncthreads();
@@ -765,7 +834,7 @@ static __global__ void k_splitk_reduce(const cf32* __restrict__ part, cf32* __re
 // This is the permute of the reference step (src/tensor.rs:453-492) fused with the planar split.
 // A 32 x 32 (r, c) tile goes through shared memory: it is read along whichever index the source
 // walks with unit stride (r_major) and written along c, so both sides stay coalesced.
-template <typename PT>  // plane element: float (split-TF32) or __nv_bfloat16 (split-BF16)
+template <typename PT>  // plane element: float (split-TF32), __nv_bfloat16 (split-BF16) or bf16p3 (three pieces)
 static __global__ void __launch_bounds__(256) k_pack_planar(const cf32* __restrict__ src, PT* __restrict__ dst,
                                                      const ll* __restrict__ tabB, const ll* __restrict__ tabR,
                                                      const ll* __restrict__ tabC, ll bt, ll R, ll K, ll Rpad, ll Kpad,
@@ -797,7 +866,7 @@ static __global__ void __launch_bounds__(256) k_pack_planar(const cf32* __restri
       if (c < Kpad) {
         const ll o = (zz * Rpad + r) * Kpad + c;
         put_split(dst, plane, o, tile[u][tx].re);
-        put_split(dst + 2 * plane, plane, o, im_sign * tile[u][tx].im);
+        put_split(dst + pieces_of<PT>() * plane, plane, o, im_sign * tile[u][tx].im);
       }
     }
     __syncthreads();
@@ -844,7 +913,7 @@ static __global__ void __launch_bounds__(256) k_pack_planar_real(const float* __
       if (c < Kpad) {
         const ll o = (zz * Rpad + r) * Kpad + c;
         put_split(dst, plane, o, tile[u][tx].re);
-        put_split(dst + 2 * plane, plane, o, im_sign * tile[u][tx].im);
+        put_split(dst + pieces_of<PT>() * plane, plane, o, im_sign * tile[u][tx].im);
       }
     }
     __syncthreads();

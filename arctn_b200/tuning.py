@@ -9,9 +9,9 @@ through a tuning table, run op by op on random inputs of the network's shapes, a
 its GEMMs plus the ops serving them (operand packs, split-K sums; a producer's epilogue that writes the next
 GEMM's packed operand counts for the producer).  Every variant is pinned on all the keys it may serve in one
 run, so a tuning pass costs one program run per variant, not per key and variant.
-Candidates are the SIMT kernels (all dtypes) and, under precision tf32x3 / bf16x3 for float32 and complex64,
-the tensor-core GEMM with either tile order or with K split across CTAs.  A candidate whose time cannot
-beat the current choice even at its kernel family's peak rate is skipped untimed.
+Candidates are the SIMT kernels (all dtypes) and, under precision tf32x3 / bf16x3 / bf16x6 for float32 and
+complex64, the tensor-core GEMM with either tile order or with K split across CTAs.  A candidate whose time
+cannot beat the current choice even at its kernel family's peak rate is skipped untimed.
 
 The resulting :class:`TuneTable` goes to ``SlicedProgram(..., tuning=table)``; it saves to and loads from
 JSON, so a table tuned once on a GPU serves later runs.  The reference has no counterpart: every GEMM there
@@ -62,7 +62,7 @@ def candidates(key, S=1):
     dtype, precision, phase, _, _, bt, m, k, n = key
     outs = bt * m * n * (S if phase == 2 else 1)
     out = []
-    if precision in (C.PREC_TF32X3, C.PREC_BF16X3) and dtype in (C.F32, C.C64):
+    if precision in (C.PREC_TF32X3, C.PREC_BF16X3, C.PREC_BF16X6) and dtype in (C.F32, C.C64):
         out.append("tc_mfast")
         mt, nt = -(-m // _TILE_M), -(-n // _TILE_N)
         if mt > 1 and nt > 1:

@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--precision", choices=["fp32", "tf32x3", "bf16x3"], default="tf32x3")
+    ap.add_argument("--precision", choices=["fp32", "tf32x3", "bf16x3", "bf16x6"], default="tf32x3")
     ap.add_argument("--nodes", type=int, default=172)
     ap.add_argument("--target-log2", type=int, default=24)
     ap.add_argument("--group", type=int, default=0, help="slices per group (0: as many as the workspace allows)")
@@ -428,7 +428,7 @@ def run_latency(args, dev, which):
     else:
         net, arrays = N.brickwork_circuit(30, 14, seed=0)
         arrays = [a.astype(np.complex64) for a in arrays]
-        dtype, precisions = np.complex64, ["tf32x3", "fp32", "bf16x3"]
+        dtype, precisions = np.complex64, ["tf32x3", "fp32", "bf16x3", "bf16x6"]
     path = A.greedy(*net.as_tuple())
     O.build()
     ref = complex(O.contract_sliced(*net.as_tuple(), path, [], [a.astype(np.complex128) for a in arrays]))

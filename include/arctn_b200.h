@@ -61,9 +61,12 @@ enum {
                                  for steps dense enough to fill a tensor-core tile; thin steps FP32.
                                  f32 steps run on the complex kernel with K folded in half into the
                                  real and imaginary parts (the real part of the product is kept) */
-  ARCTN_B200_PREC_BF16X3 = 2  /* split-BF16 (3 products, hi/lo BF16 pairs) on tcgen05 tensor cores, FP32
+  ARCTN_B200_PREC_BF16X3 = 2, /* split-BF16 (3 products, hi/lo BF16 pairs) on tcgen05 tensor cores, FP32
                                  accumulate; each operand carried to about 2^-18, for precision studies;
                                  the same step selection as TF32X3 */
+  ARCTN_B200_PREC_BF16X6 = 3  /* three-piece split-BF16 (x = h + m + l, 6 products hh hm mh hl lh mm) on tcgen05
+                                 tensor cores, FP32 accumulate: FP32-level accuracy from BF16 MMAs; the same step
+                                 selection as TF32X3 (no epilogue-fused operand packs) */
 };
 
 /* A tensor network (TensorNetwork, src/network.rs:134-143).
@@ -220,7 +223,7 @@ enum {
 };
 /* One GEMM shape and its variant.  phase: 1 for a slice-invariant GEMM (run once per execute), 2 for one run
  * per slice group; a_var / b_var: whether that operand differs per slice; bt, m, k, n: gemm_dims() of one
- * slice (src/compiled.rs:138-141).  The tensor-core variants need precision TF32X3 or BF16X3 and a C64 or
+ * slice (src/compiled.rs:138-141).  The tensor-core variants need precision TF32X3, BF16X3 or BF16X6 and a C64 or
  * F32 network; SIMT_TILE128 needs F32. */
 typedef struct {
   int dtype, precision, phase, a_var, b_var, variant;

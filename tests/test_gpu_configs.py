@@ -94,8 +94,9 @@ def brickwork():
     return net, a64, path, want, ref_c64
 
 
-# Split-BF16 with three products carries each operand to about 2^-18 and drops the lo x lo term.
-@pytest.mark.parametrize("precision,tol", [("tf32x3", 1e-5), ("fp32", 1e-5), ("bf16x3", 1e-4)])
+# Split-BF16 with three products carries each operand to about 2^-18 and drops the lo x lo term; with three
+# pieces and six products (bf16x6) it matches FP32.
+@pytest.mark.parametrize("precision,tol", [("tf32x3", 1e-5), ("fp32", 1e-5), ("bf16x3", 1e-4), ("bf16x6", 1e-5)])
 def test_brickwork_precisions_match_c128_oracle(brickwork, precision, tol):
     net, a64, path, want, ref_c64 = brickwork
     assert rel(ref_c64, want) <= 1e-5  # the reference's own complex64 executor on these inputs

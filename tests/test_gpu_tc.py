@@ -51,8 +51,9 @@ CASES = [
 
 
 # Split-TF32 carries each operand to about 2^-22 (1e-5 on these steps); split-BF16 to about 2^-18 and drops
-# the lo x lo term, about 2^-17 of each product (1e-4).
-PRECISIONS = [("tf32x3", 1e-5), ("bf16x3", 1e-4)]
+# the lo x lo term, about 2^-17 of each product (1e-4); three-piece split-BF16 carries each operand to about
+# 2^-26 and drops terms of at most about 2^-24 of each product (1e-5, like FP32).
+PRECISIONS = [("tf32x3", 1e-5), ("bf16x3", 1e-4), ("bf16x6", 1e-5)]
 
 
 @pytest.mark.parametrize("precision,tol", PRECISIONS, ids=[p for p, _ in PRECISIONS])
@@ -100,9 +101,11 @@ def test_tc_grid_contraction_matches_fp64_oracle():
     got = complex(A.contract_sliced(*net.as_tuple(), arrays, [], ssa_path=path, precision="tf32x3"))
     got32 = complex(A.contract_sliced(*net.as_tuple(), arrays, [], ssa_path=path, precision="fp32"))
     got_bf = complex(A.contract_sliced(*net.as_tuple(), arrays, [], ssa_path=path, precision="bf16x3"))
+    got_b6 = complex(A.contract_sliced(*net.as_tuple(), arrays, [], ssa_path=path, precision="bf16x6"))
     assert abs(got - want) / abs(want) <= 1e-5
     assert abs(got32 - want) / abs(want) <= 1e-5
     assert abs(got_bf - want) / abs(want) <= 1e-4
+    assert abs(got_b6 - want) / abs(want) <= 1e-5
 
 
 def test_epilogue_packs_are_bit_identical_to_separate_packs():
@@ -134,3 +137,24 @@ def test_tensor_pipe_peak_probe(kind):
     assert all(100.0 < r < 5000.0 for r in rates.values()), rates
     if kind == "bf16":
         assert rates[256] > A.tensor_pipe_peak("tf32", 256, iters=1 << 14, repeats=1)
+
+
+def test_bf16x6_rand3reg_n104_matches_fp64_oracle():
+    # rand3reg n=104, 16 slices: every dense step on the three-piece split-BF16 tensor-core kernel, within the
+    # 1e-5 the complex64 path is held to, and no further from FP64 than split-TF32 by more than 2x.
+    from arctn_b200 import networks as N
+
+    net, arrays = N.workload_rand3reg(104, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 14)
+    want = complex(O.contract_sliced(*net.as_tuple(), path, sliced, O.promote(arrays), threads=8))
+    errs = {}
+    for precision in ("bf16x6", "tf32x3"):
+        prog = A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex64, precision=precision)
+        ops = prog.describe()["ops"]
+        assert any(o["kind"] == "gemm_tc" and o["bf16x6"] == (precision == "bf16x6") for o in ops)
+        got = complex(prog.execute(arrays, f64_out=True))
+        errs[precision] = abs(got - want) / abs(want)
+    print("rand3reg n104 rel err", errs)
+    assert errs["bf16x6"] <= 1e-5
+    assert errs["bf16x6"] <= max(2 * errs["tf32x3"], 2e-6)

@@ -21,12 +21,12 @@ pytestmark = pytest.mark.gpu
 
 CODES = {np.dtype(np.float32): C.F32, np.dtype(np.float64): C.F64, np.dtype(np.complex64): C.C64,
          np.dtype(np.complex128): C.C128}
-PRECS = {"fp32": C.PREC_FP32, "tf32x3": C.PREC_TF32X3, "bf16x3": C.PREC_BF16X3}
+PRECS = {"fp32": C.PREC_FP32, "tf32x3": C.PREC_TF32X3, "bf16x3": C.PREC_BF16X3, "bf16x6": C.PREC_BF16X6}
 
 
 def valid(variant, dtype, precision):
     if variant.startswith("tc_"):
-        return precision in ("tf32x3", "bf16x3") and dtype in (C.F32, C.C64)
+        return precision in ("tf32x3", "bf16x3", "bf16x6") and dtype in (C.F32, C.C64)
     return variant != "simt_tile128" or dtype == C.F32
 
 

@@ -93,6 +93,27 @@ def test_bf16x3_programs_pack_bf16_planes_on_32_wide_k_rows():
         program(net, path, sliced, dtype=np.complex64, precision="bf16x3", tc_k_chunk=16)
 
 
+def test_bf16x6_programs_pack_six_bf16_planes():
+    # Three-piece split-BF16: the same tensor-core steps, 2-byte planes on 32-wide K rows, six planes per operand
+    # (so each pack holds 1.5x the bytes of a split-BF16 pair pack), no epilogue packs.
+    net, _ = N.workload_rand3reg(172, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 24)
+    b3 = program(net, path, sliced, dtype=np.complex64, precision="bf16x3", max_slices_per_group=4).describe()["ops"]
+    b6 = program(net, path, sliced, dtype=np.complex64, precision="bf16x6", max_slices_per_group=4).describe()["ops"]
+    tc3 = [(o["bt"], o["m"], o["k"], o["n"]) for o in b3 if o["kind"] == "gemm_tc"]
+    tc6 = [(o["bt"], o["m"], o["k"], o["n"]) for o in b6 if o["kind"] == "gemm_tc"]
+    assert tc6 and tc6 == tc3
+    assert all(o["bf16"] == 1 and o["bf16x6"] == 1 for o in b6 if o["kind"] in ("gemm_tc", "pack", "pack_tiled"))
+    assert all(o["bf16x6"] == 0 for o in b3 if o["kind"] in ("gemm_tc", "pack", "pack_tiled"))
+    assert all(o["kpad"] % 32 == 0 for o in b6 if o["kind"] in ("pack", "pack_tiled"))
+    assert not any("pack_into" in o for o in b6)
+    with pytest.raises(A.ArcTNB200Error, match="multiple of 32"):
+        program(net, path, sliced, dtype=np.complex64, precision="bf16x6", tc_k_chunk=16)
+    with pytest.raises(A.ArcTNB200Error, match="precision"):
+        program(net, path, sliced, dtype=np.complex64, precision=4)
+
+
 def test_tensor_core_epilogues_pack_the_next_gemm_operand():
     # rand3reg n=172: the producer's epilogue writes the packed operand of the GEMM that reads its result,
     # so no separate pack reads that result; gradient programs keep separate packs.
