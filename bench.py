@@ -61,6 +61,8 @@ def parse():
     ap.add_argument("--workspace-gb", type=float, default=24.0)
     ap.add_argument("--tc-k-chunk", type=int, default=0, help="K per tensor-core accumulator (0: library default)")
     ap.add_argument("--no-tune", action="store_true", help="keep the built-in GEMM heuristics (skip the autotuner)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the other configurations (grid6, brickwork, grid8, batch) after the headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, the FP32 comparison and the FP64 check")
@@ -487,7 +489,7 @@ def run_latency(args, dev, which):
                                "sample": "one full contraction, median of 5, oracle executor in the input dtype"},
                  clocks=res[head]["clocks"], precisions=res, fp64_oracle=[ref.real, ref.imag],
                  cpu_native_rel_err_vs_fp64=abs(cpu_native - ref) / abs(ref))
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_grid8(args, dev):
@@ -562,8 +564,9 @@ def run_grid8(args, dev):
     flops_fwd = p.flops
     total_ms = fwd_ms + bwd_ms
     value = 3 * flops_fwd / (total_ms * 1e-3) / 1e12  # forward F + two adjoint GEMMs per step (2F)
-    pk = peaks()
-    tf32_alg_peak = pk["bf16_tflops"] / 2 / 3  # split-TF32 4M: 3 TF32 products per real product
+    # split-TF32 4M: 3 TF32 products per real product; the TF32 pipe rate measured by the library's probe
+    tf32_pipe = max(A.tensor_pipe_peak("tf32", n, device=dev.index) for n in (128, 256))
+    tf32_alg_peak = tf32_pipe / 3
     line = _line(args, "grid8 bond6 c64 forward+adjoint TFLOP/s", value, "TFLOP/s", True, total_ms,
                  {"workload": "grid8x8_bond6_c64_adjoint", "precision": "tf32x3", "inputs_scaled_by": 4,
                   "l2": "flushed (256 MiB write) before each timed part"}, "c64",
@@ -571,8 +574,8 @@ def run_grid8(args, dev):
                  e2e=None,
                  roofline={"bound": "tensor", "achieved": value, "peak": tf32_alg_peak, "unit": "TFLOP/s",
                            "frac": value / tf32_alg_peak,
-                           "peak_source": f"{pk['source']} bf16 dense burst / 2 (TF32) / 3 (split-TF32 products)",
-                           "traffic": None},
+                           "peak_source": "measured TF32 tensor pipe (arctn_b200_tc_peak) / 3 (split-TF32 products)",
+                           "tf32_pipe_tflops": tf32_pipe, "traffic": None},
                  cpu_baseline=None, clocks=clocks, device_status=status,
                  fwd_ms=fwd_ms, bwd_ms=bwd_ms, bwd_over_fwd=bwd_ms / fwd_ms,
                  fp32_fwd_ms=fwd32, fp32_bwd_ms=bwd32, speedup_vs_fp32=(fwd32 + bwd32) / total_ms,
@@ -584,7 +587,7 @@ def run_grid8(args, dev):
                  recompute={"workspace_bytes": pr.workspace_bytes, "recomputed_steps": pr.recomputed_steps,
                             "fwd_ms": fwd_r, "bwd_ms": bwd_r, "bwd_over_fwd": bwd_r / fwd_r,
                             "bit_identical_to_kept": identical})
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_batch(args, dev):
@@ -646,12 +649,11 @@ def run_batch(args, dev):
     # (one pinned copy per network), runs the batch and returns outputs and gradients as NumPy arrays.
     host = [arrays for _, arrays in nets]
     if args.no_extras:  # device time only (profiling runs)
-        print(json.dumps(_line(args, "many-network forward+adjoint throughput", len(progs) / (ms * 1e-3),
-                               "networks/s", True, ms, {"workload": f"{len(progs)} random 3-regular networks, n in "
-                                                        "[20,50], bond in {2,3,4}, f32/c64 alternating"}, "f32+c64",
-                               gpu_launches=launches_per_call * args.steps, e2e=None, roofline=None,
-                               cpu_baseline=None, clocks=sampler.summary(), device_status=status)), flush=True)
-        return
+        return _line(args, "many-network forward+adjoint throughput", len(progs) / (ms * 1e-3),
+                     "networks/s", True, ms, {"workload": f"{len(progs)} random 3-regular networks, n in "
+                                              "[20,50], bond in {2,3,4}, f32/c64 alternating"}, "f32+c64",
+                     gpu_launches=launches_per_call * args.steps, e2e=None, roofline=None,
+                     cpu_baseline=None, clocks=sampler.summary(), device_status=status)
     h2d = sum(a.nbytes for arrays in host for a in arrays)
     d2h = sum(int(np.prod(p.output_shape)) * a[0].itemsize for p, a in zip(progs, host)) + h2d
     ws_e2e = torch.empty(max(batch.workspace_bytes, 1), dtype=torch.uint8, device=dev)
@@ -689,7 +691,7 @@ def run_batch(args, dev):
                  single_network_ms_p50=lat[len(lat) // 2], single_network_ms_p99=lat[min(len(lat) - 1,
                                                                                          int(0.99 * len(lat)))],
                  sum_of_single_network_ms=sum(lat), batch_speedup_vs_serial=sum(lat) / ms)
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -705,11 +707,12 @@ def main():
         torch.cuda.set_device(local)
         dev = torch.device("cuda", local)
         if args.workload in ("grid6", "brickwork"):
-            run_latency(args, dev, args.workload)
+            line = run_latency(args, dev, args.workload)
         elif args.workload == "grid8":
-            run_grid8(args, dev)
+            line = run_grid8(args, dev)
         else:
-            run_batch(args, dev)
+            line = run_batch(args, dev)
+        print(json.dumps(line), flush=True)
         return
     if args.impl == "reference":
         run_reference(args, rank)
@@ -907,6 +910,23 @@ def main():
                 "clocks": clocks, "device_status": status, "workspace_bytes": int(prog.workspace_bytes),
                 "result": [float(r.real), float(r.imag)]}
         line.update(extras)
+        if world == 1 and not args.no_extras and not args.no_configs:
+            # The other configurations, each measured the way its own --workload run measures it, in the same
+            # process after the headline's buffers are released.
+            del prog, ws, x, flush
+            torch.cuda.empty_cache()
+            others = {}
+            for which in ("grid6", "brickwork", "grid8", "batch"):
+                t0 = time.perf_counter()
+                try:
+                    d = (run_latency(args, dev, which) if which in ("grid6", "brickwork") else
+                         run_grid8(args, dev) if which == "grid8" else run_batch(args, dev))
+                    d["wall_s"] = round(time.perf_counter() - t0, 1)
+                except Exception as e:  # one configuration failing must not hide the headline
+                    d = {"error": f"{type(e).__name__}: {e}"}
+                others[which] = d
+                torch.cuda.empty_cache()
+            line["configs"] = others
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
