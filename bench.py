@@ -67,9 +67,11 @@ def parse():
     ap.add_argument("--no-profile", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip e2e, the FP32 comparison and the FP64 check")
     ap.add_argument("--batch-size", type=int, default=256, help="networks of --workload batch (256: config 5)")
-    ap.add_argument("--workload", choices=["rand3reg", "grid6", "brickwork", "grid8", "batch"], default="rand3reg",
-                    help="rand3reg: the sliced headline (default); grid6 / brickwork: latency and precision; "
-                         "grid8: forward + adjoint; batch: 256 uneven networks in one graph launch")
+    ap.add_argument("--workload", choices=["rand3reg", "rand3reg_n64", "grid6", "brickwork", "grid8", "batch"],
+                    default="rand3reg",
+                    help="rand3reg: the sliced headline (default); rand3reg_n64: 256 slices of the n=64 graph in "
+                         "one persistent launch; grid6 / brickwork: latency and precision; grid8: forward + adjoint; "
+                         "batch: 256 uneven networks in one graph launch")
     return ap.parse_args()
 
 
@@ -590,6 +592,56 @@ def run_grid8(args, dev):
     return line
 
 
+def run_rand3reg_n64(args, dev):
+    """rand3reg n=64, bond 2, c64, greedy, sliced to 2^7 elements -> 256 slices (the configuration as written
+    at n = 64; its stated 2^24 target needs no slicing): microseconds per sliced contraction as a graph of
+    kernel launches and under the staged scheduler, where every slice runs inside one persistent launch."""
+    import torch
+
+    import arctn_b200 as A
+    from arctn_b200 import networks as N
+    from oracle import oracle as O
+
+    net, arrays = N.workload_rand3reg(64, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 7)
+    prog = A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex64, precision="tf32x3", device=dev.index)
+    x = [torch.from_numpy(a).to(dev) for a in arrays]
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    ws = torch.empty(max(prog.workspace_bytes, 1), dtype=torch.uint8, device=dev)
+    batch = A.ProgramBatch([prog], max_lanes=8, mode="staged")
+    part = next(p for p in batch.describe()["parts"] if p["part"] == -1)
+    run = batch.bind([x], stream=stream)
+    forms = {"program": lambda: prog.execute(x, workspace=ws, stream=stream), "staged": run}
+    res = {}
+    sampler = ClockSampler(dev.index)
+    with sampler:
+        for name, fn in forms.items():
+            for _ in range(max(args.warmup, 3)):
+                fn()
+            torch.cuda.synchronize(dev)
+            ts = []
+            for _ in range(max(args.steps, 10)):
+                flush.fill_(1)
+                ts.append(_events_ms(stream, fn))
+            res[name] = 1e3 * statistics.mean(ts)
+    got = complex(batch.execute([x], workspace=run.workspace, stream=stream)[0].item())
+    want = complex(O.contract_sliced(*net.as_tuple(), path, sliced, O.promote(arrays), threads=8))
+    return _line(args, "rand3reg n64 256-slice c64 contraction latency", res["staged"], "us", False,
+                 res["staged"] / 1e3,
+                 {"workload": "rand3reg_n64_bond2_seed1_c64_greedy_target2^7_256slices", "n_slices": 2 ** len(sliced),
+                  "precision": "tf32x3", "form": "staged scheduler: one persistent interpreter launch for all slices",
+                  "l2": "flushed (256 MiB write) before each timed contraction"}, "c64",
+                 gpu_launches=(part["stages"] + sum(part["stage_launches"])) * max(args.steps, 10),
+                 e2e=None, roofline={"bound": "latency", "note": "256 slices of 2^7-element steps"},
+                 cpu_baseline=None, clocks=sampler.summary(), device_status=batch.device_status(run.workspace, stream),
+                 interpreter_launches=part["stages"], tensor_core_launches=sum(part["stage_launches"]),
+                 program_graph_us=res["program"], program_graph_launches=prog.launches,
+                 rel_err_vs_fp64_oracle=abs(got - want) / abs(want))
+
+
 def run_batch(args, dev):
     """256 uneven random 3-regular networks (half float32, half complex64): forward + adjoint of all of
     them as one graph launch; networks/s, TFLOP/s and the per-network latency distribution."""
@@ -710,6 +762,8 @@ def main():
             line = run_latency(args, dev, args.workload)
         elif args.workload == "grid8":
             line = run_grid8(args, dev)
+        elif args.workload == "rand3reg_n64":
+            line = run_rand3reg_n64(args, dev)
         else:
             line = run_batch(args, dev)
         print(json.dumps(line), flush=True)
@@ -837,6 +891,34 @@ def main():
                                    "oracle": [want.real, want.imag], "gpu": [got.real, got.imag],
                                    "oracle_wall_s": t_or, "oracle_threads": samp}
 
+    # The same contraction under the staged scheduler (ProgramBatch of one program): every slice's SIMT steps
+    # inside persistent interpreter launches, the tensor-core GEMMs and packs launched between them.
+    if world == 1 and not args.no_extras:
+        sb = A.ProgramBatch([prog], max_lanes=8, mode="staged")
+        part = next(p for p in sb.describe()["parts"] if p["part"] == -1)
+        run = sb.bind([x], stream=stream)
+        for _ in range(max(args.warmup, 3)):
+            run()
+        torch.cuda.synchronize(dev)
+        st_ms = []
+        for _ in range(args.steps):
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run()
+            e1.record(stream)
+            e1.synchronize()
+            st_ms.append(e0.elapsed_time(e1))
+        same = bool(torch.equal(sb.execute([x], workspace=run.workspace, stream=stream)[0],
+                                prog.execute(x, workspace=ws, stream=stream)))
+        extras["staged_scheduler"] = {
+            "ms_per_step": statistics.mean(st_ms), "value": prog.flops / (statistics.mean(st_ms) * 1e-3) / 1e12,
+            "unit": "TFLOP/s", "interpreter_launches": part["stages"],
+            "tensor_core_and_pack_launches": sum(part["stage_launches"]), "graph_launches_of_program": prog.launches,
+            "bit_identical_to_program": same, "device_status": sb.device_status(run.workspace, stream)}
+        del sb, run
+        torch.cuda.empty_cache()
+
     roof = None
     pk = peaks()
     if not args.no_profile:
@@ -916,10 +998,11 @@ def main():
             del prog, ws, x, flush
             torch.cuda.empty_cache()
             others = {}
-            for which in ("grid6", "brickwork", "grid8", "batch"):
+            for which in ("grid6", "rand3reg_n64", "brickwork", "grid8", "batch"):
                 t0 = time.perf_counter()
                 try:
                     d = (run_latency(args, dev, which) if which in ("grid6", "brickwork") else
+                         run_rand3reg_n64(args, dev) if which == "rand3reg_n64" else
                          run_grid8(args, dev) if which == "grid8" else run_batch(args, dev))
                     d["wall_s"] = round(time.perf_counter() - t0, 1)
                 except Exception as e:  # one configuration failing must not hide the headline

@@ -132,3 +132,28 @@ def test_batch_numpy_inputs_match_cuda_inputs(fn):
             assert len(g_ref) == len(g_got)
             for a, b in zip(g_ref, g_got):
                 assert b.shape == tuple(a.shape) and np.array_equal(a.cpu().numpy(), b)
+
+
+@pytest.mark.parametrize("nodes,target,precision", [(64, 7, "fp32"), (64, 7, "tf32x3"), (104, 14, "tf32x3")])
+def test_sliced_program_as_staged_batch(nodes, target, precision):
+    # A sliced contraction run by the staged scheduler: all its slices' SIMT steps inside persistent interpreter
+    # launches (one for rand3reg n=64, whose steps are all SIMT), the tensor-core steps launched between them.
+    # The bits equal the program's own execute, and the value matches the oracle.
+    net, arrays = N.workload_rand3reg(nodes, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** target)
+    assert len(sliced) >= 4
+    prog = A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex64, precision=precision)
+    x = [torch.from_numpy(a).cuda() for a in arrays]
+    ref = prog.execute(x)
+    batch = A.ProgramBatch([prog], max_lanes=8, mode="staged")
+    part = next(p for p in batch.describe()["parts"] if p["part"] == -1)
+    if nodes == 64:
+        assert part["stages"] == 1 and sum(part["stage_launches"]) == 0  # one persistent launch for every slice
+    else:
+        assert sum(part["stage_launches"]) > 0
+    ws = torch.empty(max(batch.workspace_bytes, 1), dtype=torch.uint8, device="cuda")
+    (out,) = run_batch(batch, "execute", [x], ws, True)
+    assert torch.equal(out, ref)
+    want = complex(O.contract_sliced(*net.as_tuple(), path, sliced, O.promote(arrays), threads=8))
+    assert abs(complex(out.item()) - want) / abs(want) <= 1e-5
