@@ -780,6 +780,8 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
         P.pk_tab[2] = tab_ll(table(2, btp));
         P.pk_tab[3] = tab_i32(chunks);
         P.pk_tab[4] = tab_i32(lane);
+        P.pk_rows = 1;
+        for (int l : lane) P.pk_rows = std::max(P.pk_rows, (l >> 16) + 1);
         P.pk_slice = (ll)bt * rpad * kpad;
         // 16-byte stores need every chunk start 4-float aligned: tile bases (row / column tables at tile
         // starts, batch table), chunk offsets inside a tile, and the slice stride (the plane stride is a
@@ -2359,7 +2361,11 @@ std::string Program::describe() const {
       case Op::GEMM_WARP: case Op::GEMM_TILE128:
         f("S", op.S); f("bt", op.bt); f("m", op.m); f("k", op.k); f("n", op.n);
         f("splits", op.splits); f("conj_a", op.conj_a); f("conj_b", op.conj_b);
-        if (op.pk.kind != Ref::NONE) { f("pack_into", (long long)op.pk.index); f("pack_vec", op.pk_vec ? 1 : 0); }
+        if (op.pk.kind != Ref::NONE) {
+          f("pack_into", (long long)op.pk.index);
+          f("pack_vec", op.pk_vec ? 1 : 0);
+          f("pack_chunk_rows", op.pk_rows);
+        }
         if (op.kind == Op::GEMM_TC) { f("bf16", op.bf16); f("bf16x6", op.six); f("real", op.real); }
         s += std::string(",\"variant\":\"") + gemm_variant_name(op.variant) + "\"";
         f("tuned", op.tuned ? 1 : 0);

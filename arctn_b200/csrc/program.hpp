@@ -106,6 +106,7 @@ struct Op {
   int pk_qbeg[5] = {0, 0, 0, 0, 0};     // chunk ranges per 32-row group of the tile
   ll pk_slice = 0;
   bool pk_vec = false;                  // every packed chunk start is 16-byte aligned (vector stores)
+  int pk_rows = 0;                      // rows a packed chunk spans (1 + its largest row offset)
 };
 
 class Program {
