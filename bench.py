@@ -528,8 +528,19 @@ def run_grid8(args, dev):
         return statistics.mean(f), statistics.mean(b), sampler.summary(), ws
 
     kw = dict(gradient=True, use_graph=False, device=dev.index)
+    # The autotuner times every GEMM variant inside the gradient program (forward and adjoint GEMMs alike).
+    tuning, tune_info = None, None
+    if not args.no_tune:
+        t0 = time.perf_counter()
+        tuning = A.autotune(*net.as_tuple(), path, (), dtype=np.complex64, precision="tf32x3",
+                            workspace_budget=40 << 30, **kw)
+        tune_info = {"tune_s": round(time.perf_counter() - t0, 1), "gemm_shapes": len(tuning),
+                     "changed_from_heuristic": sum(tuning.get(k) != tuning.timings(k).get("heuristic")
+                                                   for k in tuning.keys()),
+                     "program_ms": {"heuristics": tuning.meta.get("program_ms_before"),
+                                    "tuned": tuning.meta.get("program_ms_after")}}
     p = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex64, precision="tf32x3", workspace_budget=40 << 30,
-                        **kw)
+                        tuning=tuning, **kw)
     fwd_ms, bwd_ms, clocks, ws = measure(p)
     status = p.device_status(ws)
     del ws
@@ -558,7 +569,7 @@ def run_grid8(args, dev):
         d[1] = round(d[1] + float(t), 3)
     # Lowered budget: half the layout that keeps every intermediate -> the sweep recomputes.
     pr = A.SlicedProgram(*net.as_tuple(), path, (), dtype=np.complex64, precision="tf32x3",
-                         workspace_budget=p.workspace_bytes // 2, **kw)
+                         workspace_budget=p.workspace_bytes // 2, tuning=tuning, **kw)
     fwd_r, bwd_r, _, wsr = measure(pr)
     o_r, g_r = pr.gradient(x, workspace=wsr)
     identical = bool(torch.equal(o_r, o_tc)) and all(torch.equal(a, b) for a, b in zip(g_r, g_tc))
@@ -571,7 +582,7 @@ def run_grid8(args, dev):
     tf32_alg_peak = tf32_pipe / 3
     line = _line(args, "grid8 bond6 c64 forward+adjoint TFLOP/s", value, "TFLOP/s", True, total_ms,
                  {"workload": "grid8x8_bond6_c64_adjoint", "precision": "tf32x3", "inputs_scaled_by": 4,
-                  "l2": "flushed (256 MiB write) before each timed part"}, "c64",
+                  "l2": "flushed (256 MiB write) before each timed part", "tuning": tune_info}, "c64",
                  gpu_launches=p.launches * args.steps,
                  e2e=None,
                  roofline={"bound": "tensor", "achieved": value, "peak": tf32_alg_peak, "unit": "TFLOP/s",
