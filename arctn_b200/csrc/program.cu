@@ -617,7 +617,10 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
                              opt_.precision == PREC_BF16X6) && (dt == DT_C64 || dt == DT_F32);
     int forced = GV_AUTO;
     if (auto it = opt_.tuning.find(g.key); it != opt_.tuning.end()) forced = it->second;
-    const bool forced_tc = forced == GV_TC_MFAST || forced == GV_TC_NFAST || forced == GV_TC_SPLITK;
+    const bool forced_tc = forced == GV_TC_MFAST || forced == GV_TC_NFAST || forced == GV_TC_SPLITK ||
+                           forced == GV_TC_STREAM;
+    if (forced == GV_TC_STREAM && opt_.precision != PREC_TF32X3)
+      throw Error(E_INVALID, "tuning entry asks for the streaming-epilogue tensor-core GEMM, which is split-TF32 only");
     if (forced_tc && !tc_allowed)
       throw Error(E_INVALID, "tuning entry asks for the tensor-core GEMM, which needs precision tf32x3, bf16x3 or "
                              "bf16x6 and a float32 or complex64 network");
@@ -871,6 +874,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       g.real = real_tc;
       const ll mt = (ll)(m + tc::BM - 1) / tc::BM, nt = (ll)(n + tc::BN - 1) / tc::BN;
       g.raster = forced == GV_TC_MFAST ? 1 : forced == GV_TC_NFAST ? 0 : -1;
+      g.stream = forced == GV_TC_STREAM;
       if (g.variant == GV_AUTO) g.variant = g.splits > 1 ? GV_TC_SPLITK : (mt <= nt ? GV_TC_MFAST : GV_TC_NFAST);
       g.a = Ref{Ref::WS, pa};
       g.b = Ref{Ref::WS, pb};
@@ -1767,10 +1771,11 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
-    const std::pair<decltype(&tc::k_tc_cgemm_tf32x3), int> kerns[3] = {
+    const std::pair<decltype(&tc::k_tc_cgemm_tf32x3), int> kerns[4] = {
         {tc::k_tc_cgemm_tf32x3, tc::Fmt<tc::FMT_TF32X3>::kSmemBytes},
         {tc::k_tc_cgemm_bf16x3, tc::Fmt<tc::FMT_BF16X3>::kSmemBytes},
-        {tc::k_tc_cgemm_bf16x6, tc::Fmt<tc::FMT_BF16X6>::kSmemBytes}};
+        {tc::k_tc_cgemm_bf16x6, tc::Fmt<tc::FMT_BF16X6>::kSmemBytes},
+        {tc::k_tc_cgemm_tf32x3_stream, tc::kStreamSmemBytes}};
     for (auto [kern, smem] : kerns) {
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       // The kernel's setmaxnreg split assumes exactly kLaunchRegs registers a thread at launch.
@@ -1828,7 +1833,9 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   if (dev < 64 && !sms[dev]) CK(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
   const int n_sm = dev < 64 ? sms[dev] : 148;
   const unsigned grid = (unsigned)std::min<ll>(items, n_sm);
-  if (op.six)
+  if (op.stream)
+    tc::k_tc_cgemm_tf32x3_stream<<<grid, tc::kThreads, tc::kStreamSmemBytes, st>>>(ma, mb, args);
+  else if (op.six)
     tc::k_tc_cgemm_bf16x6<<<grid, tc::kThreads, tc::Fmt<tc::FMT_BF16X6>::kSmemBytes, st>>>(ma, mb, args);
   else if (op.bf16)
     tc::k_tc_cgemm_bf16x3<<<grid, tc::kThreads, tc::Fmt<tc::FMT_BF16X3>::kSmemBytes, st>>>(ma, mb, args);
@@ -2311,7 +2318,7 @@ void Program::execute_gradient(int part, const void* const* inputs, const void* 
 
 const char* gemm_variant_name(int v) {
   static const char* names[GV_COUNT] = {"auto", "simt_small", "simt_tile64", "simt_tile32", "simt_warp",
-                                        "simt_tile128", "simt_dot", "tc_mfast", "tc_nfast", "tc_splitk"};
+                                        "simt_tile128", "simt_dot", "tc_mfast", "tc_nfast", "tc_splitk", "tc_stream"};
   return v >= 0 && v < GV_COUNT ? names[v] : "?";
 }
 

@@ -60,6 +60,12 @@ constexpr int kChunkTiles = 2;
 // K = 16 take as long as 3 TF32 MMAs of K = 8 over the same K.  Its 6 planes per operand fill a 96 KB stage,
 // so the ring holds 2 stages, and one stage (32 of K) per TMEM chunk keeps 24 MMAs per accumulator chain.
 enum : int { FMT_TF32X3 = 0, FMT_BF16X3 = 1, FMT_BF16X6 = 2 };
+// The streaming epilogue (kStream): two staging buffers, so that the next 32-row pass is staged while the
+// previous one is stored, with per-buffer mbarriers in place of block-wide barriers; its smem comes from a
+// two-stage operand ring.  Meant for GEMMs whose epilogue outweighs their MMA work (short K).
+constexpr int kStreamStages = 2;
+constexpr int kStreamSmemBytes = kStreamStages * STAGE_BYTES + 2 * STAGING_BYTES + 1024 + 1024;
+static_assert(kStreamSmemBytes <= 232448, "shared memory above the 227 KB a block may use");
 template <int F>
 struct Fmt {
   static constexpr bool kBF16 = F != FMT_TF32X3;
@@ -460,24 +466,28 @@ __device__ __forceinline__ void store_pass(const TcArgs& args, const EpiState& e
 
 // The GEMM body for either operand format: split-TF32 (4-byte planes, 16 of K per 64-byte operand row) or
 // split-BF16 (2-byte planes, 32 of K per row).  Shared-memory layout, swizzle, TMEM and epilogue are the same.
-template <int F>
+template <int F, bool kStream = false>
 __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcArgs& args) {
   using FM = Fmt<F>;
+  static_assert(!kStream || F == FMT_TF32X3, "the streaming epilogue is built for split-TF32 operands");
   constexpr bool kBF16 = FM::kBF16;
-  constexpr int STAGES = FM::kStages, STAGE_BYTES = FM::kStageBytes, PLANES = FM::kPlanes;
+  constexpr int STAGES = kStream ? kStreamStages : FM::kStages, STAGE_BYTES = FM::kStageBytes, PLANES = FM::kPlanes;
+  constexpr int kStagingBufs = kStream ? 2 : 1;
   constexpr int kChunkTiles = FM::kChunkTiles;
   constexpr int KT_ELEMS = kBF16 ? 2 * BK : BK;  // K per 64-byte operand row
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* ring = smem;                                  // STAGES x {A planes, B planes}
   cf32* stage = reinterpret_cast<cf32*>(smem + STAGES * STAGE_BYTES);  // kStageRows x kTileStride
-  uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES + STAGING_BYTES);
+  uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES + kStagingBufs * STAGING_BYTES);
   uint64_t* full = bars;                     // TMA landed                  (count 1 + tx)
   uint64_t* empty = bars + STAGES;           // MMAs done reading a stage   (commit)
   uint64_t* accfull = bars + 2 * STAGES;     // [2] a TMEM buffer's chunk is complete (commit)
   uint64_t* accempty = accfull + 2;          // [2] the drain warps have read it      (count kDrainThreads)
   uint64_t* drain = accempty + 2;            // abort drain                 (commit)
-  volatile uint32_t* tmem_slot = (volatile uint32_t*)(drain + 1);
+  uint64_t* sfull = drain + 1;               // [2] kStream: a staging buffer holds its pass (the 2 stager warps)
+  uint64_t* sempty = sfull + 2;              // [2] kStream: its pass is stored             (the 14 epilogue warps)
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(sempty + 2);
   volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -504,6 +514,7 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
     for (int i = 0; i < STAGES; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
     for (int i = 0; i < 2; ++i) { mbar_init(&accfull[i], 1); mbar_init(&accempty[i], kDrainThreads); }
     mbar_init(drain, 1);
+    for (int i = 0; i < 2; ++i) { mbar_init(&sfull[i], 2); mbar_init(&sempty[i], kEpiWarps); }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -517,9 +528,39 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
+  // kStream: global pass gp (4 per item) uses staging buffer gp & 1 for the (gp >> 1)-th time.  A pass is
+  // stored once sfull[b] completed that use, and its buffer is staged again once sempty[b] completed the use
+  // before; every wait is bounded and gives up at once after an abort.
+  auto stream_store = [&](const EpiState& es, const EpiTile& t, int gp, int rows, int cols, bool& dead) {
+    const int b = gp & 1, u = gp >> 1;
+    if (!dead && !mbar_wait_or_abort(&sfull[b], (uint32_t)(u & 1), args.err, 3, abort_flag)) {
+      dead = true;
+      *abort_flag = 1;
+    }
+    if (!dead) store_pass(args, es, t, stage + b * kStageRows * BN, gp & 3, rows, cols, threadIdx.x - 64);
+    __syncwarp();
+    if (!dead && (threadIdx.x & 31) == 0) mbar_arrive(&sempty[b]);
+  };
   // Store helpers (warps 2, 3, 12..15): they follow the drain warps' items and barriers and share the
   // stores of every staged pass.
   auto helpers = [&]() {
+    if constexpr (kStream) {
+      const EpiState es = epi_setup(args, warp - 2, lane);
+      bool dead = false;
+      int gp = 0;
+      for (int it = blockIdx.x; it < args.n_items; it += gridDim.x, gp += BM / kStageRows) {
+        const Item w = item_of(it);
+        const ll row0 = (ll)w.tile_m * BM, col0 = (ll)w.tile_n * BN;
+        const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
+        const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
+        const EpiTile t = epi_tile(args, w.z, w.split, row0, col0, lane);
+        for (int q = 0; q < BM / kStageRows; ++q) {
+          if (*abort_flag) dead = true;
+          stream_store(es, t, gp + q, rows, cols, dead);
+        }
+      }
+      return;
+    }
     const EpiState es = epi_setup(args, warp - 2, lane);
     bool dead = false;
     for (int it = blockIdx.x; it < args.n_items; it += gridDim.x) {
@@ -667,7 +708,7 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kDrainRegs));
     const int quad = warp % 4, half = (warp - 4) / 4;
     const EpiState es = epi_setup(args, warp - 2, lane);
-    int gc = 0;
+    int gc = 0, gpass = 0;
     bool dead = false;
     for (int it = blockIdx.x; it < args.n_items; it += gridDim.x) {
       const Item w = item_of(it);
@@ -707,6 +748,33 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
       // then all 14 epilogue warps store them.
       const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
       const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
+      if constexpr (kStream) {
+        // Pass q is staged by quadrant q's two drain warps one pass early (quadrant 0 before pass 0), into
+        // buffer gp & 1 once the pass that used it before is stored; all 14 warps store every pass.
+        auto stage_pass = [&](int g) {
+          const int b = g & 1, u = g >> 1;
+          if (!dead && u > 0 && !mbar_wait_or_abort(&sempty[b], (uint32_t)((u - 1) & 1), args.err, 4, abort_flag)) {
+            dead = true;
+            *abort_flag = 1;
+          }
+          if (!dead) {
+            cf32* sb = stage + b * kStageRows * BN;
+#pragma unroll
+            for (int j = 0; j < kHalfCols; ++j) sb[stage_at(lane, half * kHalfCols + j)] = cf32{acc_re[j], acc_im[j]};
+          }
+          __syncwarp();
+          if (!dead && lane == 0) mbar_arrive(&sfull[b]);
+        };
+        if (quad == 0) stage_pass(gpass);
+#pragma unroll 1
+        for (int q = 0; q < BM / kStageRows; ++q) {
+          if (quad == q + 1) stage_pass(gpass + q + 1);
+          if (*abort_flag) dead = true;
+          stream_store(es, t, gpass + q, rows, cols, dead);
+        }
+        gpass += BM / kStageRows;
+        continue;
+      }
 #pragma unroll 1
       for (int q = 0; q < BM / kStageRows; ++q) {
         asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");  // the previous rows are out
@@ -734,6 +802,12 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3(const __
                                                                 const __grid_constant__ CUtensorMap tmB,
                                                                 TcArgs args) {
   tc_cgemm_body<FMT_TF32X3>(tmA, tmB, args);
+}
+// Split-TF32 with the streaming epilogue (two-stage operand ring, double-buffered staging).
+static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3_stream(const __grid_constant__ CUtensorMap tmA,
+                                                                       const __grid_constant__ CUtensorMap tmB,
+                                                                       TcArgs args) {
+  tc_cgemm_body<FMT_TF32X3, true>(tmA, tmB, args);
 }
 // Split-BF16: operands packed as BF16 hi/lo planes, 3 BF16 products per real product (kind::f16).
 static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_bf16x3(const __grid_constant__ CUtensorMap tmA,

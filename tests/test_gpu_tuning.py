@@ -25,6 +25,8 @@ PRECS = {"fp32": C.PREC_FP32, "tf32x3": C.PREC_TF32X3, "bf16x3": C.PREC_BF16X3, 
 
 
 def valid(variant, dtype, precision):
+    if variant == "tc_stream":
+        return precision == "tf32x3" and dtype in (C.F32, C.C64)
     if variant.startswith("tc_"):
         return precision in ("tf32x3", "bf16x3", "bf16x6") and dtype in (C.F32, C.C64)
     return variant != "simt_tile128" or dtype == C.F32
