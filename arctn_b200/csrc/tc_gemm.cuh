@@ -773,17 +773,17 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
           stream_store(es, t, gpass + q, rows, cols, dead);
         }
         gpass += BM / kStageRows;
-        continue;
-      }
+      } else {
 #pragma unroll 1
-      for (int q = 0; q < BM / kStageRows; ++q) {
-        asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");  // the previous rows are out
-        if (quad == q && !dead) {
+        for (int q = 0; q < BM / kStageRows; ++q) {
+          asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");  // the previous rows are out
+          if (quad == q && !dead) {
 #pragma unroll
-          for (int j = 0; j < kHalfCols; ++j) stage[stage_at(lane, half * kHalfCols + j)] = cf32{acc_re[j], acc_im[j]};
+            for (int j = 0; j < kHalfCols; ++j) stage[stage_at(lane, half * kHalfCols + j)] = cf32{acc_re[j], acc_im[j]};
+          }
+          asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
+          if (!dead) store_pass(args, es, t, stage, q, rows, cols, threadIdx.x - 64);
         }
-        asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
-        if (!dead) store_pass(args, es, t, stage, q, rows, cols, threadIdx.x - 64);
       }
     }
   } else {
