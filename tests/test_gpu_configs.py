@@ -11,6 +11,8 @@
   complex64 executor.
 - The product's slice-range partition (tnmpi's contract_slice_range split over k ranks) summed on the
   host agrees with the full program and the oracle to 1e-12 (complex128).
+- The full headline (256 slices) through size-independent properties: doubling an input doubles the result
+  bit for bit at every precision, and a 4-way slice-range split sums to the whole to FP64 rounding.
 """
 
 import json
@@ -186,3 +188,35 @@ def test_slice_range_partition_matches_full_program(ranks):
     want = complex(O.contract_sliced(*net.as_tuple(), path, sliced, arrays, threads=4))
     assert rel(acc, full) <= 1e-12
     assert rel(acc, want) <= 1e-12
+
+
+# The full headline (all 256 slices) through properties that hold whatever the size: scaling one input by 2 is
+# exact in floating point (no value nears FP32's range limits), so the result doubles bit for bit, at every
+# precision; and the slice ranges of a 4-way split, summed, give the full contraction to FP64 rounding.
+@pytest.mark.parametrize("precision", ["tf32x3", "fp32", "bf16x6"])
+def test_headline_full_size_scaling_is_exact(headline, precision):
+    net, arrays, path, sliced, _, _ = headline
+    x = [torch.from_numpy(a).cuda() for a in arrays]
+    prog = A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex64, precision=precision,
+                           workspace_budget=24 << 30)
+    ws = torch.empty(max(prog.workspace_bytes, 1), dtype=torch.uint8, device="cuda")
+    base = complex(prog.execute(x, f64_out=True, workspace=ws).item())
+    for i in (0, len(x) // 2):
+        y = list(x)
+        y[i] = x[i] * 2
+        got = complex(prog.execute(y, f64_out=True, workspace=ws).item())
+        assert got == 2 * base, (precision, i, got, base)
+    assert prog.device_status(ws) == 0
+
+
+def test_headline_full_size_slice_ranges_sum_to_the_whole(headline):
+    net, arrays, path, sliced, _, _ = headline
+    x = [torch.from_numpy(a).cuda() for a in arrays]
+    kw = dict(dtype=np.complex64, precision="tf32x3", workspace_budget=24 << 30)
+    whole = complex(A.SlicedProgram(*net.as_tuple(), path, sliced, **kw).execute(x, f64_out=True).item())
+    parts = []
+    for r in range(4):
+        lo, hi = A.slice_range(256, 4, r)
+        p = A.SlicedProgram(*net.as_tuple(), path, sliced, slice_begin=lo, slice_end=hi, **kw)
+        parts.append(complex(p.execute(x, f64_out=True).item()))
+    assert abs(sum(parts) - whole) <= 1e-12 * sum(abs(v) for v in parts), (parts, whole)
