@@ -618,9 +618,11 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     int forced = GV_AUTO;
     if (auto it = opt_.tuning.find(g.key); it != opt_.tuning.end()) forced = it->second;
     const bool forced_tc = forced == GV_TC_MFAST || forced == GV_TC_NFAST || forced == GV_TC_SPLITK ||
-                           forced == GV_TC_STREAM;
+                           forced == GV_TC_STREAM || forced == GV_TC_DEEP;
     if (forced == GV_TC_STREAM && opt_.precision != PREC_TF32X3)
       throw Error(E_INVALID, "tuning entry asks for the streaming-epilogue tensor-core GEMM, which is split-TF32 only");
+    if (forced == GV_TC_DEEP && opt_.precision != PREC_TF32X3)
+      throw Error(E_INVALID, "tuning entry asks for the deep-ring tensor-core GEMM, which is split-TF32 only");
     if (forced_tc && !tc_allowed)
       throw Error(E_INVALID, "tuning entry asks for the tensor-core GEMM, which needs precision tf32x3, bf16x3 or "
                              "bf16x6 and a float32 or complex64 network");
@@ -875,6 +877,8 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       const ll mt = (ll)(m + tc::BM - 1) / tc::BM, nt = (ll)(n + tc::BN - 1) / tc::BN;
       g.raster = forced == GV_TC_MFAST ? 1 : forced == GV_TC_NFAST ? 0 : -1;
       g.stream = forced == GV_TC_STREAM;
+      g.deep = forced == GV_TC_DEEP;
+      if (g.deep && g.splits > 1) g.kt_chunk *= tc::BK / tc::kDeepBK;  // the deep ring's K tiles are 8 wide
       if (g.variant == GV_AUTO) g.variant = g.splits > 1 ? GV_TC_SPLITK : (mt <= nt ? GV_TC_MFAST : GV_TC_NFAST);
       g.a = Ref{Ref::WS, pa};
       g.b = Ref{Ref::WS, pb};
@@ -1707,17 +1711,18 @@ EncodeTiled encode_fn() {
 
 // [re|im][z][rows][kpad] fp32 planes, boxes of 16 x 128 with 64-byte swizzle.
 // Split-TF32 planes are fp32 (boxes of 16 x 128), split-BF16 planes bf16 (boxes of 32 x 128): 64-byte rows either way.
-CUtensorMap plane_map(void* base, ll kpad, ll rows, ll zplanes, bool bf16) {
+// The deep-ring kernel reads 8 of K per box (32-byte rows, 32-byte swizzle) from the same planes.
+CUtensorMap plane_map(void* base, ll kpad, ll rows, ll zplanes, bool bf16, bool deep = false) {
   CUtensorMap m;
   const ll el = bf16 ? 2 : 4;
   cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows, (cuuint64_t)zplanes};
   cuuint64_t strides[2] = {(cuuint64_t)(kpad * el), (cuuint64_t)(kpad * rows * el)};
-  cuuint32_t box[3] = {(cuuint32_t)(bf16 ? 2 * tc::BK : tc::BK), (cuuint32_t)tc::BM, 1};
+  cuuint32_t box[3] = {(cuuint32_t)(deep ? tc::kDeepBK : bf16 ? 2 * tc::BK : tc::BK), (cuuint32_t)tc::BM, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = encode_fn()(&m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base,
-                           dims, strides, box, estr,
-                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                           dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           deep ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_64B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) throw Error(E_CUDA, "cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
   return m;
 }
@@ -1771,11 +1776,12 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
-    const std::pair<decltype(&tc::k_tc_cgemm_tf32x3), int> kerns[4] = {
+    const std::pair<decltype(&tc::k_tc_cgemm_tf32x3), int> kerns[5] = {
         {tc::k_tc_cgemm_tf32x3, tc::Fmt<tc::FMT_TF32X3>::kSmemBytes},
         {tc::k_tc_cgemm_bf16x3, tc::Fmt<tc::FMT_BF16X3>::kSmemBytes},
         {tc::k_tc_cgemm_bf16x6, tc::Fmt<tc::FMT_BF16X6>::kSmemBytes},
-        {tc::k_tc_cgemm_tf32x3_stream, tc::kStreamSmemBytes}};
+        {tc::k_tc_cgemm_tf32x3_stream, tc::kStreamSmemBytes},
+        {tc::k_tc_cgemm_tf32x3_deep, tc::kDeepSmemBytes}};
     for (auto [kern, smem] : kerns) {
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       // The kernel's setmaxnreg split assumes exactly kLaunchRegs registers a thread at launch.
@@ -1790,13 +1796,13 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   const ll s_eff = (op.a_var || op.b_var) ? op.S : 1;
   const ll za = (op.a_var ? op.S : 1) * op.bt, zb = (op.b_var ? op.S : 1) * op.bt;
   const ll planes = op.six ? 6 : tc::PLANES;
-  const CUtensorMap ma = plane_map(A, op.kpad, op.rpad, planes * za, op.bf16);
-  const CUtensorMap mb = plane_map(B, op.kpad, op.rpad_b, planes * zb, op.bf16);
+  const CUtensorMap ma = plane_map(A, op.kpad, op.rpad, planes * za, op.bf16, op.deep);
+  const CUtensorMap mb = plane_map(B, op.kpad, op.rpad_b, planes * zb, op.bf16, op.deep);
   tc::TcArgs args;
   args.C = (cf32*)C;
   args.m = op.m;
   args.n = op.n;
-  args.k_tiles = (int)(op.kpad / (op.bf16 ? 2 * tc::BK : tc::BK));
+  args.k_tiles = (int)(op.kpad / (op.deep ? tc::kDeepBK : op.bf16 ? 2 * tc::BK : tc::BK));
   args.za = (int)za;
   args.zb = (int)zb;
   args.bt = (int)op.bt;
@@ -1833,7 +1839,9 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   if (dev < 64 && !sms[dev]) CK(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
   const int n_sm = dev < 64 ? sms[dev] : 148;
   const unsigned grid = (unsigned)std::min<ll>(items, n_sm);
-  if (op.stream)
+  if (op.deep)
+    tc::k_tc_cgemm_tf32x3_deep<<<grid, tc::kThreads, tc::kDeepSmemBytes, st>>>(ma, mb, args);
+  else if (op.stream)
     tc::k_tc_cgemm_tf32x3_stream<<<grid, tc::kThreads, tc::kStreamSmemBytes, st>>>(ma, mb, args);
   else if (op.six)
     tc::k_tc_cgemm_bf16x6<<<grid, tc::kThreads, tc::Fmt<tc::FMT_BF16X6>::kSmemBytes, st>>>(ma, mb, args);
@@ -2318,7 +2326,8 @@ void Program::execute_gradient(int part, const void* const* inputs, const void* 
 
 const char* gemm_variant_name(int v) {
   static const char* names[GV_COUNT] = {"auto", "simt_small", "simt_tile64", "simt_tile32", "simt_warp",
-                                        "simt_tile128", "simt_dot", "tc_mfast", "tc_nfast", "tc_splitk", "tc_stream"};
+                                        "simt_tile128", "simt_dot", "tc_mfast", "tc_nfast", "tc_splitk", "tc_stream",
+                                        "tc_deep"};
   return v >= 0 && v < GV_COUNT ? names[v] : "?";
 }
 

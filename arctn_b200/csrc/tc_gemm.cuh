@@ -66,6 +66,13 @@ enum : int { FMT_TF32X3 = 0, FMT_BF16X3 = 1, FMT_BF16X6 = 2 };
 constexpr int kStreamStages = 2;
 constexpr int kStreamSmemBytes = kStreamStages * STAGE_BYTES + 2 * STAGING_BYTES + 1024 + 1024;
 static_assert(kStreamSmemBytes <= 232448, "shared memory above the 227 KB a block may use");
+// The deep-ring variant (kDeep, split-TF32): 8 of K per stage (32-byte operand rows, 32-byte swizzle), so the
+// same 192 KB ring holds six stages and keeps five in flight instead of two -- more time to hide TMA latency
+// on long-K steps.  A TMEM chunk spans four stages, the same 32 of K as otherwise.
+constexpr int kDeepBK = 8, kDeepStages = 6;
+constexpr int kDeepStageBytes = 2 * PLANES * BM * kDeepBK * 4;  // 32 KB
+constexpr int kDeepSmemBytes = kDeepStages * kDeepStageBytes + STAGING_BYTES + 1024 + 1024;
+static_assert(kDeepSmemBytes <= 232448, "shared memory above the 227 KB a block may use");
 template <int F>
 struct Fmt {
   static constexpr bool kBF16 = F != FMT_TF32X3;
@@ -182,6 +189,11 @@ __device__ __forceinline__ void tma_load_3d(const CUtensorMap* map, uint64_t* ba
 __device__ __forceinline__ uint64_t sw64_desc(uint32_t saddr) {
   return (uint64_t)((saddr & 0x3FFFF) >> 4) | (1ull << 16) | ((uint64_t)(512 >> 4) << 32) | (1ull << 46) |
          (4ull << 61);
+}
+// K-major operand tile, 32-byte swizzle: rows of 32 B, 8-row groups 256 B apart (the deep-ring stages).
+__device__ __forceinline__ uint64_t sw32_desc(uint32_t saddr) {
+  return (uint64_t)((saddr & 0x3FFFF) >> 4) | (1ull << 16) | ((uint64_t)(256 >> 4) << 32) | (1ull << 46) |
+         (6ull << 61);
 }
 // kind::tf32, FP32 accumulate, K-major A and B, M = 128, N = 128.
 __host__ __device__ constexpr uint32_t idesc_tf32(bool neg_a) {
@@ -466,15 +478,20 @@ __device__ __forceinline__ void store_pass(const TcArgs& args, const EpiState& e
 
 // The GEMM body for either operand format: split-TF32 (4-byte planes, 16 of K per 64-byte operand row) or
 // split-BF16 (2-byte planes, 32 of K per row).  Shared-memory layout, swizzle, TMEM and epilogue are the same.
-template <int F, bool kStream = false>
+template <int F, bool kStream = false, bool kDeep = false>
 __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcArgs& args) {
   using FM = Fmt<F>;
   static_assert(!kStream || F == FMT_TF32X3, "the streaming epilogue is built for split-TF32 operands");
+  static_assert(!kDeep || (F == FMT_TF32X3 && !kStream), "the deep ring is built for split-TF32 operands");
   constexpr bool kBF16 = FM::kBF16;
-  constexpr int STAGES = kStream ? kStreamStages : FM::kStages, STAGE_BYTES = FM::kStageBytes, PLANES = FM::kPlanes;
+  constexpr int STAGES = kDeep ? kDeepStages : kStream ? kStreamStages : FM::kStages;
+  constexpr int STAGE_BYTES = kDeep ? kDeepStageBytes : FM::kStageBytes, PLANES = FM::kPlanes;
+  constexpr int PLANE_BYTES = kDeep ? BM * kDeepBK * 4 : tc::PLANE_BYTES;
   constexpr int kStagingBufs = kStream ? 2 : 1;
-  constexpr int kChunkTiles = FM::kChunkTiles;
-  constexpr int KT_ELEMS = kBF16 ? 2 * BK : BK;  // K per 64-byte operand row
+  constexpr int kChunkTiles = kDeep ? 4 : FM::kChunkTiles;
+  constexpr int KT_ELEMS = kDeep ? kDeepBK : kBF16 ? 2 * BK : BK;  // K per operand row of a stage
+  constexpr int KSTEPS = kDeep ? 1 : BK / 8;                        // MMA K steps per stage (32 bytes each)
+  auto sdesc = [](uint32_t a) { return kDeep ? sw32_desc(a) : sw64_desc(a); };
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* ring = smem;                                  // STAGES x {A planes, B planes}
@@ -668,22 +685,22 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
               const uint32_t hAr = a0, lAr = a0 + PLANE_BYTES, hAi = a0 + 2 * PLANE_BYTES, lAi = a0 + 3 * PLANE_BYTES;
               const uint32_t hBr = b0, lBr = b0 + PLANE_BYTES, hBi = b0 + 2 * PLANE_BYTES, lBi = b0 + 3 * PLANE_BYTES;
   #pragma unroll
-              for (int kk = 0; kk < BK / 8; ++kk) {
+              for (int kk = 0; kk < KSTEPS; ++kk) {
                 const uint32_t o = kk * 32;  // 8 tf32 or 16 bf16 = 32 bytes along the swizzled row
                 const uint32_t acc = first ? 0u : 1u;
                 // leading terms (hi,hi), then the corrections (lo,hi) and (hi,lo), all into this chunk's buffer
-                umma<kBF16>(cr, sw64_desc(hAr + o), sw64_desc(hBr + o), id_pos, acc);
-                umma<kBF16>(ci, sw64_desc(hAr + o), sw64_desc(hBi + o), id_pos, acc);
-                umma<kBF16>(cr, sw64_desc(hAi + o), sw64_desc(hBi + o), id_neg, 1);
-                umma<kBF16>(ci, sw64_desc(hAi + o), sw64_desc(hBr + o), id_pos, 1);
-                umma<kBF16>(cr, sw64_desc(lAr + o), sw64_desc(hBr + o), id_pos, 1);
-                umma<kBF16>(ci, sw64_desc(lAr + o), sw64_desc(hBi + o), id_pos, 1);
-                umma<kBF16>(cr, sw64_desc(lAi + o), sw64_desc(hBi + o), id_neg, 1);
-                umma<kBF16>(ci, sw64_desc(lAi + o), sw64_desc(hBr + o), id_pos, 1);
-                umma<kBF16>(cr, sw64_desc(hAr + o), sw64_desc(lBr + o), id_pos, 1);
-                umma<kBF16>(ci, sw64_desc(hAr + o), sw64_desc(lBi + o), id_pos, 1);
-                umma<kBF16>(cr, sw64_desc(hAi + o), sw64_desc(lBi + o), id_neg, 1);
-                umma<kBF16>(ci, sw64_desc(hAi + o), sw64_desc(lBr + o), id_pos, 1);
+                umma<kBF16>(cr, sdesc(hAr + o), sdesc(hBr + o), id_pos, acc);
+                umma<kBF16>(ci, sdesc(hAr + o), sdesc(hBi + o), id_pos, acc);
+                umma<kBF16>(cr, sdesc(hAi + o), sdesc(hBi + o), id_neg, 1);
+                umma<kBF16>(ci, sdesc(hAi + o), sdesc(hBr + o), id_pos, 1);
+                umma<kBF16>(cr, sdesc(lAr + o), sdesc(hBr + o), id_pos, 1);
+                umma<kBF16>(ci, sdesc(lAr + o), sdesc(hBi + o), id_pos, 1);
+                umma<kBF16>(cr, sdesc(lAi + o), sdesc(hBi + o), id_neg, 1);
+                umma<kBF16>(ci, sdesc(lAi + o), sdesc(hBr + o), id_pos, 1);
+                umma<kBF16>(cr, sdesc(hAr + o), sdesc(lBr + o), id_pos, 1);
+                umma<kBF16>(ci, sdesc(hAr + o), sdesc(lBi + o), id_pos, 1);
+                umma<kBF16>(cr, sdesc(hAi + o), sdesc(lBi + o), id_neg, 1);
+                umma<kBF16>(ci, sdesc(hAi + o), sdesc(lBr + o), id_pos, 1);
                 first = false;
               }
               umma_commit(&empty[s]);
@@ -808,6 +825,12 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3_stream(c
                                                                        const __grid_constant__ CUtensorMap tmB,
                                                                        TcArgs args) {
   tc_cgemm_body<FMT_TF32X3, true>(tmA, tmB, args);
+}
+// Split-TF32 with the deep ring (six 32 KB stages of 8 of K, 32-byte swizzle).
+static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3_deep(const __grid_constant__ CUtensorMap tmA,
+                                                                     const __grid_constant__ CUtensorMap tmB,
+                                                                     TcArgs args) {
+  tc_cgemm_body<FMT_TF32X3, false, true>(tmA, tmB, args);
 }
 // Split-BF16: operands packed as BF16 hi/lo planes, 3 BF16 products per real product (kind::f16).
 static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_bf16x3(const __grid_constant__ CUtensorMap tmA,

@@ -25,7 +25,7 @@ PRECS = {"fp32": C.PREC_FP32, "tf32x3": C.PREC_TF32X3, "bf16x3": C.PREC_BF16X3, 
 
 
 def valid(variant, dtype, precision):
-    if variant == "tc_stream":
+    if variant in ("tc_stream", "tc_deep"):
         return precision == "tf32x3" and dtype in (C.F32, C.C64)
     if variant.startswith("tc_"):
         return precision in ("tf32x3", "bf16x3", "bf16x6") and dtype in (C.F32, C.C64)
