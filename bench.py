@@ -104,6 +104,40 @@ def peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
 
 
+def per_step_roofline(prog, ms, tf32_pipe_tflops, hbm_gbs):
+    """Each tensor-core GEMM shape of the program against its own bound, from the op-by-op profile `ms`:
+    the tensor bound is its split-TF32 pipe work (3 TF32 products per real product) at the measured TF32 rate,
+    the memory bound its algorithmic bytes (16 B per packed operand element read, 16 B per packed or 8 B per
+    plain output element written) at the HBM rate; the step's bound is the larger of the two times."""
+    ops = prog.describe()["ops"]
+    units = {}
+    for i, o in enumerate(ops):
+        units.setdefault(o.get("unit", i), []).append(o)
+    order = [u for u in sorted(units) if units[u][0]["kind"] != "memset"]
+    agg = {}
+    for u, t in zip(order, ms):
+        o = units[u][0]
+        if o["kind"] != "gemm_tc":
+            continue
+        S, bt, m, k, n = o["S"], o["bt"], o["m"], o["k"], o["n"]
+        a = agg.setdefault((m, k, n), {"ms": 0.0, "flops": 0.0, "bytes": 0.0, "launches": 0,
+                                       "fused_output": "pack_into" in o})
+        a["ms"] += float(t)
+        a["launches"] += 1
+        a["flops"] += 8.0 * S * bt * m * k * n
+        a["bytes"] += 16.0 * bt * ((S if o["a_var"] else 1) * m * k + (S if o["b_var"] else 1) * k * n) + \
+            (16.0 if "pack_into" in o else 8.0) * S * bt * m * n
+    out = []
+    for (m, k, n), a in sorted(agg.items(), key=lambda kv: -kv[1]["ms"]):
+        t_tensor = 3 * a["flops"] / (tf32_pipe_tflops * 1e12) * 1e3
+        t_mem = a["bytes"] / (hbm_gbs * 1e9) * 1e3
+        out.append({"m_k_n": [m, k, n], "ms": round(a["ms"], 3), "launches": a["launches"],
+                    "fused_output": a["fused_output"], "tflops": a["flops"] / (a["ms"] * 1e-3) / 1e12,
+                    "gbs": a["bytes"] / (a["ms"] * 1e-3) / 1e9, "bound": "tensor" if t_tensor >= t_mem else "hbm",
+                    "frac_of_bound": max(t_tensor, t_mem) / a["ms"]})
+    return out
+
+
 def profiled_traffic():
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary, if present."""
     p = os.path.join(ROOT, "profiles", "k_tc_cgemm_tf32x3_rand3reg_n172.md")
@@ -972,6 +1006,7 @@ def main():
                 roof["pipe_frac_of_tf32_peak"] = achieved * 3 / tf32_peak
                 roof["pipe_frac_of_tf32_n128"] = achieved * 3 / pk_tc["tf32_n128"]
                 roof["tf32_peak_source"] = "measured: arctn_b200_tc_peak (tcgen05 kind::tf32, M=128, best N)"
+                roof["per_step"] = per_step_roofline(prog, ms, tf32_peak, pk["hbm_gbs"])
         else:
             achieved = tw / (tms * 1e-3) / 1e9
             roof = {"bound": "hbm", "kernel": KIND_NAMES.get(top, str(top)), "achieved": achieved,
