@@ -1,4 +1,5 @@
-// Tensor-pipe peak probe: the dense MMA rate of this GPU for the operand kinds the GEMMs use.
+// Tensor-pipe peak probe: the dense MMA rate of this GPU for the operand kinds the GEMMs use, and the rate of the
+// split-TF32 GEMM's own MMA stream over operands laid out as its ring (kind 2).
 //
 // Every SM runs one CTA whose single issuing thread streams `iters` tcgen05.mma instructions (M = 128,
 // N = 128 or 256, K = 8 for kind::tf32 / 16 for kind::f16 with BF16 operands) over operands that stay
@@ -72,6 +73,75 @@ __global__ void __launch_bounds__(128, 1) k_tc_peak(long long iters, int* err) {
   }
 }
 
+// The split-TF32 GEMM's own MMA stream without TMA or epilogue: per iteration (one 8-wide K step) the 12 MMAs of
+// the 4M product in the kernel's order, over A and B planes laid out as the GEMM's operand ring -- three
+// 64 KB stages of 8 planes, a new stage every two iterations -- into two accumulators (Cr, Ci).  Its rate is
+// the ceiling the GEMM's MMA phase can reach with operands streaming through shared memory.
+__global__ void __launch_bounds__(128, 1) k_tc_peak_stream(long long iters, int* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint32_t* words = (uint32_t*)smem;
+  for (int i = threadIdx.x; i < tc::STAGES * tc::STAGE_BYTES / 4; i += blockDim.x) words[i] = 0x3F800000u;
+  uint64_t* bar = (uint64_t*)(smem + tc::STAGES * tc::STAGE_BYTES);
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(bar + 1);
+  const int warp = threadIdx.x / 32;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tc::smem_u32((const void*)tmem_slot)),
+                 "r"(256u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  if (threadIdx.x == 32) {
+    const uint32_t base = tc::smem_u32(smem), P = tc::PLANE_BYTES;
+    const uint32_t cr = tmem, ci = tmem + 128;
+    const uint32_t pos = tc::idesc_tf32(false), neg = tc::idesc_tf32(true);
+    for (long long i = 0; i < iters; ++i) {
+      const uint32_t o = (uint32_t)(i & 1) * 32;
+      const uint32_t a0 = base + (uint32_t)((i / 2) % tc::STAGES) * tc::STAGE_BYTES, b0 = a0 + tc::PLANES * P;
+      const uint32_t hAr = a0 + o, lAr = hAr + P, hAi = hAr + 2 * P, lAi = hAr + 3 * P;
+      const uint32_t hBr = b0 + o, lBr = hBr + P, hBi = hBr + 2 * P, lBi = hBr + 3 * P;
+      const uint32_t acc = i > 0 ? 1u : 0u;
+      tc::umma<false>(cr, tc::sw64_desc(hAr), tc::sw64_desc(hBr), pos, acc);
+      tc::umma<false>(ci, tc::sw64_desc(hAr), tc::sw64_desc(hBi), pos, acc);
+      tc::umma<false>(cr, tc::sw64_desc(hAi), tc::sw64_desc(hBi), neg, 1);
+      tc::umma<false>(ci, tc::sw64_desc(hAi), tc::sw64_desc(hBr), pos, 1);
+      tc::umma<false>(cr, tc::sw64_desc(lAr), tc::sw64_desc(hBr), pos, 1);
+      tc::umma<false>(ci, tc::sw64_desc(lAr), tc::sw64_desc(hBi), pos, 1);
+      tc::umma<false>(cr, tc::sw64_desc(lAi), tc::sw64_desc(hBi), neg, 1);
+      tc::umma<false>(ci, tc::sw64_desc(lAi), tc::sw64_desc(hBr), pos, 1);
+      tc::umma<false>(cr, tc::sw64_desc(hAr), tc::sw64_desc(lBr), pos, 1);
+      tc::umma<false>(ci, tc::sw64_desc(hAr), tc::sw64_desc(lBi), pos, 1);
+      tc::umma<false>(cr, tc::sw64_desc(hAi), tc::sw64_desc(lBi), neg, 1);
+      tc::umma<false>(ci, tc::sw64_desc(hAi), tc::sw64_desc(lBr), pos, 1);
+    }
+    tc::umma_commit(bar);
+    tc::mbar_wait(bar, 0, err, 9);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u));
+  }
+}
+
+cudaError_t launch_peak_stream(int ctas, long long iters, int* err, cudaStream_t st) {
+  constexpr int smem = tc::STAGES * tc::STAGE_BYTES + 64 + 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_tc_peak_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  k_tc_peak_stream<<<ctas, 128, smem, st>>>(iters, err);
+  return cudaGetLastError();
+}
+
 template <bool kBF16, int N>
 cudaError_t launch_peak(int ctas, long long iters, int* err, cudaStream_t st) {
   constexpr int smem = (128 + N) * 64 + 64 + 1024;
@@ -89,8 +159,9 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
     ab2::set_last_error(m);
     return code;
   };
-  if (kind != 0 && kind != 1) return fail("kind must be 0 (tf32) or 1 (bf16)", ARCTN_B200_ERR_INVALID);
+  if (kind < 0 || kind > 2) return fail("kind must be 0 (tf32), 1 (bf16) or 2 (split-TF32 GEMM stream)", ARCTN_B200_ERR_INVALID);
   if (n != 128 && n != 256) return fail("n must be 128 or 256", ARCTN_B200_ERR_INVALID);
+  if (kind == 2 && n != 128) return fail("kind 2 runs the GEMM's N = 128 MMAs", ARCTN_B200_ERR_INVALID);
   if (iters < 2 || iters > (1ull << 22)) return fail("iters must lie in [2, 2^22]", ARCTN_B200_ERR_INVALID);
   if (!status || !tflops_out) return fail("status and tflops_out must not be null", ARCTN_B200_ERR_INVALID);
   int dev = 0, sms = 0;
@@ -104,7 +175,8 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
   const long long it = (long long)iters;
   int* err = (int*)status;
   if (e == cudaSuccess) {
-    if (kind == 0) e = n == 128 ? launch_peak<false, 128>(sms, it, err, st) : launch_peak<false, 256>(sms, it, err, st);
+    if (kind == 2) e = launch_peak_stream(sms, it, err, st);
+    else if (kind == 0) e = n == 128 ? launch_peak<false, 128>(sms, it, err, st) : launch_peak<false, 256>(sms, it, err, st);
     else e = n == 128 ? launch_peak<true, 128>(sms, it, err, st) : launch_peak<true, 256>(sms, it, err, st);
   }
   if (e == cudaSuccess) e = cudaEventRecord(e1, st);
@@ -114,8 +186,8 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (e != cudaSuccess) return fail(std::string("tensor-core peak probe: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
-  const double k = kind == 0 ? 8.0 : 16.0;
-  *tflops_out = 2.0 * 128.0 * n * k * (double)iters * sms / (ms * 1e-3) / 1e12;
+  const double k = kind == 1 ? 16.0 : 8.0, per_iter = kind == 2 ? 12.0 : 1.0;  // kind 2: 12 MMAs an iteration
+  *tflops_out = 2.0 * 128.0 * n * k * per_iter * (double)iters * sms / (ms * 1e-3) / 1e12;
   ab2::set_last_error("");
   return ARCTN_B200_OK;
 }

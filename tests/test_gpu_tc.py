@@ -137,6 +137,11 @@ def test_tensor_pipe_peak_probe(kind):
     assert all(100.0 < r < 5000.0 for r in rates.values()), rates
     if kind == "bf16":
         assert rates[256] > A.tensor_pipe_peak("tf32", 256, iters=1 << 14, repeats=1)
+    else:
+        # the GEMM's own MMA sequence over streamed operands cannot beat resident operands by much
+        stream = A.tensor_pipe_peak("tf32_gemm_stream", 128, iters=1 << 12, repeats=1)
+        print("tf32 gemm stream", stream)
+        assert 100.0 < stream < 1.1 * max(rates.values()), (stream, rates)
 
 
 def test_bf16x6_rand3reg_n104_matches_fp64_oracle():
