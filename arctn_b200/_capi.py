@@ -91,6 +91,7 @@ SIGNATURES = [
     ("arctn_b200_program_create_tuned", c_int, [NETP, u64, u64p, u64, u32p, ctypes.POINTER(ProgramOptions),
                                                 ctypes.POINTER(GemmChoice), u64, ctypes.POINTER(vp)]),
     ("arctn_b200_program_gemms", c_int, [vp, ctypes.POINTER(GemmChoice), ctypes.POINTER(c_int), u64, u64p]),
+    ("arctn_b200_program_set_tc_chain", c_int, [vp, u64]),
     ("arctn_b200_program_destroy", None, [vp]),
     ("arctn_b200_program_workspace_size", u64, [vp]),
     ("arctn_b200_program_n_slices", u64, [vp]),

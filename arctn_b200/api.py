@@ -278,7 +278,7 @@ class SlicedProgram:
 
     def __init__(self, inputs, output, size_dict, ssa_path, sliced_legs=(), *, dtype="complex64",
                  precision="fp32", device=None, use_graph=True, max_slices_per_group=0, workspace_budget=0,
-                 slice_begin=0, slice_end=0, gradient=False, tc_k_chunk=0, tuning=None):
+                 slice_begin=0, slice_end=0, gradient=False, tc_k_chunk=0, tuning=None, tc_chain_k=None):
         torch = _torch()
         self.inputs = [[int(l) for l in t] for t in inputs]
         self.output = [int(l) for l in output]
@@ -318,6 +318,8 @@ class SlicedProgram:
         self._h = h
         self._lock = threading.Lock()
         L = C.lib()
+        if tc_chain_k is not None:  # K per TMEM chain of the split-TF32 GEMMs (default 64; gradient programs 32)
+            C.check(L.arctn_b200_program_set_tc_chain(h, int(tc_chain_k)), "sliced contraction failed")
         self.workspace_bytes = int(L.arctn_b200_program_workspace_size(h))
         self.n_slices = int(L.arctn_b200_program_n_slices(h))
         self.slices_per_group = int(L.arctn_b200_program_slices_per_group(h))

@@ -364,6 +364,13 @@ int arctn_b200_program_create_tuned(const arctn_b200_network* net, uint64_t n_st
   });
 }
 
+int arctn_b200_program_set_tc_chain(arctn_b200_program* p, uint64_t k_per_chain) {
+  return guarded([&] {
+    if (!p) fail("null argument");
+    p->p->set_tc_chain((int)std::min<uint64_t>(k_per_chain, 1u << 20));
+  });
+}
+
 int arctn_b200_program_gemms(const arctn_b200_program* p, arctn_b200_gemm_choice* out, int* tuned_out, uint64_t cap,
                              uint64_t* n_out) {
   return guarded([&] {

@@ -86,6 +86,7 @@ struct Op {
   int raster = -1;                      // GEMM_TC tile order: 1 m-tiles fastest, 0 n-tiles fastest, -1 smaller side fastest
   bool stream = false;                  // GEMM_TC: the streaming-epilogue kernel (two-stage ring, double staging)
   bool deep = false;                    // GEMM_TC: the deep-ring kernel (six stages of 8 of K)
+  int chunk_mul = 1;                    // GEMM_TC: TMEM accumulation chunk in units of the format's 32 of K
   // GEMM kinds: the shape key, the variant that runs (never GV_AUTO) and whether a tuning table chose it.
   GemmKey key;
   int variant = GV_AUTO;
@@ -159,6 +160,9 @@ class Program {
   u64 n_inputs() const { return plan_.n_inputs; }
   // JSON description of the launch sequence and workspace layout (host-only; no GPU needed).
   std::string describe() const;
+  // K per TMEM accumulation chain of the split-TF32 tensor-core GEMMs (32, 64 or 128): changes launch
+  // parameters only, so the next graph execute re-captures.
+  void set_tc_chain(int k_per_chain);
   // Every GEMM op in launch order: its shape key, the variant it runs and whether the tuning table chose it.
   struct GemmChoice { GemmKey key; int variant; bool tuned; size_t op; };
   std::vector<GemmChoice> gemm_choices() const;

@@ -276,6 +276,9 @@ struct TcArgs {
   // address are multiples of 4 floats: a quarter-warp then stores one chunk with 16-byte stores (4 chunks
   // per warp step, 4 stores per element quadruple instead of 16).
   int pk_vec = 0;
+  // K tiles per TMEM accumulation chunk (0: the format's default, 32 of K).  Longer chunks drain TMEM less
+  // often and let the MMA run further ahead of an epilogue, at a longer truncated-FP32 chain per chunk.
+  int chunk_tiles = 0;
 };
 
 #define AB2_TMEM_LD16(taddr, r)                                                                                   \
@@ -488,7 +491,7 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
   constexpr int STAGE_BYTES = kDeep ? kDeepStageBytes : FM::kStageBytes, PLANES = FM::kPlanes;
   constexpr int PLANE_BYTES = kDeep ? BM * kDeepBK * 4 : tc::PLANE_BYTES;
   constexpr int kStagingBufs = kStream ? 2 : 1;
-  constexpr int kChunkTiles = kDeep ? 4 : FM::kChunkTiles;
+  const int kChunkTiles = args.chunk_tiles > 0 ? args.chunk_tiles : (kDeep ? 4 : FM::kChunkTiles);
   constexpr int KT_ELEMS = kDeep ? kDeepBK : kBF16 ? 2 * BK : BK;  // K per operand row of a stage
   constexpr int KSTEPS = kDeep ? 1 : BK / 8;                        // MMA K steps per stage (32 bytes each)
   auto sdesc = [](uint32_t a) { return kDeep ? sw32_desc(a) : sw64_desc(a); };

@@ -246,6 +246,12 @@ int arctn_b200_program_create_tuned(const arctn_b200_network* net, uint64_t n_st
  * may be null); *n_out = the full count.  Host-only.  No reference counterpart. */
 int arctn_b200_program_gemms(const arctn_b200_program* program, arctn_b200_gemm_choice* out, int* tuned_out,
                              uint64_t cap, uint64_t* n_out);
+/* K summed per TMEM accumulation chain by the split-TF32 tensor-core GEMMs before the FP32 register sum: 32, 64
+ * or 128.  Programs default to 64 (32 for gradient programs, whose long-K adjoint GEMMs carry the tightest
+ * error budget).  Longer chains drain TMEM less often and let the MMAs run further ahead of each epilogue,
+ * at a longer truncated-FP32 chain per chunk.  Changes launch parameters only; the next execute re-captures
+ * its graph.  Not thread-safe against a concurrent execute of the same program.  No reference counterpart. */
+int arctn_b200_program_set_tc_chain(arctn_b200_program* program, uint64_t k_per_chain);
 void arctn_b200_program_destroy(arctn_b200_program* program);
 uint64_t arctn_b200_program_workspace_size(const arctn_b200_program* program);
 uint64_t arctn_b200_program_n_slices(const arctn_b200_program* program);

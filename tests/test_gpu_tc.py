@@ -117,7 +117,8 @@ def test_epilogue_packs_are_bit_identical_to_separate_packs():
     net, arrays = N.workload_rand3reg(104, 2, 1, np.complex64, seed=0)
     path = A.greedy(*net.as_tuple())
     sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 14)
-    kw = dict(dtype=np.complex64, precision="tf32x3", max_slices_per_group=4)
+    # the same TMEM chain length in both (forward programs default to 64 of K, gradient programs to 32)
+    kw = dict(dtype=np.complex64, precision="tf32x3", max_slices_per_group=4, tc_chain_k=64)
     fused = A.SlicedProgram(*net.as_tuple(), path, sliced, **kw)
     plain = A.SlicedProgram(*net.as_tuple(), path, sliced, gradient=True, **kw)
     assert any("pack_into" in o for o in fused.describe()["ops"])
@@ -163,3 +164,23 @@ def test_bf16x6_rand3reg_n104_matches_fp64_oracle():
     print("rand3reg n104 rel err", errs)
     assert errs["bf16x6"] <= 1e-5
     assert errs["bf16x6"] <= max(2 * errs["tf32x3"], 2e-6)
+
+
+def test_tmem_chain_lengths_match_fp64_oracle():
+    # 32, 64 (the forward default) and 128 of K per TMEM chain before the FP32 register sum: all within the
+    # 1e-5 the complex64 path is held to on rand3reg n=104 (16 slices), the error growing with the chain.
+    from arctn_b200 import _capi as C
+    from arctn_b200 import networks as N
+
+    net, arrays = N.workload_rand3reg(104, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 14)
+    want = complex(O.contract_sliced(*net.as_tuple(), path, sliced, O.promote(arrays), threads=8))
+    prog = A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex64, precision="tf32x3")
+    errs = {}
+    for k in (32, 64, 128):
+        C.check(C.lib().arctn_b200_program_set_tc_chain(prog._h, k))
+        assert all(o["tmem_chunk_k"] == k for o in prog.describe()["ops"] if o["kind"] == "gemm_tc")
+        errs[k] = abs(complex(prog.execute(arrays, f64_out=True)) - want) / abs(want)
+    print("tmem chain errors", errs)
+    assert max(errs.values()) <= 1e-5

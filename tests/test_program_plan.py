@@ -307,3 +307,21 @@ def test_gradient_program_dag_orders_every_pair_of_ops_sharing_memory(precision)
         net, arrays = nets[j]
         p = program(net, A.greedy(*net.as_tuple()), dtype=arrays[0].dtype, precision=precision, gradient=True)
         _dag_orders_every_overlap(p.describe()["ops"])
+
+
+def test_tmem_chain_defaults_and_setter():
+    # Forward split-TF32 programs sum 64 of K per TMEM chain, gradient programs 32; the setter changes every
+    # split-TF32 GEMM and rejects other lengths; BF16 formats keep theirs.
+    from arctn_b200 import _capi as C
+
+    net, _ = N.workload_rand3reg(104, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 14)
+    chains = lambda p: {o["tmem_chunk_k"] for o in p.describe()["ops"] if o["kind"] == "gemm_tc"}  # noqa: E731
+    fwd = program(net, path, sliced, dtype=np.complex64, precision="tf32x3")
+    grad = program(net, path, sliced, dtype=np.complex64, precision="tf32x3", gradient=True)
+    assert chains(fwd) == {64} and chains(grad) == {32}
+    assert chains(program(net, path, sliced, dtype=np.complex64, precision="tf32x3", tc_chain_k=128)) == {128}
+    assert chains(program(net, path, sliced, dtype=np.complex64, precision="bf16x3")) == {64}
+    assert chains(program(net, path, sliced, dtype=np.complex64, precision="bf16x6")) == {32}
+    assert C.lib().arctn_b200_program_set_tc_chain(fwd._h, 48) == C.ERR_INVALID
