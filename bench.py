@@ -11,10 +11,14 @@ elements and needs no slicing at 2^24).
 One step = one full sliced contraction (all 256 slices) of inputs resident in
 HBM.  TFLOP/s counts 8 real flops per complex MAC over every pairwise GEMM of
 every slice (the reference's per-slice work x n_slices).  The headline runs
-the split-TF32 tensor-core path; the same line reports the plain-FP32 form's
-TFLOP/s and both results' relative error against an FP64 contraction.
+the split-TF32 tensor-core path with its GEMM kernels autotuned before timing;
+the same line reports the plain-FP32 form's TFLOP/s, both results' relative
+error against an FP64 contraction, the oracle on a slice sample, the staged
+scheduler's form, the roofline per tensor-core step and, under `configs`, the
+other configurations (grid6, rand3reg n=64, brickwork, grid8, the 256-network
+batch), each also available alone through --workload.
 
-    python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference] [--precision tf32x3|fp32]
+    python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference] [--precision tf32x3|fp32|bf16x3|bf16x6]
 
 Under torchrun each rank contracts a contiguous range of slices (the
 reference's MPI slice_range, src/bin/tnmpi.rs:279-284) and one NCCL
