@@ -10,7 +10,7 @@
 // 4M complex product is 12 TF32 MMAs per 8-wide K step into TMEM accumulators:
 //   Cr += Ar*Br - Ai*Bi,  Ci += Ar*Bi + Ai*Br   for (hi,hi), (hi,lo), (lo,hi),
 // the minus through the instruction's negate-A bit.  Accumulation is FP32: short
-// chains in TMEM, summed across chains in registers.
+// chains in TMEM (32 or 64 of K), summed across chains in registers.
 //
 // Persistent: one CTA per SM walks a list of 128x128 output tiles (work items).
 // Warp roles (512 threads, four warpgroups):
@@ -48,7 +48,8 @@ static_assert(SMEM_BYTES <= 232448, "shared memory above the 227 KB a block may 
 // thread fills one buffer with kChunkTiles K tiles (all 12 products per 8-wide K step) while the drain
 // warps read the other and add it into FP32 registers with round-to-nearest.  The tensor core's FP32
 // accumulation truncates once per MMA, so keeping each TMEM chain short (24 MMAs per accumulator at
-// kChunkTiles = 2) bounds that biased error; the long sum over K happens in the drain registers.
+// kChunkTiles = 2, the format default; TcArgs::chunk_tiles doubles it for forward programs) bounds that
+// biased error; the long sum over K happens in the drain registers.
 constexpr uint32_t TMEM_COLS = 512;
 constexpr int kChunkTiles = 2;
 
