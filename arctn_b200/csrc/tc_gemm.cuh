@@ -307,6 +307,24 @@ __device__ __forceinline__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parit
   }
 }
 
+// Bounded wait until a shared-memory arrival counter reaches target (acquire); same exits as above.
+__device__ __forceinline__ bool count_wait_or_abort(const volatile uint32_t* c, uint32_t target, int* err,
+                                                    int code, volatile int* abort_flag) {
+  const unsigned long long t0 = now_ns();
+  for (uint32_t i = 1; *c < target; ++i) {
+    if ((i & 63) == 0) {
+      if (*abort_flag) return false;
+      if (now_ns() - t0 > kWaitNs) {
+        atomicCAS(err, 0, code);
+        return false;
+      }
+      __nanosleep(64);
+    }
+  }
+  __threadfence_block();
+  return true;
+}
+
 // Staging layout of 32 output rows x 128 complex columns: row r, column c sits at r * BN + (c ^ g(r mod 16)),
 // g(q) = (q & 3) << 2 | q >> 2.  A stager warp (lanes = 32 rows, one column) and a row reader (lanes = 32
 // columns) both meet 16 distinct 8-byte bank pairs per half-warp, and so does a packed chunk spanning
@@ -317,14 +335,15 @@ __device__ __forceinline__ int stage_at(int r, int c) {
 }
 
 // Per-thread epilogue state.  For the fused pack: the lane's chunk pattern (dr, dc) and this warp's
-// chunk entries, loaded once per kernel (the chunk table is the same for every tile): warp ew takes
-// chunks qbeg[q] + ew + kEpiWarps * k of quadrant q, slot s = q * kq + k, held by lane s % 32 in e0
-// (s < 32) or e1; entries past a quadrant's end hold r0 = 0x7FFF (out of every tile).
+// chunk entries, loaded once per kernel (the chunk table is the same for every tile): storer warp ew of nw
+// takes chunks qbeg[q] + ew + nw * k of quadrant q, slot s = q * kq + k, held by lane s % 32 in e0
+// (s < 32) or e1; entries past a quadrant's end hold r0 = 0x7FFF (out of every tile).  A quadrant has at
+// most 32 x 128 / 32 = 128 chunks, so kq <= 10 for 14 storers and kq <= 16 for 8: 64 slots suffice.
 struct EpiState {
   int dr = 0, dc = 0, kq = 0;
   int2 e0 = make_int2(0x7FFF0000, 0), e1 = make_int2(0x7FFF0000, 0);
 };
-__device__ __forceinline__ EpiState epi_setup(const TcArgs& args, int ew, int lane) {
+__device__ __forceinline__ EpiState epi_setup(const TcArgs& args, int ew, int lane, int nw = kEpiWarps) {
   EpiState st;
   if (!args.pk) return st;
   const int lp = __ldg(args.pk_lane + lane);
@@ -334,13 +353,13 @@ __device__ __forceinline__ EpiState epi_setup(const TcArgs& args, int ew, int la
   int most = 0;
 #pragma unroll
   for (int q = 0; q < BM / kStageRows; ++q) most = max(most, args.pk_qbeg[q + 1] - args.pk_qbeg[q]);
-  st.kq = (most + kEpiWarps - 1) / kEpiWarps;
+  st.kq = (most + nw - 1) / nw;
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     const int slot = lane + 32 * h, q = st.kq ? slot / st.kq : 0, k = st.kq ? slot % st.kq : 0;
     int2 e = make_int2(0x7FFF0000, 0);
     if (q < BM / kStageRows) {
-      const int ci = args.pk_qbeg[q] + ew + kEpiWarps * k;
+      const int ci = args.pk_qbeg[q] + ew + nw * k;
       if (ci < args.pk_qbeg[q + 1]) e = __ldg(args.pk_chunk + ci);
     }
     if (h == 0) st.e0 = e; else st.e1 = e;
@@ -378,9 +397,10 @@ __device__ __forceinline__ void put_pair(float* hi, float* lo, ll o, float x) {
 }
 
 // One pass of the epilogue store: output rows [r_lo, r_lo + 32) of the tile, staged in `stage`, written
-// by epilogue warp ew (0..13) / thread et (0..447) either as C rows or as packed 32-float chunks.
+// by storer thread et of nthreads (the 14 epilogue warps; 8 in the streaming epilogue), either as C rows or
+// as packed 32-float chunks (the warp's chunks are in es, from epi_setup with the same storer count).
 __device__ __forceinline__ void store_pass(const TcArgs& args, const EpiState& es, const EpiTile& t, const cf32* stage,
-                                           int q, int rows, int cols, int et) {
+                                           int q, int rows, int cols, int et, int nthreads = kEpiThreads) {
   const int r_lo = q * kStageRows;
   if (r_lo >= rows) return;
   if (args.pk && args.pk_vec) {
@@ -464,16 +484,16 @@ __device__ __forceinline__ void store_pass(const TcArgs& args, const EpiState& e
     const int nr = rows - r_lo < kStageRows ? rows - r_lo : kStageRows;
     cf32* cbase = t.cbase + (ll)r_lo * args.n;
     constexpr int U = 4;
-    for (int e0 = et; e0 < nr * BN; e0 += U * kEpiThreads) {
+    for (int e0 = et; e0 < nr * BN; e0 += U * nthreads) {
       cf32 v[U];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * kEpiThreads, r = e / BN, c = e % BN;
+        const int e = e0 + u * nthreads, r = e / BN, c = e % BN;
         v[u] = (e < nr * BN && c < cols) ? stage[stage_at(r, c)] : cf32{0.f, 0.f};
       }
 #pragma unroll
       for (int u = 0; u < U; ++u) {
-        const int e = e0 + u * kEpiThreads, r = e / BN, c = e % BN;
+        const int e = e0 + u * nthreads, r = e / BN, c = e % BN;
         if (e < nr * BN && c < cols) cbase[(ll)r * args.n + c] = v[u];
       }
     }
@@ -507,8 +527,11 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
   uint64_t* accempty = accfull + 2;          // [2] the drain warps have read it      (count kDrainThreads)
   uint64_t* drain = accempty + 2;            // abort drain                 (commit)
   uint64_t* sfull = drain + 1;               // [2] kStream: a staging buffer holds its pass (the 2 stager warps)
-  uint64_t* sempty = sfull + 2;              // [2] kStream: its pass is stored             (the 14 epilogue warps)
-  volatile uint32_t* tmem_slot = (volatile uint32_t*)(sempty + 2);
+  // [2] kStream: storer warps done with a staging buffer, counted over all its uses (8 per use).  A counter,
+  // not an mbarrier: a buffer's consecutive uses are staged by different quadrants, which may drift two uses
+  // apart, and a phase-parity wait cannot tell those apart.
+  volatile uint32_t* sdone = (volatile uint32_t*)(sfull + 2);
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(sfull + 4);
   volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -535,7 +558,7 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
     for (int i = 0; i < STAGES; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
     for (int i = 0; i < 2; ++i) { mbar_init(&accfull[i], 1); mbar_init(&accempty[i], kDrainThreads); }
     mbar_init(drain, 1);
-    for (int i = 0; i < 2; ++i) { mbar_init(&sfull[i], 2); mbar_init(&sempty[i], kEpiWarps); }
+    for (int i = 0; i < 2; ++i) { mbar_init(&sfull[i], 2); sdone[i] = 0; }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -549,24 +572,37 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  // kStream: global pass gp (4 per item) uses staging buffer gp & 1 for the (gp >> 1)-th time.  A pass is
-  // stored once sfull[b] completed that use, and its buffer is staged again once sempty[b] completed the use
-  // before; every wait is bounded and gives up at once after an abort.
-  auto stream_store = [&](const EpiState& es, const EpiTile& t, int gp, int rows, int cols, bool& dead) {
+  // kStream: global pass gp (4 per item) uses staging buffer gp & 1 for the (gp >> 1)-th time, u.  A pass is
+  // stored once sfull[b] completed use u, and its buffer is staged again once sdone[b] counts the stores of
+  // uses 0..u-1; every wait is bounded and gives up at once after an abort.  A storer waits on sfull[b] only
+  // after it stored use u-1 and before it stores use u, and use u+1 is staged only after that store, so the
+  // barrier is never two phases away from its waiter and the parity wait is exact.
+  // Storers of a streamed pass: the six helpers (ranks 0..5) and the two drain warps that staged it (ranks 6, 7).
+  constexpr int kStreamStorers = 8;
+  // epi_setup holds a storer's chunks of all four passes in the 64 slots of a warp's two int2 registers.
+  static_assert(BM / kStageRows * ((kStageRows * BN / 32 + kStreamStorers - 1) / kStreamStorers) <= 64,
+                "a streamed pass's packed chunks do not fit a storer warp's slots");
+  auto stream_store = [&](const EpiState& es, const EpiTile& t, int gp, int rows, int cols, bool& dead, int rank) {
     const int b = gp & 1, u = gp >> 1;
     if (!dead && !mbar_wait_or_abort(&sfull[b], (uint32_t)(u & 1), args.err, 3, abort_flag)) {
       dead = true;
       *abort_flag = 1;
     }
-    if (!dead) store_pass(args, es, t, stage + b * kStageRows * BN, gp & 3, rows, cols, threadIdx.x - 64);
+    if (!dead)
+      store_pass(args, es, t, stage + b * kStageRows * BN, gp & 3, rows, cols, rank * 32 + (threadIdx.x & 31),
+                 kStreamStorers * 32);
     __syncwarp();
-    if (!dead && (threadIdx.x & 31) == 0) mbar_arrive(&sempty[b]);
+    if (!dead && (threadIdx.x & 31) == 0) {
+      __threadfence_block();  // this warp's reads of the buffer come before the count
+      atomicAdd((uint32_t*)&sdone[b], 1u);
+    }
   };
   // Store helpers (warps 2, 3, 12..15): they follow the drain warps' items and barriers and share the
   // stores of every staged pass.
   auto helpers = [&]() {
     if constexpr (kStream) {
-      const EpiState es = epi_setup(args, warp - 2, lane);
+      const int rank = warp < 4 ? warp - 2 : warp - 10;  // warps 2, 3, 12..15 -> storer ranks 0..5
+      const EpiState es = epi_setup(args, rank, lane, kStreamStorers);
       bool dead = false;
       int gp = 0;
       for (int it = blockIdx.x; it < args.n_items; it += gridDim.x, gp += BM / kStageRows) {
@@ -577,7 +613,7 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
         const EpiTile t = epi_tile(args, w.z, w.split, row0, col0, lane);
         for (int q = 0; q < BM / kStageRows; ++q) {
           if (*abort_flag) dead = true;
-          stream_store(es, t, gp + q, rows, cols, dead);
+          stream_store(es, t, gp + q, rows, cols, dead, rank);
         }
       }
       return;
@@ -729,6 +765,7 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kDrainRegs));
     const int quad = warp % 4, half = (warp - 4) / 4;
     const EpiState es = epi_setup(args, warp - 2, lane);
+    [[maybe_unused]] const EpiState es_stream = kStream ? epi_setup(args, 6 + half, lane, 8) : EpiState{};
     int gc = 0, gpass = 0;
     bool dead = false;
     for (int it = blockIdx.x; it < args.n_items; it += gridDim.x) {
@@ -770,11 +807,14 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
       const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
       const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
       if constexpr (kStream) {
-        // Pass q is staged by quadrant q's two drain warps one pass early (quadrant 0 before pass 0), into
-        // buffer gp & 1 once the pass that used it before is stored; all 14 warps store every pass.
+        // Pass q is staged by quadrant q's two drain warps into buffer gp & 1 once the pass that used it before
+        // is stored, then stored by those two warps and the six helpers.  A drain warp's part of the epilogue
+        // ends with its own quadrant's pass, so it goes on to drain the next item while the helpers still store
+        // the later passes of this one.
         auto stage_pass = [&](int g) {
           const int b = g & 1, u = g >> 1;
-          if (!dead && u > 0 && !mbar_wait_or_abort(&sempty[b], (uint32_t)((u - 1) & 1), args.err, 4, abort_flag)) {
+          if (!dead && u > 0 &&
+              !count_wait_or_abort(&sdone[b], (uint32_t)(kStreamStorers * u), args.err, 4, abort_flag)) {
             dead = true;
             *abort_flag = 1;
           }
@@ -786,13 +826,9 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
           __syncwarp();
           if (!dead && lane == 0) mbar_arrive(&sfull[b]);
         };
-        if (quad == 0) stage_pass(gpass);
-#pragma unroll 1
-        for (int q = 0; q < BM / kStageRows; ++q) {
-          if (quad == q + 1) stage_pass(gpass + q + 1);
-          if (*abort_flag) dead = true;
-          stream_store(es, t, gpass + q, rows, cols, dead);
-        }
+        if (*abort_flag) dead = true;
+        stage_pass(gpass + quad);
+        stream_store(es_stream, t, gpass + quad, rows, cols, dead, 6 + half);
         gpass += BM / kStageRows;
       } else {
 #pragma unroll 1
