@@ -618,9 +618,11 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     int forced = GV_AUTO;
     if (auto it = opt_.tuning.find(g.key); it != opt_.tuning.end()) forced = it->second;
     const bool forced_tc = forced == GV_TC_MFAST || forced == GV_TC_NFAST || forced == GV_TC_SPLITK ||
-                           forced == GV_TC_STREAM || forced == GV_TC_DEEP;
+                           forced == GV_TC_STREAM || forced == GV_TC_DEEP || forced == GV_TC_PAIR;
     if (forced == GV_TC_STREAM && opt_.precision != PREC_TF32X3)
       throw Error(E_INVALID, "tuning entry asks for the streaming-epilogue tensor-core GEMM, which is split-TF32 only");
+    if (forced == GV_TC_PAIR && opt_.precision != PREC_TF32X3)
+      throw Error(E_INVALID, "tuning entry asks for the CTA-pair tensor-core GEMM, which is split-TF32 only");
     if (forced == GV_TC_DEEP && opt_.precision != PREC_TF32X3)
       throw Error(E_INVALID, "tuning entry asks for the deep-ring tensor-core GEMM, which is split-TF32 only");
     if (forced_tc && !tc_allowed)
@@ -878,6 +880,7 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       g.raster = forced == GV_TC_MFAST ? 1 : forced == GV_TC_NFAST ? 0 : -1;
       g.stream = forced == GV_TC_STREAM;
       g.deep = forced == GV_TC_DEEP;
+      g.pair = forced == GV_TC_PAIR;
       // Forward-only split-TF32 programs accumulate 64 of K per TMEM chain before the FP32 register sum (48 MMAs
       // per accumulator): fewer drains and a longer MMA run-ahead past each epilogue, measured about 8% faster on
       // the sliced headline's large steps for an error of 2.9e-6 instead of 2.5e-6 against FP64.  Gradient
@@ -1717,12 +1720,12 @@ EncodeTiled encode_fn() {
 // [re|im][z][rows][kpad] fp32 planes, boxes of 16 x 128 with 64-byte swizzle.
 // Split-TF32 planes are fp32 (boxes of 16 x 128), split-BF16 planes bf16 (boxes of 32 x 128): 64-byte rows either way.
 // The deep-ring kernel reads 8 of K per box (32-byte rows, 32-byte swizzle) from the same planes.
-CUtensorMap plane_map(void* base, ll kpad, ll rows, ll zplanes, bool bf16, bool deep = false) {
+CUtensorMap plane_map(void* base, ll kpad, ll rows, ll zplanes, bool bf16, bool deep = false, int box_rows = tc::BM) {
   CUtensorMap m;
   const ll el = bf16 ? 2 : 4;
   cuuint64_t dims[3] = {(cuuint64_t)kpad, (cuuint64_t)rows, (cuuint64_t)zplanes};
   cuuint64_t strides[2] = {(cuuint64_t)(kpad * el), (cuuint64_t)(kpad * rows * el)};
-  cuuint32_t box[3] = {(cuuint32_t)(deep ? tc::kDeepBK : bf16 ? 2 * tc::BK : tc::BK), (cuuint32_t)tc::BM, 1};
+  cuuint32_t box[3] = {(cuuint32_t)(deep ? tc::kDeepBK : bf16 ? 2 * tc::BK : tc::BK), (cuuint32_t)box_rows, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = encode_fn()(&m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base,
                            dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -1781,12 +1784,13 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
-    const std::pair<decltype(&tc::k_tc_cgemm_tf32x3), int> kerns[5] = {
+    const std::pair<decltype(&tc::k_tc_cgemm_tf32x3), int> kerns[6] = {
         {tc::k_tc_cgemm_tf32x3, tc::Fmt<tc::FMT_TF32X3>::kSmemBytes},
         {tc::k_tc_cgemm_bf16x3, tc::Fmt<tc::FMT_BF16X3>::kSmemBytes},
         {tc::k_tc_cgemm_bf16x6, tc::Fmt<tc::FMT_BF16X6>::kSmemBytes},
         {tc::k_tc_cgemm_tf32x3_stream, tc::kStreamSmemBytes},
-        {tc::k_tc_cgemm_tf32x3_deep, tc::kDeepSmemBytes}};
+        {tc::k_tc_cgemm_tf32x3_deep, tc::kDeepSmemBytes},
+        {tc::k_tc_cgemm_tf32x3_pair, tc::kPairSmemBytes}};
     for (auto [kern, smem] : kerns) {
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       // The kernel's setmaxnreg split assumes exactly kLaunchRegs registers a thread at launch.
@@ -1802,7 +1806,8 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   const ll za = (op.a_var ? op.S : 1) * op.bt, zb = (op.b_var ? op.S : 1) * op.bt;
   const ll planes = op.six ? 6 : tc::PLANES;
   const CUtensorMap ma = plane_map(A, op.kpad, op.rpad, planes * za, op.bf16, op.deep);
-  const CUtensorMap mb = plane_map(B, op.kpad, op.rpad_b, planes * zb, op.bf16, op.deep);
+  // A pair's CTAs each load 64 of the tile's 128 B rows.
+  const CUtensorMap mb = plane_map(B, op.kpad, op.rpad_b, planes * zb, op.bf16, op.deep, op.pair ? tc::BN / 2 : tc::BM);
   tc::TcArgs args;
   args.C = (cf32*)C;
   args.m = op.m;
@@ -1833,8 +1838,10 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
     args.kt_chunk = op.kt_chunk;
     args.part = (cf32*)D;
   }
-  // The smaller operand's tiles run fastest, so it stays in L2 while the larger one streams once.
-  const ll mt = (op.m + tc::BM - 1) / tc::BM, nt = (op.n + tc::BN - 1) / tc::BN;
+  // The smaller operand's tiles run fastest, so it stays in L2 while the larger one streams once.  A CTA
+  // pair's m-tiles are 256 rows.
+  const ll tile_rows = op.pair ? 2 * tc::BM : tc::BM;
+  const ll mt = (op.m + tile_rows - 1) / tile_rows, nt = (op.n + tc::BN - 1) / tc::BN;
   args.m_tiles = (int)mt;
   args.m_fast = op.raster >= 0 ? op.raster : (mt <= nt ? 1 : 0);
   const ll items = mt * nt * zc * op.splits;
@@ -1845,7 +1852,31 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   if (dev < 64 && !sms[dev]) CK(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
   const int n_sm = dev < 64 ? sms[dev] : 148;
   const unsigned grid = (unsigned)std::min<ll>(items, n_sm);
-  if (op.deep)
+  if (op.pair) {
+    // Clusters of two CTAs, as many as fit at once (persistent: each pair loops over items).
+    static int pairs_fit[64] = {};
+    cudaLaunchConfig_t cfg{};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.blockDim = dim3(tc::kThreads);
+    cfg.dynamicSmemBytes = tc::kPairSmemBytes;
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (dev < 64 && !pairs_fit[dev]) {
+      cfg.gridDim = dim3(2 * (unsigned)(n_sm / 2));
+      int fit = 0;
+      CK(cudaOccupancyMaxActiveClusters(&fit, tc::k_tc_cgemm_tf32x3_pair, &cfg));
+      if (fit < 1) throw Error(E_UNSUPPORTED, "no CTA pair of the tensor-core GEMM fits on this device");
+      pairs_fit[dev] = fit;
+    }
+    const ll fit = dev < 64 ? pairs_fit[dev] : n_sm / 2;
+    cfg.gridDim = dim3((unsigned)(2 * std::min<ll>(items, fit)));
+    CK(cudaLaunchKernelEx(&cfg, tc::k_tc_cgemm_tf32x3_pair, ma, mb, args));
+  } else if (op.deep)
     tc::k_tc_cgemm_tf32x3_deep<<<grid, tc::kThreads, tc::kDeepSmemBytes, st>>>(ma, mb, args);
   else if (op.stream)
     tc::k_tc_cgemm_tf32x3_stream<<<grid, tc::kThreads, tc::kStreamSmemBytes, st>>>(ma, mb, args);
@@ -2333,7 +2364,7 @@ void Program::execute_gradient(int part, const void* const* inputs, const void* 
 const char* gemm_variant_name(int v) {
   static const char* names[GV_COUNT] = {"auto", "simt_small", "simt_tile64", "simt_tile32", "simt_warp",
                                         "simt_tile128", "simt_dot", "tc_mfast", "tc_nfast", "tc_splitk", "tc_stream",
-                                        "tc_deep"};
+                                        "tc_deep", "tc_pair"};
   return v >= 0 && v < GV_COUNT ? names[v] : "?";
 }
 

@@ -24,7 +24,8 @@ enum : int { PREC_FP32 = 0, PREC_TF32X3 = 1, PREC_BF16X3 = 2, PREC_BF16X6 = 3 };
 // GEMM kernel variants a tuning table can pin per GEMM shape (the values of ARCTN_B200_GEMM_*).
 enum : int {
   GV_AUTO = 0, GV_SMALL = 1, GV_TILE64 = 2, GV_TILE32 = 3, GV_WARP = 4, GV_TILE128 = 5, GV_DOT = 6,
-  GV_TC_MFAST = 7, GV_TC_NFAST = 8, GV_TC_SPLITK = 9, GV_TC_STREAM = 10, GV_TC_DEEP = 11, GV_COUNT = 12
+  GV_TC_MFAST = 7, GV_TC_NFAST = 8, GV_TC_SPLITK = 9, GV_TC_STREAM = 10, GV_TC_DEEP = 11, GV_TC_PAIR = 12,
+  GV_COUNT = 13
 };
 // A GEMM's shape key: element type, precision, phase (1: slice-invariant, run once; 2: run per slice group),
 // which operands vary per slice, and gemm_dims (bt, m, k, n) of one slice.
@@ -86,6 +87,7 @@ struct Op {
   int raster = -1;                      // GEMM_TC tile order: 1 m-tiles fastest, 0 n-tiles fastest, -1 smaller side fastest
   bool stream = false;                  // GEMM_TC: the streaming-epilogue kernel (two-stage ring, double staging)
   bool deep = false;                    // GEMM_TC: the deep-ring kernel (six stages of 8 of K)
+  bool pair = false;                    // GEMM_TC: the CTA-pair kernel (clusters of 2, 256 x 128 tiles)
   int chunk_mul = 1;                    // GEMM_TC: TMEM accumulation chunk in units of the format's 32 of K
   // GEMM kinds: the shape key, the variant that runs (never GV_AUTO) and whether a tuning table chose it.
   GemmKey key;

@@ -74,6 +74,13 @@ constexpr int kDeepBK = 8, kDeepStages = 6;
 constexpr int kDeepStageBytes = 2 * PLANES * BM * kDeepBK * 4;  // 32 KB
 constexpr int kDeepSmemBytes = kDeepStages * kDeepStageBytes + STAGING_BYTES + 1024 + 1024;
 static_assert(kDeepSmemBytes <= 232448, "shared memory above the 227 KB a block may use");
+// The CTA-pair variant (kPair, split-TF32): two CTAs of a cluster share a 256 x 128 tile through
+// tcgen05.mma.cta_group::2, each holding its 128 rows of A and half of B (64 output columns).  A stage is
+// then 32 KB of A and 16 KB of B per CTA: a quarter less operand traffic per MMA and four stages in the ring.
+constexpr int kPairStages = 4;
+constexpr int kPairStageBytes = PLANES * PLANE_BYTES + PLANES * PLANE_BYTES / 2;  // 48 KB
+constexpr int kPairSmemBytes = kPairStages * kPairStageBytes + STAGING_BYTES + 1024 + 1024;
+static_assert(kPairSmemBytes <= 232448, "shared memory above the 227 KB a block may use");
 template <int F>
 struct Fmt {
   static constexpr bool kBF16 = F != FMT_TF32X3;
@@ -224,6 +231,83 @@ __device__ __forceinline__ void umma(uint32_t d_tmem, uint64_t a, uint64_t b, ui
 }
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// ---- CTA pairs (cta_group::2): a cluster of two CTAs on one TPC computes a 256 x 128 tile; CTA rank r holds
+// A rows 128 r .. + 127 and B rows (output columns) 64 r .. + 63 of the tile in its shared memory, and its own
+// TMEM receives output rows 128 r .. + 127.  Rank 0 (the leader) issues the MMAs for both.
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// The shared::cluster address of the same shared variable in CTA `rank` of this cluster.
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t rank) {
+  uint32_t a;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(a) : "r"(smem_u32(p)), "r"(rank));
+  return a;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// TMA load into this CTA's shared memory whose completion is counted on the leader's barrier (bar: a
+// shared::cluster address).  No multicast.
+__device__ __forceinline__ void tma_load_3d_pair(const CUtensorMap* map, uint32_t bar, void* dst, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(bar), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_remote(uint32_t bar) {
+  asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_cluster(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on a local barrier that CTAs of the cluster arrive on (acquire at cluster scope).
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity, int* err, int code) {
+  if (mbar_try_cluster(bar, parity)) return true;
+  const unsigned long long t0 = now_ns();
+  for (uint32_t i = 1;; ++i) {
+    if (mbar_try_cluster(bar, parity)) return true;
+    if ((i & 255) == 0) {
+      if (now_ns() - t0 > kWaitNs) {
+        atomicCAS(err, 0, code);
+        return false;
+      }
+      __nanosleep(128);
+    }
+  }
+}
+// kind::tf32 over the pair: M = 256 (128 rows in each CTA), N = 128 (64 B rows in each CTA).
+__host__ __device__ constexpr uint32_t idesc_tf32_pair(bool neg_a) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(BN >> 3) << 17) |
+         ((uint32_t)((2 * BM) >> 4) << 24);
+}
+__device__ __forceinline__ void umma_pair(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n}\n"
+      ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+// Arrive on the barrier at bar's offset in both CTAs of the pair once the leader's MMAs so far complete.
+__device__ __forceinline__ void umma_commit_pair_both(uint64_t* bar) {
+  const uint16_t mask = 3;
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
+      ::"r"(smem_u32(bar)), "h"(mask)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
 }
 
@@ -502,15 +586,18 @@ __device__ __forceinline__ void store_pass(const TcArgs& args, const EpiState& e
 
 // The GEMM body for either operand format: split-TF32 (4-byte planes, 16 of K per 64-byte operand row) or
 // split-BF16 (2-byte planes, 32 of K per row).  Shared-memory layout, swizzle, TMEM and epilogue are the same.
-template <int F, bool kStream = false, bool kDeep = false>
+template <int F, bool kStream = false, bool kDeep = false, bool kPair = false>
 __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUtensorMap& tmB, const TcArgs& args) {
   using FM = Fmt<F>;
   static_assert(!kStream || F == FMT_TF32X3, "the streaming epilogue is built for split-TF32 operands");
   static_assert(!kDeep || (F == FMT_TF32X3 && !kStream), "the deep ring is built for split-TF32 operands");
+  static_assert(!kPair || (F == FMT_TF32X3 && !kStream && !kDeep), "the CTA pair is built for split-TF32 operands");
   constexpr bool kBF16 = FM::kBF16;
-  constexpr int STAGES = kDeep ? kDeepStages : kStream ? kStreamStages : FM::kStages;
-  constexpr int STAGE_BYTES = kDeep ? kDeepStageBytes : FM::kStageBytes, PLANES = FM::kPlanes;
+  constexpr int STAGES = kPair ? kPairStages : kDeep ? kDeepStages : kStream ? kStreamStages : FM::kStages;
+  constexpr int STAGE_BYTES = kPair ? kPairStageBytes : kDeep ? kDeepStageBytes : FM::kStageBytes;
+  constexpr int PLANES = FM::kPlanes;
   constexpr int PLANE_BYTES = kDeep ? BM * kDeepBK * 4 : tc::PLANE_BYTES;
+  constexpr int B_PLANE_BYTES = kPair ? PLANE_BYTES / 2 : PLANE_BYTES;  // B rows per CTA: 64 in a pair
   constexpr int kStagingBufs = kStream ? 2 : 1;
   const int kChunkTiles = args.chunk_tiles > 0 ? args.chunk_tiles : (kDeep ? 4 : FM::kChunkTiles);
   constexpr int KT_ELEMS = kDeep ? kDeepBK : kBF16 ? 2 * BK : BK;  // K per operand row of a stage
@@ -536,6 +623,12 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   const int n_tiles = (int)((args.n + BN - 1) / BN);
+  // Items are taken per CTA, or per pair (items it0, it0 + it_step, ...); a pair's m-tiles are 256 rows and
+  // CTA rank r writes rows 128 r .. + 127 of each.
+  const int rank = kPair ? (int)cluster_rank() : 0;
+  const int it0 = kPair ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+  const int it_step = kPair ? (int)(gridDim.x >> 1) : (int)gridDim.x;
+  auto row0_of = [&](int tile_m) -> ll { return kPair ? (ll)tile_m * 2 * BM + rank * BM : (ll)tile_m * BM; };
   // Work item it: output tile it % tiles (raster as in TcArgs) of batch-and-split it / tiles.
   struct Item { int tile_m, tile_n, z, split, kt0, KT, zA, zB; };
   auto item_of = [&](int it) {
@@ -556,19 +649,28 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
 
   if (threadIdx.x == 0) {
     for (int i = 0; i < STAGES; ++i) { mbar_init(&full[i], 1); mbar_init(&empty[i], 1); }
-    for (int i = 0; i < 2; ++i) { mbar_init(&accfull[i], 1); mbar_init(&accempty[i], kDrainThreads); }
+    // accempty: every drain thread arrives, or in a pair one arrival per drain warp of both CTAs (the leader's)
+    for (int i = 0; i < 2; ++i) { mbar_init(&accfull[i], 1); mbar_init(&accempty[i], kPair ? 2 * kDrainWarps : kDrainThreads); }
     mbar_init(drain, 1);
     for (int i = 0; i < 2; ++i) { mbar_init(&sfull[i], 2); sdone[i] = 0; }
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32((const void*)tmem_slot)),
-                 "r"(TMEM_COLS));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    // a pair allocates collectively, one warp in each CTA: the same columns in both CTAs' TMEM
+    if constexpr (kPair) {
+      asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;"
+                   ::"r"(smem_u32((const void*)tmem_slot)), "r"(TMEM_COLS));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    } else {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                   ::"r"(smem_u32((const void*)tmem_slot)), "r"(TMEM_COLS));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  if constexpr (kPair) cluster_sync_all();  // the peer's barriers are initialised before any copy signals them
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
@@ -582,14 +684,14 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
   // epi_setup holds a storer's chunks of all four passes in the 64 slots of a warp's two int2 registers.
   static_assert(BM / kStageRows * ((kStageRows * BN / 32 + kStreamStorers - 1) / kStreamStorers) <= 64,
                 "a streamed pass's packed chunks do not fit a storer warp's slots");
-  auto stream_store = [&](const EpiState& es, const EpiTile& t, int gp, int rows, int cols, bool& dead, int rank) {
+  auto stream_store = [&](const EpiState& es, const EpiTile& t, int gp, int rows, int cols, bool& dead, int srank) {
     const int b = gp & 1, u = gp >> 1;
     if (!dead && !mbar_wait_or_abort(&sfull[b], (uint32_t)(u & 1), args.err, 3, abort_flag)) {
       dead = true;
       *abort_flag = 1;
     }
     if (!dead)
-      store_pass(args, es, t, stage + b * kStageRows * BN, gp & 3, rows, cols, rank * 32 + (threadIdx.x & 31),
+      store_pass(args, es, t, stage + b * kStageRows * BN, gp & 3, rows, cols, srank * 32 + (threadIdx.x & 31),
                  kStreamStorers * 32);
     __syncwarp();
     if (!dead && (threadIdx.x & 31) == 0) {
@@ -601,31 +703,31 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
   // stores of every staged pass.
   auto helpers = [&]() {
     if constexpr (kStream) {
-      const int rank = warp < 4 ? warp - 2 : warp - 10;  // warps 2, 3, 12..15 -> storer ranks 0..5
-      const EpiState es = epi_setup(args, rank, lane, kStreamStorers);
+      const int srank = warp < 4 ? warp - 2 : warp - 10;  // warps 2, 3, 12..15 -> storer ranks 0..5
+      const EpiState es = epi_setup(args, srank, lane, kStreamStorers);
       bool dead = false;
       int gp = 0;
-      for (int it = blockIdx.x; it < args.n_items; it += gridDim.x, gp += BM / kStageRows) {
+      for (int it = it0; it < args.n_items; it += it_step, gp += BM / kStageRows) {
         const Item w = item_of(it);
-        const ll row0 = (ll)w.tile_m * BM, col0 = (ll)w.tile_n * BN;
+        const ll row0 = row0_of(w.tile_m), col0 = (ll)w.tile_n * BN;
         const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
         const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
-        const EpiTile t = epi_tile(args, w.z, w.split, row0, col0, lane);
+        const EpiTile t = epi_tile(args, w.z, w.split, row0 < args.m ? row0 : 0, col0, lane);  // rows <= 0: unused
         for (int q = 0; q < BM / kStageRows; ++q) {
           if (*abort_flag) dead = true;
-          stream_store(es, t, gp + q, rows, cols, dead, rank);
+          stream_store(es, t, gp + q, rows, cols, dead, srank);
         }
       }
       return;
     }
     const EpiState es = epi_setup(args, warp - 2, lane);
     bool dead = false;
-    for (int it = blockIdx.x; it < args.n_items; it += gridDim.x) {
+    for (int it = it0; it < args.n_items; it += it_step) {
       const Item w = item_of(it);
-      const ll row0 = (ll)w.tile_m * BM, col0 = (ll)w.tile_n * BN;
+      const ll row0 = row0_of(w.tile_m), col0 = (ll)w.tile_n * BN;
       const int rows = (int)(args.m - row0 < BM ? args.m - row0 : BM);
       const int cols = (int)(args.n - col0 < BN ? args.n - col0 : BN);
-      const EpiTile t = epi_tile(args, w.z, w.split, row0, col0, lane);
+      const EpiTile t = epi_tile(args, w.z, w.split, row0 < args.m ? row0 : 0, col0, lane);  // rows <= 0: unused
 #pragma unroll 1
       for (int q = 0; q < BM / kStageRows; ++q) {
         asm volatile("bar.sync 1, %0;" ::"n"(kEpiThreads) : "memory");
@@ -643,7 +745,7 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
       if (lane == 0) {
         int g = 0, issued = 0;
         bool stop = false;
-        for (int it = blockIdx.x; it < args.n_items && !stop; it += gridDim.x) {
+        for (int it = it0; it < args.n_items && !stop; it += it_step) {
           const Item w = item_of(it);
           for (int t = 0; t < w.KT; ++t, ++g) {
             const int s = g % STAGES;
@@ -654,17 +756,30 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
             }
             if (*abort_flag) { stop = true; break; }
             unsigned char* dst = ring + s * STAGE_BYTES;
-            mbar_expect_tx(&full[s], STAGE_BYTES);
             const int k0 = (w.kt0 + t) * KT_ELEMS;
+            if constexpr (kPair) {
+              // Both CTAs' copies count on the leader's full[s], which expects the pair's bytes.  Rows past the
+              // operand (the upper half of a last 256-row tile) arrive as zeros and count all the same.
+              const uint32_t fb = cluster_addr(&full[s], 0);
+              if (rank == 0) mbar_expect_tx(&full[s], 2 * STAGE_BYTES);
+              const int ya = (int)row0_of(w.tile_m), yb = w.tile_n * BN + rank * (BN / 2);
   #pragma unroll
-            for (int p = 0; p < PLANES; ++p) {
-              tma_load_3d(&tmA, &full[s], dst + p * PLANE_BYTES, k0, w.tile_m * BM, w.zA + p * args.za);
-              tma_load_3d(&tmB, &full[s], dst + (PLANES + p) * PLANE_BYTES, k0, w.tile_n * BN, w.zB + p * args.zb);
+              for (int p = 0; p < PLANES; ++p) {
+                tma_load_3d_pair(&tmA, fb, dst + p * PLANE_BYTES, k0, ya, w.zA + p * args.za);
+                tma_load_3d_pair(&tmB, fb, dst + PLANES * PLANE_BYTES + p * B_PLANE_BYTES, k0, yb, w.zB + p * args.zb);
+              }
+            } else {
+              mbar_expect_tx(&full[s], STAGE_BYTES);
+  #pragma unroll
+              for (int p = 0; p < PLANES; ++p) {
+                tma_load_3d(&tmA, &full[s], dst + p * PLANE_BYTES, k0, w.tile_m * BM, w.zA + p * args.za);
+                tma_load_3d(&tmB, &full[s], dst + (PLANES + p) * PLANE_BYTES, k0, w.tile_n * BN, w.zB + p * args.zb);
+              }
             }
             issued = g + 1;
           }
         }
-        if (*abort_flag) {  // let issued copies land before the CTA retires
+        if (*abort_flag && rank == 0) {  // let issued copies land before the CTA retires (a pair's count on the leader)
           for (int t = (issued > STAGES ? issued - STAGES : 0); t < issued; ++t)
             mbar_wait(&full[t % STAGES], (t / STAGES) & 1, args.err, 7);
         }
@@ -673,17 +788,27 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
       // ------------------------------------------------------------ MMA issuer
       // gc counts chunks over all items: TMEM buffer gc & 1.  The issuer runs up to two chunks ahead
       // of the drain warps, so the next item's first chunks overlap the previous item's epilogue.
-      if (lane == 0) {
-        const uint32_t id_pos = idesc_for<kBF16>(false), id_neg = idesc_for<kBF16>(true);
+      if (lane == 0 && rank == 0) {  // in a pair, the leader issues for both CTAs
+        const uint32_t id_pos = kPair ? idesc_tf32_pair(false) : idesc_for<kBF16>(false);
+        const uint32_t id_neg = kPair ? idesc_tf32_pair(true) : idesc_for<kBF16>(true);
+        auto mma = [&](uint32_t d, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+          if constexpr (kPair) umma_pair(d, a, b, id, acc);
+          else umma<kBF16>(d, a, b, id, acc);
+        };
+        auto commit = [&](uint64_t* bar) {  // a pair's stage and accumulator barriers are signalled in both CTAs
+          if constexpr (kPair) umma_commit_pair_both(bar);
+          else umma_commit(bar);
+        };
         int g = 0, gc = 0;
         bool stop = false;
-        for (int it = blockIdx.x; it < args.n_items && !stop; it += gridDim.x) {
+        for (int it = it0; it < args.n_items && !stop; it += it_step) {
           const Item w = item_of(it);
           const int n_chunks = (w.KT + kChunkTiles - 1) / kChunkTiles;
           for (int c = 0; c < n_chunks; ++c, ++gc) {
             if (*abort_flag) { stop = true; break; }
             const int b = gc & 1;
-            if (gc >= 2 && !mbar_wait(&accempty[b], ((gc >> 1) - 1) & 1, args.err, 6)) {
+            if (gc >= 2 && !(kPair ? mbar_wait_cluster(&accempty[b], ((gc >> 1) - 1) & 1, args.err, 6)
+                                   : mbar_wait(&accempty[b], ((gc >> 1) - 1) & 1, args.err, 6))) {
               *abort_flag = 1;
               stop = true;
               break;
@@ -723,34 +848,35 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
                 continue;
               }
               const uint32_t hAr = a0, lAr = a0 + PLANE_BYTES, hAi = a0 + 2 * PLANE_BYTES, lAi = a0 + 3 * PLANE_BYTES;
-              const uint32_t hBr = b0, lBr = b0 + PLANE_BYTES, hBi = b0 + 2 * PLANE_BYTES, lBi = b0 + 3 * PLANE_BYTES;
+              const uint32_t hBr = b0, lBr = b0 + B_PLANE_BYTES, hBi = b0 + 2 * B_PLANE_BYTES, lBi = b0 + 3 * B_PLANE_BYTES;
   #pragma unroll
               for (int kk = 0; kk < KSTEPS; ++kk) {
                 const uint32_t o = kk * 32;  // 8 tf32 or 16 bf16 = 32 bytes along the swizzled row
                 const uint32_t acc = first ? 0u : 1u;
                 // leading terms (hi,hi), then the corrections (lo,hi) and (hi,lo), all into this chunk's buffer
-                umma<kBF16>(cr, sdesc(hAr + o), sdesc(hBr + o), id_pos, acc);
-                umma<kBF16>(ci, sdesc(hAr + o), sdesc(hBi + o), id_pos, acc);
-                umma<kBF16>(cr, sdesc(hAi + o), sdesc(hBi + o), id_neg, 1);
-                umma<kBF16>(ci, sdesc(hAi + o), sdesc(hBr + o), id_pos, 1);
-                umma<kBF16>(cr, sdesc(lAr + o), sdesc(hBr + o), id_pos, 1);
-                umma<kBF16>(ci, sdesc(lAr + o), sdesc(hBi + o), id_pos, 1);
-                umma<kBF16>(cr, sdesc(lAi + o), sdesc(hBi + o), id_neg, 1);
-                umma<kBF16>(ci, sdesc(lAi + o), sdesc(hBr + o), id_pos, 1);
-                umma<kBF16>(cr, sdesc(hAr + o), sdesc(lBr + o), id_pos, 1);
-                umma<kBF16>(ci, sdesc(hAr + o), sdesc(lBi + o), id_pos, 1);
-                umma<kBF16>(cr, sdesc(hAi + o), sdesc(lBi + o), id_neg, 1);
-                umma<kBF16>(ci, sdesc(hAi + o), sdesc(lBr + o), id_pos, 1);
+                mma(cr, sdesc(hAr + o), sdesc(hBr + o), id_pos, acc);
+                mma(ci, sdesc(hAr + o), sdesc(hBi + o), id_pos, acc);
+                mma(cr, sdesc(hAi + o), sdesc(hBi + o), id_neg, 1);
+                mma(ci, sdesc(hAi + o), sdesc(hBr + o), id_pos, 1);
+                mma(cr, sdesc(lAr + o), sdesc(hBr + o), id_pos, 1);
+                mma(ci, sdesc(lAr + o), sdesc(hBi + o), id_pos, 1);
+                mma(cr, sdesc(lAi + o), sdesc(hBi + o), id_neg, 1);
+                mma(ci, sdesc(lAi + o), sdesc(hBr + o), id_pos, 1);
+                mma(cr, sdesc(hAr + o), sdesc(lBr + o), id_pos, 1);
+                mma(ci, sdesc(hAr + o), sdesc(lBi + o), id_pos, 1);
+                mma(cr, sdesc(hAi + o), sdesc(lBi + o), id_neg, 1);
+                mma(ci, sdesc(hAi + o), sdesc(lBr + o), id_pos, 1);
                 first = false;
               }
-              umma_commit(&empty[s]);
+              commit(&empty[s]);
             }
             if (stop) break;
-            umma_commit(&accfull[b]);
+            commit(&accfull[b]);
           }
         }
         if (*abort_flag) {
-          umma_commit(drain);
+          if constexpr (kPair) umma_commit_pair(drain);
+          else umma_commit(drain);
           mbar_wait(drain, 0, args.err, 8);
         }
       }
@@ -768,11 +894,11 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
     [[maybe_unused]] const EpiState es_stream = kStream ? epi_setup(args, 6 + half, lane, 8) : EpiState{};
     int gc = 0, gpass = 0;
     bool dead = false;
-    for (int it = blockIdx.x; it < args.n_items; it += gridDim.x) {
+    for (int it = it0; it < args.n_items; it += it_step) {
       const Item w = item_of(it);
       const int n_chunks = (w.KT + kChunkTiles - 1) / kChunkTiles;
-      const ll row0 = (ll)w.tile_m * BM, col0 = (ll)w.tile_n * BN;
-      const EpiTile t = epi_tile(args, w.z, w.split, row0, col0, lane);  // loads overlap the drain below
+      const ll row0 = row0_of(w.tile_m), col0 = (ll)w.tile_n * BN;
+      const EpiTile t = epi_tile(args, w.z, w.split, row0 < args.m ? row0 : 0, col0, lane);  // overlaps the drain
       float acc_re[kHalfCols], acc_im[kHalfCols];
 #pragma unroll
       for (int j = 0; j < kHalfCols; ++j) acc_re[j] = acc_im[j] = 0.f;
@@ -799,7 +925,12 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
           }
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        mbar_arrive(&accempty[b]);
+        if constexpr (kPair) {  // one arrival per warp of either CTA, on the leader's barrier
+          __syncwarp();
+          if (lane == 0) mbar_arrive_remote(cluster_addr(&accempty[b], 0));
+        } else {
+          mbar_arrive(&accempty[b]);
+        }
       }
       if (*abort_flag) dead = true;
       // Epilogue, one lane quadrant (32 output rows) at a time: its two drain warps stage their rows,
@@ -849,9 +980,15 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  // A pair retires together: the leader's MMAs read the peer's shared memory and write its TMEM, and the
+  // peer's warps arrive on the leader's barriers.
+  if constexpr (kPair) cluster_sync_all();
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    if constexpr (kPair)
+      asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    else
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
   }
 }
 
@@ -865,6 +1002,12 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3_stream(c
                                                                        const __grid_constant__ CUtensorMap tmB,
                                                                        TcArgs args) {
   tc_cgemm_body<FMT_TF32X3, true>(tmA, tmB, args);
+}
+// Split-TF32 on CTA pairs (clusters of 2, cta_group::2 MMAs on 256 x 128 tiles, four 48 KB stages).
+static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3_pair(const __grid_constant__ CUtensorMap tmA,
+                                                                     const __grid_constant__ CUtensorMap tmB,
+                                                                     TcArgs args) {
+  tc_cgemm_body<FMT_TF32X3, false, false, true>(tmA, tmB, args);
 }
 // Split-TF32 with the deep ring (six 32 KB stages of 8 of K, 32-byte swizzle).
 static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3_deep(const __grid_constant__ CUtensorMap tmA,

@@ -16,6 +16,7 @@ from arctn_b200 import _capi as C
 from arctn_b200 import networks as N
 from arctn_b200 import tuning as T
 from oracle import oracle as O
+from tests.helpers import random_arrays
 
 pytestmark = pytest.mark.gpu
 
@@ -25,7 +26,7 @@ PRECS = {"fp32": C.PREC_FP32, "tf32x3": C.PREC_TF32X3, "bf16x3": C.PREC_BF16X3, 
 
 
 def valid(variant, dtype, precision):
-    if variant in ("tc_stream", "tc_deep"):
+    if variant in ("tc_stream", "tc_deep", "tc_pair"):
         return precision == "tf32x3" and dtype in (C.F32, C.C64)
     if variant.startswith("tc_"):
         return precision in ("tf32x3", "bf16x3", "bf16x6") and dtype in (C.F32, C.C64)
@@ -117,3 +118,59 @@ def test_autotune_picks_timed_winners_and_matches_oracle():
     p2 = A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex64, precision="tf32x3", tuning=back)
     assert [g["variant"] for g in p2.gemms()] == [g["variant"] for g in gs]
     assert np.array_equal(np.asarray(p2.execute(arrays, f64_out=True)), np.asarray(got))
+
+
+PAIR_STEPS = [  # (bt, m dims, k dims, n dims): m >= 256, so both CTAs of a pair hold rows; 384 and 300 leave the
+    (1, [512], [64], [256]),  # second CTA of the last 256-row tile partly or wholly past the operand
+    (1, [384], [1000], [96]),
+    (2, [300], [48], [130]),
+]
+
+
+@pytest.mark.parametrize("case", PAIR_STEPS, ids=[str(c) for c in PAIR_STEPS])
+def test_cta_pair_step_matches_single_cta_bitwise_and_fp64(case):
+    import torch
+
+    from tests.test_gpu_tc import step_network
+
+    bt, md, kd, nd = case
+    inputs, output, size = step_network(bt, md, kd, nd, seed=11 + bt)
+    arrays = random_arrays(inputs, size, np.complex64, 5)
+    x = [torch.from_numpy(a).cuda() for a in arrays]
+    outs = {}
+    for v in ("tc_mfast", "tc_pair"):
+        base = A.SlicedProgram(inputs, output, size, [(0, 1)], (), dtype=np.complex64, precision="tf32x3")
+        table = T.TuneTable()
+        for g in base.gemms():
+            table.set(T.key_of(g), v)
+        prog = A.SlicedProgram(inputs, output, size, [(0, 1)], (), dtype=np.complex64, precision="tf32x3",
+                               tuning=table)
+        assert [g["variant"] for g in prog.gemms()] == [v]
+        ws = torch.empty(max(prog.workspace_bytes, 1), dtype=torch.uint8, device="cuda")
+        outs[v] = prog.execute(x, workspace=ws).cpu().numpy()
+        assert prog.device_status(ws) == 0
+    # a pair computes each output element with the same MMA sequence as one CTA
+    assert np.array_equal(outs["tc_pair"], outs["tc_mfast"])
+    want = np.einsum(*sum(([a.astype(np.complex128), t] for a, t in zip(arrays, inputs)), []), output)
+    assert rel(outs["tc_pair"], want) <= 1e-5
+
+
+def test_cta_pair_on_fused_pack_steps_of_rand3reg_n172():
+    # slices 0..3 of the n=172 contraction: its large steps (m = 512 and 1024) write the next GEMM's packed
+    # operand from the epilogue; pinned to CTA pairs they give the single-CTA kernel's bits
+    net, arrays = N.workload_rand3reg(172, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 24)
+    kw = dict(dtype=np.complex64, precision="tf32x3", slice_begin=0, slice_end=4, workspace_budget=8 << 30)
+    base = A.SlicedProgram(*net.as_tuple(), path, sliced, **kw)
+    big = [T.key_of(g) for g in base.gemms() if g["variant"].startswith("tc_") and g["m"] >= 256]
+    assert big
+    got = {}
+    for v in ("tc_mfast", "tc_pair"):
+        table = T.TuneTable()
+        for k in big:
+            table.set(k, v)
+        prog = A.SlicedProgram(*net.as_tuple(), path, sliced, tuning=table, **kw)
+        assert any("pack_into" in o for o in prog.describe()["ops"] if o.get("variant") == v)
+        got[v] = np.asarray(prog.execute(arrays, f64_out=True))
+    assert np.array_equal(got["tc_pair"], got["tc_mfast"])

@@ -70,6 +70,10 @@ def test_candidates_respect_dtype_and_precision():
     # the deep ring: split-TF32 only, for K of at least 8 tiles
     assert "tc_deep" in T.candidates((C.C64, C.PREC_TF32X3, 2, 1, 1, 1, 512, 16384, 1024), 37)
     assert "tc_deep" not in T.candidates((C.C64, C.PREC_TF32X3, 2, 1, 1, 1, 1024, 16, 8192), 37)
+    # CTA pairs: split-TF32 only, for outputs of more than one 128-row tile
+    assert "tc_pair" in T.candidates((C.C64, C.PREC_TF32X3, 2, 1, 1, 1, 512, 16384, 1024), 37)
+    assert "tc_pair" not in T.candidates((C.C64, C.PREC_TF32X3, 2, 1, 1, 1, 128, 64, 16384), 37)
+    assert "tc_pair" not in T.candidates((C.C64, C.PREC_BF16X6, 2, 1, 1, 1, 512, 16384, 1024), 37)
 
 
 def test_table_pins_only_matching_gemms():
@@ -124,6 +128,10 @@ def test_tensor_core_pin_builds_packs_and_rejects_wrong_dtypes():
     bad.set((C.C64, C.PREC_BF16X6) + key[2:], "tc_deep")
     with pytest.raises(A.ArcTNB200Error, match="split-TF32 only"):
         A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex64, precision="bf16x6", tuning=bad)
+    bad = T.TuneTable()
+    bad.set((C.C64, C.PREC_BF16X3) + key[2:], "tc_pair")
+    with pytest.raises(A.ArcTNB200Error, match="split-TF32 only"):
+        A.SlicedProgram(*net.as_tuple(), path, sliced, dtype=np.complex64, precision="bf16x3", tuning=bad)
     bad = T.TuneTable()
     bad.set(key, "simt_tile128")
     with pytest.raises(A.ArcTNB200Error, match="float32"):
