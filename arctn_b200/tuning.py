@@ -217,7 +217,7 @@ def _key_costs(prog, arrays, reps):
 
 
 def autotune(inputs, output, size_dict, ssa_path, sliced_legs=(), *, dtype="complex64", precision="fp32",
-             device=None, table=None, reps=2, log=None, **program_kw):
+             device=None, table=None, reps=2, log=None, margin=0.03, **program_kw):
     """Tunes every GEMM shape of the program these arguments describe (``program_kw``: the other
     ``SlicedProgram`` options -- workspace budget, group size, slice range, gradient) and returns the table;
     a given ``table`` is extended, and keys it already holds are not timed again.  Needs a GPU.
@@ -225,7 +225,10 @@ def autotune(inputs, output, size_dict, ssa_path, sliced_legs=(), *, dtype="comp
     The candidates are timed inside the program itself, on random inputs of the network's shapes: one run
     with the current choices, then one run per variant with that variant pinned on every untuned key it may
     serve; each key's time is the time of its GEMMs and the ops serving them (operand packs, split-K sums).
-    A candidate that cannot beat the key's current time even at its kernel family's peak rate is not run."""
+    A candidate that cannot beat the key's current time even at its kernel family's peak rate is not run.  A
+    variant replaces the heuristic's choice only where it is faster by more than ``margin`` (a fraction of the
+    heuristic's time): repeated runs of one program differ by a few percent, and a switch on a smaller
+    difference is as likely to lose as to win."""
     import torch
 
     from .api import SlicedProgram
@@ -275,14 +278,15 @@ def autotune(inputs, output, size_dict, ssa_path, sliced_legs=(), *, dtype="comp
     # writes its consumer's packed operand from its epilogue, and a tensor-core consumer needs packs its SIMT
     # form does not.  Such a switch is kept only if the whole program gets faster, tried one key at a time in
     # order of the gain measured on the key itself (the largest few, each worth at least 0.2% of the run).
-    # Switches within one family are taken as measured.
+    # Switches within one family are taken where they beat the heuristic's choice by more than the margin.
     choice, switches = {}, []
     for k in todo:
         timed_ = {v: t for v, t in times[k].items() if t is not None}
         a = base_var[k]
         same = {v: t for v, t in timed_.items() if v.startswith("tc_") == a.startswith("tc_")}
         other = {v: t for v, t in timed_.items() if v not in same}
-        choice[k] = min(same, key=same.get)
+        best = min(same, key=same.get)
+        choice[k] = best if same[best] < (1.0 - margin) * same[a] else a
         if other:
             b = min(other, key=other.get)
             if other[b] < same[choice[k]]:

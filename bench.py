@@ -108,11 +108,13 @@ def peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "source": "fallback"}
 
 
-def per_step_roofline(prog, ms, tf32_pipe_tflops, hbm_gbs):
+def per_step_roofline(prog, ms, tf32_pipe_tflops, hbm_gbs, sustained_tflops=None):
     """Each tensor-core GEMM shape of the program against its own bound, from the op-by-op profile `ms`:
     the tensor bound is its split-TF32 pipe work (3 TF32 products per real product) at the measured TF32 rate,
     the memory bound its algorithmic bytes (16 B per packed operand element read, 16 B per packed or 8 B per
-    plain output element written) at the HBM rate; the step's bound is the larger of the two times."""
+    plain output element written) at the HBM rate; the step's bound is the larger of the two times.  With
+    `sustained_tflops` (the TF32 rate held for seconds under the power cap) each step also carries its
+    tensor work against that rate."""
     ops = prog.describe()["ops"]
     units = {}
     for i, o in enumerate(ops):
@@ -139,6 +141,8 @@ def per_step_roofline(prog, ms, tf32_pipe_tflops, hbm_gbs):
                     "fused_output": a["fused_output"], "tflops": a["flops"] / (a["ms"] * 1e-3) / 1e12,
                     "gbs": a["bytes"] / (a["ms"] * 1e-3) / 1e9, "bound": "tensor" if t_tensor >= t_mem else "hbm",
                     "frac_of_bound": max(t_tensor, t_mem) / a["ms"]})
+        if sustained_tflops:
+            out[-1]["tensor_frac_of_sustained"] = 3 * a["flops"] / (sustained_tflops * 1e12) * 1e3 / a["ms"]
     return out
 
 
@@ -1002,8 +1006,9 @@ def main():
         top = max(by, key=lambda k: by[k][0])
         tms, tw, tn = by[top]
         if top in GEMM_KINDS:
-            # The profile times each kernel on its own (an event pair per launch), and the step runs near
-            # full clock, so the denominator is the burst bf16 rate; the sustained one is reported beside it.
+            # The profile times each kernel on its own (an event pair per launch).  `frac` divides by the burst
+            # bf16 rate, the stricter denominator; the sustained one is reported beside it, and the split-TF32
+            # GEMM below is also set against the TF32 rates measured on this GPU, burst and sustained.
             achieved = tw / (tms * 1e-3) / 1e12
             peak = pk["bf16_tflops"]
             traffic = profiled_traffic()  # scaled from an ncu capture of a smaller slice group
@@ -1037,7 +1042,13 @@ def main():
                 roof["tf32_peak_source"] = ("measured: arctn_b200_tc_peak, the highest of kind::tf32 M=128 N=128/256 and "
                                             "the split-TF32 GEMM's own MMA stream")
                 roof["pipe_frac_of_gemm_stream_ceiling"] = achieved * 3 / pk_tc["tf32_gemm_stream_n128"]
-                roof["per_step"] = per_step_roofline(prog, ms, tf32_peak, pk["hbm_gbs"])
+                # The same MMA stream held for seconds (one 1.7 s launch after a warm-up launch as long), as the
+                # GEMM runs inside the step: under the 1 kW power cap the SM clock settles below its burst value,
+                # and this is the TF32 rate the tensor pipe sustains there.
+                sust = A.tensor_pipe_peak("tf32_gemm_stream", 128, iters=1 << 22, device=local, repeats=1)
+                pk_tc["tf32_gemm_stream_sustained"] = sust
+                roof["pipe_frac_of_sustained_gemm_stream"] = achieved * 3 / sust
+                roof["per_step"] = per_step_roofline(prog, ms, tf32_peak, pk["hbm_gbs"], sust)
         else:
             achieved = tw / (tms * 1e-3) / 1e9
             roof = {"bound": "hbm", "kernel": KIND_NAMES.get(top, str(top)), "achieved": achieved,

@@ -101,10 +101,13 @@ def test_autotune_picks_timed_winners_and_matches_oracle():
         times = {v: t for v, t in tm.items() if v in T.VARIANT_CODES and t is not None}
         assert tm["heuristic"] in times  # the heuristic's own choice is always timed
         assert g["variant"] == table.get(key) in times
-        # the pick is the fastest of its family (tensor core / SIMT); a switch of family was kept only where
-        # the whole program got faster
+        # the pick is the fastest of its family (tensor core / SIMT) where that beats the heuristic's choice by
+        # more than the margin (3%), else the heuristic's choice; a switch of family was kept only where the
+        # whole program got faster
         fam = {v: t for v, t in times.items() if v.startswith("tc_") == g["variant"].startswith("tc_")}
-        assert g["variant"] == min(fam, key=fam.get)
+        best = min(fam, key=fam.get)
+        if g["variant"] != best:
+            assert g["variant"] == tm["heuristic"] and fam[best] >= 0.97 * fam[tm["heuristic"]]
         if g["variant"].startswith("tc_") != tm["heuristic"].startswith("tc_"):
             w = tm["whole_program_ms"]
             assert w["after"] < w["before"]
