@@ -352,7 +352,7 @@ int arctn_b200_program_create_tuned(const arctn_b200_network* net, uint64_t n_st
     ProgramOptions po = to_options(options);
     for (u64 i = 0; i < n_table; ++i) {
       const arctn_b200_gemm_choice& e = table[i];
-      if (e.variant < ARCTN_B200_GEMM_AUTO || e.variant > ARCTN_B200_GEMM_TC_PAIR)
+      if (e.variant < ARCTN_B200_GEMM_AUTO || e.variant > ARCTN_B200_GEMM_TC_PAIR_STREAM)
         fail("tuning entry " + std::to_string(i) + ": unknown variant " + std::to_string(e.variant));
       if (e.phase != 1 && e.phase != 2) fail("tuning entry " + std::to_string(i) + ": phase must be 1 or 2");
       GemmKey k{e.dtype, e.precision, e.phase, e.a_var ? 1 : 0, e.b_var ? 1 : 0, e.bt, e.m, e.k, e.n};

@@ -618,10 +618,11 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
     int forced = GV_AUTO;
     if (auto it = opt_.tuning.find(g.key); it != opt_.tuning.end()) forced = it->second;
     const bool forced_tc = forced == GV_TC_MFAST || forced == GV_TC_NFAST || forced == GV_TC_SPLITK ||
-                           forced == GV_TC_STREAM || forced == GV_TC_DEEP || forced == GV_TC_PAIR;
+                           forced == GV_TC_STREAM || forced == GV_TC_DEEP || forced == GV_TC_PAIR ||
+                           forced == GV_TC_PAIR_STREAM;
     if (forced == GV_TC_STREAM && opt_.precision != PREC_TF32X3)
       throw Error(E_INVALID, "tuning entry asks for the streaming-epilogue tensor-core GEMM, which is split-TF32 only");
-    if (forced == GV_TC_PAIR && opt_.precision != PREC_TF32X3)
+    if ((forced == GV_TC_PAIR || forced == GV_TC_PAIR_STREAM) && opt_.precision != PREC_TF32X3)
       throw Error(E_INVALID, "tuning entry asks for the CTA-pair tensor-core GEMM, which is split-TF32 only");
     if (forced == GV_TC_DEEP && opt_.precision != PREC_TF32X3)
       throw Error(E_INVALID, "tuning entry asks for the deep-ring tensor-core GEMM, which is split-TF32 only");
@@ -878,9 +879,9 @@ void Program::build(const Network& net, const SsaPath& path, const std::vector<L
       g.real = real_tc;
       const ll mt = (ll)(m + tc::BM - 1) / tc::BM, nt = (ll)(n + tc::BN - 1) / tc::BN;
       g.raster = forced == GV_TC_MFAST ? 1 : forced == GV_TC_NFAST ? 0 : -1;
-      g.stream = forced == GV_TC_STREAM;
+      g.stream = forced == GV_TC_STREAM || forced == GV_TC_PAIR_STREAM;
       g.deep = forced == GV_TC_DEEP;
-      g.pair = forced == GV_TC_PAIR;
+      g.pair = forced == GV_TC_PAIR || forced == GV_TC_PAIR_STREAM;
       // Forward-only split-TF32 programs accumulate 64 of K per TMEM chain before the FP32 register sum (48 MMAs
       // per accumulator): fewer drains and a longer MMA run-ahead past each epilogue, measured about 8% faster on
       // the sliced headline's large steps for an error of 2.9e-6 instead of 2.5e-6 against FP64.  Gradient
@@ -1784,13 +1785,14 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 64 && !attr_set[dev]) {
-    const std::pair<decltype(&tc::k_tc_cgemm_tf32x3), int> kerns[6] = {
+    const std::pair<decltype(&tc::k_tc_cgemm_tf32x3), int> kerns[7] = {
         {tc::k_tc_cgemm_tf32x3, tc::Fmt<tc::FMT_TF32X3>::kSmemBytes},
         {tc::k_tc_cgemm_bf16x3, tc::Fmt<tc::FMT_BF16X3>::kSmemBytes},
         {tc::k_tc_cgemm_bf16x6, tc::Fmt<tc::FMT_BF16X6>::kSmemBytes},
         {tc::k_tc_cgemm_tf32x3_stream, tc::kStreamSmemBytes},
         {tc::k_tc_cgemm_tf32x3_deep, tc::kDeepSmemBytes},
-        {tc::k_tc_cgemm_tf32x3_pair, tc::kPairSmemBytes}};
+        {tc::k_tc_cgemm_tf32x3_pair, tc::kPairSmemBytes},
+        {tc::k_tc_cgemm_tf32x3_pair_stream, tc::kPairStreamSmemBytes}};
     for (auto [kern, smem] : kerns) {
       CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       // The kernel's setmaxnreg split assumes exactly kLaunchRegs registers a thread at launch.
@@ -1854,7 +1856,9 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
   const unsigned grid = (unsigned)std::min<ll>(items, n_sm);
   if (op.pair) {
     // Clusters of two CTAs, as many as fit at once (persistent: each pair loops over items).
-    static int pairs_fit[64] = {};
+    static int pairs_fit[64][2] = {};
+    const auto kern = op.stream ? tc::k_tc_cgemm_tf32x3_pair_stream : tc::k_tc_cgemm_tf32x3_pair;
+    const int kv = op.stream ? 1 : 0;
     cudaLaunchConfig_t cfg{};
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1862,20 +1866,20 @@ void launch_tc(const Op& op, void* A, void* B, void* C, void* D, void* PK, const
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
     cfg.blockDim = dim3(tc::kThreads);
-    cfg.dynamicSmemBytes = tc::kPairSmemBytes;
+    cfg.dynamicSmemBytes = op.stream ? tc::kPairStreamSmemBytes : tc::kPairSmemBytes;
     cfg.stream = st;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (dev < 64 && !pairs_fit[dev]) {
+    if (dev < 64 && !pairs_fit[dev][kv]) {
       cfg.gridDim = dim3(2 * (unsigned)(n_sm / 2));
       int fit = 0;
-      CK(cudaOccupancyMaxActiveClusters(&fit, tc::k_tc_cgemm_tf32x3_pair, &cfg));
+      CK(cudaOccupancyMaxActiveClusters(&fit, kern, &cfg));
       if (fit < 1) throw Error(E_UNSUPPORTED, "no CTA pair of the tensor-core GEMM fits on this device");
-      pairs_fit[dev] = fit;
+      pairs_fit[dev][kv] = fit;
     }
-    const ll fit = dev < 64 ? pairs_fit[dev] : n_sm / 2;
+    const ll fit = dev < 64 ? pairs_fit[dev][kv] : n_sm / 2;
     cfg.gridDim = dim3((unsigned)(2 * std::min<ll>(items, fit)));
-    CK(cudaLaunchKernelEx(&cfg, tc::k_tc_cgemm_tf32x3_pair, ma, mb, args));
+    CK(cudaLaunchKernelEx(&cfg, kern, ma, mb, args));
   } else if (op.deep)
     tc::k_tc_cgemm_tf32x3_deep<<<grid, tc::kThreads, tc::kDeepSmemBytes, st>>>(ma, mb, args);
   else if (op.stream)
@@ -2364,7 +2368,7 @@ void Program::execute_gradient(int part, const void* const* inputs, const void* 
 const char* gemm_variant_name(int v) {
   static const char* names[GV_COUNT] = {"auto", "simt_small", "simt_tile64", "simt_tile32", "simt_warp",
                                         "simt_tile128", "simt_dot", "tc_mfast", "tc_nfast", "tc_splitk", "tc_stream",
-                                        "tc_deep", "tc_pair"};
+                                        "tc_deep", "tc_pair", "tc_pair_stream"};
   return v >= 0 && v < GV_COUNT ? names[v] : "?";
 }
 

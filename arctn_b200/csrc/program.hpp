@@ -25,7 +25,7 @@ enum : int { PREC_FP32 = 0, PREC_TF32X3 = 1, PREC_BF16X3 = 2, PREC_BF16X6 = 3 };
 enum : int {
   GV_AUTO = 0, GV_SMALL = 1, GV_TILE64 = 2, GV_TILE32 = 3, GV_WARP = 4, GV_TILE128 = 5, GV_DOT = 6,
   GV_TC_MFAST = 7, GV_TC_NFAST = 8, GV_TC_SPLITK = 9, GV_TC_STREAM = 10, GV_TC_DEEP = 11, GV_TC_PAIR = 12,
-  GV_COUNT = 13
+  GV_TC_PAIR_STREAM = 13, GV_COUNT = 14
 };
 // A GEMM's shape key: element type, precision, phase (1: slice-invariant, run once; 2: run per slice group),
 // which operands vary per slice, and gemm_dims (bt, m, k, n) of one slice.

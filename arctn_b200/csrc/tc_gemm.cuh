@@ -81,6 +81,11 @@ constexpr int kPairStages = 4;
 constexpr int kPairStageBytes = PLANES * PLANE_BYTES + PLANES * PLANE_BYTES / 2;  // 48 KB
 constexpr int kPairSmemBytes = kPairStages * kPairStageBytes + STAGING_BYTES + 1024 + 1024;
 static_assert(kPairSmemBytes <= 232448, "shared memory above the 227 KB a block may use");
+// CTA pairs with the streaming epilogue: the pair's smaller stages leave room for both staging buffers beside
+// a three-stage ring.
+constexpr int kPairStreamStages = 3;
+constexpr int kPairStreamSmemBytes = kPairStreamStages * kPairStageBytes + 2 * STAGING_BYTES + 1024 + 1024;
+static_assert(kPairStreamSmemBytes <= 232448, "shared memory above the 227 KB a block may use");
 template <int F>
 struct Fmt {
   static constexpr bool kBF16 = F != FMT_TF32X3;
@@ -591,9 +596,10 @@ __device__ __forceinline__ void tc_cgemm_body(const CUtensorMap& tmA, const CUte
   using FM = Fmt<F>;
   static_assert(!kStream || F == FMT_TF32X3, "the streaming epilogue is built for split-TF32 operands");
   static_assert(!kDeep || (F == FMT_TF32X3 && !kStream), "the deep ring is built for split-TF32 operands");
-  static_assert(!kPair || (F == FMT_TF32X3 && !kStream && !kDeep), "the CTA pair is built for split-TF32 operands");
+  static_assert(!kPair || (F == FMT_TF32X3 && !kDeep), "the CTA pair is built for split-TF32 operands");
   constexpr bool kBF16 = FM::kBF16;
-  constexpr int STAGES = kPair ? kPairStages : kDeep ? kDeepStages : kStream ? kStreamStages : FM::kStages;
+  constexpr int STAGES = kPair ? (kStream ? kPairStreamStages : kPairStages)
+                               : kDeep ? kDeepStages : kStream ? kStreamStages : FM::kStages;
   constexpr int STAGE_BYTES = kPair ? kPairStageBytes : kDeep ? kDeepStageBytes : FM::kStageBytes;
   constexpr int PLANES = FM::kPlanes;
   constexpr int PLANE_BYTES = kDeep ? BM * kDeepBK * 4 : tc::PLANE_BYTES;
@@ -1008,6 +1014,11 @@ static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3_pair(con
                                                                      const __grid_constant__ CUtensorMap tmB,
                                                                      TcArgs args) {
   tc_cgemm_body<FMT_TF32X3, false, false, true>(tmA, tmB, args);
+}
+// Split-TF32 on CTA pairs with the streaming epilogue (three 48 KB stages, double-buffered staging).
+static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3_pair_stream(
+    const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, TcArgs args) {
+  tc_cgemm_body<FMT_TF32X3, true, false, true>(tmA, tmB, args);
 }
 // Split-TF32 with the deep ring (six 32 KB stages of 8 of K, 32-byte swizzle).
 static __global__ void __launch_bounds__(kThreads, 1) k_tc_cgemm_tf32x3_deep(const __grid_constant__ CUtensorMap tmA,

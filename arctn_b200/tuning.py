@@ -26,10 +26,10 @@ import time
 from . import _capi as C
 
 VARIANT_NAMES = ["auto", "simt_small", "simt_tile64", "simt_tile32", "simt_warp", "simt_tile128", "simt_dot",
-                 "tc_mfast", "tc_nfast", "tc_splitk", "tc_stream", "tc_deep", "tc_pair"]
+                 "tc_mfast", "tc_nfast", "tc_splitk", "tc_stream", "tc_deep", "tc_pair", "tc_pair_stream"]
 VARIANT_CODES = {name: code for code, name in enumerate(VARIANT_NAMES)}
 SIMT_VARIANTS = ["simt_tile64", "simt_tile32", "simt_tile128", "simt_warp", "simt_small", "simt_dot"]
-TC_VARIANTS = ["tc_mfast", "tc_nfast", "tc_splitk", "tc_stream", "tc_deep", "tc_pair"]
+TC_VARIANTS = ["tc_mfast", "tc_nfast", "tc_splitk", "tc_stream", "tc_deep", "tc_pair", "tc_pair_stream"]
 KEY_FIELDS = ("dtype", "precision", "phase", "a_var", "b_var", "bt", "m", "k", "n")
 
 # Rate ceilings used only to skip candidates that cannot win (TFLOP/s of algorithmic flops): the CUDA cores'
@@ -76,6 +76,8 @@ def candidates(key, S=1):
             out.append("tc_deep")
         if precision == C.PREC_TF32X3 and m > _TILE_M:  # a 256-row pair tile would be half empty otherwise
             out.append("tc_pair")
+            if -(-kk // _TC_K_TILE) <= 32:
+                out.append("tc_pair_stream")
     for v in SIMT_VARIANTS:
         if v == "simt_tile128" and dtype != C.F32:
             continue

@@ -224,9 +224,11 @@ enum {
                                       stages the next 32 output rows while storing the previous ones (short K) */
   ARCTN_B200_GEMM_TC_DEEP = 11,    /* split-TF32 only: six operand stages of 8 of K (32-byte swizzle) instead of
                                       three of 16, more copies in flight (long K) */
-  ARCTN_B200_GEMM_TC_PAIR = 12     /* split-TF32 only: clusters of two CTAs share 256 x 128 output tiles through
+  ARCTN_B200_GEMM_TC_PAIR = 12,    /* split-TF32 only: clusters of two CTAs share 256 x 128 output tiles through
                                       cta_group::2 MMAs, each CTA holding half of the B tile (less operand
                                       traffic per MMA, four operand stages) */
+  ARCTN_B200_GEMM_TC_PAIR_STREAM = 13 /* split-TF32 only: CTA pairs with the streaming epilogue of TC_STREAM over a
+                                      three-stage ring (short K) */
 };
 /* One GEMM shape and its variant.  phase: 1 for a slice-invariant GEMM (run once per execute), 2 for one run
  * per slice group; a_var / b_var: whether that operand differs per slice; bt, m, k, n: gemm_dims() of one

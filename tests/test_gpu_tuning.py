@@ -26,7 +26,7 @@ PRECS = {"fp32": C.PREC_FP32, "tf32x3": C.PREC_TF32X3, "bf16x3": C.PREC_BF16X3, 
 
 
 def valid(variant, dtype, precision):
-    if variant in ("tc_stream", "tc_deep", "tc_pair"):
+    if variant in ("tc_stream", "tc_deep", "tc_pair", "tc_pair_stream"):
         return precision == "tf32x3" and dtype in (C.F32, C.C64)
     if variant.startswith("tc_"):
         return precision in ("tf32x3", "bf16x3", "bf16x6") and dtype in (C.F32, C.C64)
@@ -141,7 +141,7 @@ def test_cta_pair_step_matches_single_cta_bitwise_and_fp64(case):
     arrays = random_arrays(inputs, size, np.complex64, 5)
     x = [torch.from_numpy(a).cuda() for a in arrays]
     outs = {}
-    for v in ("tc_mfast", "tc_pair"):
+    for v in ("tc_mfast", "tc_pair", "tc_pair_stream"):
         base = A.SlicedProgram(inputs, output, size, [(0, 1)], (), dtype=np.complex64, precision="tf32x3")
         table = T.TuneTable()
         for g in base.gemms():
@@ -154,6 +154,7 @@ def test_cta_pair_step_matches_single_cta_bitwise_and_fp64(case):
         assert prog.device_status(ws) == 0
     # a pair computes each output element with the same MMA sequence as one CTA
     assert np.array_equal(outs["tc_pair"], outs["tc_mfast"])
+    assert np.array_equal(outs["tc_pair_stream"], outs["tc_mfast"])
     want = np.einsum(*sum(([a.astype(np.complex128), t] for a, t in zip(arrays, inputs)), []), output)
     assert rel(outs["tc_pair"], want) <= 1e-5
 
@@ -169,7 +170,7 @@ def test_cta_pair_on_fused_pack_steps_of_rand3reg_n172():
     big = [T.key_of(g) for g in base.gemms() if g["variant"].startswith("tc_") and g["m"] >= 256]
     assert big
     got = {}
-    for v in ("tc_mfast", "tc_pair"):
+    for v in ("tc_mfast", "tc_pair", "tc_pair_stream"):
         table = T.TuneTable()
         for k in big:
             table.set(k, v)
@@ -177,3 +178,4 @@ def test_cta_pair_on_fused_pack_steps_of_rand3reg_n172():
         assert any("pack_into" in o for o in prog.describe()["ops"] if o.get("variant") == v)
         got[v] = np.asarray(prog.execute(arrays, f64_out=True))
     assert np.array_equal(got["tc_pair"], got["tc_mfast"])
+    assert np.array_equal(got["tc_pair_stream"], got["tc_mfast"])

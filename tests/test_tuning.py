@@ -74,6 +74,8 @@ def test_candidates_respect_dtype_and_precision():
     assert "tc_pair" in T.candidates((C.C64, C.PREC_TF32X3, 2, 1, 1, 1, 512, 16384, 1024), 37)
     assert "tc_pair" not in T.candidates((C.C64, C.PREC_TF32X3, 2, 1, 1, 1, 128, 64, 16384), 37)
     assert "tc_pair" not in T.candidates((C.C64, C.PREC_BF16X6, 2, 1, 1, 1, 512, 16384, 1024), 37)
+    assert "tc_pair_stream" in T.candidates((C.C64, C.PREC_TF32X3, 2, 1, 1, 1, 512, 512, 32768), 37)
+    assert "tc_pair_stream" not in T.candidates((C.C64, C.PREC_TF32X3, 2, 1, 1, 1, 512, 16384, 1024), 37)
 
 
 def test_table_pins_only_matching_gemms():
