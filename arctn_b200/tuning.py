@@ -276,39 +276,73 @@ def autotune(inputs, output, size_dict, ssa_path, sliced_legs=(), *, dtype="comp
                 times[k][v] = cost[k]
         if log:
             log(f"{v}: {len(pins)} GEMM shapes timed")
-    # A switch between a tensor-core and a SIMT variant changes more than its own GEMM: a tensor-core producer
-    # writes its consumer's packed operand from its epilogue, and a tensor-core consumer needs packs its SIMT
-    # form does not.  Such a switch is kept only if the whole program gets faster, tried one key at a time in
-    # order of the gain measured on the key itself (the largest few, each worth at least 0.2% of the run).
-    # Switches within one family are taken where they beat the heuristic's choice by more than the margin.
-    choice, switches = {}, []
-    for k in todo:
-        timed_ = {v: t for v, t in times[k].items() if t is not None}
-        a = base_var[k]
-        same = {v: t for v, t in timed_.items() if v.startswith("tc_") == a.startswith("tc_")}
-        other = {v: t for v, t in timed_.items() if v not in same}
-        best = min(same, key=same.get)
-        choice[k] = best if same[best] < (1.0 - margin) * same[a] else a
-        if other:
-            b = min(other, key=other.get)
-            if other[b] < same[choice[k]]:
-                switches.append((same[choice[k]] - other[b], k, b))
-    current = base_total
-    switches.sort(reverse=True)
-    confirmed = 0
-    for gain, k, v in switches[:8]:
-        if gain < 0.002 * base_total:
-            break
+    def with_choices(extra):
         trial = TuneTable()
         for kk in table.keys():
             trial.set(kk, table.get(kk))
         for kk, vv in choice.items():
             trial.set(kk, vv)
-        trial.set(k, v)
+        for kk, vv in extra.items():
+            trial.set(kk, vv)
+        return trial
+
+    def program_ms(trial):
         try:
-            _, _, _, total = _key_costs(build(trial), arrays, reps)
+            return _key_costs(build(trial), arrays, reps)[3]
         except torch.cuda.OutOfMemoryError:
             torch.cuda.empty_cache()
+            return None
+
+    # Within one family a variant replaces the heuristic's choice where it beats it by more than the margin.
+    choice = {}
+    for k in todo:
+        a = base_var[k]
+        same = {v: t for v, t in times[k].items()
+                if v in VARIANT_CODES and t is not None and v.startswith("tc_") == a.startswith("tc_")}
+        best = min(same, key=same.get)
+        choice[k] = best if same[best] < (1.0 - margin) * same[a] else a
+    # A variant's in-situ time is taken with that variant pinned on every key it may serve, and all GEMMs share
+    # one power budget: a variant that slows some other key draws less power and lets the clock of the whole
+    # run rise.  So a switch on a key worth more than 5% of the run is kept only if the whole program gets
+    # faster by 1% with it, tried one key at a time from the largest measured gain.
+    current = base_total
+    big = sorted(((times[k][base_var[k]] - times[k][choice[k]], k) for k in todo
+                  if choice[k] != base_var[k] and times[k][base_var[k]] > 0.05 * base_total), reverse=True)
+    confirmed_big = 0
+    if big:
+        pending = {k: choice[k] for _, k in big}
+        for _, k in big:
+            choice[k] = base_var[k]
+        start = program_ms(with_choices({}))
+        current = start if start is not None else base_total
+        for _, k in big:
+            total = program_ms(with_choices({k: pending[k]}))
+            if total is None:
+                continue
+            times[k]["whole_program_ms"] = {"before": current, "after": total}
+            if total < 0.99 * current:
+                choice[k], current = pending[k], total
+                confirmed_big += 1
+    # A switch between a tensor-core and a SIMT variant changes more than its own GEMM: a tensor-core producer
+    # writes its consumer's packed operand from its epilogue, and a tensor-core consumer needs packs its SIMT
+    # form does not.  Such a switch is kept only if the whole program gets faster, tried one key at a time in
+    # order of the gain measured on the key itself (the largest few, each worth at least 0.2% of the run).
+    switches = []
+    for k in todo:
+        timed_ = {v: t for v, t in times[k].items() if v in VARIANT_CODES and t is not None}
+        a = base_var[k]
+        other = {v: t for v, t in timed_.items() if v.startswith("tc_") != a.startswith("tc_")}
+        if other:
+            b = min(other, key=other.get)
+            if other[b] < timed_[choice[k]]:
+                switches.append((timed_[choice[k]] - other[b], k, b))
+    switches.sort(reverse=True)
+    confirmed = 0
+    for gain, k, v in switches[:8]:
+        if gain < 0.002 * base_total:
+            break
+        total = program_ms(with_choices({k: v}))
+        if total is None:
             continue
         times[k]["whole_program_ms"] = {"before": current, "after": total}
         if total < 0.998 * current:
@@ -320,6 +354,7 @@ def autotune(inputs, output, size_dict, ssa_path, sliced_legs=(), *, dtype="comp
     table.meta["program_ms_before"] = base_total
     table.meta["program_ms_after"] = current
     table.meta["family_switches_kept"] = confirmed
+    table.meta["large_key_switches_kept"] = confirmed_big
     table.meta.setdefault("device", torch.cuda.get_device_name(device))
     table.meta["tune_seconds"] = table.meta.get("tune_seconds", 0.0) + (time.perf_counter() - t0)
     del arrays

@@ -106,8 +106,10 @@ def test_autotune_picks_timed_winners_and_matches_oracle():
         # whole program got faster
         fam = {v: t for v, t in times.items() if v.startswith("tc_") == g["variant"].startswith("tc_")}
         best = min(fam, key=fam.get)
-        if g["variant"] != best:
-            assert g["variant"] == tm["heuristic"] and fam[best] >= 0.97 * fam[tm["heuristic"]]
+        if g["variant"] != best:  # kept the heuristic's: within the margin, or the whole program said no
+            assert g["variant"] == tm["heuristic"]
+            w = tm.get("whole_program_ms")
+            assert fam[best] >= 0.97 * fam[tm["heuristic"]] or (w and w["after"] >= 0.99 * w["before"])
         if g["variant"].startswith("tc_") != tm["heuristic"].startswith("tc_"):
             w = tm["whole_program_ms"]
             assert w["after"] < w["before"]
