@@ -249,9 +249,10 @@ def tensor_pipe_peak(kind="tf32", n=256, iters=1 << 16, device=None, repeats=3):
     """Measured dense tensor-pipe rate of a GPU in TFLOP/s (``arctn_b200_tc_peak``): tcgen05 MMAs with M = 128,
     N = ``n`` (128 or 256) over operands resident in shared memory, ``kind`` "tf32" or "bf16"; or
     "tf32_gemm_stream" (n = 128): the split-TF32 GEMM's own MMA sequence over operands streaming through its
-    three-stage ring layout.  Best of ``repeats`` launches after one warm-up."""
+    three-stage ring layout, every operand 1.0; "tf32_gemm_stream_random": the same over random TF32 hi / lo
+    operands.  Best of ``repeats`` launches after one warm-up."""
     torch = _torch()
-    code = {"tf32": 0, "bf16": 1, "tf32_gemm_stream": 2}[kind]
+    code = {"tf32": 0, "bf16": 1, "tf32_gemm_stream": 2, "tf32_gemm_stream_random": 3}[kind]
     dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
     with torch.cuda.device(dev):
         status = torch.zeros(1, dtype=torch.int32, device=dev)

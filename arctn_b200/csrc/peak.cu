@@ -1,5 +1,8 @@
 // Tensor-pipe peak probe: the dense MMA rate of this GPU for the operand kinds the GEMMs use, and the rate of the
-// split-TF32 GEMM's own MMA stream over operands laid out as its ring (kind 2).
+// split-TF32 GEMM's own MMA stream over operands laid out as its ring (kind 2: every operand 1.0; kind 3: random
+// TF32 hi / lo values with random signs, as the GEMM's packed operands).  The tensor pipe's power depends on how
+// many operand bits change from one MMA to the next, so under the power cap the two kinds can settle at
+// different clocks when run for seconds.
 //
 // Every SM runs one CTA whose single issuing thread streams `iters` tcgen05.mma instructions (M = 128,
 // N = 128 or 256, K = 8 for kind::tf32 / 16 for kind::f16 with BF16 operands) over operands that stay
@@ -77,11 +80,32 @@ __global__ void __launch_bounds__(128, 1) k_tc_peak(long long iters, int* err) {
 // the 4M product in the kernel's order, over A and B planes laid out as the GEMM's operand ring -- three
 // 64 KB stages of 8 planes, a new stage every two iterations -- into two accumulators (Cr, Ci).  Its rate is
 // the ceiling the GEMM's MMA phase can reach with operands streaming through shared memory.
+// A 32-bit integer mix (the MurmurHash3 finaliser), for the random operands.
+__device__ __forceinline__ uint32_t mix32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x85EBCA6Bu;
+  x ^= x >> 13;
+  x *= 0xC2B2AE35u;
+  x ^= x >> 16;
+  return x;
+}
+
+template <bool kRandom>
 __global__ void __launch_bounds__(128, 1) k_tc_peak_stream(long long iters, int* err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint32_t* words = (uint32_t*)smem;
-  for (int i = threadIdx.x; i < tc::STAGES * tc::STAGE_BYTES / 4; i += blockDim.x) words[i] = 0x3F800000u;
+  for (int i = threadIdx.x; i < tc::STAGES * tc::STAGE_BYTES / 4; i += blockDim.x) {
+    if constexpr (kRandom) {
+      // plane (i * 4 / PLANE_BYTES) % 8: even planes hold hi parts in +-[0.5, 1), odd planes lo parts about 2^-11
+      // of that; both carry a random 10-bit TF32 mantissa and a random sign
+      const uint32_t h = mix32((uint32_t)i * 0x9E3779B9u + blockIdx.x * 0x632BE5ABu + 1u);
+      const bool lo = ((i * 4 / tc::PLANE_BYTES) & 1) != 0;
+      words[i] = (h & 0x80000000u) | (lo ? 0x39800000u : 0x3F000000u) | (h & 0x007FE000u);
+    } else {
+      words[i] = 0x3F800000u;
+    }
+  }
   uint64_t* bar = (uint64_t*)(smem + tc::STAGES * tc::STAGE_BYTES);
   volatile uint32_t* tmem_slot = (volatile uint32_t*)(bar + 1);
   const int warp = threadIdx.x / 32;
@@ -134,11 +158,12 @@ __global__ void __launch_bounds__(128, 1) k_tc_peak_stream(long long iters, int*
   }
 }
 
+template <bool kRandom>
 cudaError_t launch_peak_stream(int ctas, long long iters, int* err, cudaStream_t st) {
   constexpr int smem = tc::STAGES * tc::STAGE_BYTES + 64 + 1024;
-  cudaError_t e = cudaFuncSetAttribute(k_tc_peak_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = cudaFuncSetAttribute(k_tc_peak_stream<kRandom>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  k_tc_peak_stream<<<ctas, 128, smem, st>>>(iters, err);
+  k_tc_peak_stream<kRandom><<<ctas, 128, smem, st>>>(iters, err);
   return cudaGetLastError();
 }
 
@@ -159,9 +184,11 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
     ab2::set_last_error(m);
     return code;
   };
-  if (kind < 0 || kind > 2) return fail("kind must be 0 (tf32), 1 (bf16) or 2 (split-TF32 GEMM stream)", ARCTN_B200_ERR_INVALID);
+  if (kind < 0 || kind > 3)
+    return fail("kind must be 0 (tf32), 1 (bf16), 2 (split-TF32 GEMM stream) or 3 (the stream on random operands)",
+                ARCTN_B200_ERR_INVALID);
   if (n != 128 && n != 256) return fail("n must be 128 or 256", ARCTN_B200_ERR_INVALID);
-  if (kind == 2 && n != 128) return fail("kind 2 runs the GEMM's N = 128 MMAs", ARCTN_B200_ERR_INVALID);
+  if (kind >= 2 && n != 128) return fail("kinds 2 and 3 run the GEMM's N = 128 MMAs", ARCTN_B200_ERR_INVALID);
   if (iters < 2 || iters > (1ull << 22)) return fail("iters must lie in [2, 2^22]", ARCTN_B200_ERR_INVALID);
   if (!status || !tflops_out) return fail("status and tflops_out must not be null", ARCTN_B200_ERR_INVALID);
   int dev = 0, sms = 0;
@@ -175,7 +202,8 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
   const long long it = (long long)iters;
   int* err = (int*)status;
   if (e == cudaSuccess) {
-    if (kind == 2) e = launch_peak_stream(sms, it, err, st);
+    if (kind == 2) e = launch_peak_stream<false>(sms, it, err, st);
+    else if (kind == 3) e = launch_peak_stream<true>(sms, it, err, st);
     else if (kind == 0) e = n == 128 ? launch_peak<false, 128>(sms, it, err, st) : launch_peak<false, 256>(sms, it, err, st);
     else e = n == 128 ? launch_peak<true, 128>(sms, it, err, st) : launch_peak<true, 256>(sms, it, err, st);
   }
@@ -186,7 +214,7 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (e != cudaSuccess) return fail(std::string("tensor-core peak probe: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
-  const double k = kind == 1 ? 16.0 : 8.0, per_iter = kind == 2 ? 12.0 : 1.0;  // kind 2: 12 MMAs an iteration
+  const double k = kind == 1 ? 16.0 : 8.0, per_iter = kind >= 2 ? 12.0 : 1.0;  // kinds 2, 3: 12 MMAs an iteration
   *tflops_out = 2.0 * 128.0 * n * k * per_iter * (double)iters * sms / (ms * 1e-3) / 1e12;
   ab2::set_last_error("");
   return ARCTN_B200_OK;

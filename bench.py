@@ -113,8 +113,8 @@ def per_step_roofline(prog, ms, tf32_pipe_tflops, hbm_gbs, sustained_tflops=None
     the tensor bound is its split-TF32 pipe work (3 TF32 products per real product) at the measured TF32 rate,
     the memory bound its algorithmic bytes (16 B per packed operand element read, 16 B per packed or 8 B per
     plain output element written) at the HBM rate; the step's bound is the larger of the two times.  With
-    `sustained_tflops` (the TF32 rate held for seconds under the power cap) each step also carries its
-    tensor work against that rate."""
+    `sustained_tflops` (the TF32 rate held for seconds under the power cap, on random operands) each step
+    also carries its tensor work against that rate."""
     ops = prog.describe()["ops"]
     units = {}
     for i, o in enumerate(ops):
@@ -1048,7 +1048,14 @@ def main():
                 sust = A.tensor_pipe_peak("tf32_gemm_stream", 128, iters=1 << 22, device=local, repeats=1)
                 pk_tc["tf32_gemm_stream_sustained"] = sust
                 roof["pipe_frac_of_sustained_gemm_stream"] = achieved * 3 / sust
-                roof["per_step"] = per_step_roofline(prog, ms, tf32_peak, pk["hbm_gbs"], sust)
+                # The probes above stream operands that are all 1.0.  The tensor pipe's power follows its operand
+                # bits, so the same stream over random TF32 hi / lo operands, held as long, is the rate the pipe
+                # sustains on data like the GEMM's under the power cap.
+                pk_tc["tf32_gemm_stream_random_n128"] = A.tensor_pipe_peak("tf32_gemm_stream_random", 128, device=local)
+                sust_rand = A.tensor_pipe_peak("tf32_gemm_stream_random", 128, iters=1 << 22, device=local, repeats=1)
+                pk_tc["tf32_gemm_stream_random_sustained"] = sust_rand
+                roof["pipe_frac_of_sustained_random_stream"] = achieved * 3 / sust_rand
+                roof["per_step"] = per_step_roofline(prog, ms, tf32_peak, pk["hbm_gbs"], sust_rand)
         else:
             achieved = tw / (tms * 1e-3) / 1e9
             roof = {"bound": "hbm", "kernel": KIND_NAMES.get(top, str(top)), "achieved": achieved,

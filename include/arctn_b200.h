@@ -344,7 +344,9 @@ int arctn_b200_cgemm_noalloc_status(void* cuda_stream, int* code);
  * one CTA per SM streams `iters` tcgen05.mma instructions (M = 128, N = n in {128, 256}; kind 0: TF32,
  * K = 8; kind 1: BF16, K = 16) over operands resident in shared memory, with no TMA and no epilogue.
  * kind 2 (n = 128): `iters` K steps of the split-TF32 GEMM's own 12-MMA 4M sequence over planes laid out as
- * its three-stage operand ring, a new 64 KB stage every two steps -- the ceiling of the GEMM's MMA phase.
+ * its three-stage operand ring, a new 64 KB stage every two steps -- the ceiling of the GEMM's MMA phase; every
+ * operand is 1.0.  kind 3 (n = 128): the same stream over random TF32 hi / lo operands with random signs, whose
+ * bit activity (and so power under the 1 kW cap, when run for seconds) is that of real packed operands.
  * Synchronises cuda_stream and sets *tflops_out to 2*128*n*K*MMAs / elapsed (TF32 MMA work).  `status` is a
  * device int the caller zeroed: nonzero afterwards means the final bounded wait expired.  iters in [2, 2^22]. */
 int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status, void* cuda_stream, double* tflops_out);

@@ -144,6 +144,10 @@ def test_tensor_pipe_peak_probe(kind):
         stream = A.tensor_pipe_peak("tf32_gemm_stream", 128, iters=1 << 12, repeats=1)
         print("tf32 gemm stream", stream)
         assert 0.5 * max(rates.values()) < stream < 2.0 * max(rates.values()), (stream, rates)
+        # the same stream over random hi / lo operands does the same MMA work
+        rand = A.tensor_pipe_peak("tf32_gemm_stream_random", 128, iters=1 << 12, repeats=1)
+        print("tf32 gemm stream, random operands", rand)
+        assert 0.5 * stream < rand < 2.0 * stream, (rand, stream)
 
 
 def test_bf16x6_rand3reg_n104_matches_fp64_oracle():
