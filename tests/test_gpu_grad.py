@@ -103,9 +103,9 @@ def test_grid8_bond6_c64_gradient_tf32x3_against_c128():
     # With that scaling the scalar is ~1e-35, at the bottom of FP32's range; every input is multiplied
     # by 4 (exact in binary floating point), which scales the result by 4^64 and every gradient by 4^63.
     # The contraction cancels heavily (the scalar is far below the norms of its intermediates), so even
-    # exact-FP32 arithmetic misses the c128 value by ~3e-5 relative.  tf32x3 must do as well as the FP32
-    # SIMT path: each error is bounded by twice the FP32 path's, or by 1e-5 where that is larger.  A
-    # gradient tensor's error is normwise, ||g - g_ref||_F / ||g_ref||_F.
+    # exact-FP32 arithmetic misses the c128 value by ~3e-5 relative: the scalar must do as well as the FP32
+    # SIMT path (1.7e-5 against 2.5e-5 measured).  Every gradient tensor meets 1e-5 normwise,
+    # ||g - g_ref||_F / ||g_ref||_F (at most 7.9e-6 measured; the FP32 path 5.5e-6).
     net, arrays = N.workload_grid8(6, np.complex64, seed=0)
     arrays = [a * np.float32(4.0) for a in arrays]
     path = A.greedy(*net.as_tuple())
@@ -124,12 +124,12 @@ def test_grid8_bond6_c64_gradient_tf32x3_against_c128():
         return abs(complex(o.item()) - ref) / abs(ref)
 
     assert rel(of32) <= 1e-4  # sanity of the comparison itself
-    assert rel(otc) <= max(1e-5, 2 * rel(of32)), (rel(otc), rel(of32))
+    assert rel(otc) <= max(1e-5, rel(of32)), (rel(otc), rel(of32))
     for a, f, b in zip(gtc, gf32, g64):
         a, f, b = (t.cpu().numpy().astype(np.complex128) for t in (a, f, b))
         scale = np.linalg.norm(b)
         err_tc, err_f32 = np.linalg.norm(a - b) / scale, np.linalg.norm(f - b) / scale
-        assert err_tc <= max(1e-5, 2 * err_f32), (err_tc, err_f32)
+        assert err_tc <= 1e-5, (err_tc, err_f32)
 
 
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["c128", "c64"])
