@@ -250,9 +250,11 @@ def tensor_pipe_peak(kind="tf32", n=256, iters=1 << 16, device=None, repeats=3):
     N = ``n`` (128 or 256) over operands resident in shared memory, ``kind`` "tf32" or "bf16"; or
     "tf32_gemm_stream" (n = 128): the split-TF32 GEMM's own MMA sequence over operands streaming through its
     three-stage ring layout, every operand 1.0; "tf32_gemm_stream_random": the same over random TF32 hi / lo
-    operands.  Best of ``repeats`` launches after one warm-up."""
+    operands; "bf16x6_gemm_stream_random": the three-piece split-BF16 GEMM's 24-MMA sequence over random BF16
+    pieces (BF16 MMA work).  Best of ``repeats`` launches after one warm-up."""
     torch = _torch()
-    code = {"tf32": 0, "bf16": 1, "tf32_gemm_stream": 2, "tf32_gemm_stream_random": 3}[kind]
+    code = {"tf32": 0, "bf16": 1, "tf32_gemm_stream": 2, "tf32_gemm_stream_random": 3,
+            "bf16x6_gemm_stream_random": 4}[kind]
     dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
     with torch.cuda.device(dev):
         status = torch.zeros(1, dtype=torch.int32, device=dev)

@@ -158,6 +158,79 @@ __global__ void __launch_bounds__(128, 1) k_tc_peak_stream(long long iters, int*
   }
 }
 
+// The three-piece split-BF16 GEMM's MMA stream (FMT_BF16X6) on random operands: per iteration (one 16-wide K step)
+// the 24 kind::f16 MMAs of its 4M product in the kernel's order -- products (h,h), (h,m), (m,h), (h,l), (l,h),
+// (m,m) of each real product -- over planes laid out as its two-stage ring of 96 KB stages (re h, m, l, im h,
+// m, l for A, then B), a new stage every two iterations.  Pieces are random BF16 values with random signs:
+// h in +-[0.5, 1), m about 2^-8 and l about 2^-16 of that.
+__global__ void __launch_bounds__(128, 1) k_tc_peak_six(long long iters, int* err) {
+  using FM = tc::Fmt<tc::FMT_BF16X6>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint32_t* words = (uint32_t*)smem;
+  for (int i = threadIdx.x; i < FM::kStages * FM::kStageBytes / 4; i += blockDim.x) {
+    const uint32_t h = mix32((uint32_t)i * 0x9E3779B9u + blockIdx.x * 0x632BE5ABu + 7u);
+    const int piece = ((i * 4 % FM::kStageBytes) / tc::PLANE_BYTES) % 3;  // h, m, l
+    const uint32_t base = piece == 0 ? 0x3F00u : piece == 1 ? 0x3B00u : 0x3700u;
+    const uint32_t lo16 = (h & 0x8000u) | base | (h & 0x7Fu), hi16 = ((h >> 16) & 0x8000u) | base | ((h >> 16) & 0x7Fu);
+    words[i] = hi16 << 16 | lo16;
+  }
+  uint64_t* bar = (uint64_t*)(smem + FM::kStages * FM::kStageBytes);
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(bar + 1);
+  const int warp = threadIdx.x / 32;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tc::smem_u32((const void*)tmem_slot)),
+                 "r"(256u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  if (threadIdx.x == 32) {
+    const uint32_t base = tc::smem_u32(smem), P = tc::PLANE_BYTES;
+    const uint32_t cr = tmem, ci = tmem + 128;
+    const uint32_t pos = tc::idesc_bf16(false), neg = tc::idesc_bf16(true);
+    constexpr int px[6] = {0, 0, 1, 0, 2, 1}, py[6] = {0, 1, 0, 2, 0, 1};
+    for (long long i = 0; i < iters; ++i) {
+      const uint32_t o = (uint32_t)(i & 1) * 32;
+      const uint32_t a0 = base + (uint32_t)((i / 2) % FM::kStages) * FM::kStageBytes, b0 = a0 + FM::kPlanes * P;
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        const uint32_t Ar = a0 + px[q] * P + o, Ai = Ar + 3 * P;
+        const uint32_t Br = b0 + py[q] * P + o, Bi = Br + 3 * P;
+        const uint32_t acc = (i > 0 || q > 0) ? 1u : 0u;
+        tc::umma<true>(cr, tc::sw64_desc(Ar), tc::sw64_desc(Br), pos, acc);
+        tc::umma<true>(ci, tc::sw64_desc(Ar), tc::sw64_desc(Bi), pos, acc);
+        tc::umma<true>(cr, tc::sw64_desc(Ai), tc::sw64_desc(Bi), neg, 1);
+        tc::umma<true>(ci, tc::sw64_desc(Ai), tc::sw64_desc(Br), pos, 1);
+      }
+    }
+    tc::umma_commit(bar);
+    tc::mbar_wait(bar, 0, err, 9);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u));
+  }
+}
+
+cudaError_t launch_peak_six(int ctas, long long iters, int* err, cudaStream_t st) {
+  constexpr int smem = tc::Fmt<tc::FMT_BF16X6>::kStages * tc::Fmt<tc::FMT_BF16X6>::kStageBytes + 64 + 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_tc_peak_six, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  k_tc_peak_six<<<ctas, 128, smem, st>>>(iters, err);
+  return cudaGetLastError();
+}
+
 template <bool kRandom>
 cudaError_t launch_peak_stream(int ctas, long long iters, int* err, cudaStream_t st) {
   constexpr int smem = tc::STAGES * tc::STAGE_BYTES + 64 + 1024;
@@ -184,11 +257,11 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
     ab2::set_last_error(m);
     return code;
   };
-  if (kind < 0 || kind > 3)
-    return fail("kind must be 0 (tf32), 1 (bf16), 2 (split-TF32 GEMM stream) or 3 (the stream on random operands)",
-                ARCTN_B200_ERR_INVALID);
+  if (kind < 0 || kind > 4)
+    return fail("kind must be 0 (tf32), 1 (bf16), 2 (split-TF32 GEMM stream), 3 (the stream on random operands) or "
+                "4 (the three-piece split-BF16 GEMM stream on random operands)", ARCTN_B200_ERR_INVALID);
   if (n != 128 && n != 256) return fail("n must be 128 or 256", ARCTN_B200_ERR_INVALID);
-  if (kind >= 2 && n != 128) return fail("kinds 2 and 3 run the GEMM's N = 128 MMAs", ARCTN_B200_ERR_INVALID);
+  if (kind >= 2 && n != 128) return fail("kinds 2 to 4 run the GEMMs' N = 128 MMAs", ARCTN_B200_ERR_INVALID);
   if (iters < 2 || iters > (1ull << 22)) return fail("iters must lie in [2, 2^22]", ARCTN_B200_ERR_INVALID);
   if (!status || !tflops_out) return fail("status and tflops_out must not be null", ARCTN_B200_ERR_INVALID);
   int dev = 0, sms = 0;
@@ -204,6 +277,7 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
   if (e == cudaSuccess) {
     if (kind == 2) e = launch_peak_stream<false>(sms, it, err, st);
     else if (kind == 3) e = launch_peak_stream<true>(sms, it, err, st);
+    else if (kind == 4) e = launch_peak_six(sms, it, err, st);
     else if (kind == 0) e = n == 128 ? launch_peak<false, 128>(sms, it, err, st) : launch_peak<false, 256>(sms, it, err, st);
     else e = n == 128 ? launch_peak<true, 128>(sms, it, err, st) : launch_peak<true, 256>(sms, it, err, st);
   }
@@ -214,7 +288,8 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (e != cudaSuccess) return fail(std::string("tensor-core peak probe: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
-  const double k = kind == 1 ? 16.0 : 8.0, per_iter = kind >= 2 ? 12.0 : 1.0;  // kinds 2, 3: 12 MMAs an iteration
+  // kinds 2, 3: 12 TF32 MMAs (K = 8) an iteration; kind 4: 24 BF16 MMAs (K = 16)
+  const double k = (kind == 1 || kind == 4) ? 16.0 : 8.0, per_iter = kind == 4 ? 24.0 : kind >= 2 ? 12.0 : 1.0;
   *tflops_out = 2.0 * 128.0 * n * k * per_iter * (double)iters * sms / (ms * 1e-3) / 1e12;
   ab2::set_last_error("");
   return ARCTN_B200_OK;

@@ -347,6 +347,8 @@ int arctn_b200_cgemm_noalloc_status(void* cuda_stream, int* code);
  * its three-stage operand ring, a new 64 KB stage every two steps -- the ceiling of the GEMM's MMA phase; every
  * operand is 1.0.  kind 3 (n = 128): the same stream over random TF32 hi / lo operands with random signs, whose
  * bit activity (and so power under the 1 kW cap, when run for seconds) is that of real packed operands.
+ * kind 4 (n = 128): `iters` K steps of 16 of the three-piece split-BF16 GEMM's 24-MMA sequence (kind::f16,
+ * K = 16) over random BF16 pieces laid out as its two-stage ring; the rate counts BF16 MMA work.
  * Synchronises cuda_stream and sets *tflops_out to 2*128*n*K*MMAs / elapsed (TF32 MMA work).  `status` is a
  * device int the caller zeroed: nonzero afterwards means the final bounded wait expired.  iters in [2, 2^22]. */
 int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status, void* cuda_stream, double* tflops_out);

@@ -138,6 +138,10 @@ def test_tensor_pipe_peak_probe(kind):
     assert all(100.0 < r < 5000.0 for r in rates.values()), rates
     if kind == "bf16":
         assert rates[256] > A.tensor_pipe_peak("tf32", 256, iters=1 << 14, repeats=1)
+        # the three-piece split-BF16 GEMM's MMA stream (random pieces) at the same order of rate
+        six = A.tensor_pipe_peak("bf16x6_gemm_stream_random", 128, iters=1 << 11, repeats=1)
+        print("bf16x6 gemm stream, random operands", six)
+        assert 0.5 * max(rates.values()) < six < 2.0 * max(rates.values()), (six, rates)
     else:
         # the GEMM's own MMA sequence (two interleaved accumulators, operands streaming through its ring layout)
         # runs at the same order of rate as a single accumulator chain over resident operands
