@@ -251,10 +251,11 @@ def tensor_pipe_peak(kind="tf32", n=256, iters=1 << 16, device=None, repeats=3):
     "tf32_gemm_stream" (n = 128): the split-TF32 GEMM's own MMA sequence over operands streaming through its
     three-stage ring layout, every operand 1.0; "tf32_gemm_stream_random": the same over random TF32 hi / lo
     operands; "bf16x6_gemm_stream_random": the three-piece split-BF16 GEMM's 24-MMA sequence over random BF16
-    pieces (BF16 MMA work).  Best of ``repeats`` launches after one warm-up."""
+    pieces (BF16 MMA work); "tf32_3m_stream_random": a 3M split-TF32 product's 9 MMAs per K step over random
+    operands (TF32 MMA work).  Best of ``repeats`` launches after one warm-up."""
     torch = _torch()
     code = {"tf32": 0, "bf16": 1, "tf32_gemm_stream": 2, "tf32_gemm_stream_random": 3,
-            "bf16x6_gemm_stream_random": 4}[kind]
+            "bf16x6_gemm_stream_random": 4, "tf32_3m_stream_random": 5}[kind]
     dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
     with torch.cuda.device(dev):
         status = torch.zeros(1, dtype=torch.int32, device=dev)

@@ -223,6 +223,75 @@ __global__ void __launch_bounds__(128, 1) k_tc_peak_six(long long iters, int* er
   }
 }
 
+// A 3M (Gauss) split-TF32 complex product's MMA stream on random operands, as a measurement of what that form
+// would sustain: per iteration (one 8-wide K step) 9 MMAs -- the split products (h,h), (l,h), (h,l) of
+// T1 = Ar.Br, T2 = Ai.Bi and T3 = (Ar + Ai).(Br + Bi), into three accumulators -- over six planes per operand
+// (hi and lo of Ar, Ai and Ar + Ai) in a two-stage ring of 96 KB stages.  Re = T1 - T2 and Im = T3 - T1 - T2
+// would be formed when draining; the probe only streams the MMAs.
+__global__ void __launch_bounds__(128, 1) k_tc_peak_3m(long long iters, int* err) {
+  constexpr int kPlanes = 6, kStageBytes = 2 * kPlanes * tc::PLANE_BYTES, kStages = 2;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint32_t* words = (uint32_t*)smem;
+  for (int i = threadIdx.x; i < kStages * kStageBytes / 4; i += blockDim.x) {
+    const uint32_t h = mix32((uint32_t)i * 0x9E3779B9u + blockIdx.x * 0x632BE5ABu + 11u);
+    const bool lo = ((i * 4 / tc::PLANE_BYTES) & 1) != 0;
+    words[i] = (h & 0x80000000u) | (lo ? 0x39800000u : 0x3F000000u) | (h & 0x007FE000u);
+  }
+  uint64_t* bar = (uint64_t*)(smem + kStages * kStageBytes);
+  volatile uint32_t* tmem_slot = (volatile uint32_t*)(bar + 1);
+  const int warp = threadIdx.x / 32;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tc::smem_u32((const void*)tmem_slot)),
+                 "r"(512u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  if (threadIdx.x == 32) {
+    const uint32_t base = tc::smem_u32(smem), P = tc::PLANE_BYTES;
+    const uint32_t t1 = tmem, t2 = tmem + 128, t3 = tmem + 256;
+    const uint32_t pos = tc::idesc_tf32(false);
+    for (long long i = 0; i < iters; ++i) {
+      const uint32_t o = (uint32_t)(i & 1) * 32;
+      const uint32_t a0 = base + (uint32_t)((i / 2) % kStages) * kStageBytes + o, b0 = a0 + kPlanes * P;
+      const uint32_t acc = i > 0 ? 1u : 0u;
+      // operand planes: 0/1 hi/lo of the real part, 2/3 of the imaginary part, 4/5 of their sum
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        const uint32_t d = t == 0 ? t1 : t == 1 ? t2 : t3, ah = a0 + 2 * t * P, bh = b0 + 2 * t * P;
+        tc::umma<false>(d, tc::sw64_desc(ah), tc::sw64_desc(bh), pos, acc);
+        tc::umma<false>(d, tc::sw64_desc(ah + P), tc::sw64_desc(bh), pos, 1);
+        tc::umma<false>(d, tc::sw64_desc(ah), tc::sw64_desc(bh + P), pos, 1);
+      }
+    }
+    tc::umma_commit(bar);
+    tc::mbar_wait(bar, 0, err, 9);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u));
+  }
+}
+
+cudaError_t launch_peak_3m(int ctas, long long iters, int* err, cudaStream_t st) {
+  constexpr int smem = 2 * 2 * 6 * tc::PLANE_BYTES + 64 + 1024;
+  cudaError_t e = cudaFuncSetAttribute(k_tc_peak_3m, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  k_tc_peak_3m<<<ctas, 128, smem, st>>>(iters, err);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_peak_six(int ctas, long long iters, int* err, cudaStream_t st) {
   constexpr int smem = tc::Fmt<tc::FMT_BF16X6>::kStages * tc::Fmt<tc::FMT_BF16X6>::kStageBytes + 64 + 1024;
   cudaError_t e = cudaFuncSetAttribute(k_tc_peak_six, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -257,11 +326,12 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
     ab2::set_last_error(m);
     return code;
   };
-  if (kind < 0 || kind > 4)
-    return fail("kind must be 0 (tf32), 1 (bf16), 2 (split-TF32 GEMM stream), 3 (the stream on random operands) or "
-                "4 (the three-piece split-BF16 GEMM stream on random operands)", ARCTN_B200_ERR_INVALID);
+  if (kind < 0 || kind > 5)
+    return fail("kind must be 0 (tf32), 1 (bf16), 2 (split-TF32 GEMM stream), 3 (the stream on random operands), "
+                "4 (the three-piece split-BF16 GEMM stream on random operands) or 5 (a 3M split-TF32 stream on "
+                "random operands)", ARCTN_B200_ERR_INVALID);
   if (n != 128 && n != 256) return fail("n must be 128 or 256", ARCTN_B200_ERR_INVALID);
-  if (kind >= 2 && n != 128) return fail("kinds 2 to 4 run the GEMMs' N = 128 MMAs", ARCTN_B200_ERR_INVALID);
+  if (kind >= 2 && n != 128) return fail("kinds 2 to 5 run the GEMMs' N = 128 MMAs", ARCTN_B200_ERR_INVALID);
   if (iters < 2 || iters > (1ull << 22)) return fail("iters must lie in [2, 2^22]", ARCTN_B200_ERR_INVALID);
   if (!status || !tflops_out) return fail("status and tflops_out must not be null", ARCTN_B200_ERR_INVALID);
   int dev = 0, sms = 0;
@@ -278,6 +348,7 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
     if (kind == 2) e = launch_peak_stream<false>(sms, it, err, st);
     else if (kind == 3) e = launch_peak_stream<true>(sms, it, err, st);
     else if (kind == 4) e = launch_peak_six(sms, it, err, st);
+    else if (kind == 5) e = launch_peak_3m(sms, it, err, st);
     else if (kind == 0) e = n == 128 ? launch_peak<false, 128>(sms, it, err, st) : launch_peak<false, 256>(sms, it, err, st);
     else e = n == 128 ? launch_peak<true, 128>(sms, it, err, st) : launch_peak<true, 256>(sms, it, err, st);
   }
@@ -288,8 +359,9 @@ extern "C" int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status,
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (e != cudaSuccess) return fail(std::string("tensor-core peak probe: ") + cudaGetErrorString(e), ARCTN_B200_ERR_CUDA);
-  // kinds 2, 3: 12 TF32 MMAs (K = 8) an iteration; kind 4: 24 BF16 MMAs (K = 16)
-  const double k = (kind == 1 || kind == 4) ? 16.0 : 8.0, per_iter = kind == 4 ? 24.0 : kind >= 2 ? 12.0 : 1.0;
+  // kinds 2, 3: 12 TF32 MMAs (K = 8) an iteration; kind 4: 24 BF16 MMAs (K = 16); kind 5: 9 TF32 MMAs
+  const double k = (kind == 1 || kind == 4) ? 16.0 : 8.0;
+  const double per_iter = kind == 5 ? 9.0 : kind == 4 ? 24.0 : kind >= 2 ? 12.0 : 1.0;
   *tflops_out = 2.0 * 128.0 * n * k * per_iter * (double)iters * sms / (ms * 1e-3) / 1e12;
   ab2::set_last_error("");
   return ARCTN_B200_OK;

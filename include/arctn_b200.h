@@ -349,6 +349,8 @@ int arctn_b200_cgemm_noalloc_status(void* cuda_stream, int* code);
  * bit activity (and so power under the 1 kW cap, when run for seconds) is that of real packed operands.
  * kind 4 (n = 128): `iters` K steps of 16 of the three-piece split-BF16 GEMM's 24-MMA sequence (kind::f16,
  * K = 16) over random BF16 pieces laid out as its two-stage ring; the rate counts BF16 MMA work.
+ * kind 5 (n = 128): a 3M split-TF32 complex product's 9-MMA sequence per K step (three accumulators, six
+ * random planes per operand), a measurement of that form's sustained rate; it counts TF32 MMA work.
  * Synchronises cuda_stream and sets *tflops_out to 2*128*n*K*MMAs / elapsed (TF32 MMA work).  `status` is a
  * device int the caller zeroed: nonzero afterwards means the final bounded wait expired.  iters in [2, 2^22]. */
 int arctn_b200_tc_peak(int kind, int n, uint64_t iters, void* status, void* cuda_stream, double* tflops_out);

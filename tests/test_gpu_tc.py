@@ -152,6 +152,10 @@ def test_tensor_pipe_peak_probe(kind):
         rand = A.tensor_pipe_peak("tf32_gemm_stream_random", 128, iters=1 << 12, repeats=1)
         print("tf32 gemm stream, random operands", rand)
         assert 0.5 * stream < rand < 2.0 * stream, (rand, stream)
+        # a 3M product's nine MMAs per K step into three accumulators (a measurement aid)
+        gauss = A.tensor_pipe_peak("tf32_3m_stream_random", 128, iters=1 << 12, repeats=1)
+        print("tf32 3M stream, random operands", gauss)
+        assert 0.5 * stream < gauss < 2.0 * stream, (gauss, stream)
 
 
 def test_bf16x6_rand3reg_n104_matches_fp64_oracle():
