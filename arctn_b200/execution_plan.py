@@ -249,6 +249,7 @@ class ExecutionPlan:
         self.ssa_path, self.sliced_legs, self.target_size = path, sliced, exact
         self.leg_labels = labels
         self.metrics = full
+        self.name = artifact.get("net", "network")
         self.per_slice_metrics = per
         self._artifact = artifact
 

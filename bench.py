@@ -1015,7 +1015,8 @@ def main():
             roof = {"bound": "tensor", "kernel": KIND_NAMES.get(top, str(top)), "achieved": achieved,
                     "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                     "frac_of_sustained": achieved / pk["bf16_tflops_sustained"],
-                    "peak_source": f"{pk['source']} bf16 dense burst (MEASURED_PEAKS.json)",
+                    "peak_source": "measured bf16 dense burst (MEASURED_PEAKS.json)" if pk["source"] == "measured"
+                    else "fallback bf16 dense burst of an earlier measurement (MEASURED_PEAKS.json absent)",
                     "traffic": traffic, "traffic_source": "ncu capture of a slice group of 4, scaled by slices "
                     "(profiles/k_tc_cgemm_tf32x3_rand3reg_n172.md)" if traffic else None,
                     "launches": tn, "avg_launch_ms": tms / tn,

@@ -1,0 +1,134 @@
+"""The slice-sharded plan runner (arctn_b200.tnmpi) with the product's GPU executor.
+
+Each rank runs the product's slice-range program for its contiguous range of a saved version-2 plan and the
+FP64 partials are summed by one all-reduce, as the reference's MPI runner does (src/bin/tnmpi.rs:404-496).
+One GPU per call: ranks are spawned processes that share cuda:0 and sum over gloo (their kernels never wait on
+one another); the single-rank command line runs its all-reduce over NCCL.  Results are checked against the
+oracle: 1e-5 relative for complex64, 1e-12 for float64/complex128.
+"""
+
+import datetime
+import json
+import os
+import socket
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+import torch
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import arctn_b200 as A
+from arctn_b200 import networks as N
+from arctn_b200 import tnmpi as T
+from oracle import oracle as O
+from tests.helpers import random_arrays
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rand3reg_plan(tmp):
+    """rand3reg n = 64, bond 2, sliced to 2^8 elements per slice (256 slices), complex64 inputs."""
+    net, arrays = N.workload_rand3reg(64, 2, 1, np.complex64, seed=0)
+    path = A.greedy(*net.as_tuple())
+    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 8)
+    inputs, output, size_dict = net.as_tuple()
+    plan = A.ExecutionPlan.from_path(inputs, output, size_dict, path, sliced, target_size=2 ** 8, name="rand3reg64")
+    data = os.path.join(tmp, "rand3reg64.bin")
+    A.save_tensors_bin(data, arrays)
+    return plan.save(os.path.join(tmp, "rand3reg64.json")), data, plan, arrays
+
+
+def _blocks_plan(tmp):
+    """Output-leg and internal slices of a small network, float64 / complex128 inputs."""
+    inputs, output, size_dict = [[0, 1, 2], [1, 3, 2], [1, 4]], [4, 1, 0, 3], {0: 2, 1: 3, 2: 5, 3: 2, 4: 2}
+    path, sliced = [(0, 1), (3, 2)], [2, 0]
+    plan = A.ExecutionPlan.from_path(inputs, output, size_dict, path, sliced, name="blocks")
+    arrays = random_arrays(inputs, size_dict, np.complex128, 11)
+    data = os.path.join(tmp, "blocks.bin")
+    A.save_tensors_bin(data, arrays)
+    return plan.save(os.path.join(tmp, "blocks.json")), data, plan, arrays
+
+
+def _worker(rank, world, port, argv, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        stats, total = T.run(T.parse_args(argv), device=torch.device("cuda", 0))
+        q.put((rank, stats, total))
+    finally:
+        dist.destroy_process_group()
+
+
+def _run_ranks(world, argv):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    mp.start_processes(_worker, args=(world, _free_port(), argv, q), nprocs=world, join=True, start_method="spawn")
+    return sorted((q.get(timeout=120) for _ in range(world)), key=lambda r: r[0])
+
+
+@pytest.mark.parametrize("precision", ["fp32", "tf32x3"])
+def test_two_ranks_on_the_gpu_executor_match_the_oracle(tmp_path, precision):
+    plan_path, data, plan, arrays = _rand3reg_plan(str(tmp_path))
+    want = complex(O.contract_sliced(plan.inputs, plan.output, plan.size_dict, plan.ssa_path, plan.sliced_legs,
+                                     O.promote(arrays), threads=8))
+    results = _run_ranks(2, ["--load-path", plan_path, "--data", data, "--dtype", "complex64", "--precision",
+                             precision, "--backend", "gloo", "--check"])
+    for _, stats, total in results:
+        got = complex(total)
+        assert abs(got - want) <= 1e-5 * abs(want), (got, want)
+        assert stats["n_slices"] == 256 and stats["ranks"] == 2 and stats["check"].startswith("PASS(")
+        assert stats["execution_device_seconds_max"] > 0
+        assert stats["target_size"] == 256 and stats["target_log2_size"] == 8.0
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_output_blocks_across_ranks_on_the_gpu_executor(tmp_path, world):
+    plan_path, data, plan, arrays = _blocks_plan(str(tmp_path))
+    want = O.contract_sliced(plan.inputs, plan.output, plan.size_dict, plan.ssa_path, plan.sliced_legs, arrays)
+    results = _run_ranks(world, ["--load-path", plan_path, "--data", data, "--dtype", "complex128",
+                                 "--backend", "gloo", "--check"])
+    for _, stats, total in results:
+        assert total.shape == want.shape
+        assert np.max(np.abs(total - want)) <= 1e-12 * max(1.0, np.max(np.abs(want)))
+        assert stats["check"].startswith("PASS(")
+
+
+def test_command_line_single_rank_over_nccl(tmp_path):
+    plan_path, data, plan, arrays = _rand3reg_plan(str(tmp_path))
+    env = dict(os.environ, PYTHONPATH=ROOT + os.pathsep + os.environ.get("PYTHONPATH", ""))
+    for key in ("RANK", "WORLD_SIZE", "LOCAL_RANK", "MASTER_ADDR", "MASTER_PORT"):
+        env.pop(key, None)
+    proc = subprocess.run([sys.executable, "-m", "arctn_b200.tnmpi", "--load-path", plan_path, "--data", data,
+                           "--dtype", "complex64", "--precision", "tf32x3", "--check"],
+                          capture_output=True, text=True, timeout=300, env=env, cwd=ROOT)
+    assert proc.returncode == 0, proc.stderr[-2000:]
+    stats = json.loads(proc.stdout.strip().splitlines()[-1])
+    assert stats["ranks"] == 1 and stats["backend"] == "nccl" and stats["check"].startswith("PASS(")
+    assert stats["execution_device_seconds_max"] > 0
+
+
+def test_command_line_under_the_launcher_with_two_ranks(tmp_path):
+    plan_path, data, plan, arrays = _blocks_plan(str(tmp_path))
+    env = dict(os.environ, PYTHONPATH=ROOT + os.pathsep + os.environ.get("PYTHONPATH", ""))
+    proc = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node=2",
+                           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
+                           "-m", "arctn_b200.tnmpi", "--load-path", plan_path, "--data", data,
+                           "--dtype", "complex128", "--backend", "gloo", "--check"],
+                          capture_output=True, text=True, timeout=300, env=env, cwd=ROOT)
+    assert proc.returncode == 0, proc.stderr[-2000:]
+    stats = json.loads(proc.stdout.strip().splitlines()[-1])
+    assert stats["ranks"] == 2 and stats["check"].startswith("PASS(")
+    assert stats["output_shape"] == [2, 3, 2, 2]
+
