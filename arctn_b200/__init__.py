@@ -26,6 +26,7 @@ from .api import (
     ssa_to_linear,
     tensor_pipe_peak,
 )
+from .sharding import lpt_shard, run_sharded
 from .tuning import TuneTable, autotune
 
 __all__ = [
@@ -48,8 +49,10 @@ __all__ = [
     "save_tensors_bin",
     "greedy",
     "linear_to_ssa",
+    "lpt_shard",
     "simulate_path",
     "slice_parallel_chunks",
+    "run_sharded",
     "slice_range",
     "ssa_to_linear",
     "tensor_pipe_peak",

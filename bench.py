@@ -705,6 +705,23 @@ def run_batch(args, dev):
 
     nets = N.workload_batch(args.batch_size, seed=0)
     paths = [A.greedy(*net.as_tuple()) for net, _ in nets]
+    count = len(nets)
+    world, rank = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        # The networks are independent: each rank runs its LPT share of the batch (balanced by flops) and the
+        # only collective is the max over ranks of the device time.  Device-time line only.
+        import torch.distributed as dist
+
+        from arctn_b200.sharding import lpt_shard
+
+        if count < world:
+            raise SystemExit(f"--batch-size {count} is smaller than the {world} ranks")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+        costs = [10 ** A.simulate_path(*net.as_tuple(), p)["log10_flops"] for (net, _), p in zip(nets, paths)]
+        mine = lpt_shard(costs, world)[rank]
+        nets, paths = [nets[i] for i in mine], [paths[i] for i in mine]
+        args.no_extras = True
 
     def build(tuning):
         return [A.SlicedProgram(*net.as_tuple(), path, (), dtype=arrays[0].dtype, precision="tf32x3", gradient=True,
@@ -755,6 +772,11 @@ def run_batch(args, dev):
     sampler = ClockSampler(dev.index)
     ms, status = time_batch(batch, sampler)
     status = status or lanes_status
+    if dist is not None:
+        t = torch.tensor([ms, float(status)], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, status = float(t[0].item()), int(t[1].item())
+        dist.destroy_process_group()
     # Kernels per call: one interpreter launch per stage with tasks, the staged tensor-core steps and packs
     # (+1 for a split-K sum), every kernel of the lane programs, the status collection.
     desc = batch.describe(detail=True)
@@ -774,11 +796,13 @@ def run_batch(args, dev):
     # (one pinned copy per network), runs the batch and returns outputs and gradients as NumPy arrays.
     host = [arrays for _, arrays in nets]
     if args.no_extras:  # device time only (profiling runs)
-        return _line(args, "many-network forward+adjoint throughput", len(progs) / (ms * 1e-3),
-                     "networks/s", True, ms, {"workload": f"{len(progs)} random 3-regular networks, n in "
-                                              "[20,50], bond in {2,3,4}, f32/c64 alternating"}, "f32+c64",
+        return _line(args, "many-network forward+adjoint throughput", count / (ms * 1e-3),
+                     "networks/s", True, ms, {"workload": f"{count} random 3-regular networks, n in "
+                                              "[20,50], bond in {2,3,4}, f32/c64 alternating",
+                                              "parallelism": f"LPT network shards x{world}"}, "f32+c64",
                      gpu_launches=launches_per_call * args.steps, e2e=None, roofline=None,
-                     cpu_baseline=None, clocks=sampler.summary(), device_status=status)
+                     cpu_baseline=None, clocks=sampler.summary(), device_status=status, n_gpus=world,
+                     scaling="strong" if world > 1 else "none")
     h2d = sum(a.nbytes for arrays in host for a in arrays)
     d2h = sum(int(np.prod(p.output_shape)) * a[0].itemsize for p, a in zip(progs, host)) + h2d
     ws_e2e = torch.empty(max(batch.workspace_bytes, 1), dtype=torch.uint8, device=dev)
@@ -825,7 +849,7 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload != "rand3reg":
-        if rank != 0:
+        if rank != 0 and not (args.workload == "batch" and world > 1):
             return
         import torch
 
@@ -839,7 +863,8 @@ def main():
             line = run_rand3reg_n64(args, dev)
         else:
             line = run_batch(args, dev)
-        print(json.dumps(line), flush=True)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
         return
     if args.impl == "reference":
         run_reference(args, rank)
