@@ -84,3 +84,29 @@ SMALL_NETWORKS = {
     "mixed": mixed_network(),
     "tiny6": ([[0, 1], [1, 2], [2, 3], [3, 4], [4, 5], [5, 0, 6]], [6], {0: 4, 1: 5, 2: 4, 3: 6, 4: 4, 5: 5, 6: 3}),
 }
+
+
+def spawn_ranks(fn, args, world, timeout=300):
+    """Run fn(rank, *args, q) in ``world`` spawned processes and return the ``world`` items they put on q,
+    sorted by their first field (the rank).  The queue is drained while the processes run: a child that has
+    put more than a pipe buffer holds cannot exit until its data is read, so joining first would wait forever.
+    A child that raises fails the call at once; a missing item fails it after ``timeout`` seconds."""
+    import queue
+    import time
+
+    import torch.multiprocessing as mp
+
+    q = mp.get_context("spawn").Queue()
+    pc = mp.start_processes(fn, args=tuple(args) + (q,), nprocs=world, join=False, start_method="spawn")
+    got, deadline = [], time.monotonic() + timeout
+    while len(got) < world:
+        try:
+            got.append(q.get(timeout=1.0))
+        except queue.Empty:
+            pc.join(timeout=0)  # raises if a child failed
+            if time.monotonic() > deadline:
+                raise TimeoutError(f"{len(got)} of {world} ranks reported within {timeout} s")
+    while not pc.join(timeout=1.0):
+        if time.monotonic() > deadline:
+            raise TimeoutError(f"ranks did not exit within {timeout} s")
+    return sorted(got, key=lambda item: item[0])

@@ -18,13 +18,12 @@ import numpy as np
 import pytest
 import torch
 import torch.distributed as dist
-import torch.multiprocessing as mp
 
 import arctn_b200 as A
 from arctn_b200 import networks as N
 from arctn_b200 import tnmpi as T
 from oracle import oracle as O
-from tests.helpers import random_arrays
+from tests.helpers import random_arrays, spawn_ranks
 
 pytestmark = pytest.mark.gpu
 
@@ -77,10 +76,7 @@ def _worker(rank, world, port, argv, q):
 
 
 def _run_ranks(world, argv):
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    mp.start_processes(_worker, args=(world, _free_port(), argv, q), nprocs=world, join=True, start_method="spawn")
-    return sorted((q.get(timeout=120) for _ in range(world)), key=lambda r: r[0])
+    return spawn_ranks(_worker, (world, _free_port(), argv), world)
 
 
 @pytest.mark.parametrize("precision", ["fp32", "tf32x3"])

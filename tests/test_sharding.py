@@ -3,7 +3,7 @@
 The assignment is checked for being a partition, deterministic and within the LPT bound of the best split
 (brute-forced on small cases).  The rank protocol runs on gloo ranks on CPU (world size 2 and 3), each rank
 contracting its share with the oracle: every rank ends with every network's result, in network order, equal to
-contracting each network alone.  tests/test_gpu_sharding.py runs the same protocol with ProgramBatch shares.
+contracting each network alone.  tests/test_gpu_sharding.py runs the shares as ProgramBatches on the GPU.
 """
 
 import datetime
@@ -14,12 +14,12 @@ import socket
 import numpy as np
 import pytest
 import torch.distributed as dist
-import torch.multiprocessing as mp
 
 import arctn_b200 as A
 from arctn_b200 import networks as N
 from arctn_b200.sharding import lpt_shard, run_sharded
 from oracle import oracle as O
+from tests.helpers import spawn_ranks
 
 
 def _free_port():
@@ -97,7 +97,8 @@ def _worker(rank, world, port, q):
 
         def execute_share(indices):
             ran.extend(indices)
-            return [_oracle_one(batch[i]) for i in indices]
+            # each result also carries 64 KB, so every rank's report exceeds a pipe buffer
+            return [(_oracle_one(batch[i]), np.full(8192, i, dtype=np.float64)) for i in indices]
 
         results = run_sharded([b[-1] for b in batch], execute_share, rank, world)
         q.put((rank, ran, results))
@@ -109,13 +110,11 @@ def _worker(rank, world, port, q):
 def test_ranks_run_their_shares_and_gather_every_result(world):
     batch = _batch()
     want = [_oracle_one(b) for b in batch]
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    mp.start_processes(_worker, args=(world, _free_port(), q), nprocs=world, join=True, start_method="spawn")
-    got = sorted((q.get(timeout=60) for _ in range(world)), key=lambda r: r[0])
+    got = spawn_ranks(_worker, (world, _free_port()), world)
     shares = lpt_shard([b[-1] for b in batch], world)
     for rank, ran, results in got:
         assert ran == shares[rank]  # each rank contracted exactly its LPT share
         assert len(results) == len(batch)
-        for r, w in zip(results, want):
+        for i, ((r, pad), w) in enumerate(zip(results, want)):
             assert np.array_equal(r, w)
+            assert np.array_equal(pad, np.full(8192, i, dtype=np.float64))

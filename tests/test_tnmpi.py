@@ -16,12 +16,11 @@ import numpy as np
 import pytest
 import torch
 import torch.distributed as dist
-import torch.multiprocessing as mp
 
 import arctn_b200 as A
 from arctn_b200 import tnmpi as T
 from oracle import oracle as O
-from tests.helpers import random_arrays
+from tests.helpers import random_arrays, spawn_ranks
 
 # Dense networks (legs numbered in first-occurrence order), with their SSA paths and sliced legs.
 CASES = {
@@ -82,11 +81,7 @@ def _worker(rank, world, port, argv, executor_name, q):
 
 
 def _run_ranks(world, argv, executor="oracle"):
-    ctx = mp.get_context("spawn")
-    q = ctx.Queue()
-    mp.start_processes(_worker, args=(world, _free_port(), argv, executor, q), nprocs=world, join=True,
-                       start_method="spawn")
-    return sorted((q.get(timeout=30) for _ in range(world)), key=lambda r: r[0])
+    return spawn_ranks(_worker, (world, _free_port(), argv, executor), world)
 
 
 @pytest.mark.parametrize("world", [2, 3])
