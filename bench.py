@@ -258,6 +258,15 @@ def oracle_workload(n_nodes, target_log2):
     return net, arrays, path, sliced, name, flops
 
 
+def product_library_loaded():
+    """Whether this process has mapped the product library (read from /proc/self/maps)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return any("libarctn_b200" in line for line in f)
+    except OSError:
+        return None
+
+
 def host_threads():
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
 
@@ -380,7 +389,8 @@ def run_reference(args, rank):
                              "sample": cb["sample"]},
             "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference Rust executor cannot be built in this image (no cargo/rustc, crates not "
-                    "vendored); its CPU restatement (oracle/) is timed instead, on a sample of slices"}
+                    "vendored); its CPU restatement (oracle/) is timed instead, on a sample of slices",
+            "product_library_loaded": product_library_loaded()}
     print(json.dumps(line), flush=True)
 
 
