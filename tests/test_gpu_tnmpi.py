@@ -134,3 +134,48 @@ def test_command_line_under_the_launcher_with_two_ranks(tmp_path):
     assert stats["ranks"] == 2 and stats["check"].startswith("PASS(")
     assert stats["output_shape"] == [2, 3, 2, 2]
 
+
+
+def _ranks_sum(inputs, output, size_dict, path, sliced, arrays, ranks, dtype):
+    """The product's slice-range programs of ``ranks`` ranks, run in turn and summed in FP64, as the reference's
+    in-process rank tests do (src/bin/tnmpi.rs:540-583); ranks whose range is empty contribute nothing."""
+    n = int(np.prod([size_dict[l] for l in sliced])) if sliced else 1
+    total = None
+    for rank in range(ranks):
+        b, e = A.slice_range(n, ranks, rank)
+        if b == e:
+            continue
+        prog = A.SlicedProgram(inputs, output, size_dict, path, sliced, dtype=dtype, slice_begin=b, slice_end=e)
+        part = np.asarray(prog.execute(arrays, f64_out=True))
+        total = part if total is None else total + part
+    return total
+
+
+def test_output_blocks_land_in_place_for_every_axis_position():
+    # src/bin/tnmpi.rs:539-583: sliced output legs at the front, middle and back of a three-axis output,
+    # alone and with the internal legs 3 and 4, over four ranks.
+    inputs, output, size_dict = [[0, 3], [3, 1, 4], [4, 2]], [0, 1, 2], {0: 2, 1: 3, 2: 2, 3: 2, 4: 3}
+    path = [(0, 1), (3, 2)]
+    arrays = random_arrays(inputs, size_dict, np.float64, 7)
+    want = O.execute(inputs, output, size_dict, path, arrays)
+    for sliced in ([1], [2, 0], [1, 3], [4, 1, 0, 3], [0, 1, 2]):
+        got = _ranks_sum(inputs, output, size_dict, path, sliced, arrays, 4, np.float64)
+        assert got.shape == want.shape
+        assert np.max(np.abs(got - want)) < 1e-12, sliced
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64, np.complex64, np.complex128])
+def test_matrix_slice_products_over_three_ranks_are_exact(dtype):
+    # src/bin/tnmpi.rs:607-680: a 2x2 . 2x2 product with internal, output and mixed slices over three ranks
+    # (some ranges empty); small integer parts keep every product and sum exact.
+    real = np.array([1.0, 2.0, 3.0, 4.0, 5.0, 6.0, 7.0, 8.0])
+    imag = np.array([1.0, -1.0, 2.0, 0.0, 0.0, 1.0, -1.0, 2.0])
+    vals = real + 1j * imag if np.dtype(dtype).kind == "c" else real
+    a, b = (np.asarray(v, dtype=dtype).reshape(2, 2) for v in (vals[:4], vals[4:]))
+    want = a.astype(np.complex128) @ b.astype(np.complex128)
+    if np.dtype(dtype).kind == "f":
+        assert np.array_equal(want.real, [[19.0, 22.0], [43.0, 50.0]])
+    inputs, output, size_dict = [[0, 1], [1, 2]], [0, 2], {0: 2, 1: 2, 2: 2}
+    for sliced in ([], [1], [0], [2, 0], [1, 2, 0]):
+        got = _ranks_sum(inputs, output, size_dict, [(0, 1)], sliced, [a, b], 3, dtype)
+        assert np.array_equal(got, want if np.dtype(dtype).kind == "c" else want.real), (sliced, got)
