@@ -186,3 +186,27 @@ def test_command_line_failure_exits_3_on_every_rank(tmp_path):
     assert proc.returncode != 0
     assert "tnmpi rank 0" in proc.stderr and "tnmpi rank 1" in proc.stderr
     assert proc.stderr.count("exitcode  : 3") == 2
+
+
+@pytest.mark.parametrize("dtype", ["f32", "f64", "complex64", "complex128"])
+def test_check_passes_and_catches_a_wrong_total(tmp_path, dtype):
+    # src/bin/tnmpi.rs:645-671: the single-process comparison passes on the right total and fails once one
+    # element moves by one unit (the imaginary unit for complex dtypes).
+    plan_path, data_path, _ = _save_case(str(tmp_path), "output_and_internal", T.DTYPES[dtype])
+    plan = A.ExecutionPlan.load(plan_path)
+    arrays = A.load_tensors_bin(data_path, plan.inputs, plan.size_dict, T.DTYPES[dtype])
+    args = T.parse_args(["--load-path", plan_path, "--dtype", dtype, "--check"])
+    n = int(np.prod([plan.size_dict[l] for l in plan.sliced_legs]))
+    total = oracle_executor(plan, arrays, args, 0, n, None)().numpy()
+    assert T._check_result(plan, arrays, args, total, n, oracle_executor, None).startswith("PASS(")
+    bad = total.copy()
+    bad.reshape(-1)[0] += 1j if np.iscomplexobj(bad) else 1.0
+    with pytest.raises(RuntimeError, match="single-process comparison failed"):
+        T._check_result(plan, arrays, args, bad, n, oracle_executor, None)
+
+
+def test_check_is_skipped_above_the_size_limits():
+    # src/bin/tnmpi.rs:386-388
+    big = np.zeros(T.CHECK_MAX_NUMEL + 1)
+    assert T._check_result(None, None, None, big, 1, None, None).startswith("skipped")
+    assert T._check_result(None, None, None, np.zeros(1), T.CHECK_MAX_SLICES + 1, None, None).startswith("skipped")
