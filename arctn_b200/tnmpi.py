@@ -20,7 +20,9 @@ Differences from the reference, each deliberate:
 - ``--check`` compares with a single-process execution of all slices on rank 0's GPU;
 - besides the wall clock, each rank times its execute and the all-reduce with CUDA events, and the line
   reports the maximum over ranks (``execution_device_seconds_max``);
-- version-1 plans with ``--net`` are not read (only self-contained version-2 plans).
+- version-1 plans with ``--net`` are not read (only self-contained version-2 plans);
+- ``--broadcast-inputs``: rank 0 alone reads (or generates) the inputs and one broadcast of all their bytes
+  replicates them, over NVLink with NCCL, so the other ranks need no access to the data file.
 
 Failures follow the reference's ``require_all`` (src/bin/tnmpi.rs:165-177): a rank that fails reports its
 error, every rank learns of it through an all-reduce(MAX) of a failure flag before the next collective, and
@@ -47,6 +49,7 @@ Execute the saved SSA path and sliced indices; no path search is performed.
   --seed <N>           Seed for example inputs when --data is omitted (default 1)
   --backend <NAME>     nccl (default) or gloo for the all-reduce
   --check              Compare a small result with single-process execution
+  --broadcast-inputs   Rank 0 alone reads (or generates) the inputs; one broadcast replicates them
   --help               Show this help
 
 Version 2 plans contain the network; every rank must read identical input data.
@@ -77,6 +80,7 @@ class Args:
         self.seed = 1
         self.backend = "nccl"
         self.check = False
+        self.broadcast_inputs = False
 
 
 def parse_args(argv):
@@ -88,6 +92,9 @@ def parse_args(argv):
             return None
         if flag == "--check":
             args.check = True
+            continue
+        if flag == "--broadcast-inputs":
+            args.broadcast_inputs = True
             continue
         if flag == "--net":
             raise UsageError("--net (version 1 plans) is not supported; save a version 2 plan")
@@ -172,6 +179,31 @@ class _Group:
         self.dist.broadcast_object_list(box, src=0, device=self.cdev if self.backend == "nccl" else None)
         return box[0]
 
+    def replicate_inputs(self, plan, dtype, load):
+        """Every rank's copy of the inputs from one broadcast of rank 0's bytes.  Only rank 0 calls ``load``;
+        a failure there stops every rank before the broadcast.  With NCCL the copies are device tensors."""
+        torch = self.torch
+        dt = np.dtype(DTYPES[dtype])
+        shapes = [tuple(plan.size_dict[l] for l in legs) for legs in plan.inputs]
+        counts = [int(np.prod(sh, dtype=np.int64)) for sh in shapes]
+        arrays = self.require_all(lambda: load() if self.rank == 0 else None)
+        buf = torch.empty(sum(counts) * dt.itemsize, dtype=torch.uint8, device=self.cdev)
+        if self.rank == 0 and buf.numel():
+            host = np.concatenate([np.ascontiguousarray(a, dtype=dt).reshape(-1) for a in arrays]).view(np.uint8)
+            buf.copy_(torch.from_numpy(host))
+        if buf.numel():
+            self.dist.broadcast(buf, src=0)
+        tdt = {"f": {4: torch.float32, 8: torch.float64}, "c": {8: torch.complex64, 16: torch.complex128}}
+        out, off = [], 0
+        for sh, n in zip(shapes, counts):
+            piece = buf[off:off + n * dt.itemsize]
+            off += n * dt.itemsize
+            if self.backend == "nccl":
+                out.append(piece.view(tdt[dt.kind][dt.itemsize]).reshape(sh))
+            else:
+                out.append(piece.numpy().view(dt).reshape(sh).copy())
+        return out
+
     def sum_(self, t):
         """In-place all-reduce(SUM) of an FP64 (real or complex) tensor."""
         flat = self.torch.view_as_real(t) if t.is_complex() else t
@@ -202,7 +234,8 @@ def gpu_range_executor(plan, arrays, args, begin, end, device):
     prog = SlicedProgram(plan.inputs, plan.output, plan.size_dict, plan.ssa_path, plan.sliced_legs,
                          dtype=DTYPES[args.dtype], precision=args.precision, device=device.index,
                          slice_begin=0 if whole else begin, slice_end=0 if whole else end)
-    x = [torch.from_numpy(np.ascontiguousarray(a)).to(device) for a in arrays]
+    x = [a.to(device) if torch.is_tensor(a) else torch.from_numpy(np.ascontiguousarray(a)).to(device)
+         for a in arrays]
     ws = torch.empty(max(prog.workspace_bytes, 1), dtype=torch.uint8, device=device)
 
     def call():
@@ -268,9 +301,12 @@ def run(args, *, device=None, executor=gpu_range_executor):
     plan = g.require_all(decode)
     n_slices = int(math.prod(plan.size_dict[l] for l in plan.sliced_legs))
     out_shape = tuple(plan.size_dict[l] for l in plan.output)
-    arrays = g.require_all(lambda: load_tensors_bin(args.data_file, plan.inputs, plan.size_dict,
-                                                    DTYPES[args.dtype]) if args.data_file
-                           else example_inputs(plan, args.dtype, args.seed))
+    def load():
+        if args.data_file:
+            return load_tensors_bin(args.data_file, plan.inputs, plan.size_dict, DTYPES[args.dtype])
+        return example_inputs(plan, args.dtype, args.seed)
+
+    arrays = g.replicate_inputs(plan, args.dtype, load) if args.broadcast_inputs else g.require_all(load)
     begin, end = slice_range(n_slices, g.size, g.rank)
     call = g.require_all(lambda: executor(plan, arrays, args, begin, end, device) if begin < end else None)
     wide = _wide_dtype(args.dtype)

@@ -145,12 +145,12 @@ def test_example_inputs_are_seeded_and_uniform(tmp_path):
 def test_options():
     assert T.parse_args(["--help"]) is None
     args = T.parse_args(["--load-path", "p.json", "--dtype", "complex64", "--precision", "tf32x3", "--seed", "9",
-                         "--check", "--backend", "gloo", "--data", "t.bin"])
-    assert (args.load_path, args.dtype, args.precision, args.seed, args.check, args.backend, args.data_file) == \
-        ("p.json", "complex64", "tf32x3", 9, True, "gloo", "t.bin")
+                         "--check", "--backend", "gloo", "--data", "t.bin", "--broadcast-inputs"])
+    assert (args.load_path, args.dtype, args.precision, args.seed, args.check, args.backend, args.data_file,
+            args.broadcast_inputs) == ("p.json", "complex64", "tf32x3", 9, True, "gloo", "t.bin", True)
     defaults = T.parse_args(["--load-path", "p.json"])
-    assert (defaults.dtype, defaults.precision, defaults.seed, defaults.check, defaults.backend) == \
-        ("f64", "fp32", 1, False, "nccl")
+    assert (defaults.dtype, defaults.precision, defaults.seed, defaults.check, defaults.backend,
+            defaults.broadcast_inputs) == ("f64", "fp32", 1, False, "nccl", False)
     for argv, msg in [([], "--load-path"), (["--load-path"], "requires a value"),
                       (["--load-path", "--check"], "requires a value"),
                       (["--load-path", "p", "--dtype", "c64"], "--dtype must be"),
@@ -210,3 +210,41 @@ def test_check_is_skipped_above_the_size_limits():
     big = np.zeros(T.CHECK_MAX_NUMEL + 1)
     assert T._check_result(None, None, None, big, 1, None, None).startswith("skipped")
     assert T._check_result(None, None, None, np.zeros(1), T.CHECK_MAX_SLICES + 1, None, None).startswith("skipped")
+
+
+def _worker_per_rank(rank, world, port, argvs, q):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        try:
+            stats, total = T.run(T.parse_args(argvs[rank]), device=torch.device("cpu"), executor=oracle_executor)
+            q.put((rank, "ok", stats, total))
+        except T.RankFailure as exc:
+            q.put((rank, "failed", str(exc), None))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("dtype", ["f32", "complex128"])
+def test_broadcast_inputs_need_the_data_file_on_rank0_only(tmp_path, world, dtype):
+    plan_path, data_path, arrays = _save_case(str(tmp_path), "output_and_internal", T.DTYPES[dtype])
+    inputs, output, size_dict, path, sliced = CASES["output_and_internal"]
+    want = O.contract_sliced(inputs, output, size_dict, path, sliced, O.promote(arrays))
+    common = ["--load-path", plan_path, "--dtype", dtype, "--backend", "gloo", "--broadcast-inputs", "--check"]
+    argvs = [common + ["--data", data_path if r == 0 else str(tmp_path / "absent.bin")] for r in range(world)]
+    results = spawn_ranks(_worker_per_rank, (world, _free_port(), argvs), world)
+    for rank, status, stats, total in results:
+        assert status == "ok", stats
+        assert np.max(np.abs(total - want)) < 1e-12
+        assert stats["check"].startswith("PASS(")
+
+
+def test_broadcast_inputs_stop_every_rank_when_rank0_cannot_read(tmp_path):
+    plan_path, data_path, _ = _save_case(str(tmp_path), "internal")
+    argv = ["--load-path", plan_path, "--data", str(tmp_path / "absent.bin"), "--backend", "gloo",
+            "--broadcast-inputs"]
+    results = spawn_ranks(_worker_per_rank, (2, _free_port(), [argv, argv]), 2)
+    assert [r[1] for r in results] == ["failed", "failed"]
+    assert "absent.bin" in results[0][2] and results[1][2] == "another rank failed"
