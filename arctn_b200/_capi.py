@@ -68,6 +68,8 @@ SIGNATURES = [
     ("arctn_b200_simulate_path", c_int, [NETP, u64, u64p, ctypes.POINTER(c_double)]),
     ("arctn_b200_greedy", c_int, [NETP, u64p, u64p]),
     ("arctn_b200_find_slices_to_size", c_int, [NETP, u64, u64p, u64, u32p, u64p, ctypes.POINTER(c_int)]),
+    ("arctn_b200_find_slices_with_output", c_int,
+     [NETP, u64, u64p, u64, c_int, u32p, u64p, ctypes.POINTER(c_int)]),
     ("arctn_b200_slice_parallel_chunks", u64, [u64, u64]),
     ("arctn_b200_slice_plan_check", c_int, [NETP, u64, u64p, u64, u32p, u64, ctypes.POINTER(c_double),
                                             ctypes.POINTER(c_int)]),

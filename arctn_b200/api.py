@@ -23,6 +23,7 @@ from __future__ import annotations
 import ctypes
 import math
 import operator
+import sys
 import threading
 import time
 
@@ -215,16 +216,24 @@ def greedy(inputs, output, size_dict):
     return [(int(buf[2 * s]), int(buf[2 * s + 1])) for s in range(ns.value)]
 
 
-def find_slices_to_size(inputs, output, size_dict, ssa_path, target_size):
-    """Sliced legs meeting ``target_size`` elements per intermediate, or None (src/slice.rs:209-215)."""
+def find_slices_to_size(inputs, output, size_dict, ssa_path, target_size, allow_output_slicing=False):
+    """Sliced legs meeting ``target_size`` elements per intermediate, or None (src/slice.rs:209-215).  With
+    ``allow_output_slicing`` output legs may be chosen too, the reference's opt-in output-index slicing
+    (src/slice.rs:254-289)."""
     net = C.NetworkArgs(inputs, output, size_dict)
     n, p = C.path_array(ssa_path)
     buf = np.zeros(max(1, len(net.size_dict)), dtype=np.uint32)
     nl = C.u64(0)
     found = ctypes.c_int(0)
-    C.check(C.lib().arctn_b200_find_slices_to_size(net.ptr, n, p.ctypes.data_as(C.u64p), int(target_size),
-                                                   buf.ctypes.data_as(C.u32p), ctypes.byref(nl),
-                                                   ctypes.byref(found)), "slice search")
+    if allow_output_slicing:
+        rc = C.lib().arctn_b200_find_slices_with_output(net.ptr, n, p.ctypes.data_as(C.u64p), int(target_size), 1,
+                                                        buf.ctypes.data_as(C.u32p), ctypes.byref(nl),
+                                                        ctypes.byref(found))
+    else:
+        rc = C.lib().arctn_b200_find_slices_to_size(net.ptr, n, p.ctypes.data_as(C.u64p), int(target_size),
+                                                    buf.ctypes.data_as(C.u32p), ctypes.byref(nl),
+                                                    ctypes.byref(found))
+    C.check(rc, "slice search")
     return [int(x) for x in buf[: nl.value]] if found.value else None
 
 
@@ -1269,27 +1278,84 @@ class ArcTNCompiledContraction:
                 f"n_steps={len(self.ssa_path)})")
 
 
-def arctn_contract(inputs, output, size_dict, arrays, *, target_size=None, backend="b200", ssa_path=None,
-                   sliced_legs=None, precision="fp32", return_info=False):
-    """Plan (when no path is given), optionally slice, and execute on the B200 executor.
+_AUTO_PRESETS = ("light", "heavy")
+_SLICING_MODES = ("fixed", "dynamic")
 
-    Mirrors ``arctn_contract`` (pybind/python/arctn/__init__.py:903-1072).  The
-    reference plans with its closed-source engine; here the public greedy
-    planner (src/paths/greedy.rs:317-320) and ``find_slices_to_size``
-    (src/slice.rs:209-215) produce the path and slices unless they are given.
-    """
-    backend = _validate_backend(backend)
-    inputs_i, output_i, size_i, _ = _to_int_labels(inputs, output, size_dict)
+
+def _validate_planning_options(preset, seed, target_size, slicing_mode, max_time, flops_weight, read_write_weight,
+                               allow_output_slicing):
+    """The reference's argument checks for ``arctn_contract`` (pybind/python/arctn/__init__.py:70-150), with the
+    same exception types; returns the normalised (target_size, max_time, weights)."""
+    if not isinstance(preset, str) or preset not in _AUTO_PRESETS:
+        raise ValueError(f"preset must be 'light' or 'heavy', got {preset!r}")
+    if isinstance(seed, bool):
+        raise TypeError("seed must be an integer, not bool")
+    operator.index(seed)
     if target_size is not None:
-        target_size = operator.index(target_size)
+        if isinstance(target_size, bool):
+            raise TypeError("target_size must be an integer, not bool")
+        try:
+            target_size = operator.index(target_size)
+        except TypeError as exc:
+            raise TypeError(f"target_size must be an integer, got {target_size!r}") from exc
         if target_size < 1:
             raise ValueError(f"target_size must be >= 1, got {target_size}")
+        if target_size > sys.maxsize:
+            raise OverflowError(f"target_size={target_size} exceeds this platform's usize range {sys.maxsize}")
+    if not isinstance(slicing_mode, str) or slicing_mode not in _SLICING_MODES:
+        raise ValueError(f"slicing_mode must be 'fixed' or 'dynamic', got {slicing_mode!r}")
+    if slicing_mode == "dynamic" and target_size is None:
+        raise ValueError("slicing_mode='dynamic' requires target_size")
+    if max_time is not None:
+        try:
+            max_time = float(max_time)
+        except (TypeError, ValueError) as exc:
+            raise TypeError("max_time must be a finite number of seconds greater than 0") from exc
+        if not math.isfinite(max_time) or max_time <= 0.0:
+            raise ValueError("max_time must be a finite number of seconds greater than 0")
+    weights = []
+    for name, value in (("flops_weight", flops_weight), ("read_write_weight", read_write_weight)):
+        if isinstance(value, bool):
+            raise TypeError(f"{name} must be a finite non-negative number, not bool")
+        try:
+            value = float(value)
+        except (TypeError, ValueError) as exc:
+            raise TypeError(f"{name} must be a finite non-negative number") from exc
+        if not math.isfinite(value) or value < 0.0:
+            raise ValueError(f"{name} must be a finite non-negative number")
+        weights.append(value)
+    if weights == [0.0, 0.0]:
+        raise ValueError("flops_weight and read_write_weight cannot both be 0")
+    if not isinstance(allow_output_slicing, bool):
+        raise TypeError("allow_output_slicing must be a bool")
+    return target_size, max_time, tuple(weights)
+
+
+def arctn_contract(inputs, output, size_dict, arrays, *, preset="heavy", seed=0, target_size=None,
+                   slicing_mode="fixed", max_time=None, backend="b200", flops_weight=1.0, read_write_weight=64.0,
+                   return_info=False, allow_output_slicing=False, ssa_path=None, sliced_legs=None,
+                   precision="fp32"):
+    """Plan (when no path is given), optionally slice, and execute on the B200 executor.
+
+    Mirrors ``arctn_contract`` (pybind/python/arctn/__init__.py:903-1072): the same keywords, checked the same
+    way.  The reference plans with its closed-source engine, which ``preset``, ``seed``, ``max_time`` and the
+    weights steer; here the public greedy planner (src/paths/greedy.rs:317-320) and the slice search
+    (src/slice.rs:209-289) produce the path and slices unless ``ssa_path`` / ``sliced_legs`` are given, so
+    those planner options are validated and reported but do not change the plan.  ``slicing_mode="dynamic"``
+    lets the reference change the path while slicing; this planner keeps it, which that mode allows.
+    ``allow_output_slicing`` lets the slice search pick output legs; the output is then assembled from blocks.
+    """
+    target_size, max_time, (flops_weight, read_write_weight) = _validate_planning_options(
+        preset, seed, target_size, slicing_mode, max_time, flops_weight, read_write_weight, allow_output_slicing)
+    backend = _validate_backend(backend)
+    inputs_i, output_i, size_i, _ = _to_int_labels(inputs, output, size_dict)
     t0 = time.perf_counter()
     ssa = [tuple(p) for p in ssa_path] if ssa_path is not None else greedy(inputs_i, output_i, size_i)
     if sliced_legs is None:
         sliced_legs = []
         if target_size is not None:
-            found = find_slices_to_size(inputs_i, output_i, size_i, ssa, target_size)
+            found = find_slices_to_size(inputs_i, output_i, size_i, ssa, target_size,
+                                        allow_output_slicing=allow_output_slicing)
             if found is None:
                 raise ValueError(f"target_size (log2={math.log2(target_size):.6g}) is unreachable: no slicing "
                                  "meets it")
@@ -1299,9 +1365,13 @@ def arctn_contract(inputs, output, size_dict, arrays, *, target_size=None, backe
     result = contract_sliced(inputs_i, output_i, size_i, arrays, sliced_legs, ssa_path=ssa, precision=precision)
     exec_wall = time.perf_counter() - t1
     if return_info:
-        info = {"path": ssa, "sliced_legs": list(sliced_legs), "execution_backend": backend,
-                "execution_implementation": "arctn_b200.contract_sliced", "planning_wall_s": plan_wall,
-                "execution_wall_s": exec_wall, "target_size": target_size}
+        info = {"path": ssa, "sliced_legs": list(sliced_legs), "sliced": bool(sliced_legs),
+                "execution_backend": backend, "execution_implementation": "arctn_b200.contract_sliced",
+                "planning_wall_s": plan_wall, "execution_wall_s": exec_wall, "target_size": target_size,
+                "target_log2_size": math.log2(target_size) if target_size is not None else None,
+                "allow_output_slicing": allow_output_slicing, "preset": preset, "seed": seed,
+                "slicing_mode": slicing_mode, "max_time": max_time, "flops_weight": flops_weight,
+                "read_write_weight": read_write_weight, "planner": "greedy + find_slices_to_size"}
         info.update(simulate_path(inputs_i, output_i, size_i, ssa))
         return result, info
     return result

@@ -178,6 +178,19 @@ int arctn_b200_find_slices_to_size(const arctn_b200_network* net, uint64_t n_ste
   });
 }
 
+int arctn_b200_find_slices_with_output(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
+                                       uint64_t target_size, int allow_output_slicing, uint32_t* legs_out,
+                                       uint64_t* n_legs_out, int* found) {
+  return guarded([&] {
+    std::vector<Leg> legs;
+    bool ok = find_slices_to_size(to_network(net), to_path(n_steps, ssa_path), target_size, legs,
+                                  allow_output_slicing != 0);
+    *found = ok ? 1 : 0;
+    *n_legs_out = legs.size();
+    for (size_t i = 0; i < legs.size(); ++i) legs_out[i] = legs[i];
+  });
+}
+
 int arctn_b200_slice_plan_check(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
                                 uint64_t n_sliced, const uint32_t* sliced_legs, uint64_t target_size,
                                 double per_slice_stats_out[6], int* fits_out) {

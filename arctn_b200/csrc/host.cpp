@@ -402,10 +402,10 @@ u64 slice_parallel_chunks(u64 n_slices, u64 out_numel) {
   return (n_slices + chunk - 1) / chunk;
 }
 
-static bool sliceable(const Network& net, Leg leg) {  // src/slice.rs:139-150
+static bool sliceable(const Network& net, Leg leg, bool allow_output) {  // src/slice.rs:136-150
   auto it = net.size.find(leg);
   if (it == net.size.end() || it->second == 0) return false;
-  if (std::find(net.output.begin(), net.output.end(), leg) != net.output.end()) return false;
+  if (!allow_output && std::find(net.output.begin(), net.output.end(), leg) != net.output.end()) return false;
   bool held = false;
   for (auto& t : net.inputs) {
     auto c = std::count(t.begin(), t.end(), leg);
@@ -470,7 +470,8 @@ bool slice_result_fits_target_size(const Network& net, const SsaPath& path, cons
   return path_fits_target_size(cur, path, target);
 }
 
-bool find_slices_to_size(const Network& net, const SsaPath& path, u64 target, std::vector<Leg>& out) {
+bool find_slices_to_size(const Network& net, const SsaPath& path, u64 target, std::vector<Leg>& out,
+                         bool allow_output) {
   if (target == 0) return false;
   auto fits = [&](const Network& cur, const std::vector<Leg>& legs) { return legs_fit(cur, legs, target); };
   std::vector<Leg> sliced;
@@ -491,11 +492,13 @@ bool find_slices_to_size(const Network& net, const SsaPath& path, u64 target, st
     if (ok) { out = sliced; return true; }
     // src/slice.rs:557-589: most over-target intermediates, then larger leg, then smaller id.
     std::map<Leg, std::pair<u64, double>> score;
+    // With output slicing, a unary contraction (no steps) still has its output to fit (src/slice.rs:565-566).
+    if (allow_output && net.n_tensors() == 1) sl.push_back(cur.output);
     for (auto& legs : sl) {
       if (fits(cur, legs)) continue;
       for (Leg l : legs) {
         double d = cur.log2_dim(l);
-        if (d <= 0.0 || !sliceable(net, l)) continue;
+        if (d <= 0.0 || !sliceable(net, l, allow_output)) continue;
         auto ins = score.emplace(l, std::make_pair(u64(0), d));
         ins.first->second.first += 1;
       }

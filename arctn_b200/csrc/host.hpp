@@ -58,8 +58,10 @@ PathStats simulate_path(const Network& net, const SsaPath& path, std::vector<std
 
 // greedy (src/paths/greedy.rs:307-320): costmod 1, zero temperature, one branch.
 SsaPath greedy_path(const Network& net);
-// find_slices_to_size (src/slice.rs:209-215); false where the reference returns None.
-bool find_slices_to_size(const Network& net, const SsaPath& path, u64 target, std::vector<Leg>& legs_out);
+// find_slices_to_size (src/slice.rs:209-215); false where the reference returns None.  allow_output: output
+// legs may be chosen too (find_slices_until_for_target_with_output_slicing, src/slice.rs:254-289).
+bool find_slices_to_size(const Network& net, const SsaPath& path, u64 target, std::vector<Leg>& legs_out,
+                         bool allow_output = false);
 // src/slice.rs:893-905
 u64 slice_parallel_chunks(u64 n_slices, u64 out_numel);
 // src/slice.rs:152-176: uniqueness, presence and no repetition inside one input.

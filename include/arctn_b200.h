@@ -19,6 +19,7 @@
  *   simulate_path_full (metrics)                    src/path.rs:239-434
  *   greedy                                          src/paths/greedy.rs:317-320
  *   find_slices_to_size                             src/slice.rs:209-215
+ *   find_slices_with_output                         src/slice.rs:254-289
  *   PyO3 CompiledContraction.compile/execute/stats  pybind/src/lib.rs:384-454
  *   PyO3 contract_sliced                            pybind/src/lib.rs:692-765
  */
@@ -102,6 +103,12 @@ int arctn_b200_greedy(const arctn_b200_network* net, uint64_t* ssa_out, uint64_t
  * reference returns None. */
 int arctn_b200_find_slices_to_size(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
                                    uint64_t target_size, uint32_t* legs_out, uint64_t* n_legs_out, int* found);
+/* The same search with output legs allowed when allow_output_slicing != 0: the opt-in output-index slicing of
+ * find_slices_until_for_target_with_output_slicing with no deadline (src/slice.rs:254-289, 557-589); a unary
+ * network's output counts as its one intermediate. */
+int arctn_b200_find_slices_with_output(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path,
+                                       uint64_t target_size, int allow_output_slicing, uint32_t* legs_out,
+                                       uint64_t* n_legs_out, int* found);
 /* Audit of a saved slice plan (src/execution_plan.rs:817-890, src/slice.rs:102-130): validates the sliced
  * legs (validate_slice_legs, src/slice.rs:152-176), writes the per-slice path metrics (sliced legs set to
  * dimension 1; same order as arctn_b200_simulate_path) and, for target_size > 0, *fits_out = 1 when every

@@ -1232,8 +1232,10 @@ static bool legs_feasible(const Net& net, const std::vector<Leg>& legs, usize ta
   return true;
 }
 
-// src/slice.rs:209-215, 254-288, 557-589
-static bool find_slices_to_size(const Net& net, const Path& path, usize target, std::vector<Leg>& out_legs) {
+// src/slice.rs:209-215, 254-288, 557-589.  allow_output: output legs may be sliced too
+// (find_slices_until_for_target_with_output_slicing with no deadline, src/slice.rs:254-289).
+static bool find_slices_to_size(const Net& net, const Path& path, usize target, std::vector<Leg>& out_legs,
+                                bool allow_output = false) {
   if (target == 0) return false;
   std::vector<Leg> sliced;
   for (;;) {
@@ -1254,11 +1256,13 @@ static bool find_slices_to_size(const Net& net, const Path& path, usize target, 
     }
     if (feasible) { out_legs = sliced; return true; }
     std::map<Leg, std::pair<usize, double>> score;
+    // A unary contraction has no steps but still produces its output (src/slice.rs:565-566).
+    if (allow_output && net.n() == 1) step_legs.push_back(cur.output);
     for (auto& sl : step_legs) {
       if (legs_feasible(cur, sl, target)) continue;
       for (Leg l : sl) {
         double d = cur.log2_dim(l);
-        if (d <= 0.0 || !slice_leg_allowed(net, l, false)) continue;
+        if (d <= 0.0 || !slice_leg_allowed(net, l, allow_output)) continue;
         auto it = score.find(l);
         if (it == score.end()) score[l] = {1, d};
         else it->second.first += 1;
@@ -1486,6 +1490,21 @@ int oracle_find_slices_to_size(uint64_t n_inputs, const uint64_t* offs, const ui
     Net net = make_net(n_inputs, offs, legs, n_out, out, n_sizes, size_legs, size_dims);
     std::vector<Leg> sl;
     bool ok = find_slices_to_size(net, make_path(n_steps, pairs), target, sl);
+    *found = ok ? 1 : 0;
+    *n_legs_out = sl.size();
+    for (size_t i = 0; i < sl.size(); ++i) legs_out[i] = sl[i];
+  })
+}
+
+// The same search with output legs allowed when allow_output_slicing != 0.
+int oracle_find_slices_with_output(uint64_t n_inputs, const uint64_t* offs, const uint32_t* legs, uint64_t n_out,
+                                   const uint32_t* out, uint64_t n_sizes, const uint32_t* size_legs,
+                                   const uint64_t* size_dims, uint64_t n_steps, const uint64_t* pairs, uint64_t target,
+                                   int allow_output_slicing, uint32_t* legs_out, uint64_t* n_legs_out, int* found) {
+  GUARD({
+    Net net = make_net(n_inputs, offs, legs, n_out, out, n_sizes, size_legs, size_dims);
+    std::vector<Leg> sl;
+    bool ok = find_slices_to_size(net, make_path(n_steps, pairs), target, sl, allow_output_slicing != 0);
     *found = ok ? 1 : 0;
     *n_legs_out = sl.size();
     for (size_t i = 0; i < sl.size(); ++i) legs_out[i] = sl[i];

@@ -66,6 +66,8 @@ def lib():
         L.oracle_greedy.argtypes = _NET_ARGS + [_u64p, _u64p]
         L.oracle_find_slices_to_size.argtypes = _NET_ARGS + [
             ctypes.c_uint64, _u64p, ctypes.c_uint64, _u32p, _u64p, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_find_slices_with_output.argtypes = _NET_ARGS + [
+            ctypes.c_uint64, _u64p, ctypes.c_uint64, ctypes.c_int, _u32p, _u64p, ctypes.POINTER(ctypes.c_int)]
         L.oracle_slice_parallel_chunks.argtypes = [ctypes.c_uint64, ctypes.c_uint64]
         L.oracle_slice_parallel_chunks.restype = ctypes.c_uint64
         _lib = L
@@ -197,15 +199,17 @@ def greedy(inputs, output, size_dict):
     return [(int(buf[2 * s]), int(buf[2 * s + 1])) for s in range(ns.value)]
 
 
-def find_slices_to_size(inputs, output, size_dict, ssa_path, target_size):
-    """Returns the sliced legs, or ``None`` where the reference returns ``None``."""
+def find_slices_to_size(inputs, output, size_dict, ssa_path, target_size, allow_output_slicing=False):
+    """Returns the sliced legs, or ``None`` where the reference returns ``None``.  ``allow_output_slicing``
+    lets output legs be chosen too (src/slice.rs:254-289)."""
     net = _Net(inputs, output, size_dict)
     n, p = _path_arr(ssa_path)
     buf = np.zeros(max(1, net.n_sizes), dtype=np.uint32)
     nl = ctypes.c_uint64(0)
     found = ctypes.c_int(0)
-    _check(lib().oracle_find_slices_to_size(*net.args(), n, p.ctypes.data_as(_u64p), int(target_size),
-                                            buf.ctypes.data_as(_u32p), ctypes.byref(nl), ctypes.byref(found)))
+    _check(lib().oracle_find_slices_with_output(*net.args(), n, p.ctypes.data_as(_u64p), int(target_size),
+                                                1 if allow_output_slicing else 0, buf.ctypes.data_as(_u32p),
+                                                ctypes.byref(nl), ctypes.byref(found)))
     return [int(x) for x in buf[: nl.value]] if found.value else None
 
 

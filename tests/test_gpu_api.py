@@ -82,3 +82,20 @@ def test_compiled_contraction_facade_matches_oracle(precision):
     assert cc.last_execute_wall_s is not None
     with pytest.raises(ValueError):
         A.ArcTNCompiledContraction.compile(inputs, output, size, ssa_path=path, backend="auto")
+
+
+def test_arctn_contract_with_output_slicing_matches_oracle():
+    # allow_output_slicing (pybind/python/arctn/__init__.py:903-1072): the slice search may pick output legs, and
+    # the output is assembled from their blocks.
+    net = N.random_connected(7, 2, [2, 3, 4], 2, 7301)
+    arrays = random_arrays(net.inputs, net.size_dict, np.complex128, 5)
+    inputs, output, size, internal = labelled(net)
+    got, info = A.arctn_contract(inputs, output, size, arrays, target_size=4, allow_output_slicing=True,
+                                 backend="b200", return_info=True)
+    path = O.greedy(*internal)
+    sliced = O.find_slices_to_size(*internal, path, 4, allow_output_slicing=True)
+    assert list(info["sliced_legs"]) == list(sliced)
+    assert any(l in internal[1] for l in sliced)  # at least one output leg is sliced
+    want = O.execute(*internal, path, arrays)
+    assert np.asarray(got).shape == want.shape
+    assert np.max(np.abs(np.asarray(got) - want)) <= 1e-12 * max(1.0, np.max(np.abs(want)))

@@ -157,3 +157,51 @@ def test_linear_ssa_roundtrip():
     assert A.linear_to_ssa(lin, 3) == ssa
     with pytest.raises(ValueError):
         A.linear_to_ssa([(0, 5)], 3)
+
+
+def test_output_slicing_is_opt_in_for_a_unary_network():
+    # src/slice.rs:1180-1196: a unary network's output can be fitted only by slicing one of its output legs.
+    inputs, output, size_dict = [[0, 1]], [1, 0], {0: 2, 1: 3}
+    for find in (A.find_slices_to_size, O.find_slices_to_size):
+        assert find(inputs, output, size_dict, [], 2) is None
+        assert find(inputs, output, size_dict, [], 2, allow_output_slicing=True) == [1]
+
+
+def test_output_slicing_skips_a_leg_repeated_inside_one_input():
+    # src/slice.rs:1226-1238: the traced output leg cannot be sliced, so no slicing meets the target.
+    for find in (A.find_slices_to_size, O.find_slices_to_size):
+        assert find([[0, 0]], [0], {0: 2}, [], 1, allow_output_slicing=True) is None
+
+
+def _open_networks():
+    nets = {}
+    for seed in range(30):
+        net = N.random_connected(3 + seed % 6, 2, [2, 3, 4], 1 + seed % 3, seed + 7300)
+        nets[f"open{seed}"] = net.as_tuple()
+    return nets
+
+
+@pytest.mark.parametrize("name", sorted(_open_networks()))
+def test_output_slicing_matches_oracle(name):
+    inputs, output, size_dict = _open_networks()[name]
+    path = A.greedy(inputs, output, size_dict)
+    for target in (1, 2, 4, 8, 16, 64):
+        got = A.find_slices_to_size(inputs, output, size_dict, path, target, allow_output_slicing=True)
+        assert got == O.find_slices_to_size(inputs, output, size_dict, path, target, allow_output_slicing=True)
+        assert A.find_slices_to_size(inputs, output, size_dict, path, target) == \
+            O.find_slices_to_size(inputs, output, size_dict, path, target)
+        if got is not None:
+            # every per-slice intermediate fits
+            sub = dict(size_dict)
+            for l in got:
+                sub[l] = 1
+            assert A.simulate_path(inputs, output, sub, path)["log2_max_size"] <= np.log2(target) + 1e-12
+
+
+def test_output_slicing_does_choose_output_legs():
+    chosen = 0
+    for inputs, output, size_dict in _open_networks().values():
+        path = A.greedy(inputs, output, size_dict)
+        got = A.find_slices_to_size(inputs, output, size_dict, path, 4, allow_output_slicing=True)
+        chosen += got is not None and any(l in output for l in got)
+    assert chosen >= 10
