@@ -5,6 +5,8 @@ reached through the C ABI of ``include/arctn_b200.h``.  There is no CPU
 fallback: executing without a CUDA device raises ``ValueError``.
 """
 
+__version__ = "0.2.0"
+
 from ._capi import ArcTNB200Error
 from .execution_plan import ExecutionPlan, PlanValidationError, load_tensors_bin, save_tensors_bin
 from .api import (
@@ -16,6 +18,7 @@ from .api import (
     ProgramBatch,
     SlicedProgram,
     arctn_contract,
+    build_info,
     contract_sliced,
     find_slices_to_size,
     greedy,
@@ -43,6 +46,7 @@ __all__ = [
     "TuneTable",
     "autotune",
     "arctn_contract",
+    "build_info",
     "contract_sliced",
     "find_slices_to_size",
     "load_tensors_bin",

@@ -237,6 +237,20 @@ def find_slices_to_size(inputs, output, size_dict, ssa_path, target_size, allow_
     return [int(x) for x in buf[: nl.value]] if found.value else None
 
 
+def build_info():
+    """Identity of the loaded library, the counterpart of the reference's ``build_info`` (pybind/src/lib.rs:
+    470-493): the package version, the C-ABI version of ``libarctn_b200.so``, where it was loaded from, the GPU
+    architecture it was compiled for, the host platform and the executor's features.  Host-only."""
+    import platform
+
+    return {"version": __import__("arctn_b200").__version__, "abi_version": int(C.lib().arctn_b200_abi_version()),
+            "library": C.lib()._name, "target_gpu_arch": "sm_100a", "target_arch": platform.machine(),
+            "target_os": platform.system().lower(), "target_pointer_width": ctypes.sizeof(ctypes.c_void_p) * 8,
+            "features": {"dtypes": ["f32", "f64", "complex64", "complex128"],
+                         "precisions": ["fp32", "tf32x3", "bf16x3", "bf16x6"], "tensor_cores": "tcgen05",
+                         "adjoint": True, "output_slicing": True, "batch": True, "autotuner": True}}
+
+
 def slice_range(count, ranks, rank):
     """Contiguous slice range [begin, end) of one rank (src/bin/tnmpi.rs:278-284); empty when ranks > count."""
     if ranks < 1 or not 0 <= rank < ranks:

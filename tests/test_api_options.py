@@ -49,3 +49,17 @@ def test_unreachable_target_is_reported_before_execution():
     # Every leg of a 1x1 product is an output leg: without output slicing nothing meets target 1.
     with pytest.raises(ValueError, match="unreachable"):
         A.arctn_contract([["a"], ["b"]], ["a", "b"], {"a": 2, "b": 2}, None, target_size=1, backend="b200")
+
+
+def test_build_info_reports_the_loaded_library():
+    # pybind/src/lib.rs:470-493: the loaded extension's identity.
+    import os
+    import re
+
+    info = A.build_info()
+    header = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                               "arctn_b200.h")).read()
+    assert info["abi_version"] == int(re.search(r"#define ARCTN_B200_ABI_VERSION (\d+)u", header).group(1))
+    assert os.path.basename(info["library"]) == "libarctn_b200.so" and os.path.exists(info["library"])
+    assert info["version"] == A.__version__ and info["target_gpu_arch"] == "sm_100a"
+    assert info["target_pointer_width"] == 64 and "tf32x3" in info["features"]["precisions"]
