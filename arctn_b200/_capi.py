@@ -63,6 +63,7 @@ class GemmChoice(ctypes.Structure):
 # (name, restype, argtypes) for every symbol the header declares.
 NETP = ctypes.POINTER(Network)
 SIGNATURES = [
+    ("arctn_b200_debug_inject_failure", c_int, [c_int, c_int]),
     ("arctn_b200_abi_version", u32, []),
     ("arctn_b200_last_error", ctypes.c_char_p, []),
     ("arctn_b200_simulate_path", c_int, [NETP, u64, u64p, ctypes.POINTER(c_double)]),

@@ -6,6 +6,7 @@
 // with the step's result legs as output, which classifies every leg the same
 // way plan_pairwise does (src/compiled.rs:481-602).
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -58,6 +59,23 @@ int guarded(F&& f) {
   } catch (std::exception& e) {
     g_last_error = e.what();
     return ARCTN_B200_ERR_INVALID;
+  }
+}
+
+// Host-side fault injection for tests of the error paths.  A test arms a countdown per site; the armed call
+// fails at its entry, before any CUDA work, with the status and message of a failed CUDA allocation.  Nothing
+// reaches the GPU.  Site 0: program and batch execute / gradient calls; site 1: program and batch creation.
+std::atomic<int> g_inject[2];
+
+void maybe_inject(int site) {
+  int c = g_inject[site].load();
+  while (c > 0) {
+    if (g_inject[site].compare_exchange_weak(c, c - 1)) {
+      if (c == 1)
+        throw Error(E_CUDA, "cudaErrorMemoryAllocation: out of memory (injected by arctn_b200_debug_inject_failure, "
+                            "site " + std::to_string(site) + ")");
+      return;
+    }
   }
 }
 
@@ -149,6 +167,14 @@ Program& stage_program(arctn_b200_plan* pl, int kind, u64 idx, int dtype, int pr
 extern "C" {
 
 uint32_t arctn_b200_abi_version(void) { return ARCTN_B200_ABI_VERSION; }
+
+int arctn_b200_debug_inject_failure(int site, int countdown) {
+  return guarded([&] {
+    if (site < 0 || site > 1) fail("site must be 0 (execute / gradient) or 1 (create)");
+    if (countdown < 0) fail("countdown must be >= 0");
+    g_inject[site].store(countdown);
+  });
+}
 const char* arctn_b200_last_error(void) { return g_last_error.c_str(); }
 
 int arctn_b200_simulate_path(const arctn_b200_network* net, uint64_t n_steps, const uint64_t* ssa_path, double stats_out[6]) {
@@ -344,6 +370,7 @@ int arctn_b200_program_create(const arctn_b200_network* net, uint64_t n_steps, c
                               uint64_t n_sliced, const uint32_t* sliced_legs, const arctn_b200_program_options* options,
                               arctn_b200_program** program_out) {
   return guarded([&] {
+    maybe_inject(1);
     if (!program_out) fail("program_out is null");
     if (n_sliced && !sliced_legs) fail("sliced_legs is null");
     std::vector<Leg> sl(sliced_legs, sliced_legs + n_sliced);
@@ -358,6 +385,7 @@ int arctn_b200_program_create_tuned(const arctn_b200_network* net, uint64_t n_st
                                     const arctn_b200_program_options* options, const arctn_b200_gemm_choice* table,
                                     uint64_t n_table, arctn_b200_program** program_out) {
   return guarded([&] {
+    maybe_inject(1);
     if (!program_out) fail("program_out is null");
     if (n_sliced && !sliced_legs) fail("sliced_legs is null");
     if (n_table && !table) fail("table is null");
@@ -414,6 +442,7 @@ uint64_t arctn_b200_program_recomputed_steps(const arctn_b200_program* p) {
 int arctn_b200_program_execute(arctn_b200_program* p, const void* const* inputs, void* output, void* workspace,
                                uint64_t workspace_bytes, void* cuda_stream) {
   return guarded([&] {
+    maybe_inject(0);
     if (!p || !inputs) fail("null argument");
     p->p->execute(inputs, output, false, workspace, workspace_bytes, (cudaStream_t)cuda_stream);
   });
@@ -422,6 +451,7 @@ int arctn_b200_program_execute(arctn_b200_program* p, const void* const* inputs,
 int arctn_b200_program_execute_f64out(arctn_b200_program* p, const void* const* inputs, void* output_f64,
                                       void* workspace, uint64_t workspace_bytes, void* cuda_stream) {
   return guarded([&] {
+    maybe_inject(0);
     if (!p || !inputs) fail("null argument");
     p->p->execute(inputs, output_f64, true, workspace, workspace_bytes, (cudaStream_t)cuda_stream);
   });
@@ -431,6 +461,7 @@ int arctn_b200_program_execute_stripped(arctn_b200_program* p, const void* const
                                         void* workspace, uint64_t workspace_bytes, void* cuda_stream,
                                         double* log10_exponent) {
   return guarded([&] {
+    maybe_inject(0);
     if (!p || !inputs || !log10_exponent) fail("null argument");
     p->p->execute_stripped(inputs, output, workspace, workspace_bytes, (cudaStream_t)cuda_stream, log10_exponent);
   });
@@ -440,6 +471,7 @@ int arctn_b200_program_gradient(arctn_b200_program* p, int part, const void* con
                                 void* const* grad_inputs, void* output, void* workspace, uint64_t workspace_bytes,
                                 void* cuda_stream) {
   return guarded([&] {
+    maybe_inject(0);
     if (!p || !inputs) fail("null argument");
     if (part < 0 || part > 2) fail("part must be 0, 1 or 2");
     p->p->execute_gradient(part, inputs, grad_output, grad_inputs, output, workspace, workspace_bytes,
@@ -463,6 +495,7 @@ int arctn_b200_program_describe(const arctn_b200_program* p, char* buf, uint64_t
 int arctn_b200_batch_create_mode(arctn_b200_program* const* programs, uint64_t n_programs, int max_lanes, int mode,
                                  arctn_b200_batch** batch_out) {
   return guarded([&] {
+    maybe_inject(1);
     if (!programs || !batch_out) fail("null argument");
     std::vector<Program*> ps;
     for (uint64_t j = 0; j < n_programs; ++j) {
@@ -508,6 +541,7 @@ uint64_t arctn_b200_batch_lanes(const arctn_b200_batch* b) { return b ? b->b->n_
 int arctn_b200_batch_execute(arctn_b200_batch* batch, const void* const* const* inputs, void* const* outputs,
                              void* workspace, uint64_t workspace_bytes, void* cuda_stream) {
   return guarded([&] {
+    maybe_inject(0);
     if (!batch) fail("batch is null");
     batch->b->run(-1, inputs, nullptr, nullptr, outputs, workspace, workspace_bytes, (cudaStream_t)cuda_stream);
   });
@@ -517,6 +551,7 @@ int arctn_b200_batch_gradient(arctn_b200_batch* batch, const void* const* const*
                               const void* const* grad_outputs, void* const* const* grads, void* const* outputs,
                               void* workspace, uint64_t workspace_bytes, void* cuda_stream) {
   return guarded([&] {
+    maybe_inject(0);
     if (!batch) fail("batch is null");
     batch->b->run(0, inputs, grad_outputs, grads, outputs, workspace, workspace_bytes, (cudaStream_t)cuda_stream);
   });

@@ -393,6 +393,11 @@ int arctn_b200_batch_describe(const arctn_b200_batch* batch, int detail, char* b
 /* Test hook of the interpreter's bounded waits: runs it on one task whose dependency nothing completes,
  * synchronises cuda_stream and sets *code to the error word left (16 once the 2 s wait expired). */
 int arctn_b200_batch_wait_selftest(void* cuda_stream, int* code);
+/* Host-side fault injection for tests of the error paths; no counterpart in the reference.  Arms a countdown for
+ * one site: the countdown-th next call of that site fails at its entry, before any CUDA work, with
+ * ARCTN_B200_ERR_CUDA and the message of a failed CUDA allocation; 0 disarms.  Site 0: program and batch
+ * execute, execute_stripped and gradient calls; site 1: program and batch creation.  Process-wide. */
+int arctn_b200_debug_inject_failure(int site, int countdown);
 void arctn_b200_batch_destroy(arctn_b200_batch* batch);
 uint64_t arctn_b200_batch_workspace_size(const arctn_b200_batch* batch);
 uint64_t arctn_b200_batch_lanes(const arctn_b200_batch* batch);
