@@ -8,7 +8,6 @@ has no fault injection; these hooks stand in for the failures a GPU run could me
 GPU.  tests/test_gpu_failure.py checks that a program keeps working after an injected failure.
 """
 
-
 import numpy as np
 import pytest
 
