@@ -205,3 +205,16 @@ def test_output_slicing_does_choose_output_legs():
         got = A.find_slices_to_size(inputs, output, size_dict, path, 4, allow_output_slicing=True)
         chosen += got is not None and any(l in output for l in got)
     assert chosen >= 10
+
+
+def test_max_leg_id_is_safe_and_an_unused_leg_is_rejected():
+    # tests/sparse_leg_ids.rs:14-42: leg id u32::MAX in simulation, greedy and a program plan; a size_dict leg
+    # that no input uses is rejected, as the reference's network validation does.
+    top = 2 ** 32 - 1
+    net = ([[top], [top]], [top], {top: 2})
+    assert A.greedy(*net) == [(0, 1)]
+    assert A.simulate_path(*net, [(0, 1)]) == O.simulate_path(*net, [(0, 1)])
+    assert A.simulate_path(*net, [(0, 1)])["log10_flops"] == pytest.approx(np.log10(2.0))
+    assert A.SlicedProgram(*net, [(0, 1)], (), dtype=np.float64).describe()["ops"]
+    with pytest.raises(ValueError, match="not used by any input"):
+        A.simulate_path([[0]], [0], {0: 2, top: 2}, [])
