@@ -339,10 +339,43 @@ class ExecutionPlan:
         return SlicedProgram(self.inputs, self.output, self.size_dict, self.ssa_path, self.sliced_legs,
                              dtype=dtype, precision=precision, **kw)
 
-    def execute(self, arrays, *, precision="fp32", **kw):
-        """Contract the plan's network on the GPU: sum internal slices, assemble output blocks."""
+    def compile(self, *, backend="b200"):
+        """An ``ArcTNCompiledContraction`` of an unsliced plan for repeated execution
+        (pybind/python/arctn/_execution_plan.py:474-487); sliced plans are rejected as there."""
+        from .api import ArcTNCompiledContraction
+
+        if self.sliced_legs:
+            raise PlanValidationError("sliced plans cannot be compiled by ArcTNCompiledContraction; call "
+                                      "plan.execute(...)")
+        return ArcTNCompiledContraction.compile(self.inputs, self.output, self.size_dict, ssa_path=self.ssa_path,
+                                                backend=backend)
+
+    def execute(self, arrays, *, backend="b200", return_info=False, precision="fp32", **kw):
+        """Contract the plan's network on the GPU: sum internal slices, assemble output blocks
+        (pybind/python/arctn/_execution_plan.py:489-577).  ``return_info`` adds the reference's timing fields;
+        the wall time covers the synchronous call, inputs staged and the result returned."""
+        import time
+
+        from .api import _validate_backend
+
+        backend = _validate_backend(backend)
+        try:
+            arrays = tuple(arrays)
+        except TypeError as exc:
+            raise PlanValidationError("arrays must be a sequence") from exc
         self.validate(arrays)
-        return self.program(dtype=arrays[0].dtype, precision=precision, **kw).execute(arrays)
+        t0 = time.perf_counter()
+        prog = self.program(dtype=arrays[0].dtype, precision=precision, **kw)
+        t1 = time.perf_counter()
+        result = prog.execute(arrays)
+        t2 = time.perf_counter()
+        if not return_info:
+            return result
+        return result, {"plan_schema": SCHEMA, "plan_schema_version": SCHEMA_VERSION, "execution_backend": backend,
+                        "execution_implementation": "arctn_b200.SlicedProgram", "precision": precision,
+                        "expression_compile_wall_s": t1 - t0, "execution_setup_wall_s": t1 - t0,
+                        "execution_dispatch_wall_s": t2 - t1, "execution_wall_s": t2 - t0,
+                        "execution_timing_scope": "synchronous_host_wall", "sliced_legs": list(self.sliced_legs)}
 
     def __repr__(self):
         return (f"ExecutionPlan(n_inputs={len(self.inputs)}, n_steps={len(self.ssa_path)}, "

@@ -177,3 +177,23 @@ def test_saved_sliced_plan_executes_on_the_gpu(tmp_path):
     got = complex(loaded.execute(data))
     want = complex(O.contract_sliced(inputs, [], sizes, path, sliced, [a.astype(np.complex128) for a in data]))
     assert abs(got - want) <= 1e-5 * abs(want)
+
+
+def test_compile_and_execute_options_follow_the_reference():
+    # pybind/python/arctn/_execution_plan.py:474-500: compile() serves unsliced plans only; execute() takes an
+    # explicit backend and checks it before anything runs.
+    unsliced = ExecutionPlan.from_path(TRI_INPUTS, [], TRI_SIZES, TRI_PATH)
+    compiled = unsliced.compile(backend="b200")
+    assert isinstance(compiled, A.ArcTNCompiledContraction) and compiled.backend == "b200"
+    assert [tuple(p) for p in compiled.ssa_path] == TRI_PATH
+    sliced = ExecutionPlan.from_path(TRI_INPUTS, [], TRI_SIZES, TRI_PATH, [0])
+    with pytest.raises(PlanValidationError, match="sliced plans cannot be compiled"):
+        sliced.compile()
+    arrays = [np.ones((2, 2))] * 3
+    for bad in ("auto", "native", ""):
+        with pytest.raises(ValueError, match="backend"):
+            sliced.execute(arrays, backend=bad)
+    with pytest.raises(PlanValidationError, match="sequence"):
+        sliced.execute(5)
+    with pytest.raises(PlanValidationError, match="arrays length"):
+        sliced.execute(arrays[:2])
