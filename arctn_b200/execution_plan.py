@@ -252,6 +252,55 @@ class ExecutionPlan:
         self.name = artifact.get("net", "network")
         self.per_slice_metrics = per
         self._artifact = artifact
+        self._frozen = True
+
+    def __setattr__(self, name, value):
+        if getattr(self, "_frozen", False):
+            raise AttributeError("ExecutionPlan is immutable")
+        object.__setattr__(self, name, value)
+
+    # ------------------------------------------------------------------ the reference plan object's properties
+    # (pybind/python/arctn/_execution_plan.py:223-282)
+    @property
+    def schema(self):
+        return SCHEMA
+
+    @property
+    def schema_version(self):
+        return SCHEMA_VERSION
+
+    @property
+    def path_format(self):
+        return PATH_FORMAT
+
+    @property
+    def planning(self):
+        return json.loads(json.dumps(self._artifact.get("planning", {})))
+
+    @property
+    def provenance(self):
+        return json.loads(json.dumps(self._artifact.get("provenance", {})))
+
+    @property
+    def network_canon(self):
+        return self._artifact["network_canon"]
+
+    @property
+    def is_sliced(self):
+        return bool(self.sliced_legs)
+
+    def to_linear_path(self):
+        """The opt_einsum linear form of the SSA path (pybind/python/arctn/_execution_plan.py:455-457)."""
+        from .api import ssa_to_linear
+
+        return tuple(tuple(p) for p in ssa_to_linear(self.ssa_path, len(self.inputs)))
+
+    def __eq__(self, other):
+        if not isinstance(other, ExecutionPlan):
+            return NotImplemented
+        return self.to_dict() == other.to_dict()
+
+    __hash__ = None
 
     # ------------------------------------------------------------------ construction / persistence
     @classmethod
@@ -317,20 +366,50 @@ class ExecutionPlan:
         return dest
 
     # ------------------------------------------------------------------ execution
-    def validate(self, arrays):
-        """Array count, shapes and one shared dtype against the plan's network."""
-        arrays = list(arrays)
+    def validate(self, inputs=None, output=None, size_dict=None, *, arrays=None):
+        """A caller's network (any hashable labels, numbered densely in first-occurrence order) and the
+        arrays' count, shapes and one shared dtype against the plan (pybind/python/arctn/_execution_plan.py:
+        402-453)."""
+        import operator
+
+        given = (inputs is not None, output is not None, size_dict is not None)
+        if any(given) and not all(given):
+            raise TypeError("inputs, output, and size_dict must be provided together")
+        if all(given):
+            ids = {}
+            for leg in [l for t in inputs for l in t] + list(output):
+                ids.setdefault(leg, len(ids))
+            try:
+                cand = ([[ids[l] for l in t] for t in inputs], [ids[l] for l in output],
+                        {ids[l]: int(d) for l, d in size_dict.items() if l in ids})
+            except (TypeError, ValueError) as exc:
+                raise PlanValidationError(f"caller network is invalid: {exc}") from exc
+            if len(cand[2]) != len(size_dict) or cand != (self.inputs, self.output, self.size_dict):
+                raise PlanValidationError("caller network does not match the embedded plan network")
+        if arrays is None:
+            return None
+        try:
+            arrays = tuple(arrays)
+        except TypeError as exc:
+            raise PlanValidationError("arrays must be a sequence") from exc
         if len(arrays) != len(self.inputs):
             raise PlanValidationError(f"arrays length {len(arrays)} does not match {len(self.inputs)} plan inputs")
         dt = None
         for i, (a, legs) in enumerate(zip(arrays, self.inputs)):
+            if not hasattr(a, "shape") or not hasattr(a, "dtype"):
+                raise PlanValidationError(f"arrays[{i}] must provide shape and dtype")
+            try:
+                got = tuple(operator.index(d) for d in a.shape)
+            except TypeError as exc:
+                raise PlanValidationError(f"arrays[{i}] has invalid shape or dtype: {exc}") from exc
             shape = tuple(self.size_dict[l] for l in legs)
-            if tuple(int(d) for d in a.shape) != shape:
-                raise PlanValidationError(f"arrays[{i}] shape {tuple(a.shape)} does not match {shape}")
+            if got != shape:
+                raise PlanValidationError(f"arrays[{i}] shape {got} does not match {shape}")
             if dt is None:
-                dt = a.dtype
-            elif a.dtype != dt:
+                dt = str(a.dtype)
+            elif str(a.dtype) != dt:
                 raise PlanValidationError("all arrays must use the same dtype")
+        return None
 
     def program(self, *, dtype="complex64", precision="fp32", **kw):
         """A SlicedProgram for this plan (all slices, FP64 cross-slice sum)."""
@@ -363,7 +442,7 @@ class ExecutionPlan:
             arrays = tuple(arrays)
         except TypeError as exc:
             raise PlanValidationError("arrays must be a sequence") from exc
-        self.validate(arrays)
+        self.validate(arrays=arrays)
         t0 = time.perf_counter()
         prog = self.program(dtype=arrays[0].dtype, precision=precision, **kw)
         t1 = time.perf_counter()

@@ -197,3 +197,30 @@ def test_compile_and_execute_options_follow_the_reference():
         sliced.execute(5)
     with pytest.raises(PlanValidationError, match="arrays length"):
         sliced.execute(arrays[:2])
+
+
+def test_plan_object_surface_follows_the_reference():
+    # pybind/python/arctn/_execution_plan.py:220-282, 402-472, 579-582
+    plan = ExecutionPlan.from_path(TRI_INPUTS, [], TRI_SIZES, TRI_PATH, [0], labels=LABELS, name="triangle")
+    assert (plan.schema, plan.schema_version, plan.path_format) == ("arctn-execution-plan", 2, "ssa-v1")
+    assert plan.is_sliced and not ExecutionPlan.from_path(TRI_INPUTS, [], TRI_SIZES, TRI_PATH).is_sliced
+    assert plan.network_canon == network_canon(TRI_INPUTS, [], TRI_SIZES)
+    assert plan.provenance["source"] == "arctn_b200" and plan.planning == {}
+    assert plan.to_linear_path() == ((0, 1), (0, 1))
+    with pytest.raises(AttributeError, match="immutable"):
+        plan.ssa_path = []
+    assert plan == ExecutionPlan.from_dict(plan.to_dict())
+    assert plan != ExecutionPlan.from_path(TRI_INPUTS, [], TRI_SIZES, TRI_PATH, [1], labels=LABELS, name="triangle")
+    # a caller's network with its own labels, numbered in first-occurrence order
+    plan.validate([["i", "j"], ["i", "k"], ["j", "k"]], [], {"i": 2, "j": 2, "k": 2})
+    with pytest.raises(PlanValidationError, match="does not match the embedded"):
+        plan.validate([["i", "j"], ["i", "k"], ["j", "k"]], [], {"i": 2, "j": 3, "k": 2})
+    with pytest.raises(PlanValidationError, match="does not match the embedded"):
+        plan.validate([["i", "j"], ["i", "k"], ["j", "k"]], [], {"i": 2, "j": 2, "k": 2, "z": 2})
+    with pytest.raises(TypeError, match="together"):
+        plan.validate([["i", "j"]], [])
+    plan.validate(arrays=[np.zeros((2, 2))] * 3)
+    with pytest.raises(PlanValidationError, match="shape and dtype"):
+        plan.validate(arrays=[[0.0, 0.0]] * 3)
+    with pytest.raises(PlanValidationError, match="same dtype"):
+        plan.validate(arrays=[np.zeros((2, 2)), np.zeros((2, 2)), np.zeros((2, 2), np.float32)])
