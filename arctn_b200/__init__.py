@@ -8,7 +8,7 @@ fallback: executing without a CUDA device raises ``ValueError``.
 __version__ = "0.2.0"
 
 from ._capi import ArcTNB200Error
-from .execution_plan import ExecutionPlan, PlanValidationError, load_tensors_bin, save_tensors_bin
+from .execution_plan import ExecutionPlan, PlanValidationError, arctn_plan, load_tensors_bin, save_tensors_bin
 from .api import (
     ArcTNCompiledContraction,
     CompiledContraction,
@@ -46,6 +46,7 @@ __all__ = [
     "TuneTable",
     "autotune",
     "arctn_contract",
+    "arctn_plan",
     "build_info",
     "contract_sliced",
     "find_slices_to_size",

@@ -305,7 +305,7 @@ class ExecutionPlan:
     # ------------------------------------------------------------------ construction / persistence
     @classmethod
     def from_path(cls, inputs, output, size_dict, ssa_path, sliced_legs=(), *, target_size=None, labels=None,
-                  name="network"):
+                  name="network", planning=None, source="arctn_b200"):
         """A fresh v2 artifact for a network, path and slice set (complete_execution_plan_v2,
         src/execution_plan.rs:131-208).  The network must already be dense (legs 0.. in first-occurrence order)."""
         inputs = [[int(l) for l in t] for t in inputs]
@@ -326,7 +326,7 @@ class ExecutionPlan:
             "metrics": dict(full, log2_n_slices=n_log2,
                             sliced_log10_flops_total=per["log10_flops"] + n_log2 * _LOG10_2,
                             sliced_log2_max_size=per["log2_max_size"]),
-            "planning": {}, "provenance": {"source": "arctn_b200"},
+            "planning": dict(planning or {}), "provenance": {"source": source},
         }
         if target_size is not None:
             art.update(target_size=int(target_size), memory_target_log2_elements=math.log2(target_size),
@@ -488,3 +488,45 @@ def save_tensors_bin(path, arrays):
         for a in arrays:
             a = np.asarray(a)
             f.write(np.array(a, dtype=a.dtype.newbyteorder("<"), order="C").tobytes())
+
+
+def arctn_plan(inputs, output, size_dict, *, preset="heavy", seed=0, target_size=None, slicing_mode="fixed",
+               max_time=None, flops_weight=1.0, read_write_weight=64.0, rate_enabled=True,
+               allow_output_slicing=False):
+    """Plan once and return an immutable ``ExecutionPlan`` (``arctn_plan``,
+    pybind/python/arctn/_execution_plan.py:593-646), with the same keywords and checks.
+
+    The reference plans with its closed-source engine; here the public greedy path (src/paths/greedy.rs:
+    317-320) and the slice search (src/slice.rs:209-289) make the plan, so the engine-only options are checked
+    and recorded under ``planning`` but do not change it.  Legs are numbered densely in first-occurrence order
+    and the caller's labels are kept as ``network_leg_labels`` (as strings) when they stay distinct."""
+    import math as _math
+
+    from .api import _to_int_labels, _validate_planning_options, find_slices_to_size, greedy
+
+    target_size, max_time, (flops_weight, read_write_weight) = _validate_planning_options(
+        preset, seed, target_size, slicing_mode, max_time, flops_weight, read_write_weight, allow_output_slicing)
+    if not isinstance(rate_enabled, bool):
+        raise TypeError("rate_enabled must be a bool")
+    inputs = tuple(tuple(term) for term in inputs)
+    output = tuple(output)
+    if not hasattr(size_dict, "items"):
+        raise TypeError("size_dict must be a mapping from leg label to positive integer dimension")
+    inputs_i, output_i, size_i, label_of = _to_int_labels(inputs, output, dict(size_dict.items()))
+    path = greedy(inputs_i, output_i, size_i)
+    sliced = []
+    if target_size is not None:
+        found = find_slices_to_size(inputs_i, output_i, size_i, path, target_size,
+                                    allow_output_slicing=allow_output_slicing)
+        if found is None:
+            raise ValueError(f"target_size (log2={_math.log2(target_size):.6g}) is unreachable: no slicing meets it")
+        sliced = found
+    labels = [None] * len(label_of)
+    for label, leg in label_of.items():
+        labels[leg] = str(label)
+    planning = {"preset": preset, "seed": seed, "slicing_mode": slicing_mode, "allow_output_slicing":
+                allow_output_slicing, "flops_weight": flops_weight, "read_write_weight": read_write_weight,
+                "method": "greedy"}
+    return ExecutionPlan.from_path(inputs_i, output_i, size_i, path, sliced, target_size=target_size,
+                                   labels=labels if len(set(labels)) == len(labels) else None, planning=planning,
+                                   source="arctn_plan")

@@ -224,3 +224,34 @@ def test_plan_object_surface_follows_the_reference():
         plan.validate(arrays=[[0.0, 0.0]] * 3)
     with pytest.raises(PlanValidationError, match="same dtype"):
         plan.validate(arrays=[np.zeros((2, 2)), np.zeros((2, 2)), np.zeros((2, 2), np.float32)])
+
+
+def test_arctn_plan_plans_with_greedy_and_the_slice_search(tmp_path):
+    # pybind/python/arctn/_execution_plan.py:593-646 with the public planner
+    from arctn_b200 import networks as N
+    from oracle import oracle as O
+
+    net = N.rand_regular(40, 3, 2, 1)
+    names = {l: f"e{l}" for l in net.size_dict}
+    inputs = [[names[l] for l in t] for t in net.inputs]
+    size = {names[l]: d for l, d in net.size_dict.items()}
+    plan = A.arctn_plan(inputs, [], size, target_size=2 ** 6, preset="light", seed=3)
+    ids = {}
+    for lab in [l for t in inputs for l in t]:
+        ids.setdefault(lab, len(ids))
+    dense = ([[ids[l] for l in t] for t in inputs], [], {ids[l]: d for l, d in size.items()})
+    path = O.greedy(*dense)
+    assert [tuple(p) for p in plan.ssa_path] == [tuple(p) for p in path]
+    assert plan.sliced_legs == O.find_slices_to_size(*dense, path, 2 ** 6) and plan.is_sliced
+    assert plan.target_size == 2 ** 6 and plan.leg_labels == sorted(ids, key=ids.get)
+    assert plan.planning["preset"] == "light" and plan.planning["seed"] == 3
+    plan.validate(inputs, [], size)
+    assert ExecutionPlan.load(plan.save(tmp_path / "plan.json")) == plan
+    with pytest.raises(ValueError, match="unreachable"):
+        A.arctn_plan([["a"], ["b"]], ["a", "b"], {"a": 2, "b": 2}, target_size=1)
+    blocks = A.arctn_plan([["a"], ["b"]], ["a", "b"], {"a": 2, "b": 2}, target_size=2, allow_output_slicing=True)
+    assert blocks.sliced_legs and set(blocks.sliced_legs) <= {0, 1}
+    with pytest.raises(TypeError, match="rate_enabled"):
+        A.arctn_plan([["a"]], ["a"], {"a": 2}, rate_enabled=1)
+    with pytest.raises(ValueError, match="preset"):
+        A.arctn_plan([["a"]], ["a"], {"a": 2}, preset="x")
