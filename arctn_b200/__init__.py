@@ -8,7 +8,8 @@ fallback: executing without a CUDA device raises ``ValueError``.
 __version__ = "0.2.0"
 
 from ._capi import ArcTNB200Error
-from .execution_plan import ExecutionPlan, PlanValidationError, arctn_plan, load_tensors_bin, save_tensors_bin
+from .execution_plan import (ArcTNExecutionPlan, ExecutionPlan, PlanValidationError, arctn_plan, load_tensors_bin,
+                             save_tensors_bin)
 from .api import (
     ArcTNCompiledContraction,
     CompiledContraction,
@@ -33,8 +34,10 @@ from .sharding import lpt_shard, run_sharded
 from .tuning import TuneTable, autotune
 
 __all__ = [
+    "__version__",
     "ArcTNB200Error",
     "ArcTNCompiledContraction",
+    "ArcTNExecutionPlan",
     "ExecutionPlan",
     "PlanValidationError",
     "CompiledContraction",

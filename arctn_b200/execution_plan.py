@@ -461,6 +461,11 @@ class ExecutionPlan:
                 f"n_sliced_legs={len(self.sliced_legs)}, target_size={self.target_size!r})")
 
 
+
+# The reference's name for the plan object (pybind/python/arctn/_execution_plan.py:117).
+ArcTNExecutionPlan = ExecutionPlan
+
+
 def load_tensors_bin(path, inputs, size_dict, dtype):
     """Input tensors from a little-endian data file (load_tensors_bin, src/network.rs:81-132)."""
     dt = np.dtype(dtype).newbyteorder("<")

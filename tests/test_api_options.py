@@ -63,3 +63,12 @@ def test_build_info_reports_the_loaded_library():
     assert os.path.basename(info["library"]) == "libarctn_b200.so" and os.path.exists(info["library"])
     assert info["version"] == A.__version__ and info["target_gpu_arch"] == "sm_100a"
     assert info["target_pointer_width"] == 64 and "tf32x3" in info["features"]["precisions"]
+
+
+def test_the_reference_public_names_for_the_path_exist():
+    # pybind/python/arctn/__init__.py:171-183: the names on the contraction path (the planner-only ones --
+    # ArcTNOptimizer, arctn_path, arctn_tree, arctn_schedule, arctn_simplify -- are not part of this executor).
+    for name in ("__version__", "ArcTNExecutionPlan", "ArcTNCompiledContraction", "PlanValidationError",
+                 "arctn_plan", "arctn_contract"):
+        assert name in A.__all__ and hasattr(A, name)
+    assert issubclass(A.PlanValidationError, ValueError)
